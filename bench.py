@@ -1,0 +1,388 @@
+"""Benchmark: time to relative residual 1e-10 of the semi-implicit pressure
+Poisson solve (PinCFlow.jl PoissonSolver) on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--config c2|c5|c1] [--method mixed|fp64]
+
+A step is one complete solve_poisson! (operator assembly, preconditioned
+BiCGSTAB to FP64 true relative residual 1e-10, unscaling into dpip) of the
+configuration's seeded synthetic workload.  `value` is the device time per
+solve with inputs resident in HBM (CUDA events on the solver's stream, max
+over ranks); `e2e` is the same solve through the public host-array entry
+point with its host<->device copies inside the timed region.  The default
+workload (c2, 256 x 256 x 128) holds a 3.4 GB FP64 + 0.8 GB FP32 operator,
+far larger than the 126 MB L2, so no flush is needed between steps.
+
+--impl reference times the reference algorithm on the host cores (the CPU
+oracle, a C++ restatement of the Julia code; Julia is not available): each
+step runs the operator assembly plus a bounded number of BiCGSTAB
+iterations on the full workload, scaled to a complete solve by the
+oracle's own iteration count for that workload.
+Multi-GPU runs are independent replicas (the solve does not shard across
+GPUs in this build): weak scaling, one solve per rank per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "pincflow.jl_b200")
+sys.path[:0] = [REPO, PKG]
+
+import numpy as np  # noqa: E402
+
+METRIC = "time to rel. residual 1e-10: learned+FP32-refined vs plain FP64 BiCGSTAB, 1 B200"
+WORKLOADS = {
+    "c2": "256x256x128 pseudo-incompressible, stretched terrain-following grid, Gaussian mountain 1 km, "
+          "isothermal 250 K, RHS N(0,1) seed 12345",
+    "c5": "512x512x192 pseudo-incompressible, 20 Gaussian ridges <= 2 km, wave-packet RHS",
+    "c1": "periodic hill 40x1x40 Boussinesq (one of its 200 solves)",
+}
+
+
+def make_workload(name, seed_offset=0):
+    from pincflow_poisson import configs
+    if name == "c2":
+        return configs.c2(seed=12345 + seed_offset)
+    if name == "c5":
+        return configs.c5(seed=5 + seed_offset)
+    if name == "c1":
+        return configs.c1(seed=seed_offset, step=0)
+    raise SystemExit(f"unknown config {name}")
+
+
+def load_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(config):
+    """Per-launch DRAM bytes of the FP32 stencil from the committed ncu summary, or None."""
+    p = os.path.join(REPO, "profiles", f"stencil_apply32_{config}.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        for line in fh:
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        under = [v for v in sm if v > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(under), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- CPU arm --
+
+def oracle_sample(cfg, iters, threads=None):
+    """Oracle FP64 assembly + `iters` BiCGSTAB iterations on the full workload.
+    Returns (seconds_assembly, seconds_per_iteration, threads)."""
+    from oracle import oracle as O
+    O.build()
+    if threads:
+        O.set_threads(threads)
+    dom, f = cfg["dom"], cfg["fields"]
+    d = O.dims(dom.nx, dom.ny, dom.nz, dom.nbx)
+    t0 = time.perf_counter()
+    coef = O.compute_operator(d, O.MODELS[cfg["model"]], f, cfg["rho"], cfg["betar"], cfg["dt"],
+                              cfg["rayleigh_factor"])
+    t1 = time.perf_counter()
+    _, info = O.bicgstab(d, coef, f["dx"], f["dy"], cfg["rhs"], tolerance=1e-30, tolerance_is_relative=True,
+                         poisson_iterations=iters)
+    t2 = time.perf_counter()
+    return t1 - t0, (t2 - t1) / max(info["niter"], 1), O.get_threads()
+
+
+def oracle_iterations(config):
+    p = os.path.join(REPO, "tests", "golden", f"{config}_fp64_oracle.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return int(json.load(fh)["niter"]), "oracle full solve (tests/golden)"
+    return None, None
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    cfg = make_workload(args.config)
+    niter, src = oracle_iterations(args.config)
+    if niter is None:
+        niter, src = args.ref_iterations, "--ref-iterations"
+    threads = os.cpu_count()
+    times = []
+    for step in range(args.warmup + args.steps):
+        t_asm, t_it, used = oracle_sample(cfg, args.ref_sample_iters, threads)
+        if step >= args.warmup:
+            times.append(t_asm + t_it * niter)
+    value = statistics.mean(times)
+    sample = (f"per step: oracle FP64 operator assembly + {args.ref_sample_iters} BiCGSTAB iterations of the "
+              f"{args.config} workload on {used} threads, scaled to {niter} iterations ({src})")
+    line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"{args.config}: {WORKLOADS[args.config]}", "method": "plain FP64 BiCGSTAB "
+                       "with the reference preconditioner (CPU restatement of the Julia code)"},
+            "cpu_baseline": {"value": value, "unit": "s", "cores": used, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- GPU arm --
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import pincflow_poisson as pcf
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist = dist_mod
+
+    cfg = make_workload(args.config, seed_offset=rank)
+    dom, f = cfg["dom"], cfg["fields"]
+    dev = torch.device("cuda", local_rank)
+    s = pcf.PoissonSolver(dom, cfg["model"], device=local_rank)
+    s.set_grid(f)
+    s.set_background(f)
+
+    def dev_tensor(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    d_rhs, d_rho, d_betar = dev_tensor(cfg["rhs"]), dev_tensor(cfg["rho"]), dev_tensor(cfg["betar"])
+    d_dpip = torch.zeros(dom.halo_shape, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+
+    nl_fast = pcf.PoissonNamelist(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000,
+                                  precision=args.method, residual="true")
+    nl_plain = pcf.PoissonNamelist(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000,
+                                   precision="fp64", residual="true")
+
+    def solve_dev(nl):
+        info = s.solve_poisson_device(d_rhs.data_ptr(), d_rho.data_ptr(), d_betar.data_ptr(), cfg["dt"],
+                                      cfg["rayleigh_factor"], cfg["tolref"], nl, d_dpip.data_ptr())
+        if info.errflag:
+            raise RuntimeError(f"solve did not converge: {info}")
+        return info
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        solve_dev(nl_fast)
+
+    # --- headline: device-resident inputs, profiled -----------------------
+    s.profile(True)
+    l0 = s.launch_count
+    barrier()
+    infos = []
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            infos.append(solve_dev(nl_fast))
+        barrier()
+    launches = s.launch_count - l0
+    prof = s.profile_read()
+    s.profile(False)
+    ms = [i.timings_ms["total"] for i in infos]
+    ms_per_step = max_over_ranks(statistics.mean(ms))
+    value = ms_per_step / 1e3
+
+    # --- plain FP64 BiCGSTAB on the same inputs ---------------------------
+    barrier()
+    plain = [solve_dev(nl_plain) for _ in range(args.plain_steps)]
+    barrier()
+    plain_s = max_over_ranks(statistics.mean(i.timings_ms["total"] for i in plain)) / 1e3
+
+    # --- end to end through the host-array entry point --------------------
+    h_rhs = torch.from_numpy(np.ascontiguousarray(cfg["rhs"])).pin_memory().numpy()
+    h_rho = torch.from_numpy(np.ascontiguousarray(cfg["rho"])).pin_memory().numpy()
+    h_betar = torch.from_numpy(np.ascontiguousarray(cfg["betar"])).pin_memory().numpy()
+    h_dpip = torch.zeros(dom.halo_shape, dtype=torch.float64).pin_memory().numpy()
+    barrier()
+    e2e_ms, e2e_wall = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        info = s.solve_poisson(h_rhs, h_rho, h_betar, cfg["dt"], cfg["rayleigh_factor"], cfg["tolref"],
+                               nl_fast, h_dpip)
+        e2e_wall.append(time.perf_counter() - t0)
+        if info.errflag:
+            raise RuntimeError(f"e2e solve did not converge: {info}")
+        e2e_ms.append(info.timings_ms["total"])
+    barrier()
+    e2e_s = max_over_ranks(statistics.mean(e2e_ms)) / 1e3
+    n = dom.nx * dom.ny * dom.nz
+    nh = int(np.prod(dom.halo_shape))
+    h2d = 8 * (n + 2 * nh)
+    d2h = 8 * n
+
+    if rank != 0:
+        s.close()
+        return
+
+    # --- roofline of the dominant kernel (FP32 Total apply) ---------------
+    peak, peak_kind = load_peaks()
+    a32 = prof["apply32"] if args.method == "mixed" else prof["apply64"]
+    kernel_ms = a32["ms"] / max(a32["count"], 1)
+    bytes_per_launch = a32["bytes"] / max(a32["count"], 1)
+    achieved = bytes_per_launch / (kernel_ms * 1e-3) / 1e9 if kernel_ms > 0 else 0.0
+    total_prof_ms = sum(v["ms"] for v in prof.values())
+    shares = {k: round(v["ms"] / total_prof_ms, 4) for k, v in prof.items() if v["count"]} if total_prof_ms else {}
+    per_kernel = {k: {"launches": v["count"], "ms_per_launch": v["ms"] / v["count"],
+                      "gbs": v["bytes"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] > 0 else None}
+                  for k, v in prof.items() if v["count"]}
+
+    last = infos[-1]
+    line = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if args.method == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {WORKLOADS[args.config]}",
+                   "method": ("FP32 BiCGSTAB sweeps inside FP64 iterative refinement, reference preconditioner"
+                              if args.method == "mixed" else "plain FP64 BiCGSTAB"),
+                   "convergence": "FP64 true residual RMS(b-Ax)/RMS(b) <= 1e-10",
+                   "l2": "inputs larger than L2 (operator 3.4 GB FP64 + 0.8 GB FP32), no flush",
+                   "parallelism": f"replicas x{world}"},
+        "plain_fp64_s": plain_s, "speedup_vs_plain_fp64": plain_s / value,
+        "iterations": last.niter, "refinements": last.nrefine, "true_residual": last.true_residual,
+        "plain_fp64_iterations": plain[-1].niter,
+        "solves_per_s": world / value,
+        "cell_updates_per_s": world * n * (2 * last.niter) / value,
+        "gpu_launches": launches,
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "wall_s": statistics.mean(e2e_wall)},
+        "roofline": {"bound": "hbm", "kernel": "k_stencil Total apply FP32 (fused dot)" if args.method == "mixed"
+                     else "k_stencil Total apply FP64", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": ncu_traffic(args.config),
+                     "algorithmic_bytes_per_launch": bytes_per_launch, "ms_per_launch": kernel_ms},
+        "kernel_shares": shares, "kernels": per_kernel,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        niter, src = oracle_iterations(args.config)
+        if niter is None:
+            niter, src = plain[-1].niter, "the GPU FP64 solve's iteration count"
+        t_asm, t_it, used = oracle_sample(cfg, args.ref_sample_iters, os.cpu_count())
+        line["cpu_baseline"] = {
+            "value": t_asm + t_it * niter, "unit": "s", "cores": used, "kind": "port",
+            "sample": f"oracle FP64 assembly + {args.ref_sample_iters} BiCGSTAB iterations of the same workload, "
+                      f"scaled to {niter} iterations ({src})"}
+    print(json.dumps(line), flush=True)
+    s.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--ref-sample-iters", type=int, default=3)
+    ap.add_argument("--ref-iterations", type=int, default=450)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,231 @@
+/*
+ * pincflow_poisson.h -- C ABI of the B200 (sm_100a) semi-implicit pressure
+ * Poisson solver that replaces PinCFlow.jl's PoissonSolver hot path.
+ *
+ * The entry points mirror the reference's Julia functions so that a Julia
+ * method (package extension or shim) can `ccall` them
+ * with the arrays it already owns:
+ *
+ *   pcf_solve              <- solve_poisson!(state, dt, rayleigh_factor, tolref)
+ *                             src/PoissonSolver/solve_poisson!.jl:39-75
+ *                             (operator assembly + BiCGSTAB + unscaling into dpip)
+ *   pcf_compute_operator   <- compute_operator!(state, dt, rayleigh_factor)
+ *                             src/PoissonSolver/compute_operator!.jl:40-1606
+ *   pcf_apply_operator     <- apply_operator!(sin, ls, Total() | Horizontal(), state)
+ *                             src/PoissonSolver/apply_operator!.jl:48-479
+ *   pcf_apply_preconditioner <- apply_preconditioner!(sin, sout, state)
+ *                             src/PoissonSolver/apply_preconditioner!.jl:40-124
+ *   pcf_bicgstab           <- apply_bicgstab!(state, tolref)
+ *                             src/PoissonSolver/apply_bicgstab!.jl:24-150
+ *   pcf_global_dot         <- compute_global_dot_product(a, b, state)
+ *                             src/MPIOperations/compute_global_dot_product.jl:22-36
+ *   pcf_set_grid / pcf_set_background
+ *                          <- the State fields these read: Grid.jac, Grid.met
+ *                             (src/Types/FoundationalTypes/Grid.jl:243-313) and
+ *                             Atmosphere.pbar/rhobar/thetabar/n2
+ *                             (src/Types/FoundationalTypes/Atmosphere.jl:278-323)
+ *   pcf_params             <- PoissonNamelist
+ *                             (src/Types/NamelistTypes/PoissonNamelist.jl:38-66)
+ *                             plus SpongeNamelist.damp_horizontal_wind_on_rhs
+ *
+ * Array conventions are the reference's: FP64, column-major (x fastest, then
+ * y, then z).  "Haloed" arrays have (nx + 2 nbx, ny + 2 nby, nz + 2 nbz)
+ * elements like every PinCFlow field; "interior" arrays have (nx, ny, nz)
+ * elements like Poisson.rhs / Poisson.solution.  The 25 operator planes are
+ * stored one after another (plane stride nx*ny*nz) in the field order of the
+ * reference Tensor struct (src/Types/PoissonTypes/Tensor.jl:70-96), given by
+ * enum pcf_coef below.  `met` is passed as its three used planes, met[:,:,:,1,3],
+ * met[:,:,:,2,3] and met[:,:,:,3,3], which are contiguous blocks of the
+ * reference's 5-D array.
+ *
+ * Single GPU, single MPI rank: x and y are periodic, z has solid walls.
+ *
+ * Host pointers are read during the call only and never retained.  Entry
+ * points whose name ends in _device take device pointers (resident in the
+ * handle's GPU memory) and run on the handle's stream.
+ *
+ * Return codes: 0 on success, a negative PCF_E* code otherwise.
+ * Non-convergence is not an error code: it sets result->errflag = 1 and
+ * result->niter = poisson_iterations, as the reference returns
+ * (true, niter) (apply_bicgstab!.jl:146-149).
+ */
+#ifndef PINCFLOW_POISSON_H
+#define PINCFLOW_POISSON_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PCF_ABI_VERSION 1
+
+enum pcf_status {
+    PCF_OK = 0,
+    PCF_EINVAL = -1,      /* bad argument (dt == 0: solve_poisson!.jl:52-54 raises) */
+    PCF_ENOMEM = -2,      /* device allocation failed */
+    PCF_ECUDA = -3,       /* CUDA runtime error */
+    PCF_ENOTREADY = -4,   /* grid or background not set */
+    PCF_EBREAKDOWN = -5,  /* BiCGSTAB breakdown: a zero or non-finite scalar */
+    PCF_ENONFINITE = -6,  /* non-finite value in the inputs or the residual */
+    PCF_ENODEVICE = -7,   /* no usable sm_100 device */
+    PCF_ERANGE = -8       /* size beyond a documented limit */
+};
+
+enum pcf_model {
+    PCF_MODEL_BOUSSINESQ = 0,
+    PCF_MODEL_PSEUDO_INCOMPRESSIBLE = 1,
+    PCF_MODEL_COMPRESSIBLE = 2
+};
+
+/* Operator plane order = field order of the reference Tensor struct. */
+enum pcf_coef {
+    PCF_AC = 0, PCF_AL, PCF_AR, PCF_AB, PCF_AF, PCF_AD, PCF_AU,
+    PCF_ALD, PCF_ALU, PCF_ARD, PCF_ARU, PCF_ABD, PCF_ABU, PCF_AFD, PCF_AFU,
+    PCF_ADD, PCF_AUU, PCF_ALDD, PCF_ALUU, PCF_ARDD, PCF_ARUU, PCF_ABDD, PCF_ABUU,
+    PCF_AFDD, PCF_AFUU, PCF_NCOEF
+};
+
+enum pcf_precision {
+    PCF_PRECISION_FP64 = 0,   /* the reference's arithmetic: FP64 everywhere */
+    PCF_PRECISION_MIXED = 1,  /* FP32 inner BiCGSTAB inside FP64 iterative refinement */
+    PCF_PRECISION_FP32 = 2    /* component entry points only: FP32 operator copy */
+};
+
+enum pcf_residual {
+    PCF_RESIDUAL_RECURSIVE = 0, /* reference test: RMS of the recursive residual */
+    PCF_RESIDUAL_TRUE = 1       /* FP64 true residual b - A x decides convergence */
+};
+
+enum pcf_operator_mode { PCF_TOTAL = 0, PCF_HORIZONTAL = 1 };
+
+typedef struct {
+    int nx, ny, nz;      /* interior sizes (x_size, y_size, z_size on one rank) */
+    int nbx, nby, nbz;   /* halo widths of the caller's haloed arrays (reference: 3) */
+    int model;           /* enum pcf_model (AtmosphereNamelist.model) */
+    int device;          /* CUDA device ordinal */
+} pcf_dims;
+
+typedef struct {
+    /* PoissonNamelist (PoissonNamelist.jl:48-66 defaults) */
+    double tolerance;              /* 1e-8 */
+    int poisson_iterations;        /* 1000 */
+    int preconditioner;            /* 1 */
+    double dtau;                   /* 1.0 */
+    int preconditioner_iterations; /* 2 */
+    int tolerance_is_relative;     /* 0 */
+    /* SpongeNamelist */
+    int damp_horizontal_wind_on_rhs; /* 0 */
+    /* Additions without a reference counterpart; defaults reproduce the reference. */
+    int precision;                 /* PCF_PRECISION_FP64 */
+    int residual;                  /* PCF_RESIDUAL_RECURSIVE */
+    double inner_tolerance;        /* mixed: relative reduction per FP32 sweep (1e-5) */
+    int max_refinements;           /* mixed: cap on FP64 refinement sweeps (20) */
+    int learned;                   /* 0: off; 1: learned warm start + flexible BiCGSTAB */
+    int check_interval;            /* iterations between host checks of the status word (16) */
+} pcf_params;
+
+typedef struct {
+    int errflag;           /* 1 when not converged, as the reference's errflag */
+    int niter;             /* BiCGSTAB iterations (summed over refinement sweeps) */
+    int nrefine;           /* FP64 refinement sweeps (mixed precision) */
+    int status;            /* PCF_OK or PCF_EBREAKDOWN / PCF_ENONFINITE */
+    double residual;       /* final relative residual as tested (recursive or true) */
+    double true_residual;  /* FP64 RMS(b - A x) / RMS(b) */
+    double b_norm;         /* RMS of the initial residual */
+    double ms_upload;      /* host -> device copies */
+    double ms_assemble;    /* operator assembly + preconditioner factors */
+    double ms_solve;       /* Krylov iterations */
+    double ms_download;    /* device -> host copies */
+    double ms_total;
+} pcf_result;
+
+typedef struct pcf_handle pcf_handle;
+
+/* Fills *p with the reference defaults. */
+int pcf_params_default(pcf_params *p);
+
+/* Allocates all device memory of one solver instance (one `State`). */
+int pcf_create(pcf_handle **h, const pcf_dims *dims);
+int pcf_destroy(pcf_handle *h);
+const char *pcf_strerror(int code);
+
+/* Grid: non-dimensional spacings and haloed jac, met13, met23, met33. */
+int pcf_set_grid(pcf_handle *h, double dx, double dy, double dz, const double *jac,
+                 const double *met13, const double *met23, const double *met33);
+
+/* Background: haloed pbar, rhobar, n2; thetabar is read for the Compressible
+ * model only (may be NULL otherwise). */
+int pcf_set_background(pcf_handle *h, const double *pbar, const double *rhobar,
+                       const double *thetabar, const double *n2);
+
+/* solve_poisson!: assembles the operator from the haloed predictand rho, the
+ * haloed sponge coefficient betar and (Compressible only, else NULL) the
+ * haloed predictand p, solves A s = rhs (interior rhs from compute_lhs!) and
+ * writes dpip = s / sqrt(pbar^2/rhobar) / dt into the interior of the haloed
+ * array dpip (halo cells untouched).  tolref is compute_lhs!'s return value. */
+int pcf_solve(pcf_handle *h, const double *rhs, const double *rho, const double *betar,
+              const double *p, double dt, double rayleigh_factor, double tolref,
+              const pcf_params *prm, double *dpip, pcf_result *res);
+
+/* Same with device-resident inputs and output (haloed layouts as above). */
+int pcf_solve_device(pcf_handle *h, const double *d_rhs, const double *d_rho,
+                     const double *d_betar, const double *d_p, double dt,
+                     double rayleigh_factor, double tolref, const pcf_params *prm,
+                     double *d_dpip, pcf_result *res);
+
+/* compute_operator!: fills the handle's operator; if coef is not NULL the 25
+ * FP64 planes are also copied to the host (25 * nx*ny*nz doubles). */
+int pcf_compute_operator(pcf_handle *h, const double *rho, const double *betar, const double *p,
+                         double dt, double rayleigh_factor, int damp_horizontal_wind_on_rhs,
+                         double *coef);
+
+/* Loads 25 FP64 operator planes (Tensor order) instead of assembling them,
+ * as if compute_operator! had produced them. */
+int pcf_set_operator(pcf_handle *h, const double *coef);
+
+/* apply_operator!: ls = A sin (mode PCF_TOTAL) or its horizontal part
+ * (PCF_HORIZONTAL); interior arrays.  precision PCF_PRECISION_FP64 uses the
+ * FP64 planes, PCF_PRECISION_FP32 the FP32 copy (inputs rounded to FP32). */
+int pcf_apply_operator(pcf_handle *h, const double *sin_, double *ls, int mode, int precision);
+
+/* apply_preconditioner!: sout = M sin with prm->dtau and
+ * prm->preconditioner_iterations; interior arrays. */
+int pcf_apply_preconditioner(pcf_handle *h, const double *sin_, double *sout,
+                             const pcf_params *prm, int precision);
+
+/* apply_bicgstab!: solves A s = rhs with the handle's current operator;
+ * interior arrays. */
+int pcf_bicgstab(pcf_handle *h, const double *rhs, double tolref, const pcf_params *prm,
+                 double *solution, pcf_result *res);
+
+/* compute_global_dot_product: deterministic FP64 sum of a[i]*b[i] over the
+ * interior (n = nx*ny*nz elements); result in *out. */
+int pcf_global_dot(pcf_handle *h, const double *a, const double *b, double *out);
+
+/* Device memory held by the handle, in bytes. */
+long long pcf_device_bytes(const pcf_handle *h);
+
+/* Instrumentation (no reference counterpart).  Kernels launched by the handle
+ * since creation; per-kernel-class device time measured with CUDA events on
+ * the handle's stream while profiling is on.  Launches issued after a
+ * BiCGSTAB run converged (which return at once) are not counted.
+ * `bytes` is the algorithmic traffic of the counted launches. */
+enum pcf_prof_tag {
+    PCF_PROF_APPLY32 = 0,   /* Total operator apply, FP32, fused dots */
+    PCF_PROF_APPLY64 = 1,   /* Total operator apply, FP64, fused dots / residual */
+    PCF_PROF_PSEUDO32 = 2,  /* Horizontal apply + pseudo-time step, FP32 */
+    PCF_PROF_PSEUDO64 = 3,
+    PCF_PROF_THOMAS32 = 4,  /* column tridiagonal sweeps, FP32 */
+    PCF_PROF_THOMAS64 = 5,
+    PCF_PROF_UPDATE32 = 6,  /* BiCGSTAB vector updates, FP32 */
+    PCF_PROF_UPDATE64 = 7,
+    PCF_PROF_ASSEMBLE = 8,  /* operator assembly + factors */
+    PCF_PROF_NTAGS = 9
+};
+long long pcf_launch_count(const pcf_handle *h);
+int pcf_profile_enable(pcf_handle *h, int on);  /* also clears the accumulators */
+int pcf_profile_read(const pcf_handle *h, int tag, double *ms, long long *count, double *bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PINCFLOW_POISSON_H */

@@ -1,0 +1,202 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+The oracle is a literal FP64 C++ restatement of PinCFlow.jl's Poisson path
+(see pcf_oracle.h for the per-function reference citations).  Only tests/,
+``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use this module;
+the product never imports it.
+
+Parity status: PARITY UNPINNED by reference golden vectors (the reference
+ships none for the Poisson path and Julia cannot run here); pinned instead to
+analytic known-answer tests in tests/test_oracle_kat.py.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libpcf_oracle.so")
+
+NCOEF = 25
+# Plane order of the reference Tensor struct (src/Types/PoissonTypes/Tensor.jl:70-96).
+COEF_NAMES = ["ac", "al", "ar", "ab", "af", "ad", "au", "ald", "alu", "ard", "aru", "abd",
+              "abu", "afd", "afu", "add", "auu", "aldd", "aluu", "ardd", "aruu", "abdd",
+              "abuu", "afdd", "afuu"]
+MODELS = {"Boussinesq": 0, "PseudoIncompressible": 1, "Compressible": 2}
+
+
+class Dims(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("nx", "ny", "nz", "nbx", "nby", "nbz", "ko", "z_size")]
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        d = ctypes.POINTER(ctypes.c_double)
+        _lib.or_dot.restype = ctypes.c_double
+        _lib.or_compute_lhs.restype = ctypes.c_double
+        _lib.or_grid.restype = ctypes.c_int
+        _lib.or_solve_poisson.restype = ctypes.c_int
+        del d
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _pn(a):
+    return None if a is None else _p(a)
+
+
+def dims(nx, ny, nz, nb=3):
+    return Dims(nx, ny, nz, nb, nb, nb, 0, nz)
+
+
+def halo_shape(d: Dims):
+    """Shape of a haloed field in C order (k, j, i): x is fastest as in Julia."""
+    return (d.nz + 2 * d.nbz, d.ny + 2 * d.nby, d.nx + 2 * d.nbx)
+
+
+def interior_shape(d: Dims):
+    return (d.nz, d.ny, d.nx)
+
+
+def set_threads(n: int):
+    lib().or_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return lib().or_get_threads()
+
+
+def constants() -> dict:
+    out = np.zeros(12)
+    lib().or_constants(_p(out))
+    keys = ["gamma", "kappa", "rsp", "g", "rhoref", "pref", "lref", "tref", "thetaref",
+            "g_ndim", "ma", "sig"]
+    return dict(zip(keys, out.tolist()))
+
+
+def grid(d: Dims, lx, ly, lz, stretch_exp, hb_dim):
+    hs = halo_shape(d)
+    jac, m13, m23, m33, zc = (np.zeros(hs) for _ in range(5))
+    dxyz = np.zeros(3)
+    hb = np.ascontiguousarray(hb_dim, dtype=np.float64).reshape(d.ny, d.nx)
+    rc = lib().or_grid(ctypes.byref(d), ctypes.c_double(lx), ctypes.c_double(ly),
+                       ctypes.c_double(lz), ctypes.c_double(stretch_exp), _p(hb), _p(jac),
+                       _p(m13), _p(m23), _p(m33), _p(zc), _p(dxyz))
+    if rc != 0:
+        raise ValueError("impossible vertical grid stretching")
+    return dict(jac=jac, met13=m13, met23=m23, met33=m33, zc=zc, dx=dxyz[0], dy=dxyz[1],
+                dz=dxyz[2])
+
+
+def atmosphere(d: Dims, background: int, params, jac, zc, dz):
+    hs = halo_shape(d)
+    pbar, thetabar, rhobar, n2 = (np.zeros(hs) for _ in range(4))
+    prm = np.asarray(params, dtype=np.float64)
+    rc = lib().or_atmosphere(ctypes.byref(d), background, _p(prm), _p(jac), _p(zc),
+                             ctypes.c_double(dz), _p(pbar), _p(thetabar), _p(rhobar), _p(n2))
+    assert rc == 0
+    return dict(pbar=pbar, thetabar=thetabar, rhobar=rhobar, n2=n2)
+
+
+def sponge_sin2(d: Dims, zc, zr, lz, dt):
+    betar = np.zeros(halo_shape(d))
+    lib().or_sponge_sin2(ctypes.byref(d), _p(zc), ctypes.c_double(zr), ctypes.c_double(lz),
+                         ctypes.c_double(dt), _p(betar))
+    return betar
+
+
+def compute_operator(d: Dims, model, f: dict, rho, betar, dt, rayleigh_factor,
+                     damp_horizontal_wind_on_rhs=False, p=None):
+    coef = np.zeros((NCOEF,) + interior_shape(d))
+    lib().or_compute_operator(
+        ctypes.byref(d), int(model), ctypes.c_double(f["dx"]), ctypes.c_double(f["dy"]),
+        ctypes.c_double(f["dz"]), _p(f["jac"]), _p(f["met13"]), _p(f["met23"]),
+        _p(f["met33"]), _p(f["pbar"]), _p(f["rhobar"]), _pn(f.get("thetabar")), _p(f["n2"]),
+        _p(rho), _p(betar), _pn(p), ctypes.c_double(dt), ctypes.c_double(rayleigh_factor),
+        int(bool(damp_horizontal_wind_on_rhs)), _p(coef))
+    return coef
+
+
+def apply_operator(d: Dims, coef, s, horizontal=False):
+    out = np.zeros(interior_shape(d))
+    lib().or_apply_operator(ctypes.byref(d), _p(coef), _p(np.ascontiguousarray(s)), _p(out),
+                            int(bool(horizontal)))
+    return out
+
+
+def apply_preconditioner(d: Dims, coef, dx, dy, dtau, iters, s):
+    out = np.zeros(interior_shape(d))
+    lib().or_apply_preconditioner(ctypes.byref(d), _p(coef), ctypes.c_double(dx),
+                                  ctypes.c_double(dy), ctypes.c_double(dtau), int(iters),
+                                  _p(np.ascontiguousarray(s)), _p(out))
+    return out
+
+
+def bicgstab(d: Dims, coef, dx, dy, rhs, tolerance=1e-8, poisson_iterations=1000,
+             preconditioner=True, dtau=1.0, preconditioner_iterations=2,
+             tolerance_is_relative=False, tolref=1.0):
+    sol = np.zeros(interior_shape(d))
+    out = np.zeros(4)
+    lib().or_bicgstab(ctypes.byref(d), _p(coef), ctypes.c_double(dx), ctypes.c_double(dy),
+                      ctypes.c_double(tolerance), int(poisson_iterations), int(bool(preconditioner)),
+                      ctypes.c_double(dtau), int(preconditioner_iterations),
+                      int(bool(tolerance_is_relative)), ctypes.c_double(tolref),
+                      _p(np.ascontiguousarray(rhs)), _p(sol), _p(out))
+    return sol, dict(errflag=bool(out[0]), niter=int(out[1]), residual=out[2], b_norm=out[3])
+
+
+def solve_poisson(d: Dims, model, f: dict, rho, betar, rhs, dt, rayleigh_factor, tolref=1.0,
+                  damp_horizontal_wind_on_rhs=False, p=None, tolerance=1e-8,
+                  poisson_iterations=1000, preconditioner=True, dtau=1.0,
+                  preconditioner_iterations=2, tolerance_is_relative=False):
+    dpip = np.zeros(halo_shape(d))
+    out = np.zeros(4)
+    rc = lib().or_solve_poisson(
+        ctypes.byref(d), int(model), ctypes.c_double(f["dx"]), ctypes.c_double(f["dy"]),
+        ctypes.c_double(f["dz"]), _p(f["jac"]), _p(f["met13"]), _p(f["met23"]),
+        _p(f["met33"]), _p(f["pbar"]), _p(f["rhobar"]), _pn(f.get("thetabar")), _p(f["n2"]),
+        _p(rho), _p(betar), _pn(p), ctypes.c_double(dt), ctypes.c_double(rayleigh_factor),
+        int(bool(damp_horizontal_wind_on_rhs)), ctypes.c_double(tolerance),
+        int(poisson_iterations), int(bool(preconditioner)), ctypes.c_double(dtau),
+        int(preconditioner_iterations), int(bool(tolerance_is_relative)),
+        ctypes.c_double(tolref), _p(np.ascontiguousarray(rhs)), _p(dpip), _p(out))
+    if rc != 0:
+        raise ZeroDivisionError("Error in solve_poisson!: dt = 0.0!")
+    return dpip, dict(errflag=bool(out[0]), niter=int(out[1]), residual=out[2], b_norm=out[3])
+
+
+def compute_lhs(d: Dims, f: dict, u, v, w):
+    c = constants()
+    rhs = np.zeros(interior_shape(d))
+    tolref = lib().or_compute_lhs(ctypes.byref(d), ctypes.c_double(f["dx"]),
+                                  ctypes.c_double(f["dy"]), ctypes.c_double(f["dz"]),
+                                  ctypes.c_double(c["ma"]), ctypes.c_double(c["kappa"]),
+                                  _p(f["jac"]), _p(f["pbar"]), _p(f["rhobar"]), _p(u), _p(v),
+                                  _p(w), _p(rhs))
+    return rhs, tolref
+
+
+def dot(a, b) -> float:
+    a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+    b = np.ascontiguousarray(b, dtype=np.float64).ravel()
+    return lib().or_dot(ctypes.c_long(a.size), _p(a), _p(b))

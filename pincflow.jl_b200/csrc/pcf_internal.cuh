@@ -1,0 +1,130 @@
+// pcf_internal.cuh -- shared definitions of the sm_100a Poisson solver.
+//
+// Device data layout (all interior arrays x fastest, no padding):
+//   vectors             n = nx*ny*nz elements, index i + nx*(j + ny*k)
+//   operator planes     25 planes of n elements each, plane c at offset c*n,
+//                       in the reference Tensor order (enum pcf_coef)
+//   Thomas factors      3 planes (P, M, Q) of n elements: the pivots of the
+//                       preconditioner's vertical tridiagonal systems, which
+//                       depend only on ac, ad, au and d_eta
+//   haloed fields       (nx+2nbx)*(ny+2nby)*(nz+2nbz) FP64, the caller's layout
+// FP64 and FP32 copies of the operator and factors are both kept: FP64 for
+// the reference-precision path and the true residual, FP32 for the inner
+// iterations of the mixed-precision solve.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/pincflow_poisson.h"
+
+#define PCF_CUDA_TRY(expr)                                    \
+    do {                                                      \
+        cudaError_t e_ = (expr);                              \
+        if (e_ != cudaSuccess) return pcf_set_cuda_error(e_); \
+    } while (0)
+
+int pcf_set_cuda_error(cudaError_t e);
+
+namespace pcf {
+
+constexpr int kNumCoef = PCF_NCOEF;
+constexpr int kMaxPartials = 16384;  // per-block partial sums of one reduction
+
+// Scalars of one BiCGSTAB run, resident on the device so that no host round
+// trip is needed between the kernels of an iteration.
+struct KrylovScalars {
+    double rho;       // <r, r0> of the current iterate
+    double alpha, omega, beta;
+    double res;       // RMS of the recursive residual
+    double b_norm;    // RMS of the initial residual
+    double tol;       // relative tolerance on res / b_norm
+    double ncell;     // x_size * y_size * z_size
+    double last_dot[2];
+    int iter;         // completed iterations
+    int maxit;
+    int done;         // 1 once converged, failed or broken down
+    int converged;
+    int status;       // PCF_OK, PCF_EBREAKDOWN, PCF_ENONFINITE
+    int pad;
+};
+
+// Finalisation performed by the last block of a fused reduction kernel.
+enum FinalOp : int {
+    FIN_STORE = 0,   // last_dot[0..1] = sums
+    FIN_INIT = 1,    // sums[0] = <r, r>: b_norm, rho and the early exit
+    FIN_ALPHA = 2,   // sums[0] = <v, r0>: alpha = rho / <v, r0>
+    FIN_OMEGA = 3,   // sums[0] = <t, s>, sums[1] = <t, t>: omega
+    FIN_RESID = 4    // sums[0] = <r, r>, sums[1] = <r, r0>: test, beta, rho
+};
+
+struct ReduceCtx {
+    double *partials;         // [2 * kMaxPartials]
+    unsigned int *ticket;     // zero between uses
+    KrylovScalars *scal;
+    double *out;              // FIN_STORE target (may be null)
+    int op;
+};
+
+struct Dims {
+    int nx, ny, nz;
+    long long n;    // nx*ny*nz
+    int plane;      // nx*ny
+};
+
+// Kernel-timing records (pcf_profile_*): one CUDA event pair per tagged
+// launch, kept with the BiCGSTAB iteration it belongs to so that launches
+// made after convergence (which return at once) can be left out.
+struct ProfRec {
+    cudaEvent_t a, b;
+    int tag;
+    int iter;
+    double bytes;
+};
+struct ProfAcc {
+    double ms;
+    long long count;
+    double bytes;
+};
+struct ProfState;  // defined in pcf_solver.cu
+
+}  // namespace pcf
+
+// The opaque handle of the C ABI.
+struct pcf_handle {
+    pcf_dims dims;
+    pcf::Dims d;
+    int nxx, nyy, nzz;
+    long long nh;  // haloed element count
+    double dx, dy, dz;
+    int grid_set, background_set, operator_set;
+    cudaStream_t stream;
+    cudaEvent_t ev[8];
+
+    // haloed FP64 fields
+    double *jac, *met13, *met23, *met33, *pbar, *rhobar, *thetabar, *n2;
+    double *rho, *betar, *p;
+    // operator and Thomas factors
+    double *coef64;
+    float *coef32;
+    double *fac64;
+    float *fac32;
+    double fac_deta;  // d_eta the factors were built with (NaN: none)
+    // FP64 Krylov vectors
+    double *x64, *r64, *r064, *p64, *v64, *s64, *t64, *za64, *zb64, *b64, *w64;
+    // FP32 Krylov vectors
+    float *x32, *r32, *r032, *p32, *v32, *s32, *t32, *za32, *zb32;
+    // reductions
+    double *partials;
+    unsigned int *ticket;
+    pcf::KrylovScalars *scal64, *scal32;
+    double *dot_out;
+    pcf::KrylovScalars *h_scal;  // pinned mirror
+    long long bytes;
+    // instrumentation
+    long long launches;          // kernels launched by this handle
+    int prof_on;                 // record per-launch events
+    int prof_iter;               // iteration index of the launches being issued
+    pcf::ProfState *prof;
+    pcf::ProfAcc prof_acc[PCF_PROF_NTAGS];
+};

@@ -1,0 +1,563 @@
+// pcf_kernels.cuh -- device kernels of the Krylov loop, templated on the
+// working precision T (double for the reference path and the true residual,
+// float for the inner iterations of the mixed-precision solve).
+//
+//   k_stencil   25-point operator apply (apply_operator!.jl:48-479), Total or
+//               Horizontal, with fused epilogues (dot products for BiCGSTAB,
+//               the preconditioner's pseudo-time step, the true residual)
+//   k_thomas    the preconditioner's per-column tridiagonal solve
+//               (apply_preconditioner!.jl:73-111) with fused input forming
+//   k_update    BiCGSTAB solution / residual updates with fused dots
+//               (apply_bicgstab!.jl:110-123)
+// All global sums accumulate in FP64 and are reduced deterministically: one
+// partial per block, then the last block to finish sums the partials in block
+// order and runs the scalar step of the iteration (KrylovScalars).
+#pragma once
+
+#include "pcf_internal.cuh"
+
+namespace pcf {
+
+// ---------------------------------------------------------------- helpers --
+
+template <typename T, int V>
+struct Vec;
+template <>
+struct Vec<float, 4> {
+    using type = float4;
+};
+template <>
+struct Vec<float, 2> {
+    using type = float2;
+};
+template <>
+struct Vec<float, 1> {
+    using type = float;
+};
+template <>
+struct Vec<double, 2> {
+    using type = double2;
+};
+template <>
+struct Vec<double, 1> {
+    using type = double;
+};
+
+template <typename T, int V>
+__device__ __forceinline__ void load_vec(const T *__restrict__ p, T (&v)[V]) {
+    using VT = typename Vec<T, V>::type;
+    const VT x = __ldg(reinterpret_cast<const VT *>(p));
+    const T *e = reinterpret_cast<const T *>(&x);
+#pragma unroll
+    for (int q = 0; q < V; ++q) v[q] = e[q];
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void store_vec(T *__restrict__ p, const T (&v)[V]) {
+    using VT = typename Vec<T, V>::type;
+    VT x;
+    T *e = reinterpret_cast<T *>(&x);
+#pragma unroll
+    for (int q = 0; q < V; ++q) e[q] = v[q];
+    *reinterpret_cast<VT *>(p) = x;
+}
+
+__device__ __forceinline__ int wrap(int x, int n) {
+    x %= n;
+    return x < 0 ? x + n : x;
+}
+
+// Block-wide sum of NV values; the result is valid in thread 0.  The order
+// of additions depends only on blockDim, so it is deterministic.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *sh) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+    const int lane = tid & 31, warp = tid >> 5, nw = (nthreads + 31) >> 5;
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) sh[q * 32 + warp] = v[q];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            v[q] = lane < nw ? sh[q * 32 + lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+        }
+    }
+}
+
+__device__ __forceinline__ bool finite(double x) { return isfinite(x); }
+
+// Scalar step run by one thread once all partial sums of a kernel are in.
+template <int NV>
+__device__ void finalize(const ReduceCtx &c, const double (&s)[NV]) {
+    KrylovScalars *k = c.scal;
+    switch (c.op) {
+        case FIN_STORE:
+#pragma unroll
+            for (int q = 0; q < NV; ++q) c.out[q] = s[q];
+            break;
+        case FIN_INIT: {  // apply_bicgstab!.jl:63-76
+            const double res = sqrt(s[0] / k->ncell);
+            k->res = res;
+            k->b_norm = res;
+            k->rho = s[0];
+            k->alpha = 0.0;
+            k->omega = 0.0;
+            k->beta = 0.0;
+            k->iter = 0;
+            k->converged = 0;
+            k->status = PCF_OK;
+            k->done = 0;
+            if (!finite(res)) {
+                k->status = PCF_ENONFINITE;
+                k->done = 1;
+            } else if (res == 0.0 || res / res <= k->tol) {
+                k->converged = 1;
+                k->done = 1;
+            }
+            break;
+        }
+        case FIN_ALPHA: {  // :93-95
+            k->last_dot[0] = s[0];
+            const double alpha = k->rho / s[0];
+            k->alpha = alpha;
+            if (!finite(alpha)) {
+                k->status = PCF_EBREAKDOWN;
+                k->done = 1;
+            }
+            break;
+        }
+        case FIN_OMEGA: {  // :107-109
+            const double omega = s[0] / s[1];
+            k->omega = omega;
+            if (!finite(omega) || omega == 0.0) {
+                k->status = PCF_EBREAKDOWN;
+                k->done = 1;
+            }
+            break;
+        }
+        case FIN_RESID: {  // :119-143
+            k->iter += 1;
+            const double res = sqrt(s[0] / k->ncell);
+            k->res = res;
+            if (!finite(res)) {
+                k->status = PCF_ENONFINITE;
+                k->done = 1;
+            } else if (res / k->b_norm <= k->tol) {
+                k->converged = 1;
+                k->done = 1;
+            } else if (k->iter >= k->maxit) {
+                k->done = 1;
+            } else {
+                const double beta = k->alpha / k->omega * s[1] / k->rho;
+                k->beta = beta;
+                k->rho = s[1];
+                if (!finite(beta)) {
+                    k->status = PCF_EBREAKDOWN;
+                    k->done = 1;
+                }
+            }
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+// Writes this block's partial sums; the last block sums all partials in block
+// order and runs finalize().  All threads of the block must call it.
+template <int NV>
+__device__ void reduce_finalize(const ReduceCtx &c, double (&v)[NV]) {
+    __shared__ double sh[NV * 32];
+    __shared__ int is_last;
+    block_sum<NV>(v, sh);
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+    const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) c.partials[q * kMaxPartials + bid] = v[q];
+        __threadfence();
+        const unsigned t = atomicAdd(c.ticket, 1u);
+        is_last = (t == nblk - 1);
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+    for (unsigned b = tid; b < nblk; b += nthreads)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[q] += __ldcg(c.partials + q * kMaxPartials + b);
+    block_sum<NV>(acc, sh);
+    if (tid == 0) {
+        finalize<NV>(c, acc);
+        *c.ticket = 0u;
+        __threadfence();
+    }
+}
+
+__device__ __forceinline__ bool krylov_done(const KrylovScalars *s) {
+    return s != nullptr && *((volatile const int *)&s->done) != 0;
+}
+
+// ----------------------------------------------------------- stencil apply --
+
+enum Epi : int {
+    EPI_STORE = 0,    // out = A s
+    EPI_DOT1 = 1,     // out = A s;  sum out*w1                      (<v, r0>)
+    EPI_DOT2 = 2,     // out = A s;  sum out*w1, sum out*out         (<t, s>, <t, t>)
+    EPI_PSEUDO = 3,   // out = s + d_eta (L_h s - b)                 (pseudo-time step)
+    EPI_RESID = 4     // out = b - A s;  sum out*out                 (true residual)
+};
+
+template <typename T>
+struct StencilArgs {
+    const T *coef;        // 25 planes
+    const T *s;           // input vector
+    T *out;
+    const T *w1;          // EPI_DOT1/2: second operand; EPI_PSEUDO/RESID: b
+    int nx, ny, nz;
+    long long n;
+    double deta;
+    ReduceCtx red;
+    const KrylovScalars *guard;  // skip when guard->done (may be null)
+};
+
+// Shared-memory ring of z-planes of the input: NS slots of (TY+2) x (TX*V+2)
+// values (one ghost ring, periodic in x and y, zero outside the walls).
+// Each block marches up a z-chunk of kc levels; every level reads one new
+// plane, so s is read from L2/HBM about once per apply while the 25
+// coefficient planes stream through with 128-bit loads along x.
+template <typename T, int V, int TX, int TY>
+struct Ring {
+    static constexpr int W = TX * V;
+    static constexpr int RW = W + 2;
+    static constexpr int NR = TY + 2;
+    static constexpr int NS = 6;
+    static constexpr int ROWS_PER_THREAD = (NR + TY - 1) / TY;
+};
+
+template <typename T, int V, int TX, int TY>
+__device__ __forceinline__ void ring_fetch(const T *__restrict__ s, int nx, int ny, int nz, int x0, int y0,
+                                           int kk, T (&rv)[Ring<T, V, TX, TY>::ROWS_PER_THREAD][V], T &hv) {
+    using R = Ring<T, V, TX, TY>;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const bool inz = kk >= 0 && kk < nz;
+    const long long zoff = (long long)nx * ny * (inz ? kk : 0);
+#pragma unroll
+    for (int q = 0; q < R::ROWS_PER_THREAD; ++q) {
+        const int rr = ty + q * TY;
+        if (rr < R::NR && inz) {
+            const int y = wrap(y0 - 1 + rr, ny);
+            const int x = wrap(x0 + tx * V, nx);
+            load_vec<T, V>(s + zoff + (long long)nx * y + x, rv[q]);
+        } else {
+#pragma unroll
+            for (int e = 0; e < V; ++e) rv[q][e] = T(0);
+        }
+    }
+    const int lt = tx + TX * ty;
+    hv = T(0);
+    if (lt < 2 * R::NR && inz) {
+        const int rr = lt >> 1;
+        const int y = wrap(y0 - 1 + rr, ny);
+        const int x = (lt & 1) ? wrap(x0 + R::W, nx) : wrap(x0 - 1, nx);
+        hv = __ldg(s + zoff + (long long)nx * y + x);
+    }
+}
+
+template <typename T, int V, int TX, int TY>
+__device__ __forceinline__ void ring_store(T *slot, const T (&rv)[Ring<T, V, TX, TY>::ROWS_PER_THREAD][V], T hv) {
+    using R = Ring<T, V, TX, TY>;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+    for (int q = 0; q < R::ROWS_PER_THREAD; ++q) {
+        const int rr = ty + q * TY;
+        if (rr < R::NR)
+#pragma unroll
+            for (int e = 0; e < V; ++e) slot[rr * R::RW + 1 + tx * V + e] = rv[q][e];
+    }
+    const int lt = tx + TX * ty;
+    if (lt < 2 * R::NR) {
+        const int rr = lt >> 1;
+        slot[rr * R::RW + ((lt & 1) ? R::W + 1 : 0)] = hv;
+    }
+}
+
+template <typename T, int V, int TX, int TY, bool HORIZ, int EPI>
+__global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
+    using R = Ring<T, V, TX, TY>;
+    __shared__ __align__(16) T sm[R::NS][R::NR * R::RW];
+    if (krylov_done(a.guard)) return;
+
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x0 = blockIdx.x * R::W, y0 = blockIdx.y * TY;
+    const int k0 = blockIdx.z * kc;
+    const int k1 = min(k0 + kc, a.nz);
+    const int x = x0 + tx * V, y = y0 + ty;
+    const bool active = x < a.nx && y < a.ny;
+    const long long plane = (long long)a.nx * a.ny;
+    const long long n = a.n;
+
+    double d0 = 0.0, d1 = 0.0;
+    T rv[R::ROWS_PER_THREAD][V];
+    T hv;
+    // prologue: planes k0-2 .. k0+2
+#pragma unroll
+    for (int dz = -2; dz <= 2; ++dz) {
+        const int kk = k0 + dz;
+        ring_fetch<T, V, TX, TY>(a.s, a.nx, a.ny, a.nz, x0, y0, kk, rv, hv);
+        ring_store<T, V, TX, TY>(sm[(kk + 12) % R::NS], rv, hv);
+    }
+    __syncthreads();
+
+    const int r = ty + 1;
+    for (int k = k0; k < k1; ++k) {
+        // prefetch plane k+3 into registers while level k is computed
+        ring_fetch<T, V, TX, TY>(a.s, a.nx, a.ny, a.nz, x0, y0, k + 3, rv, hv);
+        if (active) {
+            const long long base = plane * k + (long long)a.nx * y + x;
+            T c[PCF_NCOEF][V];
+#pragma unroll
+            for (int p = 0; p < PCF_NCOEF; ++p) {
+                if (HORIZ && (p == PCF_AC || p == PCF_AD || p == PCF_AU)) continue;
+                load_vec<T, V>(a.coef + (long long)p * n + base, c[p]);
+            }
+            const T *sm2 = sm[(k + 10) % R::NS], *sm1 = sm[(k + 11) % R::NS], *s0 = sm[(k + 12) % R::NS],
+                    *sp1 = sm[(k + 13) % R::NS], *sp2 = sm[(k + 14) % R::NS];
+            T res[V];
+#pragma unroll
+            for (int e = 0; e < V; ++e) {
+                const int cc = 1 + tx * V + e;
+                const int ic = r * R::RW + cc;
+                const int il = ic - 1, ir = ic + 1, ib = ic - R::RW, iff = ic + R::RW;
+                T acc;
+                if (HORIZ) {
+                    acc = c[PCF_AL][e] * s0[il];
+                } else {
+                    acc = c[PCF_AC][e] * s0[ic];
+                    acc = fma(c[PCF_AD][e], sm1[ic], acc);
+                    acc = fma(c[PCF_AU][e], sp1[ic], acc);
+                    acc = fma(c[PCF_AL][e], s0[il], acc);
+                }
+                acc = fma(c[PCF_AR][e], s0[ir], acc);
+                acc = fma(c[PCF_AB][e], s0[ib], acc);
+                acc = fma(c[PCF_AF][e], s0[iff], acc);
+                acc = fma(c[PCF_ALD][e], sm1[il], acc);
+                acc = fma(c[PCF_ALU][e], sp1[il], acc);
+                acc = fma(c[PCF_ARD][e], sm1[ir], acc);
+                acc = fma(c[PCF_ARU][e], sp1[ir], acc);
+                acc = fma(c[PCF_ABD][e], sm1[ib], acc);
+                acc = fma(c[PCF_ABU][e], sp1[ib], acc);
+                acc = fma(c[PCF_AFD][e], sm1[iff], acc);
+                acc = fma(c[PCF_AFU][e], sp1[iff], acc);
+                acc = fma(c[PCF_ADD][e], sm2[ic], acc);
+                acc = fma(c[PCF_AUU][e], sp2[ic], acc);
+                acc = fma(c[PCF_ALDD][e], sm2[il], acc);
+                acc = fma(c[PCF_ALUU][e], sp2[il], acc);
+                acc = fma(c[PCF_ARDD][e], sm2[ir], acc);
+                acc = fma(c[PCF_ARUU][e], sp2[ir], acc);
+                acc = fma(c[PCF_ABDD][e], sm2[ib], acc);
+                acc = fma(c[PCF_ABUU][e], sp2[ib], acc);
+                acc = fma(c[PCF_AFDD][e], sm2[iff], acc);
+                acc = fma(c[PCF_AFUU][e], sp2[iff], acc);
+                res[e] = acc;
+            }
+            if (EPI == EPI_STORE) {
+                store_vec<T, V>(a.out + base, res);
+            } else if (EPI == EPI_DOT1 || EPI == EPI_DOT2) {
+                T w[V];
+                load_vec<T, V>(a.w1 + base, w);
+#pragma unroll
+                for (int e = 0; e < V; ++e) {
+                    d0 += (double)res[e] * (double)w[e];
+                    if (EPI == EPI_DOT2) d1 += (double)res[e] * (double)res[e];
+                }
+                store_vec<T, V>(a.out + base, res);
+            } else if (EPI == EPI_PSEUDO) {
+                T b[V];
+                load_vec<T, V>(a.w1 + base, b);
+                const T deta = (T)a.deta;
+#pragma unroll
+                for (int e = 0; e < V; ++e) res[e] = s0[r * R::RW + 1 + tx * V + e] + deta * (res[e] - b[e]);
+                store_vec<T, V>(a.out + base, res);
+            } else if (EPI == EPI_RESID) {
+                T b[V];
+                load_vec<T, V>(a.w1 + base, b);
+#pragma unroll
+                for (int e = 0; e < V; ++e) {
+                    res[e] = b[e] - res[e];
+                    d0 += (double)res[e] * (double)res[e];
+                }
+                store_vec<T, V>(a.out + base, res);
+            }
+        }
+        ring_store<T, V, TX, TY>(sm[(k + 15) % R::NS], rv, hv);
+        __syncthreads();
+    }
+
+    if (EPI == EPI_DOT1 || EPI == EPI_RESID) {
+        double v[1] = {d0};
+        reduce_finalize<1>(a.red, v);
+    } else if (EPI == EPI_DOT2) {
+        double v[2] = {d0, d1};
+        reduce_finalize<2>(a.red, v);
+    }
+}
+
+// --------------------------------------------------------- Thomas sweeps --
+
+enum ThomasIn : int {
+    TH_B = 0,       // rhs = -d_eta b                          (first pseudo-time step)
+    TH_T = 1,       // rhs = t (in place allowed)              (later pseudo-time steps)
+    TH_SUPD = 2,    // s = r - alpha v (stored); rhs = -d_eta s
+    TH_PUPD = 3     // p = r + beta (p - omega v) (stored); rhs = -d_eta p
+};
+
+template <typename T>
+struct ThomasArgs {
+    const T *fac;   // P, M, Q planes
+    const T *in;    // TH_B: b; TH_T: t
+    const T *r, *v;
+    T *vec;         // TH_SUPD: s (out); TH_PUPD: p (in/out)
+    T *out;
+    int plane, nz;
+    long long n;
+    double deta;
+    const KrylovScalars *scal;  // alpha, beta, omega; skip when done
+};
+
+// One thread per column, lanes along x (coalesced).  Forward elimination
+// writes y_k to out, back substitution overwrites it with the solution.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(128) k_thomas(ThomasArgs<T> a) {
+    if (krylov_done(a.scal)) return;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= a.plane) return;
+    const T *P = a.fac, *M = a.fac + a.n, *Q = a.fac + 2 * a.n;
+    const T deta = (T)a.deta;
+    T alpha = 0, beta = 0, omega = 0;
+    if (MODE == TH_SUPD || MODE == TH_PUPD) {
+        alpha = (T)a.scal->alpha;
+        beta = (T)a.scal->beta;
+        omega = (T)a.scal->omega;
+    }
+    T y = 0;
+#pragma unroll 4
+    for (int k = 0; k < a.nz; ++k) {
+        const long long o = col + (long long)a.plane * k;
+        T rhs;
+        if (MODE == TH_B) {
+            rhs = -deta * __ldg(a.in + o);
+        } else if (MODE == TH_T) {
+            rhs = a.in[o];
+        } else if (MODE == TH_SUPD) {
+            const T sv = a.r[o] - alpha * a.v[o];
+            a.vec[o] = sv;
+            rhs = -deta * sv;
+        } else {
+            const T pv = a.r[o] + beta * (a.vec[o] - omega * a.v[o]);
+            a.vec[o] = pv;
+            rhs = -deta * pv;
+        }
+        y = rhs * __ldg(P + o) + __ldg(M + o) * y;
+        a.out[o] = y;
+    }
+    T xs = y;
+#pragma unroll 4
+    for (int k = a.nz - 2; k >= 0; --k) {
+        const long long o = col + (long long)a.plane * k;
+        xs = a.out[o] + __ldg(Q + o) * xs;
+        a.out[o] = xs;
+    }
+}
+
+// ------------------------------------------------------- vector updates --
+
+template <typename T>
+struct UpdateArgs {
+    T *x, *r;
+    const T *p, *s, *t, *r0;
+    long long n;
+    ReduceCtx red;
+    KrylovScalars *scal;
+};
+
+// x += alpha p + omega s; r = s - omega t; sums <r, r> and <r, r0>
+// (apply_bicgstab!.jl:110-120).
+template <typename T>
+__global__ void __launch_bounds__(256) k_update(UpdateArgs<T> a) {
+    if (krylov_done(a.scal)) return;
+    const T alpha = (T)a.scal->alpha, omega = (T)a.scal->omega;
+    double rr = 0.0, rr0 = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const T sv = a.s[i];
+        a.x[i] = a.x[i] + (alpha * a.p[i] + omega * sv);
+        const T rv = sv - omega * a.t[i];
+        a.r[i] = rv;
+        rr += (double)rv * (double)rv;
+        rr0 += (double)rv * (double)a.r0[i];
+    }
+    double v[2] = {rr, rr0};
+    reduce_finalize<2>(a.red, v);
+}
+
+// Start of a BiCGSTAB run from x = 0: r0 = r = p = b, x = 0, sum <b, b>
+// (apply_bicgstab!.jl:44-67).
+template <typename T>
+__global__ void __launch_bounds__(256) k_init(const T *__restrict__ b, T *x, T *r, T *r0, T *p, long long n,
+                                              ReduceCtx red) {
+    double bb = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const T v = b[i];
+        x[i] = T(0);
+        r[i] = v;
+        r0[i] = v;
+        p[i] = v;
+        bb += (double)v * (double)v;
+    }
+    double v[1] = {bb};
+    reduce_finalize<1>(red, v);
+}
+
+// Generic sum of a*b (compute_global_dot_product).
+template <typename T>
+__global__ void __launch_bounds__(256) k_dot(const T *__restrict__ a, const T *__restrict__ b, long long n,
+                                             ReduceCtx red) {
+    double s = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        s += (double)a[i] * (double)b[i];
+    double v[1] = {s};
+    reduce_finalize<1>(red, v);
+}
+
+// Without preconditioner: s = r - alpha v or p = r + beta (p - omega v).
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_axpy_noprec(const T *r, const T *v, T *vec, long long n,
+                                                     const KrylovScalars *scal) {
+    if (krylov_done(scal)) return;
+    const T alpha = (T)scal->alpha, beta = (T)scal->beta, omega = (T)scal->omega;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (MODE == TH_SUPD)
+            vec[i] = r[i] - alpha * v[i];
+        else
+            vec[i] = r[i] + beta * (vec[i] - omega * v[i]);
+    }
+}
+
+}  // namespace pcf

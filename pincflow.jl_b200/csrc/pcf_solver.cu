@@ -1,0 +1,973 @@
+// pcf_solver.cu -- the C ABI of include/pincflow_poisson.h: handle life cycle,
+// uploads, the BiCGSTAB driver (reference FP64 and mixed FP32/FP64) and the
+// component entry points.
+//
+// The Krylov loop follows apply_bicgstab!.jl:24-150 step by step; every
+// scalar (alpha, omega, beta, the residual test) lives on the device and is
+// computed by the last block of the kernel that produces its dot products, so
+// an iteration is a fixed sequence of launches with no host round trip.  The
+// host only polls the status word every `check_interval` iterations; kernels
+// launched after convergence see the done flag and return at once.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "pcf_kernels.cuh"
+
+namespace {
+thread_local cudaError_t g_last_cuda = cudaSuccess;
+}
+
+int pcf_set_cuda_error(cudaError_t e) {
+    g_last_cuda = e;
+    return e == cudaErrorMemoryAllocation ? PCF_ENOMEM : PCF_ECUDA;
+}
+
+int pcf_launch_assemble(pcf_handle *h, double dt, double rf, int damp_h);
+int pcf_launch_factors(pcf_handle *h, double deta);
+
+namespace pcf {
+
+// --------------------------------------------------------- instrumentation --
+
+struct ProfState {
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    std::vector<ProfRec> pending;
+};
+
+static cudaEvent_t prof_event(pcf_handle *h) {
+    ProfState *ps = h->prof;
+    if (ps->used == ps->pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        ps->pool.push_back(e);
+    }
+    return ps->pool[ps->used++];
+}
+
+// Times one launch when profiling is on; counts it always.
+struct ProfScope {
+    pcf_handle *h;
+    int tag;
+    double bytes;
+    cudaEvent_t a = nullptr;
+    ProfScope(pcf_handle *h_, int tag_, double bytes_) : h(h_), tag(tag_), bytes(bytes_) {
+        h->launches += 1;
+        if (h->prof_on && h->prof) {
+            a = prof_event(h);
+            if (a) cudaEventRecord(a, h->stream);
+        }
+    }
+    ~ProfScope() {
+        if (a) {
+            cudaEvent_t b = prof_event(h);
+            if (b) {
+                cudaEventRecord(b, h->stream);
+                h->prof->pending.push_back({a, b, tag, h->prof_iter, bytes});
+            }
+        }
+    }
+};
+
+// Accumulates the pending records (after a stream synchronisation); records
+// of iterations >= keep_below (launched after convergence) are dropped.
+static void prof_flush(pcf_handle *h, int keep_below) {
+    ProfState *ps = h->prof;
+    if (!ps) return;
+    if (!ps->pending.empty()) {
+        cudaStreamSynchronize(h->stream);
+        for (const ProfRec &r : ps->pending) {
+            if (r.iter >= 0 && r.iter >= keep_below) continue;
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) continue;
+            ProfAcc &acc = h->prof_acc[r.tag];
+            acc.ms += ms;
+            acc.count += 1;
+            acc.bytes += r.bytes;
+        }
+    }
+    ps->pending.clear();
+    ps->used = 0;
+}
+
+// ------------------------------------------------------------ launchers --
+
+static int num_sms() {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+static ReduceCtx red(pcf_handle *h, KrylovScalars *scal, int op, double *out = nullptr) {
+    ReduceCtx c;
+    c.partials = h->partials;
+    c.ticket = h->ticket;
+    c.scal = scal;
+    c.out = out;
+    c.op = op;
+    return c;
+}
+
+// Levels per block: enough z-chunks for ~8 blocks per SM, at least 8 levels
+// per chunk (each chunk re-reads 4 halo planes), at most kMaxPartials blocks.
+static int pick_kc(long long xyblocks, int nz) {
+    const long long want = 8LL * num_sms();
+    long long chunks = (want + xyblocks - 1) / xyblocks;
+    if (chunks < 1) chunks = 1;
+    long long kc = (nz + chunks - 1) / chunks;
+    if (kc < 8) kc = 8;
+    if (kc > nz) kc = nz;
+    while (kc < nz && xyblocks * ((nz + kc - 1) / kc) > kMaxPartials) kc = std::min<long long>(2 * kc, nz);
+    return (int)kc;
+}
+
+template <typename T, int V, int TX, bool HORIZ, int EPI>
+static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a) {
+    constexpr int TY = 128 / TX;
+    constexpr int W = TX * V;
+    const long long gx = (a.nx + W - 1) / W, gy = (a.ny + TY - 1) / TY;
+    const int kc = pick_kc(gx * gy, a.nz);
+    // one partial sum per block: the grid must fit the partials buffer
+    if (gx * gy * ((a.nz + kc - 1) / kc) > kMaxPartials || gy > 65535) return PCF_ERANGE;
+    const dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)((a.nz + kc - 1) / kc));
+    const dim3 block(TX, TY, 1);
+    // algorithmic words per cell: coefficient planes + input + output (+ second operand)
+    const int words = (HORIZ ? 22 : 25) + 2 + (EPI == EPI_STORE ? 0 : 1);
+    const int tag = HORIZ ? (sizeof(T) == 4 ? PCF_PROF_PSEUDO32 : PCF_PROF_PSEUDO64)
+                          : (sizeof(T) == 4 ? PCF_PROF_APPLY32 : PCF_PROF_APPLY64);
+    ProfScope ps(h, tag, (double)words * sizeof(T) * (double)a.n);
+    k_stencil<T, V, TX, TY, HORIZ, EPI><<<grid, block, 0, h->stream>>>(a, kc);
+    PCF_CUDA_TRY(cudaGetLastError());
+    return PCF_OK;
+}
+
+template <typename T, bool HORIZ, int EPI>
+static int launch_stencil(pcf_handle *h, StencilArgs<T> a) {
+    a.nx = h->d.nx;
+    a.ny = h->d.ny;
+    a.nz = h->d.nz;
+    a.n = h->d.n;
+    constexpr int VMAX = sizeof(T) == 4 ? 4 : 2;
+    const bool vec = (a.nx % VMAX) == 0;
+    const int wide = vec ? 32 * VMAX : 32;
+    if (a.nx >= wide) {
+        if (vec) return launch_stencil_cfg<T, VMAX, 32, HORIZ, EPI>(h, a);
+        return launch_stencil_cfg<T, 1, 32, HORIZ, EPI>(h, a);
+    }
+    if (vec) return launch_stencil_cfg<T, VMAX, 8, HORIZ, EPI>(h, a);
+    return launch_stencil_cfg<T, 1, 8, HORIZ, EPI>(h, a);
+}
+
+template <typename T, int MODE>
+static int launch_thomas(pcf_handle *h, const ThomasArgs<T> &a) {
+    const int bs = 128;
+    // input forming + P, M (forward) + y write, y read, Q, solution write
+    const int words = (MODE == TH_B || MODE == TH_T ? 1 : (MODE == TH_SUPD ? 3 : 4)) + 6;
+    ProfScope ps(h, sizeof(T) == 4 ? PCF_PROF_THOMAS32 : PCF_PROF_THOMAS64, (double)words * sizeof(T) * (double)a.n);
+    k_thomas<T, MODE><<<(a.plane + bs - 1) / bs, bs, 0, h->stream>>>(a);
+    PCF_CUDA_TRY(cudaGetLastError());
+    return PCF_OK;
+}
+
+static unsigned vec_grid(long long n) {
+    long long g = (n + 255) / 256;
+    const long long cap = 4LL * num_sms();
+    return (unsigned)(g < cap ? (g < 1 ? 1 : g) : cap);
+}
+
+// --------------------------------------------------------- precision views --
+
+template <typename T>
+struct Work {
+    const T *coef, *fac;
+    T *x, *r, *r0, *p, *v, *s, *t, *za, *zb;
+    KrylovScalars *scal;
+};
+
+static Work<double> work64(pcf_handle *h) {
+    return {h->coef64, h->fac64, h->x64, h->r64, h->r064, h->p64, h->v64, h->s64, h->t64, h->za64, h->zb64,
+            h->scal64};
+}
+static Work<float> work32(pcf_handle *h) {
+    return {h->coef32, h->fac32, h->x32, h->r32, h->r032, h->p32, h->v32, h->s32, h->t32, h->za32, h->zb32,
+            h->scal32};
+}
+
+static double deta_of(const pcf_handle *h, double dtau) {
+    // apply_preconditioner!.jl:58
+    return dtau / (2 * (1 / (h->dx * h->dx) + 1 / (h->dy * h->dy)));
+}
+
+static int ensure_factors(pcf_handle *h, double deta) {
+    if (h->fac_deta == deta) return PCF_OK;
+    // ac, ad, au read; P, M, Q written in FP64 and FP32
+    ProfScope ps(h, PCF_PROF_ASSEMBLE, (3.0 * 8 + 3.0 * 12) * (double)h->d.n);
+    return pcf_launch_factors(h, deta);
+}
+
+// M(b) with `iters` pseudo-time steps (apply_preconditioner!.jl:53-121).  The
+// first step's Thomas input is formed by MODE (b itself, or the BiCGSTAB
+// s / p update, written back to bvec).  Returns the buffer that holds M b.
+template <typename T, int MODE>
+static int precond_apply(pcf_handle *h, const Work<T> &w, T *bvec, int iters, double deta,
+                         const KrylovScalars *guard, T **result) {
+    ThomasArgs<T> ta;
+    ta.fac = w.fac;
+    ta.in = bvec;
+    ta.r = w.r;
+    ta.v = w.v;
+    ta.vec = bvec;
+    ta.out = w.za;
+    ta.plane = h->d.plane;
+    ta.nz = h->d.nz;
+    ta.n = h->d.n;
+    ta.deta = deta;
+    ta.scal = guard;
+    int rc = launch_thomas<T, MODE>(h, ta);
+    if (rc) return rc;
+    T *cur = w.za, *other = w.zb;
+    for (int m = 1; m < iters; ++m) {
+        StencilArgs<T> sa;
+        sa.coef = w.coef;
+        sa.s = cur;
+        sa.out = other;
+        sa.w1 = bvec;
+        sa.deta = deta;
+        sa.guard = guard;
+        rc = launch_stencil<T, true, EPI_PSEUDO>(h, sa);
+        if (rc) return rc;
+        ThomasArgs<T> tb = ta;
+        tb.in = other;
+        tb.out = other;
+        rc = launch_thomas<T, TH_T>(h, tb);
+        if (rc) return rc;
+        T *tmp = cur;
+        cur = other;
+        other = tmp;
+    }
+    *result = cur;
+    return PCF_OK;
+}
+
+struct LoopCfg {
+    int precond, pc_iters;
+    double deta;
+};
+
+// One BiCGSTAB iteration, apply_bicgstab!.jl:81-143.
+template <typename T>
+static int bicgstab_iteration(pcf_handle *h, const Work<T> &w, const LoopCfg &c) {
+    int rc;
+    T *z = nullptr;
+    // p = r + beta (p - omega v); z = M p
+    if (c.precond) {
+        rc = precond_apply<T, TH_PUPD>(h, w, w.p, c.pc_iters, c.deta, w.scal, &z);
+    } else {
+        h->launches += 1;
+        k_axpy_noprec<T, TH_PUPD><<<vec_grid(h->d.n), 256, 0, h->stream>>>(w.r, w.v, w.p, h->d.n, w.scal);
+        rc = cudaGetLastError() == cudaSuccess ? PCF_OK : PCF_ECUDA;
+        z = w.p;
+    }
+    if (rc) return rc;
+    // v = A z; alpha = <r, r0> / <v, r0>
+    {
+        StencilArgs<T> sa;
+        sa.coef = w.coef;
+        sa.s = z;
+        sa.out = w.v;
+        sa.w1 = w.r0;
+        sa.deta = 0;
+        sa.red = red(h, w.scal, FIN_ALPHA);
+        sa.guard = w.scal;
+        rc = launch_stencil<T, false, EPI_DOT1>(h, sa);
+        if (rc) return rc;
+    }
+    // s = r - alpha v; z = M s
+    if (c.precond) {
+        rc = precond_apply<T, TH_SUPD>(h, w, w.s, c.pc_iters, c.deta, w.scal, &z);
+    } else {
+        h->launches += 1;
+        k_axpy_noprec<T, TH_SUPD><<<vec_grid(h->d.n), 256, 0, h->stream>>>(w.r, w.v, w.s, h->d.n, w.scal);
+        rc = cudaGetLastError() == cudaSuccess ? PCF_OK : PCF_ECUDA;
+        z = w.s;
+    }
+    if (rc) return rc;
+    // t = A z; omega = <t, s> / <t, t>
+    {
+        StencilArgs<T> sa;
+        sa.coef = w.coef;
+        sa.s = z;
+        sa.out = w.t;
+        sa.w1 = w.s;
+        sa.deta = 0;
+        sa.red = red(h, w.scal, FIN_OMEGA);
+        sa.guard = w.scal;
+        rc = launch_stencil<T, false, EPI_DOT2>(h, sa);
+        if (rc) return rc;
+    }
+    // x += alpha p + omega s; r = s - omega t; residual test, beta
+    {
+        UpdateArgs<T> ua;
+        ua.x = w.x;
+        ua.r = w.r;
+        ua.p = w.p;
+        ua.s = w.s;
+        ua.t = w.t;
+        ua.r0 = w.r0;
+        ua.n = h->d.n;
+        ua.red = red(h, w.scal, FIN_RESID);
+        ua.scal = w.scal;
+        ProfScope ps(h, sizeof(T) == 4 ? PCF_PROF_UPDATE32 : PCF_PROF_UPDATE64, 7.0 * sizeof(T) * (double)h->d.n);
+        k_update<T><<<vec_grid(h->d.n), 256, 0, h->stream>>>(ua);
+        PCF_CUDA_TRY(cudaGetLastError());
+    }
+    return PCF_OK;
+}
+
+struct RunOut {
+    int iters, converged, status;
+    double res, b_norm;
+};
+
+// A complete BiCGSTAB run on A x = b (b in w.r on entry is not required: b
+// is the `b` argument), x0 = 0.  On convergence x <- M x as at
+// apply_bicgstab!.jl:132-135.  Result vector: *xout (x or a z buffer).
+template <typename T>
+static int bicgstab_run(pcf_handle *h, const Work<T> &w, const T *b, double tol, int maxit, const LoopCfg &c,
+                        int check_interval, bool precondition_unconverged, T **xout, RunOut *out) {
+    // scalar block
+    KrylovScalars init;
+    std::memset(&init, 0, sizeof(init));
+    init.tol = tol;
+    init.maxit = maxit;
+    init.ncell = (double)h->d.n;
+    PCF_CUDA_TRY(cudaMemcpyAsync(w.scal, &init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemsetAsync(w.v, 0, sizeof(T) * h->d.n, h->stream));
+    h->launches += 1;
+    k_init<T><<<vec_grid(h->d.n), 256, 0, h->stream>>>(b, w.x, w.r, w.r0, w.p, h->d.n, red(h, w.scal, FIN_INIT));
+    PCF_CUDA_TRY(cudaGetLastError());
+    if (check_interval < 1) check_interval = 16;
+    int launched = 0;
+    for (;;) {
+        const int nb = std::min(check_interval, maxit - launched);
+        for (int q = 0; q < nb; ++q) {
+            h->prof_iter = launched + q;
+            int rc = bicgstab_iteration<T>(h, w, c);
+            if (rc) return rc;
+        }
+        launched += nb;
+        PCF_CUDA_TRY(cudaMemcpyAsync(h->h_scal, w.scal, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, h->stream));
+        PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        if (h->h_scal->done || launched >= maxit) break;
+    }
+    const KrylovScalars s = *h->h_scal;
+    h->prof_iter = -1;
+    prof_flush(h, s.iter);
+    out->iters = s.iter;
+    out->converged = s.converged;
+    out->status = s.status;
+    out->res = s.b_norm > 0 ? s.res / s.b_norm : 0.0;
+    out->b_norm = s.b_norm;
+    *xout = w.x;
+    const bool finish = s.converged || (precondition_unconverged && s.status == PCF_OK);
+    if (finish && s.iter > 0 && c.precond) {
+        T *z = nullptr;
+        int rc = precond_apply<T, TH_B>(h, w, w.x, c.pc_iters, c.deta, nullptr, &z);
+        if (rc) return rc;
+        *xout = z;
+    }
+    return PCF_OK;
+}
+
+// ------------------------------------------------------- small kernels --
+
+__global__ void k_to_float(const double *__restrict__ a, float *__restrict__ b, long long n, double scale) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)(a[i] * scale);
+}
+__global__ void k_to_double(const float *__restrict__ a, double *__restrict__ b, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (double)a[i];
+}
+__global__ void k_axpy_f2d(const float *__restrict__ e, double *__restrict__ x, long long n, double scale) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] += (double)e[i] * scale;
+}
+__global__ void k_coef_to_float(const double *__restrict__ a, float *__restrict__ b, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+// dpip = (1/dt) * s / sqrt(pbar^2 / rhobar) on the interior (solve_poisson!.jl:65-72);
+// dst is haloed with offsets (ox, oy, oz) and pitches (sx, sy), or compact.
+__global__ void k_unscale(const double *__restrict__ x, const double *__restrict__ pbar,
+                          const double *__restrict__ rhobar, double dtinv, int nx, int ny, int nz, int nbx, int nby,
+                          int nbz, int nxx, int nyy, double *__restrict__ dst, int ox, int oy, int oz, int sx, int sy) {
+    const long long n = (long long)nx * ny * nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+        const long long hh = (i + nbx) + (long long)nxx * ((j + nby) + (long long)nyy * (k + nbz));
+        const double pb = pbar[hh];
+        const double sol = x[c] / sqrt(pb * pb / rhobar[hh]);
+        dst[(i + ox) + (long long)sx * ((j + oy) + (long long)sy * (k + oz))] = dtinv * sol;
+    }
+}
+
+}  // namespace pcf
+
+using namespace pcf;
+
+// ================================================================== C ABI ==
+
+extern "C" {
+
+const char *pcf_strerror(int code) {
+    switch (code) {
+        case PCF_OK: return "success";
+        case PCF_EINVAL: return "invalid argument";
+        case PCF_ENOMEM: return "device memory allocation failed";
+        case PCF_ECUDA: return "CUDA runtime error";
+        case PCF_ENOTREADY: return "grid or background not set";
+        case PCF_EBREAKDOWN: return "BiCGSTAB breakdown (zero or non-finite scalar)";
+        case PCF_ENONFINITE: return "non-finite value in the inputs or the residual";
+        case PCF_ENODEVICE: return "no usable sm_100 CUDA device";
+        case PCF_ERANGE: return "size beyond a documented limit";
+        default: return "unknown error";
+    }
+}
+
+int pcf_params_default(pcf_params *p) {
+    if (!p) return PCF_EINVAL;
+    // PoissonNamelist.jl:48-56
+    p->tolerance = 1.0e-8;
+    p->poisson_iterations = 1000;
+    p->preconditioner = 1;
+    p->dtau = 1.0;
+    p->preconditioner_iterations = 2;
+    p->tolerance_is_relative = 0;
+    p->damp_horizontal_wind_on_rhs = 0;  // SpongeNamelist default
+    p->precision = PCF_PRECISION_FP64;
+    p->residual = PCF_RESIDUAL_RECURSIVE;
+    p->inner_tolerance = 1.0e-5;
+    p->max_refinements = 20;
+    p->learned = 0;
+    p->check_interval = 16;
+    return PCF_OK;
+}
+
+static int dalloc(pcf_handle *h, void **p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return pcf_set_cuda_error(e);
+    h->bytes += (long long)bytes;
+    return PCF_OK;
+}
+
+int pcf_destroy(pcf_handle *h) {
+    if (!h) return PCF_OK;
+    int dev = h->dims.device;
+    cudaSetDevice(dev);
+    void *ptrs[] = {h->jac, h->met13, h->met23, h->met33, h->pbar, h->rhobar, h->thetabar, h->n2, h->rho, h->betar,
+                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->x64, h->r64, h->r064, h->p64, h->v64, h->s64,
+                    h->t64, h->za64, h->zb64, h->b64, h->w64, h->x32, h->r32, h->r032, h->p32, h->v32, h->s32,
+                    h->t32, h->za32, h->zb32, h->partials, h->ticket, h->scal64, h->scal32, h->dot_out};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    if (h->h_scal) cudaFreeHost(h->h_scal);
+    if (h->prof) {
+        for (cudaEvent_t e : h->prof->pool) cudaEventDestroy(e);
+        delete h->prof;
+    }
+    for (auto &e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return PCF_OK;
+}
+
+int pcf_create(pcf_handle **out, const pcf_dims *dims) {
+    if (!out || !dims) return PCF_EINVAL;
+    *out = nullptr;
+    // nz >= 4: the four vertical boundary cases of the operator must be distinct levels.
+    if (dims->nx < 1 || dims->ny < 1 || dims->nz < 4 || dims->nbx < 1 || dims->nby < 1 || dims->nbz < 2)
+        return PCF_EINVAL;
+    if (dims->model < 0 || dims->model > 2) return PCF_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || dims->device < 0 || dims->device >= ndev) return PCF_ENODEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dims->device) != cudaSuccess || prop.major < 10) return PCF_ENODEVICE;
+    PCF_CUDA_TRY(cudaSetDevice(dims->device));
+
+    pcf_handle *h = new pcf_handle;
+    std::memset(h, 0, sizeof(*h));
+    h->dims = *dims;
+    h->d.nx = dims->nx;
+    h->d.ny = dims->ny;
+    h->d.nz = dims->nz;
+    h->d.n = (long long)dims->nx * dims->ny * dims->nz;
+    h->d.plane = dims->nx * dims->ny;
+    h->nxx = dims->nx + 2 * dims->nbx;
+    h->nyy = dims->ny + 2 * dims->nby;
+    h->nzz = dims->nz + 2 * dims->nbz;
+    h->nh = (long long)h->nxx * h->nyy * h->nzz;
+    h->fac_deta = std::nan("");
+    h->prof_iter = -1;
+    h->prof = new ProfState();
+    int rc = PCF_OK;
+    auto fail = [&](int code) {
+        pcf_destroy(h);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PCF_ECUDA);
+    for (auto &e : h->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) return fail(PCF_ECUDA);
+    const size_t nh8 = sizeof(double) * (size_t)h->nh;
+    const size_t n8 = sizeof(double) * (size_t)h->d.n, n4 = sizeof(float) * (size_t)h->d.n;
+    double **fields[] = {&h->jac, &h->met13, &h->met23, &h->met33, &h->pbar, &h->rhobar, &h->thetabar, &h->n2,
+                         &h->rho, &h->betar, &h->p};
+    for (double **f : fields)
+        if ((rc = dalloc(h, (void **)f, nh8))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->coef64, n8 * PCF_NCOEF))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->coef32, n4 * PCF_NCOEF))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->fac64, n8 * 3))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->fac32, n4 * 3))) return fail(rc);
+    double **v64[] = {&h->x64, &h->r64, &h->r064, &h->p64, &h->v64, &h->s64, &h->t64, &h->za64, &h->zb64, &h->b64,
+                      &h->w64};
+    for (double **v : v64)
+        if ((rc = dalloc(h, (void **)v, n8))) return fail(rc);
+    float **v32[] = {&h->x32, &h->r32, &h->r032, &h->p32, &h->v32, &h->s32, &h->t32, &h->za32, &h->zb32};
+    for (float **v : v32)
+        if ((rc = dalloc(h, (void **)v, n4))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->partials, sizeof(double) * 2 * kMaxPartials))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->ticket, sizeof(unsigned int) * 4))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->scal64, sizeof(KrylovScalars)))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->scal32, sizeof(KrylovScalars)))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->dot_out, sizeof(double) * 4))) return fail(rc);
+    if (cudaMallocHost((void **)&h->h_scal, sizeof(KrylovScalars)) != cudaSuccess) return fail(PCF_ENOMEM);
+    if (cudaMemsetAsync(h->ticket, 0, sizeof(unsigned int) * 4, h->stream) != cudaSuccess) return fail(PCF_ECUDA);
+    // fields a caller may legitimately leave unset read as zero
+    if (cudaMemsetAsync(h->thetabar, 0, nh8, h->stream) != cudaSuccess) return fail(PCF_ECUDA);
+    if (cudaMemsetAsync(h->p, 0, nh8, h->stream) != cudaSuccess) return fail(PCF_ECUDA);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return fail(PCF_ECUDA);
+    *out = h;
+    return PCF_OK;
+}
+
+long long pcf_device_bytes(const pcf_handle *h) { return h ? h->bytes : 0; }
+
+int pcf_set_grid(pcf_handle *h, double dx, double dy, double dz, const double *jac, const double *met13,
+                 const double *met23, const double *met33) {
+    if (!h || !jac || !met13 || !met23 || !met33 || !(dx > 0) || !(dy > 0) || !(dz > 0)) return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    const size_t b = sizeof(double) * (size_t)h->nh;
+    h->dx = dx;
+    h->dy = dy;
+    h->dz = dz;
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->jac, jac, b, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->met13, met13, b, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->met23, met23, b, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->met33, met33, b, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->grid_set = 1;
+    h->fac_deta = std::nan("");
+    return PCF_OK;
+}
+
+int pcf_set_background(pcf_handle *h, const double *pbar, const double *rhobar, const double *thetabar,
+                       const double *n2) {
+    if (!h || !pbar || !rhobar || !n2) return PCF_EINVAL;
+    if (h->dims.model == PCF_MODEL_COMPRESSIBLE && !thetabar) return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    const size_t b = sizeof(double) * (size_t)h->nh;
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->pbar, pbar, b, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->rhobar, rhobar, b, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->n2, n2, b, cudaMemcpyHostToDevice, h->stream));
+    if (thetabar) PCF_CUDA_TRY(cudaMemcpyAsync(h->thetabar, thetabar, b, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->background_set = 1;
+    return PCF_OK;
+}
+
+static int assemble_device(pcf_handle *h, double dt, double rf, int damp_h) {
+    if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
+    // about 9 haloed fields read, 25 FP64 + 25 FP32 planes written per cell
+    ProfScope ps(h, PCF_PROF_ASSEMBLE, (9.0 * 8 + 25.0 * 12) * (double)h->d.n);
+    int rc = pcf_launch_assemble(h, dt, rf, damp_h);
+    if (rc) return rc;
+    h->operator_set = 1;
+    return PCF_OK;
+}
+
+int pcf_compute_operator(pcf_handle *h, const double *rho, const double *betar, const double *p, double dt,
+                         double rayleigh_factor, int damp_h, double *coef) {
+    if (!h || !rho || !betar) return PCF_EINVAL;
+    if (h->dims.model == PCF_MODEL_COMPRESSIBLE && !p) return PCF_EINVAL;
+    if (dt == 0.0) return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    const size_t b = sizeof(double) * (size_t)h->nh;
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->rho, rho, b, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->betar, betar, b, cudaMemcpyHostToDevice, h->stream));
+    if (p) PCF_CUDA_TRY(cudaMemcpyAsync(h->p, p, b, cudaMemcpyHostToDevice, h->stream));
+    int rc = assemble_device(h, dt, rayleigh_factor, damp_h);
+    if (rc) return rc;
+    if (coef)
+        PCF_CUDA_TRY(cudaMemcpyAsync(coef, h->coef64, sizeof(double) * h->d.n * PCF_NCOEF, cudaMemcpyDeviceToHost,
+                                     h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
+}
+
+int pcf_set_operator(pcf_handle *h, const double *coef) {
+    if (!h || !coef) return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    const long long m = h->d.n * PCF_NCOEF;
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->coef64, coef, sizeof(double) * m, cudaMemcpyHostToDevice, h->stream));
+    k_coef_to_float<<<vec_grid(m), 256, 0, h->stream>>>(h->coef64, h->coef32, m);
+    PCF_CUDA_TRY(cudaGetLastError());
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->operator_set = 1;
+    h->fac_deta = std::nan("");
+    return PCF_OK;
+}
+
+// Upload an interior vector into d64 and, for FP32, a rounded copy into d32.
+static int upload_vec(pcf_handle *h, const double *src, double *d64, float *d32) {
+    PCF_CUDA_TRY(cudaMemcpyAsync(d64, src, sizeof(double) * h->d.n, cudaMemcpyHostToDevice, h->stream));
+    if (d32) {
+        k_to_float<<<vec_grid(h->d.n), 256, 0, h->stream>>>(d64, d32, h->d.n, 1.0);
+        PCF_CUDA_TRY(cudaGetLastError());
+    }
+    return PCF_OK;
+}
+
+int pcf_apply_operator(pcf_handle *h, const double *sin_, double *ls, int mode, int precision) {
+    if (!h || !sin_ || !ls || (mode != PCF_TOTAL && mode != PCF_HORIZONTAL)) return PCF_EINVAL;
+    if (!h->operator_set) return PCF_ENOTREADY;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    int rc;
+    if (precision == PCF_PRECISION_FP32) {
+        if ((rc = upload_vec(h, sin_, h->b64, h->s32))) return rc;
+        StencilArgs<float> a;
+        a.coef = h->coef32;
+        a.s = h->s32;
+        a.out = h->t32;
+        a.w1 = nullptr;
+        a.deta = 0;
+        a.guard = nullptr;
+        rc = mode == PCF_TOTAL ? launch_stencil<float, false, EPI_STORE>(h, a)
+                               : launch_stencil<float, true, EPI_STORE>(h, a);
+        if (rc) return rc;
+        k_to_double<<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->t32, h->w64, h->d.n);
+        PCF_CUDA_TRY(cudaGetLastError());
+    } else {
+        if ((rc = upload_vec(h, sin_, h->b64, nullptr))) return rc;
+        StencilArgs<double> a;
+        a.coef = h->coef64;
+        a.s = h->b64;
+        a.out = h->w64;
+        a.w1 = nullptr;
+        a.deta = 0;
+        a.guard = nullptr;
+        rc = mode == PCF_TOTAL ? launch_stencil<double, false, EPI_STORE>(h, a)
+                               : launch_stencil<double, true, EPI_STORE>(h, a);
+        if (rc) return rc;
+    }
+    PCF_CUDA_TRY(cudaMemcpyAsync(ls, h->w64, sizeof(double) * h->d.n, cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
+}
+
+int pcf_apply_preconditioner(pcf_handle *h, const double *sin_, double *sout, const pcf_params *prm, int precision) {
+    if (!h || !sin_ || !sout || !prm || prm->preconditioner_iterations < 1) return PCF_EINVAL;
+    if (!h->operator_set) return PCF_ENOTREADY;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    const double deta = deta_of(h, prm->dtau);
+    int rc = ensure_factors(h, deta);
+    if (rc) return rc;
+    if (precision == PCF_PRECISION_FP32) {
+        if ((rc = upload_vec(h, sin_, h->b64, h->s32))) return rc;
+        float *z = nullptr;
+        rc = precond_apply<float, TH_B>(h, work32(h), h->s32, prm->preconditioner_iterations, deta, nullptr, &z);
+        if (rc) return rc;
+        k_to_double<<<vec_grid(h->d.n), 256, 0, h->stream>>>(z, h->w64, h->d.n);
+        PCF_CUDA_TRY(cudaGetLastError());
+    } else {
+        if ((rc = upload_vec(h, sin_, h->s64, nullptr))) return rc;
+        double *z = nullptr;
+        rc = precond_apply<double, TH_B>(h, work64(h), h->s64, prm->preconditioner_iterations, deta, nullptr, &z);
+        if (rc) return rc;
+        PCF_CUDA_TRY(cudaMemcpyAsync(h->w64, z, sizeof(double) * h->d.n, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    PCF_CUDA_TRY(cudaMemcpyAsync(sout, h->w64, sizeof(double) * h->d.n, cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
+}
+
+int pcf_global_dot(pcf_handle *h, const double *a, const double *b, double *out) {
+    if (!h || !a || !b || !out) return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->s64, a, sizeof(double) * h->d.n, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->t64, b, sizeof(double) * h->d.n, cudaMemcpyHostToDevice, h->stream));
+    k_dot<double><<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->s64, h->t64, h->d.n, red(h, nullptr, FIN_STORE, h->dot_out));
+    PCF_CUDA_TRY(cudaGetLastError());
+    PCF_CUDA_TRY(cudaMemcpyAsync(out, h->dot_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
+}
+
+// FP64 true residual r = b - A x (into r64) and its RMS.
+static int true_residual(pcf_handle *h, const double *b, const double *x, double *rms) {
+    StencilArgs<double> a;
+    a.coef = h->coef64;
+    a.s = x;
+    a.out = h->w64;
+    a.w1 = b;
+    a.deta = 0;
+    a.guard = nullptr;
+    a.red = red(h, nullptr, FIN_STORE, h->dot_out);
+    int rc = launch_stencil<double, false, EPI_RESID>(h, a);
+    if (rc) return rc;
+    double rr = 0;
+    PCF_CUDA_TRY(cudaMemcpyAsync(&rr, h->dot_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    *rms = std::sqrt(rr / (double)h->d.n);
+    return PCF_OK;
+}
+
+// Solves A x = b64 (device) according to prm; the solution ends in *xres
+// (a device FP64 buffer owned by the handle).
+static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, const double **xres, pcf_result *res) {
+    const double tol = prm->tolerance_is_relative ? prm->tolerance : prm->tolerance / tolref;  // :49-53
+    LoopCfg c;
+    c.precond = prm->preconditioner;
+    c.pc_iters = prm->preconditioner_iterations;
+    c.deta = deta_of(h, prm->dtau);
+    if (c.precond && c.pc_iters < 1) return PCF_EINVAL;
+    int rc;
+    if (c.precond && (rc = ensure_factors(h, c.deta))) return rc;
+    const int maxit = prm->poisson_iterations;
+
+    if (prm->precision != PCF_PRECISION_MIXED) {
+        double *x = nullptr;
+        RunOut ro;
+        rc = bicgstab_run<double>(h, work64(h), h->b64, tol, maxit, c, prm->check_interval, false, &x, &ro);
+        if (rc) return rc;
+        res->niter = ro.iters;
+        res->nrefine = 0;
+        res->status = ro.status;
+        res->errflag = ro.converged ? 0 : 1;
+        res->residual = ro.res;
+        res->b_norm = ro.b_norm;
+        *xres = x;
+        double tr = 0;
+        if ((rc = true_residual(h, h->b64, x, &tr))) return rc;
+        res->true_residual = ro.b_norm > 0 ? tr / ro.b_norm : 0.0;
+        if (prm->residual == PCF_RESIDUAL_TRUE && !res->errflag && res->true_residual > tol) res->errflag = 1;
+        return PCF_OK;
+    }
+
+    // Mixed precision: FP64 iterative refinement around FP32 BiCGSTAB sweeps.
+    // x64 accumulates the correction; r64 = b - A x64 is the FP64 true residual.
+    PCF_CUDA_TRY(cudaMemsetAsync(h->x64, 0, sizeof(double) * h->d.n, h->stream));
+    double rnorm = 0;
+    if ((rc = true_residual(h, h->b64, h->x64, &rnorm))) return rc;
+    const double b_norm = rnorm;
+    res->b_norm = b_norm;
+    res->niter = 0;
+    res->nrefine = 0;
+    res->status = PCF_OK;
+    res->errflag = 0;
+    *xres = h->x64;
+    if (!std::isfinite(b_norm)) {
+        res->status = PCF_ENONFINITE;
+        res->errflag = 1;
+        return PCF_OK;
+    }
+    if (b_norm == 0.0 || 1.0 <= tol) {
+        res->residual = 0.0;
+        res->true_residual = 0.0;
+        return PCF_OK;
+    }
+    Work<float> w = work32(h);
+    double rel = 1.0;
+    while (rel > tol && res->nrefine < prm->max_refinements && res->niter < maxit) {
+        // inner right-hand side: the FP64 residual, normalised to RMS 1
+        const double scale = 1.0 / rnorm;
+        k_to_float<<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->w64, w.s, h->d.n, scale);
+        PCF_CUDA_TRY(cudaGetLastError());
+        // do not over-solve the last sweep
+        double tin = prm->inner_tolerance;
+        const double need = 0.5 * tol / rel;
+        if (need > tin) tin = need;
+        float *e = nullptr;
+        RunOut ro;
+        rc = bicgstab_run<float>(h, w, w.s, tin, maxit - res->niter, c, prm->check_interval, true, &e, &ro);
+        if (rc) return rc;
+        res->niter += ro.iters;
+        res->nrefine += 1;
+        if (ro.status != PCF_OK || ro.iters == 0) {
+            res->status = ro.status != PCF_OK ? ro.status : PCF_EBREAKDOWN;
+            break;
+        }
+        k_axpy_f2d<<<vec_grid(h->d.n), 256, 0, h->stream>>>(e, h->x64, h->d.n, rnorm);
+        PCF_CUDA_TRY(cudaGetLastError());
+        if ((rc = true_residual(h, h->b64, h->x64, &rnorm))) return rc;
+        rel = rnorm / b_norm;
+        if (!std::isfinite(rel)) {
+            res->status = PCF_ENONFINITE;
+            break;
+        }
+    }
+    res->residual = rel;
+    res->true_residual = rel;
+    res->errflag = rel <= tol ? 0 : 1;
+    return PCF_OK;
+}
+
+static float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+
+static int solve_common(pcf_handle *h, double dt, double rf, double tolref, const pcf_params *prm, pcf_result *res,
+                        const double **x) {
+    // solve_poisson!.jl:52-54
+    if (dt == 0.0) return PCF_EINVAL;
+    int rc;
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[1], h->stream));
+    if ((rc = assemble_device(h, dt, rf, prm->damp_horizontal_wind_on_rhs))) return rc;
+    if (prm->preconditioner && (rc = ensure_factors(h, deta_of(h, prm->dtau)))) return rc;
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[2], h->stream));
+    if ((rc = krylov_solve(h, tolref, prm, x, res))) return rc;
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[3], h->stream));
+    return PCF_OK;
+}
+
+int pcf_solve(pcf_handle *h, const double *rhs, const double *rho, const double *betar, const double *p, double dt,
+              double rayleigh_factor, double tolref, const pcf_params *prm, double *dpip, pcf_result *res) {
+    if (!h || !rhs || !rho || !betar || !prm || !dpip || !res) return PCF_EINVAL;
+    if (h->dims.model == PCF_MODEL_COMPRESSIBLE && !p) return PCF_EINVAL;
+    std::memset(res, 0, sizeof(*res));
+    if (dt == 0.0) return PCF_EINVAL;
+    if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    const size_t hb = sizeof(double) * (size_t)h->nh;
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[0], h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->rho, rho, hb, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->betar, betar, hb, cudaMemcpyHostToDevice, h->stream));
+    if (p) PCF_CUDA_TRY(cudaMemcpyAsync(h->p, p, hb, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->b64, rhs, sizeof(double) * h->d.n, cudaMemcpyHostToDevice, h->stream));
+    const double *x = nullptr;
+    int rc = solve_common(h, dt, rayleigh_factor, tolref, prm, res, &x);
+    if (rc) return rc;
+    if (!res->errflag) {
+        k_unscale<<<vec_grid(h->d.n), 256, 0, h->stream>>>(x, h->pbar, h->rhobar, 1.0 / dt, h->d.nx, h->d.ny,
+                                                           h->d.nz, h->dims.nbx, h->dims.nby, h->dims.nbz, h->nxx,
+                                                           h->nyy, h->w64, 0, 0, 0, h->d.nx, h->d.ny);
+        PCF_CUDA_TRY(cudaGetLastError());
+        cudaMemcpy3DParms cp;
+        std::memset(&cp, 0, sizeof(cp));
+        cp.srcPtr = make_cudaPitchedPtr((void *)h->w64, sizeof(double) * h->d.nx, h->d.nx, h->d.ny);
+        cp.dstPtr = make_cudaPitchedPtr((void *)dpip, sizeof(double) * h->nxx, h->nxx, h->nyy);
+        cp.dstPos = make_cudaPos(sizeof(double) * h->dims.nbx, h->dims.nby, h->dims.nbz);
+        cp.extent = make_cudaExtent(sizeof(double) * h->d.nx, h->d.ny, h->d.nz);
+        cp.kind = cudaMemcpyDeviceToHost;
+        PCF_CUDA_TRY(cudaMemcpy3DAsync(&cp, h->stream));
+    }
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[4], h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    res->ms_upload = elapsed(h->ev[0], h->ev[1]);
+    res->ms_assemble = elapsed(h->ev[1], h->ev[2]);
+    res->ms_solve = elapsed(h->ev[2], h->ev[3]);
+    res->ms_download = elapsed(h->ev[3], h->ev[4]);
+    res->ms_total = elapsed(h->ev[0], h->ev[4]);
+    prof_flush(h, 0);
+    return PCF_OK;
+}
+
+int pcf_solve_device(pcf_handle *h, const double *d_rhs, const double *d_rho, const double *d_betar,
+                     const double *d_p, double dt, double rayleigh_factor, double tolref, const pcf_params *prm,
+                     double *d_dpip, pcf_result *res) {
+    if (!h || !d_rhs || !d_rho || !d_betar || !prm || !d_dpip || !res) return PCF_EINVAL;
+    if (h->dims.model == PCF_MODEL_COMPRESSIBLE && !d_p) return PCF_EINVAL;
+    std::memset(res, 0, sizeof(*res));
+    if (dt == 0.0) return PCF_EINVAL;
+    if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    const size_t hb = sizeof(double) * (size_t)h->nh;
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[0], h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->rho, d_rho, hb, cudaMemcpyDeviceToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->betar, d_betar, hb, cudaMemcpyDeviceToDevice, h->stream));
+    if (d_p) PCF_CUDA_TRY(cudaMemcpyAsync(h->p, d_p, hb, cudaMemcpyDeviceToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->b64, d_rhs, sizeof(double) * h->d.n, cudaMemcpyDeviceToDevice, h->stream));
+    const double *x = nullptr;
+    int rc = solve_common(h, dt, rayleigh_factor, tolref, prm, res, &x);
+    if (rc) return rc;
+    if (!res->errflag) {
+        k_unscale<<<vec_grid(h->d.n), 256, 0, h->stream>>>(x, h->pbar, h->rhobar, 1.0 / dt, h->d.nx, h->d.ny,
+                                                           h->d.nz, h->dims.nbx, h->dims.nby, h->dims.nbz, h->nxx,
+                                                           h->nyy, d_dpip, h->dims.nbx, h->dims.nby, h->dims.nbz,
+                                                           h->nxx, h->nyy);
+        PCF_CUDA_TRY(cudaGetLastError());
+    }
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[4], h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    res->ms_upload = elapsed(h->ev[0], h->ev[1]);
+    res->ms_assemble = elapsed(h->ev[1], h->ev[2]);
+    res->ms_solve = elapsed(h->ev[2], h->ev[3]);
+    res->ms_download = elapsed(h->ev[3], h->ev[4]);
+    res->ms_total = elapsed(h->ev[0], h->ev[4]);
+    prof_flush(h, 0);
+    return PCF_OK;
+}
+
+int pcf_bicgstab(pcf_handle *h, const double *rhs, double tolref, const pcf_params *prm, double *solution,
+                 pcf_result *res) {
+    if (!h || !rhs || !prm || !solution || !res) return PCF_EINVAL;
+    std::memset(res, 0, sizeof(*res));
+    if (!h->operator_set) return PCF_ENOTREADY;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[0], h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->b64, rhs, sizeof(double) * h->d.n, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[2], h->stream));
+    const double *x = nullptr;
+    int rc = krylov_solve(h, tolref, prm, &x, res);
+    if (rc) return rc;
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[3], h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(solution, x, sizeof(double) * h->d.n, cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[4], h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    res->ms_upload = elapsed(h->ev[0], h->ev[2]);
+    res->ms_solve = elapsed(h->ev[2], h->ev[3]);
+    res->ms_download = elapsed(h->ev[3], h->ev[4]);
+    res->ms_total = elapsed(h->ev[0], h->ev[4]);
+    prof_flush(h, 0);
+    return PCF_OK;
+}
+
+long long pcf_launch_count(const pcf_handle *h) { return h ? h->launches : 0; }
+
+int pcf_profile_enable(pcf_handle *h, int on) {
+    if (!h) return PCF_EINVAL;
+    prof_flush(h, 0);
+    h->prof_on = on ? 1 : 0;
+    for (auto &a : h->prof_acc) a = ProfAcc{0.0, 0, 0.0};
+    return PCF_OK;
+}
+
+int pcf_profile_read(const pcf_handle *h, int tag, double *ms, long long *count, double *bytes) {
+    if (!h || tag < 0 || tag >= PCF_PROF_NTAGS) return PCF_EINVAL;
+    if (ms) *ms = h->prof_acc[tag].ms;
+    if (count) *count = h->prof_acc[tag].count;
+    if (bytes) *bytes = h->prof_acc[tag].bytes;
+    return PCF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,12 @@
+"""B200 (sm_100a) drop-in for PinCFlow.jl's semi-implicit pressure Poisson solve.
+
+The compute lives in libpincflow_poisson.so (include/pincflow_poisson.h);
+this package is its host-side mirror of the reference interface
+(PoissonSolver.solve_poisson, apply_operator, apply_preconditioner, ...)
+plus the caller-side construction of the grid, background and workloads.
+"""
+from . import configs, fields
+from ._lib import PoissonError, load
+from .solver import PoissonNamelist, PoissonSolver, SolveInfo
+
+__all__ = ["PoissonNamelist", "PoissonSolver", "SolveInfo", "PoissonError", "load", "fields", "configs"]

@@ -1,0 +1,145 @@
+"""ctypes binding of libpincflow_poisson.so (include/pincflow_poisson.h).
+
+The library is the product: there is no fallback.  Loading fails loudly if
+the shared object is missing; calls fail loudly (PoissonError) on any
+non-zero return code.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libpincflow_poisson.so")
+
+# enum values of include/pincflow_poisson.h
+PCF_OK = 0
+PCF_EINVAL = -1
+PCF_ENOMEM = -2
+PCF_ECUDA = -3
+PCF_ENOTREADY = -4
+PCF_EBREAKDOWN = -5
+PCF_ENONFINITE = -6
+PCF_ENODEVICE = -7
+PCF_ERANGE = -8
+
+MODEL = {"Boussinesq": 0, "PseudoIncompressible": 1, "Compressible": 2}
+PRECISION = {"fp64": 0, "mixed": 1, "fp32": 2}
+RESIDUAL = {"recursive": 0, "true": 1}
+TOTAL, HORIZONTAL = 0, 1
+NCOEF = 25
+
+EXPORTS = [
+    "pcf_params_default", "pcf_create", "pcf_destroy", "pcf_strerror", "pcf_set_grid",
+    "pcf_set_background", "pcf_solve", "pcf_solve_device", "pcf_compute_operator",
+    "pcf_set_operator", "pcf_apply_operator", "pcf_apply_preconditioner", "pcf_bicgstab",
+    "pcf_global_dot", "pcf_device_bytes", "pcf_launch_count", "pcf_profile_enable", "pcf_profile_read",
+]
+PROF_TAGS = ["apply32", "apply64", "pseudo32", "pseudo64", "thomas32", "thomas64", "update32", "update64",
+             "assemble"]
+
+
+class PcfDims(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("nbx", ctypes.c_int), ("nby", ctypes.c_int), ("nbz", ctypes.c_int),
+                ("model", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+class PcfParams(ctypes.Structure):
+    _fields_ = [("tolerance", ctypes.c_double), ("poisson_iterations", ctypes.c_int),
+                ("preconditioner", ctypes.c_int), ("dtau", ctypes.c_double),
+                ("preconditioner_iterations", ctypes.c_int),
+                ("tolerance_is_relative", ctypes.c_int),
+                ("damp_horizontal_wind_on_rhs", ctypes.c_int), ("precision", ctypes.c_int),
+                ("residual", ctypes.c_int), ("inner_tolerance", ctypes.c_double),
+                ("max_refinements", ctypes.c_int), ("learned", ctypes.c_int),
+                ("check_interval", ctypes.c_int)]
+
+
+class PcfResult(ctypes.Structure):
+    _fields_ = [("errflag", ctypes.c_int), ("niter", ctypes.c_int), ("nrefine", ctypes.c_int),
+                ("status", ctypes.c_int), ("residual", ctypes.c_double),
+                ("true_residual", ctypes.c_double), ("b_norm", ctypes.c_double),
+                ("ms_upload", ctypes.c_double), ("ms_assemble", ctypes.c_double),
+                ("ms_solve", ctypes.c_double), ("ms_download", ctypes.c_double),
+                ("ms_total", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class PoissonError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        super().__init__(f"{what}: {strerror(code)} ({code})")
+
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Loads the solver library (once).  Raises OSError if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise OSError(f"libpincflow_poisson.so not found at {p}; run pincflow.jl_b200/build.py")
+    lib = ctypes.CDLL(p)
+    P = ctypes.POINTER
+    dp = P(ctypes.c_double)
+    vp = ctypes.c_void_p
+    lib.pcf_strerror.restype = ctypes.c_char_p
+    lib.pcf_strerror.argtypes = [ctypes.c_int]
+    lib.pcf_params_default.argtypes = [P(PcfParams)]
+    lib.pcf_create.argtypes = [P(vp), P(PcfDims)]
+    lib.pcf_destroy.argtypes = [vp]
+    lib.pcf_set_grid.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp]
+    lib.pcf_set_background.argtypes = [vp, dp, dp, dp, dp]
+    lib.pcf_solve.argtypes = [vp, dp, dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                              P(PcfParams), dp, P(PcfResult)]
+    lib.pcf_solve_device.argtypes = [vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, P(PcfParams), vp, P(PcfResult)]
+    lib.pcf_compute_operator.argtypes = [vp, dp, dp, dp, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_int, dp]
+    lib.pcf_set_operator.argtypes = [vp, dp]
+    lib.pcf_apply_operator.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_int]
+    lib.pcf_apply_preconditioner.argtypes = [vp, dp, dp, P(PcfParams), ctypes.c_int]
+    lib.pcf_bicgstab.argtypes = [vp, dp, ctypes.c_double, P(PcfParams), dp, P(PcfResult)]
+    lib.pcf_global_dot.argtypes = [vp, dp, dp, dp]
+    lib.pcf_device_bytes.restype = ctypes.c_longlong
+    lib.pcf_device_bytes.argtypes = [vp]
+    lib.pcf_launch_count.restype = ctypes.c_longlong
+    lib.pcf_launch_count.argtypes = [vp]
+    lib.pcf_profile_enable.argtypes = [vp, ctypes.c_int]
+    lib.pcf_profile_read.argtypes = [vp, ctypes.c_int, dp, P(ctypes.c_longlong), dp]
+    for name in EXPORTS:
+        getattr(lib, name).restype = getattr(lib, name).restype or ctypes.c_int
+    lib.pcf_strerror.restype = ctypes.c_char_p
+    lib.pcf_device_bytes.restype = ctypes.c_longlong
+    lib.pcf_launch_count.restype = ctypes.c_longlong
+    _lib = lib
+    return lib
+
+
+def strerror(code: int) -> str:
+    try:
+        return load().pcf_strerror(int(code)).decode()
+    except OSError:
+        return f"error {code}"
+
+
+def check(code: int, what: str):
+    if code != PCF_OK:
+        raise PoissonError(code, what)
+
+
+def dptr(a):
+    """Pointer of a C-contiguous float64 numpy array (or None)."""
+    if a is None:
+        return None
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]):
+        raise TypeError("expected a C-contiguous float64 numpy array")
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))

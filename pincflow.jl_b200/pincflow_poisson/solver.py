@@ -1,0 +1,229 @@
+"""Host mirror of the reference's PoissonSolver interface over the C ABI.
+
+Names and argument meanings follow the Julia functions they stand in for:
+
+  PoissonNamelist          src/Types/NamelistTypes/PoissonNamelist.jl:38-66
+  PoissonSolver.solve_poisson       solve_poisson!(state, dt, rayleigh_factor, tolref)
+                                    src/PoissonSolver/solve_poisson!.jl:39-75
+  PoissonSolver.compute_operator    compute_operator!(state, dt, rayleigh_factor)
+  PoissonSolver.apply_operator      apply_operator!(sin, ls, Total()/Horizontal(), state)
+  PoissonSolver.apply_preconditioner apply_preconditioner!(sin, sout, state)
+  PoissonSolver.apply_bicgstab      apply_bicgstab!(state, tolref)
+  PoissonSolver.compute_global_dot_product
+                                    src/MPIOperations/compute_global_dot_product.jl:22-36
+
+Error behaviour follows the reference: dt == 0 raises (solve_poisson!.jl:52-54);
+non-convergence is returned as (errflag=True, niter) and leaves dpip
+untouched (apply_bicgstab!.jl:146-149, solve_poisson!.jl:61-63).
+Every compute call goes through libpincflow_poisson.so on the GPU; there
+is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .fields import Domain
+
+
+@dataclass
+class PoissonNamelist:
+    tolerance: float = 1.0e-8
+    poisson_iterations: int = 1000
+    preconditioner: bool = True
+    dtau: float = 1.0
+    preconditioner_iterations: int = 2
+    initial_cleaning: bool = True
+    tolerance_is_relative: bool = False
+    # SpongeNamelist.damp_horizontal_wind_on_rhs
+    damp_horizontal_wind_on_rhs: bool = False
+    # additions without a reference counterpart (defaults reproduce the reference)
+    precision: str = "fp64"          # "fp64" | "mixed"
+    residual: str = "recursive"      # "recursive" | "true"
+    inner_tolerance: float = 1.0e-5
+    max_refinements: int = 20
+    learned: bool = False
+    check_interval: int = 16
+
+    def to_c(self) -> _lib.PcfParams:
+        p = _lib.PcfParams()
+        _lib.load().pcf_params_default(ctypes.byref(p))
+        p.tolerance = float(self.tolerance)
+        p.poisson_iterations = int(self.poisson_iterations)
+        p.preconditioner = int(bool(self.preconditioner))
+        p.dtau = float(self.dtau)
+        p.preconditioner_iterations = int(self.preconditioner_iterations)
+        p.tolerance_is_relative = int(bool(self.tolerance_is_relative))
+        p.damp_horizontal_wind_on_rhs = int(bool(self.damp_horizontal_wind_on_rhs))
+        p.precision = _lib.PRECISION[self.precision]
+        p.residual = _lib.RESIDUAL[self.residual]
+        p.inner_tolerance = float(self.inner_tolerance)
+        p.max_refinements = int(self.max_refinements)
+        p.learned = int(bool(self.learned))
+        p.check_interval = int(self.check_interval)
+        return p
+
+
+@dataclass
+class SolveInfo:
+    errflag: bool
+    niter: int
+    nrefine: int = 0
+    status: int = 0
+    residual: float = 0.0
+    true_residual: float = 0.0
+    b_norm: float = 0.0
+    timings_ms: dict = field(default_factory=dict)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class PoissonSolver:
+    """One device-resident solver instance: the `Poisson` workspace of one
+    `State` (src/Types/PoissonTypes/Poisson.jl:53-89) plus the grid and
+    background fields the operator is assembled from."""
+
+    def __init__(self, dom: Domain, model: str = "PseudoIncompressible", device: int = 0):
+        self.lib = _lib.load()
+        self.dom = dom
+        self.model = model
+        d = _lib.PcfDims(dom.nx, dom.ny, dom.nz, dom.nbx, dom.nby, dom.nbz, _lib.MODEL[model], device)
+        self._h = ctypes.c_void_p()
+        _lib.check(self.lib.pcf_create(ctypes.byref(self._h), ctypes.byref(d)), "pcf_create")
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if self._h:
+            self.lib.pcf_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.lib.pcf_device_bytes(self._h))
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.lib.pcf_launch_count(self._h))
+
+    def profile(self, on: bool = True):
+        _lib.check(self.lib.pcf_profile_enable(self._h, int(bool(on))), "pcf_profile_enable")
+
+    def profile_read(self) -> dict:
+        out = {}
+        for tag, name in enumerate(_lib.PROF_TAGS):
+            ms, cnt, by = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double()
+            _lib.check(self.lib.pcf_profile_read(self._h, tag, ctypes.byref(ms), ctypes.byref(cnt),
+                                                 ctypes.byref(by)), "pcf_profile_read")
+            out[name] = dict(ms=ms.value, count=cnt.value, bytes=by.value)
+        return out
+
+    # -- state ------------------------------------------------------------
+    def set_grid(self, g: dict):
+        self._keep_grid = [_f64(g[k]) for k in ("jac", "met13", "met23", "met33")]
+        _lib.check(self.lib.pcf_set_grid(self._h, g["dx"], g["dy"], g["dz"],
+                                         *[_lib.dptr(a) for a in self._keep_grid]), "pcf_set_grid")
+        self.dx, self.dy, self.dz = g["dx"], g["dy"], g["dz"]
+
+    def set_background(self, a: dict):
+        th = _f64(a["thetabar"]) if a.get("thetabar") is not None else None
+        arrs = [_f64(a["pbar"]), _f64(a["rhobar"]), th, _f64(a["n2"])]
+        _lib.check(self.lib.pcf_set_background(self._h, *[_lib.dptr(x) for x in arrs]),
+                   "pcf_set_background")
+
+    # -- the reference's entry points ------------------------------------
+    def solve_poisson(self, rhs, rho, betar, dt, rayleigh_factor, tolref, namelist: PoissonNamelist,
+                      dpip, p=None) -> SolveInfo:
+        """solve_poisson!: returns SolveInfo (errflag, niter, ...) and writes
+        the interior of the haloed array dpip in place."""
+        if dt == 0.0:
+            raise ZeroDivisionError("Error in solve_poisson!: dt = 0.0!")
+        if not (isinstance(dpip, np.ndarray) and dpip.dtype == np.float64 and dpip.flags["C_CONTIGUOUS"]):
+            raise TypeError("dpip must be a C-contiguous float64 array")
+        res = _lib.PcfResult()
+        prm = namelist.to_c()
+        args = [_f64(rhs), _f64(rho), _f64(betar), None if p is None else _f64(p)]
+        _lib.check(self.lib.pcf_solve(self._h, *[_lib.dptr(a) for a in args], float(dt),
+                                      float(rayleigh_factor), float(tolref), ctypes.byref(prm),
+                                      _lib.dptr(dpip), ctypes.byref(res)), "pcf_solve")
+        return _info(res)
+
+    def compute_operator(self, rho, betar, dt, rayleigh_factor, damp_horizontal_wind_on_rhs=False,
+                         p=None, return_coef=True):
+        coef = np.zeros((_lib.NCOEF,) + self.dom.interior_shape) if return_coef else None
+        args = [_f64(rho), _f64(betar), None if p is None else _f64(p)]
+        _lib.check(self.lib.pcf_compute_operator(self._h, *[_lib.dptr(a) for a in args], float(dt),
+                                                 float(rayleigh_factor),
+                                                 int(bool(damp_horizontal_wind_on_rhs)),
+                                                 _lib.dptr(coef)), "pcf_compute_operator")
+        return coef
+
+    def set_operator(self, coef):
+        c = _f64(coef)
+        _lib.check(self.lib.pcf_set_operator(self._h, _lib.dptr(c)), "pcf_set_operator")
+
+    def apply_operator(self, sin, horizontal=False, precision="fp64"):
+        out = np.zeros(self.dom.interior_shape)
+        _lib.check(self.lib.pcf_apply_operator(self._h, _lib.dptr(_f64(sin)), _lib.dptr(out),
+                                               _lib.HORIZONTAL if horizontal else _lib.TOTAL,
+                                               _lib.PRECISION[precision]), "pcf_apply_operator")
+        return out
+
+    def apply_preconditioner(self, sin, namelist: PoissonNamelist, precision="fp64"):
+        out = np.zeros(self.dom.interior_shape)
+        prm = namelist.to_c()
+        _lib.check(self.lib.pcf_apply_preconditioner(self._h, _lib.dptr(_f64(sin)), _lib.dptr(out),
+                                                     ctypes.byref(prm), _lib.PRECISION[precision]),
+                   "pcf_apply_preconditioner")
+        return out
+
+    def apply_bicgstab(self, rhs, tolref, namelist: PoissonNamelist):
+        sol = np.zeros(self.dom.interior_shape)
+        res = _lib.PcfResult()
+        prm = namelist.to_c()
+        _lib.check(self.lib.pcf_bicgstab(self._h, _lib.dptr(_f64(rhs)), float(tolref), ctypes.byref(prm),
+                                         _lib.dptr(sol), ctypes.byref(res)), "pcf_bicgstab")
+        return sol, _info(res)
+
+    def compute_global_dot_product(self, a, b) -> float:
+        out = ctypes.c_double()
+        _lib.check(self.lib.pcf_global_dot(self._h, _lib.dptr(_f64(a)), _lib.dptr(_f64(b)),
+                                           ctypes.byref(out)), "pcf_global_dot")
+        return out.value
+
+    def solve_poisson_device(self, d_rhs: int, d_rho: int, d_betar: int, dt, rayleigh_factor, tolref,
+                             namelist: PoissonNamelist, d_dpip: int, d_p: int | None = None) -> SolveInfo:
+        """solve_poisson! on device-resident inputs (raw device pointers)."""
+        res = _lib.PcfResult()
+        prm = namelist.to_c()
+        _lib.check(self.lib.pcf_solve_device(self._h, ctypes.c_void_p(d_rhs), ctypes.c_void_p(d_rho),
+                                             ctypes.c_void_p(d_betar),
+                                             None if d_p is None else ctypes.c_void_p(d_p), float(dt),
+                                             float(rayleigh_factor), float(tolref), ctypes.byref(prm),
+                                             ctypes.c_void_p(d_dpip), ctypes.byref(res)),
+                   "pcf_solve_device")
+        return _info(res)
+
+
+def _info(res: _lib.PcfResult) -> SolveInfo:
+    d = res.as_dict()
+    return SolveInfo(errflag=bool(d["errflag"]), niter=int(d["niter"]), nrefine=int(d["nrefine"]),
+                     status=int(d["status"]), residual=d["residual"], true_residual=d["true_residual"],
+                     b_norm=d["b_norm"],
+                     timings_ms={k[3:]: d[k] for k in d if k.startswith("ms_")})

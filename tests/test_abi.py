@@ -1,0 +1,113 @@
+"""CPU: the C-ABI library loads, exports every entry point the header
+declares, and its Python mirror agrees with the header's struct layouts and
+defaults.  No GPU needed (no compute calls)."""
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+HEADER = os.path.join(REPO, "include", "pincflow_poisson.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(pcf_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol(pcf):
+    lib = pcf.load()
+    names = declared_functions()
+    assert len(names) >= 18
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # nm view of the shared object, independent of ctypes
+    out = subprocess.run(["nm", "-D", "--defined-only", pcf._lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (pcf_\w+)", out))
+    assert set(names) <= exported, set(names) - exported
+
+
+def _c_layout():
+    code = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "pincflow_poisson.h"
+#define F(T, m) printf(#T "." #m " %zu\n", offsetof(T, m));
+int main(void) {
+  printf("pcf_dims %zu\npcf_params %zu\npcf_result %zu\n", sizeof(pcf_dims), sizeof(pcf_params), sizeof(pcf_result));
+  F(pcf_params, dtau) F(pcf_params, inner_tolerance) F(pcf_params, check_interval)
+  F(pcf_result, residual) F(pcf_result, ms_total) F(pcf_dims, device)
+  return 0;
+}
+"""
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "l.c")
+        exe = os.path.join(d, "l")
+        open(c, "w").write(code)
+        subprocess.run(["gcc", "-I", os.path.dirname(HEADER), c, "-o", exe], check=True)
+        lines = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
+    return {ln.split()[0]: int(ln.split()[1]) for ln in lines if ln.strip()}
+
+
+def test_struct_layouts_match_header(pcf):
+    L = pcf._lib
+    c = _c_layout()
+    assert ctypes.sizeof(L.PcfDims) == c["pcf_dims"]
+    assert ctypes.sizeof(L.PcfParams) == c["pcf_params"]
+    assert ctypes.sizeof(L.PcfResult) == c["pcf_result"]
+    assert L.PcfParams.dtau.offset == c["pcf_params.dtau"]
+    assert L.PcfParams.inner_tolerance.offset == c["pcf_params.inner_tolerance"]
+    assert L.PcfParams.check_interval.offset == c["pcf_params.check_interval"]
+    assert L.PcfResult.residual.offset == c["pcf_result.residual"]
+    assert L.PcfResult.ms_total.offset == c["pcf_result.ms_total"]
+    assert L.PcfDims.device.offset == c["pcf_dims.device"]
+
+
+def test_params_default_mirror_poisson_namelist(pcf):
+    p = pcf._lib.PcfParams()
+    assert pcf.load().pcf_params_default(ctypes.byref(p)) == 0
+    # PoissonNamelist.jl:48-56
+    assert p.tolerance == 1e-8 and p.poisson_iterations == 1000 and p.preconditioner == 1
+    assert p.dtau == 1.0 and p.preconditioner_iterations == 2 and p.tolerance_is_relative == 0
+    assert p.damp_horizontal_wind_on_rhs == 0 and p.precision == 0 and p.residual == 0 and p.learned == 0
+    nl = pcf.PoissonNamelist().to_c()
+    for name, _ in pcf._lib.PcfParams._fields_:
+        assert getattr(nl, name) == getattr(p, name), name
+
+
+def test_error_codes_and_null_arguments(pcf):
+    lib = pcf.load()
+    assert lib.pcf_strerror(0) == b"success"
+    assert b"invalid" in lib.pcf_strerror(-1)
+    assert lib.pcf_create(None, None) == pcf._lib.PCF_EINVAL
+    assert lib.pcf_params_default(None) == pcf._lib.PCF_EINVAL
+    assert lib.pcf_destroy(None) == 0
+    assert lib.pcf_solve(None, None, None, None, None, 1.0, 1.0, 1.0, None, None, None) == pcf._lib.PCF_EINVAL
+    assert lib.pcf_profile_read(None, 0, None, None, None) == pcf._lib.PCF_EINVAL
+    assert lib.pcf_launch_count(None) == 0
+
+
+def test_create_rejects_bad_dims_before_touching_a_device(pcf):
+    lib = pcf.load()
+    h = ctypes.c_void_p()
+    for dims in [(8, 8, 3, 3, 3, 3, 0, 0), (0, 8, 8, 3, 3, 3, 0, 0), (8, 8, 8, 3, 3, 1, 0, 0),
+                 (8, 8, 8, 3, 3, 3, 7, 0)]:
+        d = pcf._lib.PcfDims(*dims)
+        assert lib.pcf_create(ctypes.byref(h), ctypes.byref(d)) == pcf._lib.PCF_EINVAL
+
+
+def test_no_device_is_an_error_not_a_fallback(pcf):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(pcf.PoissonError) as e:
+        pcf.PoissonSolver(pcf.fields.Domain(8, 8, 8))
+    assert e.value.code == pcf._lib.PCF_ENODEVICE
