@@ -117,10 +117,11 @@ typedef struct {
     /* Additions without a reference counterpart; defaults reproduce the reference. */
     int precision;                 /* PCF_PRECISION_FP64 */
     int residual;                  /* PCF_RESIDUAL_RECURSIVE */
-    double inner_tolerance;        /* mixed: relative reduction per FP32 sweep (1e-5) */
-    int max_refinements;           /* mixed: cap on FP64 refinement sweeps (20) */
+    double inner_tolerance;        /* mixed: FP64 reliable update each time the FP32 residual fell by this factor (1e-2) */
+    int max_refinements;           /* mixed: cap on restarts of the FP32 iteration after a breakdown (5) */
     int learned;                   /* 0: off; 1: learned warm start + flexible BiCGSTAB */
     int check_interval;            /* iterations between host checks of the status word (16) */
+    int restart_interval;          /* mixed: restart the Krylov recurrences at every n-th reliable update (1; 0: never) */
 } pcf_params;
 
 typedef struct {
@@ -219,9 +220,15 @@ enum pcf_prof_tag {
     PCF_PROF_UPDATE32 = 6,  /* BiCGSTAB vector updates, FP32 */
     PCF_PROF_UPDATE64 = 7,
     PCF_PROF_ASSEMBLE = 8,  /* operator assembly + factors */
-    PCF_PROF_NTAGS = 9
+    PCF_PROF_RELIABLE = 9,  /* FP64 true-residual applies of reliable updates (mostly skipped launches) */
+    PCF_PROF_NTAGS = 10
 };
 long long pcf_launch_count(const pcf_handle *h);
+/* Relative recursive residual after each BiCGSTAB iteration of the last
+ * solve (refinement sweeps concatenated, relative to the original b); the
+ * reference prints only the final value (apply_bicgstab!.jl:124-127).
+ * Copies min(cap, *n) entries; *n receives the total count. */
+int pcf_residual_history(pcf_handle *h, double *out, int cap, int *n);
 int pcf_profile_enable(pcf_handle *h, int on);  /* also clears the accumulators */
 int pcf_profile_read(const pcf_handle *h, int tag, double *ms, long long *count, double *bytes);
 

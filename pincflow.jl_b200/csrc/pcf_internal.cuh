@@ -30,6 +30,7 @@ namespace pcf {
 
 constexpr int kNumCoef = PCF_NCOEF;
 constexpr int kMaxPartials = 16384;  // per-block partial sums of one reduction
+constexpr int kHistCap = 65536;      // residual-history entries kept per solve
 
 // Scalars of one BiCGSTAB run, resident on the device so that no host round
 // trip is needed between the kernels of an iteration.
@@ -41,12 +42,29 @@ struct KrylovScalars {
     double tol;       // relative tolerance on res / b_norm
     double ncell;     // x_size * y_size * z_size
     double last_dot[2];
+    double *hist;     // recursive relative residual per iteration (may be null)
+    double hist_scale;// multiplies res / b_norm (refinement sweeps: the sweep's start residual)
+    int hist_off, hist_cap;
     int iter;         // completed iterations
     int maxit;
     int done;         // 1 once converged, failed or broken down
     int converged;
     int status;       // PCF_OK, PCF_EBREAKDOWN, PCF_ENONFINITE
-    int pad;
+    // Reliable updates (mixed precision): the FP32 iteration folds its
+    // correction into the FP64 solution and restarts its residual from the
+    // FP64 true residual whenever the recursive residual fell by ru_delta.
+    int reliable;     // 1: convergence is decided by the FP64 true residual
+    int update;       // 1: a reliable update is pending
+    int last_update;  // iteration of the last reliable update
+    double ru_delta;  // trigger: res <= ru_delta * max res since the last update
+    double res_max;   // max recursive residual since the last update
+    double res_true;  // last FP64 true relative residual
+    double bnorm64;   // RMS of the FP64 right-hand side
+    double alpha_omega;  // alpha / omega of the iteration that triggered the update
+    int nupdates;
+    int restart_every;   // restart the Krylov recurrences (r0 = p = r_true) at every n-th update (0: never)
+    int restart_now;     // set by FIN_RU_TRUE for the pending update
+    int pad2;
 };
 
 // Finalisation performed by the last block of a fused reduction kernel.
@@ -55,7 +73,9 @@ enum FinalOp : int {
     FIN_INIT = 1,    // sums[0] = <r, r>: b_norm, rho and the early exit
     FIN_ALPHA = 2,   // sums[0] = <v, r0>: alpha = rho / <v, r0>
     FIN_OMEGA = 3,   // sums[0] = <t, s>, sums[1] = <t, t>: omega
-    FIN_RESID = 4    // sums[0] = <r, r>, sums[1] = <r, r0>: test, beta, rho
+    FIN_RESID = 4,   // sums[0] = <r, r>, sums[1] = <r, r0>: test, beta, rho
+    FIN_RU_TRUE = 5, // sums[0] = |b - A x|^2 (FP64): reliable-update convergence test
+    FIN_RU_RHO = 6   // sums[0] = <r_true, r0>: beta and rho after the residual replacement
 };
 
 struct ReduceCtx {
@@ -109,16 +129,22 @@ struct pcf_handle {
     float *coef32;
     double *fac64;
     float *fac32;
+    // difference form of the FP32 operator for pi = s / fcscal (k_build_diff)
+    float *coefB32;
+    double *fc64, *fch;  // fcscal on the interior and on the haloed grid
+    float *rfc32;        // 1 / fcscal on the interior
     double fac_deta;  // d_eta the factors were built with (NaN: none)
     // FP64 Krylov vectors
     double *x64, *r64, *r064, *p64, *v64, *s64, *t64, *za64, *zb64, *b64, *w64;
     // FP32 Krylov vectors
-    float *x32, *r32, *r032, *p32, *v32, *s32, *t32, *za32, *zb32;
+    float *x32, *r32, *r032, *p32, *v32, *s32, *t32, *za32, *zb32, *zc32, *zd32;
     // reductions
     double *partials;
     unsigned int *ticket;
     pcf::KrylovScalars *scal64, *scal32;
     double *dot_out;
+    double *hist;                // residual history of the last solve (kHistCap entries)
+    int hist_len;
     pcf::KrylovScalars *h_scal;  // pinned mirror
     long long bytes;
     // instrumentation

@@ -148,9 +148,30 @@ __device__ void finalize(const ReduceCtx &c, const double (&s)[NV]) {
             k->iter += 1;
             const double res = sqrt(s[0] / k->ncell);
             k->res = res;
+            // reliable mode: the FP32 right-hand side is b / RMS(b), so res is
+            // already relative to the original b
+            if (k->hist && k->hist_off + k->iter - 1 < k->hist_cap)
+                k->hist[k->hist_off + k->iter - 1] = k->reliable ? res : k->hist_scale * res / k->b_norm;
             if (!finite(res)) {
                 k->status = PCF_ENONFINITE;
                 k->done = 1;
+            } else if (k->reliable) {
+                // the FP64 true residual decides; trigger a reliable update on a
+                // residual drop by ru_delta, on reaching tol, or at the cap
+                const double rel = res;
+                if (rel > k->res_max) k->res_max = rel;
+                if (rel <= k->tol || rel <= k->ru_delta * k->res_max || k->iter >= k->maxit) {
+                    k->update = 1;
+                    k->alpha_omega = k->alpha / k->omega;
+                } else {
+                    const double beta = k->alpha / k->omega * s[1] / k->rho;
+                    k->beta = beta;
+                    k->rho = s[1];
+                    if (!finite(beta)) {
+                        k->status = PCF_EBREAKDOWN;
+                        k->done = 1;
+                    }
+                }
             } else if (res / k->b_norm <= k->tol) {
                 k->converged = 1;
                 k->done = 1;
@@ -164,6 +185,41 @@ __device__ void finalize(const ReduceCtx &c, const double (&s)[NV]) {
                     k->status = PCF_EBREAKDOWN;
                     k->done = 1;
                 }
+            }
+            break;
+        }
+        case FIN_RU_TRUE: {  // sums[0] = |b - A x64|^2 after folding the correction
+            const double rt = sqrt(s[0] / k->ncell) / k->bnorm64;
+            k->res_true = rt;
+            k->nupdates += 1;
+            if (k->hist && k->hist_off + k->iter - 1 < k->hist_cap && k->iter > 0)
+                k->hist[k->hist_off + k->iter - 1] = rt;
+            if (!finite(rt)) {
+                k->status = PCF_ENONFINITE;
+                k->done = 1;
+                k->update = 0;
+            } else if (rt <= k->tol) {
+                k->converged = 1;
+                k->done = 1;
+                k->update = 0;
+            } else if (k->iter >= k->maxit) {
+                k->done = 1;
+                k->update = 0;
+            }
+            k->restart_now = k->restart_every > 0 && (k->nupdates % k->restart_every) == 0;
+            break;
+        }
+        case FIN_RU_RHO: {  // sums[0] = <r_true, r0>: continue the recurrences on the true residual
+            // (after a restart r0 = r_true, so sums[0] = <r, r> and p = r)
+            const double beta = k->restart_now ? 0.0 : k->alpha_omega * s[0] / k->rho;
+            k->beta = beta;
+            k->rho = s[0];
+            k->res_max = k->res_true;
+            k->update = 0;
+            k->last_update = k->iter;
+            if (!finite(beta)) {
+                k->status = PCF_EBREAKDOWN;
+                k->done = 1;
             }
             break;
         }
@@ -211,6 +267,11 @@ __device__ __forceinline__ bool krylov_done(const KrylovScalars *s) {
     return s != nullptr && *((volatile const int *)&s->done) != 0;
 }
 
+// Guard of the reliable-update kernels: run only while an update is pending.
+__device__ __forceinline__ bool no_update_pending(const KrylovScalars *s) {
+    return *((volatile const int *)&s->done) != 0 || *((volatile const int *)&s->update) == 0;
+}
+
 // ----------------------------------------------------------- stencil apply --
 
 enum Epi : int {
@@ -230,8 +291,9 @@ struct StencilArgs {
     int nx, ny, nz;
     long long n;
     double deta;
-    ReduceCtx red;
-    const KrylovScalars *guard;  // skip when guard->done (may be null)
+    ReduceCtx red{};
+    const KrylovScalars *guard = nullptr;  // skip when guard->done (may be null)
+    int guard_update = 0;                  // 1: run only while guard->update is pending
 };
 
 // Shared-memory ring of z-planes of the input: NS slots of (TY+2) x (TX*V+2)
@@ -295,11 +357,19 @@ __device__ __forceinline__ void ring_store(T *slot, const T (&rv)[Ring<T, V, TX,
     }
 }
 
-template <typename T, int V, int TX, int TY, bool HORIZ, int EPI>
+// DIFF: the operator is given in zero-row-sum difference form for the
+// variable pi = s / fcscal: plane AC holds the row-sum defect d (about 0) and
+// every other plane B_nb = A_nb fcscal_nb, so that
+//     (A s)_c = d pi_c + sum_nb B_nb (pi_nb - pi_c).
+// Rounding B to FP32 then perturbs face fluxes but keeps the operator's null
+// space (pi = const) exact, which a rounded A in the plain form does not:
+// its smooth-mode error grows like eps32 / (k h)^2 and stalls the FP32
+// Krylov iteration on large grids.
+template <typename T, int V, int TX, int TY, bool HORIZ, int EPI, bool DIFF = false>
 __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
     using R = Ring<T, V, TX, TY>;
     __shared__ __align__(16) T sm[R::NS][R::NR * R::RW];
-    if (krylov_done(a.guard)) return;
+    if (a.guard_update ? no_update_pending(a.guard) : krylov_done(a.guard)) return;
 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int x0 = blockIdx.x * R::W, y0 = blockIdx.y * TY;
@@ -343,6 +413,36 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
                 const int ic = r * R::RW + cc;
                 const int il = ic - 1, ir = ic + 1, ib = ic - R::RW, iff = ic + R::RW;
                 T acc;
+                if (DIFF) {
+                    const T pc = s0[ic];
+                    acc = c[PCF_AC][e] * pc;
+                    acc = fma(c[PCF_AD][e], sm1[ic] - pc, acc);
+                    acc = fma(c[PCF_AU][e], sp1[ic] - pc, acc);
+                    acc = fma(c[PCF_AL][e], s0[il] - pc, acc);
+                    acc = fma(c[PCF_AR][e], s0[ir] - pc, acc);
+                    acc = fma(c[PCF_AB][e], s0[ib] - pc, acc);
+                    acc = fma(c[PCF_AF][e], s0[iff] - pc, acc);
+                    acc = fma(c[PCF_ALD][e], sm1[il] - pc, acc);
+                    acc = fma(c[PCF_ALU][e], sp1[il] - pc, acc);
+                    acc = fma(c[PCF_ARD][e], sm1[ir] - pc, acc);
+                    acc = fma(c[PCF_ARU][e], sp1[ir] - pc, acc);
+                    acc = fma(c[PCF_ABD][e], sm1[ib] - pc, acc);
+                    acc = fma(c[PCF_ABU][e], sp1[ib] - pc, acc);
+                    acc = fma(c[PCF_AFD][e], sm1[iff] - pc, acc);
+                    acc = fma(c[PCF_AFU][e], sp1[iff] - pc, acc);
+                    acc = fma(c[PCF_ADD][e], sm2[ic] - pc, acc);
+                    acc = fma(c[PCF_AUU][e], sp2[ic] - pc, acc);
+                    acc = fma(c[PCF_ALDD][e], sm2[il] - pc, acc);
+                    acc = fma(c[PCF_ALUU][e], sp2[il] - pc, acc);
+                    acc = fma(c[PCF_ARDD][e], sm2[ir] - pc, acc);
+                    acc = fma(c[PCF_ARUU][e], sp2[ir] - pc, acc);
+                    acc = fma(c[PCF_ABDD][e], sm2[ib] - pc, acc);
+                    acc = fma(c[PCF_ABUU][e], sp2[ib] - pc, acc);
+                    acc = fma(c[PCF_AFDD][e], sm2[iff] - pc, acc);
+                    acc = fma(c[PCF_AFUU][e], sp2[iff] - pc, acc);
+                    res[e] = acc;
+                    continue;
+                }
                 if (HORIZ) {
                     acc = c[PCF_AL][e] * s0[il];
                 } else {
@@ -432,6 +532,7 @@ struct ThomasArgs {
     const T *r, *v;
     T *vec;         // TH_SUPD: s (out); TH_PUPD: p (in/out)
     T *out;
+    const T *post = nullptr;    // if set, the stored solution is multiplied by post (1 / fcscal)
     int plane, nz;
     long long n;
     double deta;
@@ -475,6 +576,17 @@ __global__ void __launch_bounds__(128) k_thomas(ThomasArgs<T> a) {
         a.out[o] = y;
     }
     T xs = y;
+    if (a.post) {
+        const long long o = col + (long long)a.plane * (a.nz - 1);
+        a.out[o] = xs * __ldg(a.post + o);
+#pragma unroll 4
+        for (int k = a.nz - 2; k >= 0; --k) {
+            const long long q = col + (long long)a.plane * k;
+            xs = a.out[q] + __ldg(Q + q) * xs;
+            a.out[q] = xs * __ldg(a.post + q);
+        }
+        return;
+    }
 #pragma unroll 4
     for (int k = a.nz - 2; k >= 0; --k) {
         const long long o = col + (long long)a.plane * k;
@@ -489,14 +601,18 @@ template <typename T>
 struct UpdateArgs {
     T *x, *r;
     const T *p, *s, *t, *r0;
+    const T *zp, *zs;  // FLEX: the preconditioned directions M p and M s
     long long n;
     ReduceCtx red;
     KrylovScalars *scal;
 };
 
 // x += alpha p + omega s; r = s - omega t; sums <r, r> and <r, r0>
-// (apply_bicgstab!.jl:110-120).
-template <typename T>
+// (apply_bicgstab!.jl:110-120).  FLEX accumulates the preconditioned
+// directions instead (x += alpha M p + omega M s), which keeps x consistent
+// with the recursive residual when M is evaluated in FP32 and so is not
+// exactly linear; no final x <- M x is then needed.
+template <typename T, bool FLEX>
 __global__ void __launch_bounds__(256) k_update(UpdateArgs<T> a) {
     if (krylov_done(a.scal)) return;
     const T alpha = (T)a.scal->alpha, omega = (T)a.scal->omega;
@@ -504,7 +620,10 @@ __global__ void __launch_bounds__(256) k_update(UpdateArgs<T> a) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.n;
          i += (long long)gridDim.x * blockDim.x) {
         const T sv = a.s[i];
-        a.x[i] = a.x[i] + (alpha * a.p[i] + omega * sv);
+        if (FLEX)
+            a.x[i] = a.x[i] + (alpha * a.zp[i] + omega * a.zs[i]);
+        else
+            a.x[i] = a.x[i] + (alpha * a.p[i] + omega * sv);
         const T rv = sv - omega * a.t[i];
         a.r[i] = rv;
         rr += (double)rv * (double)rv;
@@ -543,6 +662,76 @@ __global__ void __launch_bounds__(256) k_dot(const T *__restrict__ a, const T *_
         s += (double)a[i] * (double)b[i];
     double v[1] = {s};
     reduce_finalize<1>(red, v);
+}
+
+// Reliable update, step 1: x64 += bnorm64 * fcscal * x32 (the FP32 iteration
+// solves for pi = s / fcscal with the right-hand side scaled by 1 / bnorm64);
+// x32 = 0.
+__global__ void __launch_bounds__(256) k_ru_fold(float *x32, double *x64, const double *__restrict__ fc, long long n,
+                                                const KrylovScalars *scal) {
+    if (no_update_pending(scal)) return;
+    const double sc = scal->bnorm64;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        x64[i] += sc * fc[i] * (double)x32[i];
+        x32[i] = 0.0f;
+    }
+}
+
+// Difference-form FP32 operator (see k_stencil, DIFF): B_nb = A_nb fcscal_nb for
+// the 24 neighbours and the row-sum defect sum_all A_nb fcscal_nb in plane AC,
+// all formed in FP64; also fcscal and 1 / fcscal on the interior.
+// fch: fcscal on the haloed grid (halo >= 1 in x, y and >= 2 in z).
+__global__ void __launch_bounds__(128) k_build_diff(const double *__restrict__ A, const double *__restrict__ fch,
+                                                   int nx, int ny, int nz, int nbx, int nby, int nbz, int nxx,
+                                                   int nyy, float *__restrict__ B, double *__restrict__ fc64,
+                                                   float *__restrict__ rfc32) {
+    const long long n = (long long)nx * ny * nz;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+    const long long sy = nxx, sz = (long long)nxx * nyy;
+    const long long h = (i + nbx) + sy * (j + nby) + sz * (k + nbz);
+    // (di, dj, dk) of each plane in Tensor order
+    const signed char off[PCF_NCOEF][3] = {
+        {0, 0, 0},  {-1, 0, 0}, {1, 0, 0},  {0, -1, 0}, {0, 1, 0},  {0, 0, -1}, {0, 0, 1},  {-1, 0, -1}, {-1, 0, 1},
+        {1, 0, -1}, {1, 0, 1},  {0, -1, -1}, {0, -1, 1}, {0, 1, -1}, {0, 1, 1},  {0, 0, -2}, {0, 0, 2},  {-1, 0, -2},
+        {-1, 0, 2}, {1, 0, -2}, {1, 0, 2},  {0, -1, -2}, {0, -1, 2}, {0, 1, -2}, {0, 1, 2}};
+    double defect = 0.0;
+    for (int p = 0; p < PCF_NCOEF; ++p) {
+        const double b = A[(long long)p * n + c] * fch[h + off[p][0] + sy * off[p][1] + sz * off[p][2]];
+        defect += b;
+        if (p != PCF_AC) B[(long long)p * n + c] = (float)b;
+    }
+    B[(long long)PCF_AC * n + c] = (float)defect;
+    fc64[c] = fch[h];
+    rfc32[c] = (float)(1.0 / fch[h]);
+}
+
+// fcscal = sqrt(pbar^2 / rhobar) on the haloed grid, or 1 where no background is set.
+__global__ void k_fcscal_halo(const double *__restrict__ pbar, const double *__restrict__ rhobar, double *out,
+                              long long nh, int have_background) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nh; q += (long long)gridDim.x * blockDim.x)
+        out[q] = have_background ? sqrt(pbar[q] * pbar[q] / rhobar[q]) : 1.0;
+}
+
+// Reliable update, step 3 (after r64 = b - A x64 in FP64): r32 = r64 / bnorm64
+// and <r32, r0> for the restarted recurrences.
+__global__ void __launch_bounds__(256) k_ru_convert(const double *__restrict__ r64, float *r32, float *r0,
+                                                   long long n, ReduceCtx red) {
+    if (no_update_pending(red.scal)) return;
+    const double sc = 1.0 / red.scal->bnorm64;
+    const bool restart = red.scal->restart_now != 0;
+    double acc = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float v = (float)(r64[i] * sc);
+        r32[i] = v;
+        if (restart) r0[i] = v;
+        acc += (double)v * (double)(restart ? v : r0[i]);
+    }
+    double s[1] = {acc};
+    reduce_finalize<1>(red, s);
 }
 
 // Without preconditioner: s = r - alpha v or p = r + beta (p - omega v).

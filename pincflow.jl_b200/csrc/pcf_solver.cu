@@ -129,7 +129,7 @@ static int pick_kc(long long xyblocks, int nz) {
     return (int)kc;
 }
 
-template <typename T, int V, int TX, bool HORIZ, int EPI>
+template <typename T, int V, int TX, bool HORIZ, int EPI, bool DIFF>
 static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a) {
     constexpr int TY = 128 / TX;
     constexpr int W = TX * V;
@@ -141,15 +141,16 @@ static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a) {
     const dim3 block(TX, TY, 1);
     // algorithmic words per cell: coefficient planes + input + output (+ second operand)
     const int words = (HORIZ ? 22 : 25) + 2 + (EPI == EPI_STORE ? 0 : 1);
-    const int tag = HORIZ ? (sizeof(T) == 4 ? PCF_PROF_PSEUDO32 : PCF_PROF_PSEUDO64)
-                          : (sizeof(T) == 4 ? PCF_PROF_APPLY32 : PCF_PROF_APPLY64);
+    const int tag = a.guard_update ? PCF_PROF_RELIABLE
+                    : HORIZ        ? (sizeof(T) == 4 ? PCF_PROF_PSEUDO32 : PCF_PROF_PSEUDO64)
+                                   : (sizeof(T) == 4 ? PCF_PROF_APPLY32 : PCF_PROF_APPLY64);
     ProfScope ps(h, tag, (double)words * sizeof(T) * (double)a.n);
-    k_stencil<T, V, TX, TY, HORIZ, EPI><<<grid, block, 0, h->stream>>>(a, kc);
+    k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF><<<grid, block, 0, h->stream>>>(a, kc);
     PCF_CUDA_TRY(cudaGetLastError());
     return PCF_OK;
 }
 
-template <typename T, bool HORIZ, int EPI>
+template <typename T, bool HORIZ, int EPI, bool DIFF = false>
 static int launch_stencil(pcf_handle *h, StencilArgs<T> a) {
     a.nx = h->d.nx;
     a.ny = h->d.ny;
@@ -159,11 +160,20 @@ static int launch_stencil(pcf_handle *h, StencilArgs<T> a) {
     const bool vec = (a.nx % VMAX) == 0;
     const int wide = vec ? 32 * VMAX : 32;
     if (a.nx >= wide) {
-        if (vec) return launch_stencil_cfg<T, VMAX, 32, HORIZ, EPI>(h, a);
-        return launch_stencil_cfg<T, 1, 32, HORIZ, EPI>(h, a);
+        if (vec) return launch_stencil_cfg<T, VMAX, 32, HORIZ, EPI, DIFF>(h, a);
+        return launch_stencil_cfg<T, 1, 32, HORIZ, EPI, DIFF>(h, a);
     }
-    if (vec) return launch_stencil_cfg<T, VMAX, 8, HORIZ, EPI>(h, a);
-    return launch_stencil_cfg<T, 1, 8, HORIZ, EPI>(h, a);
+    if (vec) return launch_stencil_cfg<T, VMAX, 8, HORIZ, EPI, DIFF>(h, a);
+    return launch_stencil_cfg<T, 1, 8, HORIZ, EPI, DIFF>(h, a);
+}
+
+// Total apply of the Krylov loop: plain form, or the FP32 difference form.
+template <typename T, int EPI>
+static int apply_total(pcf_handle *h, const StencilArgs<T> &a, bool diff) {
+    if constexpr (sizeof(T) == 4) {
+        if (diff) return launch_stencil<T, false, EPI, true>(h, a);
+    }
+    return launch_stencil<T, false, EPI>(h, a);
 }
 
 template <typename T, int MODE>
@@ -188,22 +198,45 @@ static unsigned vec_grid(long long n) {
 template <typename T>
 struct Work {
     const T *coef, *fac;
-    T *x, *r, *r0, *p, *v, *s, *t, *za, *zb;
+    T *x, *r, *r0, *p, *v, *s, *t, *za, *zb, *zc, *zd;  // (za, zb): M p chain, (zc, zd): M s chain
     KrylovScalars *scal;
+    const T *coefT;  // planes of the Total apply inside the loop
+    const T *post;   // 1 / fcscal when the loop variable is pi = s / fcscal
 };
 
 static Work<double> work64(pcf_handle *h) {
+    // the reference form consumes M p before M s is formed: one chain suffices
     return {h->coef64, h->fac64, h->x64, h->r64, h->r064, h->p64, h->v64, h->s64, h->t64, h->za64, h->zb64,
-            h->scal64};
+            h->za64, h->zb64, h->scal64, h->coef64, nullptr};
 }
 static Work<float> work32(pcf_handle *h) {
     return {h->coef32, h->fac32, h->x32, h->r32, h->r032, h->p32, h->v32, h->s32, h->t32, h->za32, h->zb32,
-            h->scal32};
+            h->zc32, h->zd32, h->scal32, h->coef32, nullptr};
+}
+// The FP32 loop of the mixed solve: difference-form operator on pi = s / fcscal.
+static Work<float> work32_pi(pcf_handle *h) {
+    Work<float> w = work32(h);
+    w.coefT = h->coefB32;
+    w.post = h->rfc32;
+    return w;
 }
 
 static double deta_of(const pcf_handle *h, double dtau) {
     // apply_preconditioner!.jl:58
     return dtau / (2 * (1 / (h->dx * h->dx) + 1 / (h->dy * h->dy)));
+}
+
+// Difference-form FP32 operator (k_build_diff) from the FP64 operator; the
+// variable is pi = s / fcscal, with fcscal = 1 when no background is set.
+static int build_diff(pcf_handle *h, int have_background) {
+    h->launches += 2;
+    k_fcscal_halo<<<vec_grid(h->nh), 256, 0, h->stream>>>(h->pbar, h->rhobar, h->fch, h->nh, have_background);
+    PCF_CUDA_TRY(cudaGetLastError());
+    k_build_diff<<<(unsigned)((h->d.n + 127) / 128), 128, 0, h->stream>>>(
+        h->coef64, h->fch, h->d.nx, h->d.ny, h->d.nz, h->dims.nbx, h->dims.nby, h->dims.nbz, h->nxx, h->nyy,
+        h->coefB32, h->fc64, h->rfc32);
+    PCF_CUDA_TRY(cudaGetLastError());
+    return PCF_OK;
 }
 
 static int ensure_factors(pcf_handle *h, double deta) {
@@ -218,22 +251,28 @@ static int ensure_factors(pcf_handle *h, double deta) {
 // s / p update, written back to bvec).  Returns the buffer that holds M b.
 template <typename T, int MODE>
 static int precond_apply(pcf_handle *h, const Work<T> &w, T *bvec, int iters, double deta,
-                         const KrylovScalars *guard, T **result) {
+                         const KrylovScalars *guard, T **result, T *o1 = nullptr, T *o2 = nullptr,
+                         const T *post = nullptr) {
+    if (!o1) {
+        o1 = w.za;
+        o2 = w.zb;
+    }
     ThomasArgs<T> ta;
     ta.fac = w.fac;
     ta.in = bvec;
     ta.r = w.r;
     ta.v = w.v;
     ta.vec = bvec;
-    ta.out = w.za;
+    ta.out = o1;
     ta.plane = h->d.plane;
     ta.nz = h->d.nz;
     ta.n = h->d.n;
     ta.deta = deta;
     ta.scal = guard;
+    ta.post = iters == 1 ? post : nullptr;  // the last pseudo-time step returns M b / fcscal
     int rc = launch_thomas<T, MODE>(h, ta);
     if (rc) return rc;
-    T *cur = w.za, *other = w.zb;
+    T *cur = o1, *other = o2;
     for (int m = 1; m < iters; ++m) {
         StencilArgs<T> sa;
         sa.coef = w.coef;
@@ -247,6 +286,7 @@ static int precond_apply(pcf_handle *h, const Work<T> &w, T *bvec, int iters, do
         ThomasArgs<T> tb = ta;
         tb.in = other;
         tb.out = other;
+        tb.post = m == iters - 1 ? post : nullptr;
         rc = launch_thomas<T, TH_T>(h, tb);
         if (rc) return rc;
         T *tmp = cur;
@@ -260,39 +300,69 @@ static int precond_apply(pcf_handle *h, const Work<T> &w, T *bvec, int iters, do
 struct LoopCfg {
     int precond, pc_iters;
     double deta;
+    int flex;      // accumulate x from the preconditioned directions (FP32 inner loop)
+    int reliable;  // fold into the FP64 solution and restart r from the true residual
 };
+
+// Reliable update (mixed precision): x64 += bnorm64 x32, r64 = b - A64 x64
+// with the FP64 convergence test, r32 = r64 / bnorm64, <r32, r0>.  The three
+// launches return at once unless the last FIN_RESID raised the update flag.
+static int reliable_update(pcf_handle *h) {
+    KrylovScalars *sc = h->scal32;
+    h->launches += 1;
+    k_ru_fold<<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->x32, h->x64, h->fc64, h->d.n, sc);
+    PCF_CUDA_TRY(cudaGetLastError());
+    StencilArgs<double> a;
+    a.coef = h->coef64;
+    a.s = h->x64;
+    a.out = h->w64;
+    a.w1 = h->b64;
+    a.deta = 0;
+    a.guard = sc;
+    a.guard_update = 1;
+    a.red = red(h, sc, FIN_RU_TRUE);
+    int rc = launch_stencil<double, false, EPI_RESID>(h, a);
+    if (rc) return rc;
+    h->launches += 1;
+    k_ru_convert<<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->w64, h->r32, h->r032, h->d.n, red(h, sc, FIN_RU_RHO));
+    PCF_CUDA_TRY(cudaGetLastError());
+    return PCF_OK;
+}
 
 // One BiCGSTAB iteration, apply_bicgstab!.jl:81-143.
 template <typename T>
 static int bicgstab_iteration(pcf_handle *h, const Work<T> &w, const LoopCfg &c) {
     int rc;
-    T *z = nullptr;
+    T *z = nullptr, *zp = nullptr;
     // p = r + beta (p - omega v); z = M p
     if (c.precond) {
-        rc = precond_apply<T, TH_PUPD>(h, w, w.p, c.pc_iters, c.deta, w.scal, &z);
+        rc = precond_apply<T, TH_PUPD>(h, w, w.p, c.pc_iters, c.deta, w.scal, &z, nullptr, nullptr, w.post);
+        zp = z;
     } else {
         h->launches += 1;
         k_axpy_noprec<T, TH_PUPD><<<vec_grid(h->d.n), 256, 0, h->stream>>>(w.r, w.v, w.p, h->d.n, w.scal);
         rc = cudaGetLastError() == cudaSuccess ? PCF_OK : PCF_ECUDA;
         z = w.p;
+        zp = z;
     }
     if (rc) return rc;
     // v = A z; alpha = <r, r0> / <v, r0>
     {
         StencilArgs<T> sa;
-        sa.coef = w.coef;
+        sa.coef = w.coefT;
         sa.s = z;
         sa.out = w.v;
         sa.w1 = w.r0;
         sa.deta = 0;
         sa.red = red(h, w.scal, FIN_ALPHA);
         sa.guard = w.scal;
-        rc = launch_stencil<T, false, EPI_DOT1>(h, sa);
+        rc = apply_total<T, EPI_DOT1>(h, sa, w.post != nullptr);
         if (rc) return rc;
     }
     // s = r - alpha v; z = M s
     if (c.precond) {
-        rc = precond_apply<T, TH_SUPD>(h, w, w.s, c.pc_iters, c.deta, w.scal, &z);
+        rc = precond_apply<T, TH_SUPD>(h, w, w.s, c.pc_iters, c.deta, w.scal, &z, c.flex ? w.zc : w.za,
+                                       c.flex ? w.zd : w.zb, w.post);
     } else {
         h->launches += 1;
         k_axpy_noprec<T, TH_SUPD><<<vec_grid(h->d.n), 256, 0, h->stream>>>(w.r, w.v, w.s, h->d.n, w.scal);
@@ -303,14 +373,14 @@ static int bicgstab_iteration(pcf_handle *h, const Work<T> &w, const LoopCfg &c)
     // t = A z; omega = <t, s> / <t, t>
     {
         StencilArgs<T> sa;
-        sa.coef = w.coef;
+        sa.coef = w.coefT;
         sa.s = z;
         sa.out = w.t;
         sa.w1 = w.s;
         sa.deta = 0;
         sa.red = red(h, w.scal, FIN_OMEGA);
         sa.guard = w.scal;
-        rc = launch_stencil<T, false, EPI_DOT2>(h, sa);
+        rc = apply_total<T, EPI_DOT2>(h, sa, w.post != nullptr);
         if (rc) return rc;
     }
     // x += alpha p + omega s; r = s - omega t; residual test, beta
@@ -322,18 +392,24 @@ static int bicgstab_iteration(pcf_handle *h, const Work<T> &w, const LoopCfg &c)
         ua.s = w.s;
         ua.t = w.t;
         ua.r0 = w.r0;
+        ua.zp = zp;
+        ua.zs = z;
         ua.n = h->d.n;
         ua.red = red(h, w.scal, FIN_RESID);
         ua.scal = w.scal;
         ProfScope ps(h, sizeof(T) == 4 ? PCF_PROF_UPDATE32 : PCF_PROF_UPDATE64, 7.0 * sizeof(T) * (double)h->d.n);
-        k_update<T><<<vec_grid(h->d.n), 256, 0, h->stream>>>(ua);
+        if (c.flex)
+            k_update<T, true><<<vec_grid(h->d.n), 256, 0, h->stream>>>(ua);
+        else
+            k_update<T, false><<<vec_grid(h->d.n), 256, 0, h->stream>>>(ua);
         PCF_CUDA_TRY(cudaGetLastError());
     }
+    if (c.reliable) return reliable_update(h);
     return PCF_OK;
 }
 
 struct RunOut {
-    int iters, converged, status;
+    int iters, converged, status, nupdates;
     double res, b_norm;
 };
 
@@ -342,13 +418,23 @@ struct RunOut {
 // apply_bicgstab!.jl:132-135.  Result vector: *xout (x or a z buffer).
 template <typename T>
 static int bicgstab_run(pcf_handle *h, const Work<T> &w, const T *b, double tol, int maxit, const LoopCfg &c,
-                        int check_interval, bool precondition_unconverged, T **xout, RunOut *out) {
+                        int check_interval, bool precondition_unconverged, T **xout, RunOut *out,
+                        int hist_off = 0, double hist_scale = 1.0, double bnorm64 = 0.0, double ru_delta = 0.0,
+                        int restart_every = 0) {
     // scalar block
     KrylovScalars init;
     std::memset(&init, 0, sizeof(init));
     init.tol = tol;
     init.maxit = maxit;
     init.ncell = (double)h->d.n;
+    init.hist = h->hist;
+    init.hist_cap = kHistCap;
+    init.hist_off = hist_off;
+    init.hist_scale = hist_scale;
+    init.reliable = c.reliable;
+    init.bnorm64 = bnorm64;
+    init.ru_delta = ru_delta;
+    init.restart_every = restart_every;
     PCF_CUDA_TRY(cudaMemcpyAsync(w.scal, &init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
     PCF_CUDA_TRY(cudaMemsetAsync(w.v, 0, sizeof(T) * h->d.n, h->stream));
     h->launches += 1;
@@ -371,14 +457,16 @@ static int bicgstab_run(pcf_handle *h, const Work<T> &w, const T *b, double tol,
     const KrylovScalars s = *h->h_scal;
     h->prof_iter = -1;
     prof_flush(h, s.iter);
+    h->hist_len = std::min(hist_off + s.iter, kHistCap);
     out->iters = s.iter;
     out->converged = s.converged;
     out->status = s.status;
-    out->res = s.b_norm > 0 ? s.res / s.b_norm : 0.0;
+    out->res = c.reliable ? s.res_true : (s.b_norm > 0 ? s.res / s.b_norm : 0.0);
     out->b_norm = s.b_norm;
+    out->nupdates = s.nupdates;
     *xout = w.x;
     const bool finish = s.converged || (precondition_unconverged && s.status == PCF_OK);
-    if (finish && s.iter > 0 && c.precond) {
+    if (finish && s.iter > 0 && c.precond && !c.flex) {
         T *z = nullptr;
         int rc = precond_apply<T, TH_B>(h, w, w.x, c.pc_iters, c.deta, nullptr, &z);
         if (rc) return rc;
@@ -397,9 +485,17 @@ __global__ void k_to_double(const float *__restrict__ a, double *__restrict__ b,
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         b[i] = (double)a[i];
 }
-__global__ void k_axpy_f2d(const float *__restrict__ e, double *__restrict__ x, long long n, double scale) {
+// x += scale * fc * e (fc may be null: 1)
+__global__ void k_axpy_f2d(const float *__restrict__ e, double *__restrict__ x, const double *__restrict__ fc,
+                           long long n, double scale) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        x[i] += (double)e[i] * scale;
+        x[i] += (double)e[i] * scale * (fc ? fc[i] : 1.0);
+}
+// pi = s / fcscal in FP32 (for the difference-form operator entry point)
+__global__ void k_to_pi(const double *__restrict__ s, const float *__restrict__ rfc, float *__restrict__ pi,
+                        long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        pi[i] = (float)(s[i] * (double)rfc[i]);
 }
 __global__ void k_coef_to_float(const double *__restrict__ a, float *__restrict__ b, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -455,10 +551,11 @@ int pcf_params_default(pcf_params *p) {
     p->damp_horizontal_wind_on_rhs = 0;  // SpongeNamelist default
     p->precision = PCF_PRECISION_FP64;
     p->residual = PCF_RESIDUAL_RECURSIVE;
-    p->inner_tolerance = 1.0e-5;
-    p->max_refinements = 20;
+    p->inner_tolerance = 1.0e-2;
+    p->max_refinements = 5;
     p->learned = 0;
     p->check_interval = 16;
+    p->restart_interval = 1;
     return PCF_OK;
 }
 
@@ -474,9 +571,12 @@ int pcf_destroy(pcf_handle *h) {
     int dev = h->dims.device;
     cudaSetDevice(dev);
     void *ptrs[] = {h->jac, h->met13, h->met23, h->met33, h->pbar, h->rhobar, h->thetabar, h->n2, h->rho, h->betar,
-                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->x64, h->r64, h->r064, h->p64, h->v64, h->s64,
+                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch,
+                    h->x64, h->r64, h->r064, h->p64, h->v64, h->s64,
                     h->t64, h->za64, h->zb64, h->b64, h->w64, h->x32, h->r32, h->r032, h->p32, h->v32, h->s32,
-                    h->t32, h->za32, h->zb32, h->partials, h->ticket, h->scal64, h->scal32, h->dot_out};
+                    h->t32, h->za32, h->zb32, h->zc32, h->zd32, h->partials, h->ticket, h->scal64, h->scal32,
+                    h->dot_out,
+                    h->hist};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -537,11 +637,16 @@ int pcf_create(pcf_handle **out, const pcf_dims *dims) {
     if ((rc = dalloc(h, (void **)&h->coef32, n4 * PCF_NCOEF))) return fail(rc);
     if ((rc = dalloc(h, (void **)&h->fac64, n8 * 3))) return fail(rc);
     if ((rc = dalloc(h, (void **)&h->fac32, n4 * 3))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->coefB32, n4 * PCF_NCOEF))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->fc64, n8))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->rfc32, n4))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->fch, nh8))) return fail(rc);
     double **v64[] = {&h->x64, &h->r64, &h->r064, &h->p64, &h->v64, &h->s64, &h->t64, &h->za64, &h->zb64, &h->b64,
                       &h->w64};
     for (double **v : v64)
         if ((rc = dalloc(h, (void **)v, n8))) return fail(rc);
-    float **v32[] = {&h->x32, &h->r32, &h->r032, &h->p32, &h->v32, &h->s32, &h->t32, &h->za32, &h->zb32};
+    float **v32[] = {&h->x32, &h->r32, &h->r032, &h->p32, &h->v32, &h->s32, &h->t32, &h->za32, &h->zb32,
+                     &h->zc32, &h->zd32};
     for (float **v : v32)
         if ((rc = dalloc(h, (void **)v, n4))) return fail(rc);
     if ((rc = dalloc(h, (void **)&h->partials, sizeof(double) * 2 * kMaxPartials))) return fail(rc);
@@ -549,6 +654,7 @@ int pcf_create(pcf_handle **out, const pcf_dims *dims) {
     if ((rc = dalloc(h, (void **)&h->scal64, sizeof(KrylovScalars)))) return fail(rc);
     if ((rc = dalloc(h, (void **)&h->scal32, sizeof(KrylovScalars)))) return fail(rc);
     if ((rc = dalloc(h, (void **)&h->dot_out, sizeof(double) * 4))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->hist, sizeof(double) * kHistCap))) return fail(rc);
     if (cudaMallocHost((void **)&h->h_scal, sizeof(KrylovScalars)) != cudaSuccess) return fail(PCF_ENOMEM);
     if (cudaMemsetAsync(h->ticket, 0, sizeof(unsigned int) * 4, h->stream) != cudaSuccess) return fail(PCF_ECUDA);
     // fields a caller may legitimately leave unset read as zero
@@ -597,11 +703,13 @@ int pcf_set_background(pcf_handle *h, const double *pbar, const double *rhobar, 
 static int assemble_device(pcf_handle *h, double dt, double rf, int damp_h) {
     if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
     // about 9 haloed fields read, 25 FP64 + 25 FP32 planes written per cell
-    ProfScope ps(h, PCF_PROF_ASSEMBLE, (9.0 * 8 + 25.0 * 12) * (double)h->d.n);
-    int rc = pcf_launch_assemble(h, dt, rf, damp_h);
-    if (rc) return rc;
+    {
+        ProfScope ps(h, PCF_PROF_ASSEMBLE, (9.0 * 8 + 25.0 * 12) * (double)h->d.n);
+        int rc = pcf_launch_assemble(h, dt, rf, damp_h);
+        if (rc) return rc;
+    }
     h->operator_set = 1;
-    return PCF_OK;
+    return build_diff(h, 1);
 }
 
 int pcf_compute_operator(pcf_handle *h, const double *rho, const double *betar, const double *p, double dt,
@@ -629,10 +737,13 @@ int pcf_set_operator(pcf_handle *h, const double *coef) {
     const long long m = h->d.n * PCF_NCOEF;
     PCF_CUDA_TRY(cudaMemcpyAsync(h->coef64, coef, sizeof(double) * m, cudaMemcpyHostToDevice, h->stream));
     k_coef_to_float<<<vec_grid(m), 256, 0, h->stream>>>(h->coef64, h->coef32, m);
+    h->launches += 1;
     PCF_CUDA_TRY(cudaGetLastError());
-    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
     h->operator_set = 1;
     h->fac_deta = std::nan("");
+    int rc = build_diff(h, h->background_set);
+    if (rc) return rc;
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
     return PCF_OK;
 }
 
@@ -651,7 +762,24 @@ int pcf_apply_operator(pcf_handle *h, const double *sin_, double *ls, int mode, 
     if (!h->operator_set) return PCF_ENOTREADY;
     PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
     int rc;
-    if (precision == PCF_PRECISION_FP32) {
+    if (precision == PCF_PRECISION_MIXED) {
+        // the FP32 difference-form operator of the mixed solve, applied to s
+        if (mode != PCF_TOTAL) return PCF_EINVAL;
+        if ((rc = upload_vec(h, sin_, h->b64, nullptr))) return rc;
+        k_to_pi<<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->b64, h->rfc32, h->s32, h->d.n);
+        h->launches += 1;
+        PCF_CUDA_TRY(cudaGetLastError());
+        StencilArgs<float> a;
+        a.coef = h->coefB32;
+        a.s = h->s32;
+        a.out = h->t32;
+        a.w1 = nullptr;
+        a.deta = 0;
+        if ((rc = launch_stencil<float, false, EPI_STORE, true>(h, a))) return rc;
+        k_to_double<<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->t32, h->w64, h->d.n);
+        h->launches += 1;
+        PCF_CUDA_TRY(cudaGetLastError());
+    } else if (precision == PCF_PRECISION_FP32) {
         if ((rc = upload_vec(h, sin_, h->b64, h->s32))) return rc;
         StencilArgs<float> a;
         a.coef = h->coef32;
@@ -748,6 +876,8 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
     c.precond = prm->preconditioner;
     c.pc_iters = prm->preconditioner_iterations;
     c.deta = deta_of(h, prm->dtau);
+    c.flex = 0;
+    c.reliable = 0;
     if (c.precond && c.pc_iters < 1) return PCF_EINVAL;
     int rc;
     if (c.precond && (rc = ensure_factors(h, c.deta))) return rc;
@@ -794,35 +924,47 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
         res->true_residual = 0.0;
         return PCF_OK;
     }
-    Work<float> w = work32(h);
+    // One FP32 BiCGSTAB iteration on b / RMS(b) with reliable updates: the
+    // FP32 correction is folded into x64 and the FP32 residual replaced by the
+    // FP64 true residual whenever it fell by inner_tolerance (device-side, see
+    // reliable_update).  A breakdown restarts the FP32 iteration from the
+    // current FP64 residual (at most max_refinements times).
+    Work<float> w = work32_pi(h);
+    LoopCfg cm = c;
+    cm.flex = 1;
+    cm.reliable = 1;
     double rel = 1.0;
-    while (rel > tol && res->nrefine < prm->max_refinements && res->niter < maxit) {
-        // inner right-hand side: the FP64 residual, normalised to RMS 1
-        const double scale = 1.0 / rnorm;
-        k_to_float<<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->w64, w.s, h->d.n, scale);
+    int restarts = 0;
+    for (;;) {
+        k_to_float<<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->w64, w.s, h->d.n, 1.0 / b_norm);
+        h->launches += 1;
         PCF_CUDA_TRY(cudaGetLastError());
-        // do not over-solve the last sweep
-        double tin = prm->inner_tolerance;
-        const double need = 0.5 * tol / rel;
-        if (need > tin) tin = need;
         float *e = nullptr;
         RunOut ro;
-        rc = bicgstab_run<float>(h, w, w.s, tin, maxit - res->niter, c, prm->check_interval, true, &e, &ro);
+        rc = bicgstab_run<float>(h, w, w.s, tol, maxit - res->niter, cm, prm->check_interval, false, &e, &ro,
+                                 res->niter, 1.0, b_norm, prm->inner_tolerance, prm->restart_interval);
         if (rc) return rc;
         res->niter += ro.iters;
-        res->nrefine += 1;
-        if (ro.status != PCF_OK || ro.iters == 0) {
-            res->status = ro.status != PCF_OK ? ro.status : PCF_EBREAKDOWN;
-            break;
+        res->nrefine += ro.nupdates;
+        if (ro.nupdates > 0) rel = ro.res;
+        if (ro.converged) break;
+        if (ro.status == PCF_EBREAKDOWN && restarts < prm->max_refinements && res->niter < maxit) {
+            // fold what the broken-down iteration accumulated, then restart from the true residual
+            k_axpy_f2d<<<vec_grid(h->d.n), 256, 0, h->stream>>>(w.x, h->x64, h->fc64, h->d.n, b_norm);
+            h->launches += 1;
+            PCF_CUDA_TRY(cudaGetLastError());
+            if ((rc = true_residual(h, h->b64, h->x64, &rnorm))) return rc;
+            rel = rnorm / b_norm;
+            restarts += 1;
+            if (!std::isfinite(rel)) {
+                res->status = PCF_ENONFINITE;
+                break;
+            }
+            if (rel <= tol) break;
+            continue;
         }
-        k_axpy_f2d<<<vec_grid(h->d.n), 256, 0, h->stream>>>(e, h->x64, h->d.n, rnorm);
-        PCF_CUDA_TRY(cudaGetLastError());
-        if ((rc = true_residual(h, h->b64, h->x64, &rnorm))) return rc;
-        rel = rnorm / b_norm;
-        if (!std::isfinite(rel)) {
-            res->status = PCF_ENONFINITE;
-            break;
-        }
+        res->status = ro.status;
+        break;
     }
     res->residual = rel;
     res->true_residual = rel;
@@ -953,6 +1095,18 @@ int pcf_bicgstab(pcf_handle *h, const double *rhs, double tolref, const pcf_para
 }
 
 long long pcf_launch_count(const pcf_handle *h) { return h ? h->launches : 0; }
+
+int pcf_residual_history(pcf_handle *h, double *out, int cap, int *n) {
+    if (!h || !n || (cap > 0 && !out)) return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    const int m = std::min(cap, h->hist_len);
+    *n = h->hist_len;
+    if (m > 0) {
+        PCF_CUDA_TRY(cudaMemcpyAsync(out, h->hist, sizeof(double) * m, cudaMemcpyDeviceToHost, h->stream));
+        PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
+    return PCF_OK;
+}
 
 int pcf_profile_enable(pcf_handle *h, int on) {
     if (!h) return PCF_EINVAL;

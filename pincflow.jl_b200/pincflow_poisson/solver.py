@@ -43,10 +43,11 @@ class PoissonNamelist:
     # additions without a reference counterpart (defaults reproduce the reference)
     precision: str = "fp64"          # "fp64" | "mixed"
     residual: str = "recursive"      # "recursive" | "true"
-    inner_tolerance: float = 1.0e-5
-    max_refinements: int = 20
+    inner_tolerance: float = 1.0e-2   # mixed: residual drop between FP64 reliable updates
+    max_refinements: int = 5          # mixed: restarts of the FP32 iteration after a breakdown
     learned: bool = False
     check_interval: int = 16
+    restart_interval: int = 1         # mixed: Krylov restart at every n-th reliable update (0: never)
 
     def to_c(self) -> _lib.PcfParams:
         p = _lib.PcfParams()
@@ -64,6 +65,7 @@ class PoissonNamelist:
         p.max_refinements = int(self.max_refinements)
         p.learned = int(bool(self.learned))
         p.check_interval = int(self.check_interval)
+        p.restart_interval = int(self.restart_interval)
         return p
 
 
@@ -124,6 +126,15 @@ class PoissonSolver:
 
     def profile(self, on: bool = True):
         _lib.check(self.lib.pcf_profile_enable(self._h, int(bool(on))), "pcf_profile_enable")
+
+    def residual_history(self) -> np.ndarray:
+        """Relative recursive residual after each iteration of the last solve."""
+        n = ctypes.c_int()
+        _lib.check(self.lib.pcf_residual_history(self._h, None, 0, ctypes.byref(n)), "pcf_residual_history")
+        out = np.zeros(max(n.value, 1))
+        _lib.check(self.lib.pcf_residual_history(self._h, _lib.dptr(out), n.value, ctypes.byref(n)),
+                   "pcf_residual_history")
+        return out[:n.value]
 
     def profile_read(self) -> dict:
         out = {}

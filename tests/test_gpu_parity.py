@@ -226,3 +226,45 @@ def test_gpu_matches_golden_fixtures(pcf):
             sol, info = s.apply_bicgstab(gold[f"{name}/rhs"], 1.0, nl)
             assert not info.errflag
             assert rel_err(_drop_null(cfg, sol), _drop_null(cfg, gold[f"{name}/solution"])) < 1e-8
+
+
+@pytest.mark.parametrize("name", ["hill", "mtn", "odd", "rho", "comp", "wide"])
+def test_difference_form_fp32_operator(name, solvers, oracle):
+    """The FP32 operator of the mixed solve (zero-row-sum difference form in
+    pi = s / fcscal) applied to s equals A s to FP32 accuracy."""
+    cfg, s = solvers(name)
+    d, coef = oracle_operator(oracle, cfg)
+    s.set_operator(coef)
+    x = np.random.default_rng(15).standard_normal(cfg["dom"].interior_shape)
+    ref = oracle.apply_operator(d, coef, x)
+    got = s.apply_operator(x, precision="mixed")
+    assert rel_err(got, ref) < 5e-6
+    if cfg["model"] == "Compressible":
+        return  # dpdpi makes the compressible operator nonsingular
+    # exact null space: A fcscal = 0 also in FP32
+    from pincflow_poisson import fields as F
+    fc = F.fcscal(cfg["dom"], cfg["fields"])
+    a_fc = s.apply_operator(fc, precision="mixed")
+    a_fc32 = s.apply_operator(fc, precision="fp32")
+    scale = np.abs(coef[0]).max() * np.abs(fc).max()
+    assert np.abs(a_fc).max() <= 1e-6 * scale
+    assert np.abs(a_fc).max() <= np.abs(a_fc32).max()
+
+
+def test_mixed_precision_iteration_count_at_scale(pcf):
+    """On a stretched 128 x 96 x 48 mountain grid the reliable-update FP32 solve
+    reaches the FP64 true residual 1e-10 within 25 % of the FP64 iteration count."""
+    from pincflow_poisson import configs as C
+    cfg = C.c2(nx=128, ny=96, nz=48)
+    with pcf.PoissonSolver(cfg["dom"], cfg["model"]) as s:
+        s.set_grid(cfg["fields"])
+        s.set_background(cfg["fields"])
+        s.compute_operator(cfg["rho"], cfg["betar"], cfg["dt"], cfg["rayleigh_factor"], return_coef=False)
+        kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=5000, residual="true")
+        _, i64 = s.apply_bicgstab(cfg["rhs"], 1.0, pcf.PoissonNamelist(precision="fp64", **kw))
+        x, imx = s.apply_bicgstab(cfg["rhs"], 1.0, pcf.PoissonNamelist(precision="mixed", **kw))
+        hist = s.residual_history()
+    assert not i64.errflag and not imx.errflag, (i64, imx)
+    assert imx.true_residual <= 1e-10
+    assert imx.niter <= 1.25 * i64.niter + 5, (imx.niter, i64.niter)
+    assert len(hist) == imx.niter and hist[-1] <= 1e-10
