@@ -47,9 +47,12 @@ WORKLOADS = {
 }
 
 
-def make_workload(name, seed_offset=0):
+def make_workload(name, seed_offset=0, size=None):
     from pincflow_poisson import configs
     if name == "c2":
+        if size:
+            nx, ny, nz = (int(v) for v in size.lower().split("x"))
+            return configs.c2(seed=12345 + seed_offset, nx=nx, ny=ny, nz=nz)
         return configs.c2(seed=12345 + seed_offset)
     if name == "c5":
         return configs.c5(seed=5 + seed_offset)
@@ -168,7 +171,7 @@ def oracle_iterations(config):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    cfg = make_workload(args.config)
+    cfg = make_workload(args.config, size=args.size)
     niter, src = oracle_iterations(args.config)
     if niter is None:
         niter, src = args.ref_iterations, "--ref-iterations"
@@ -204,7 +207,7 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist_mod
         dist = dist_mod
 
-    cfg = make_workload(args.config, seed_offset=rank)
+    cfg = make_workload(args.config, seed_offset=rank, size=args.size)
     dom, f = cfg["dom"], cfg["fields"]
     dev = torch.device("cuda", local_rank)
     s = pcf.PoissonSolver(dom, cfg["model"], device=local_rank)
@@ -352,6 +355,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--size", default=None, help="c2 only: NXxNYxNZ instead of 256x256x128 (profiling captures)")
     ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--ref-sample-iters", type=int, default=3)

@@ -554,44 +554,85 @@ __global__ void __launch_bounds__(128) k_thomas(ThomasArgs<T> a) {
         beta = (T)a.scal->beta;
         omega = (T)a.scal->omega;
     }
+    // The sweeps are serial in k, so each thread has only its own column's
+    // loads to hide HBM latency with.  They are issued in batches of D levels
+    // ahead of the batch's stores: with in-place outputs the compiler may not
+    // move a load above an earlier store, which otherwise serialises one
+    // round trip per level.
+    constexpr int D = 8;
+    const long long pl = a.plane;
     T y = 0;
-#pragma unroll 4
-    for (int k = 0; k < a.nz; ++k) {
-        const long long o = col + (long long)a.plane * k;
-        T rhs;
-        if (MODE == TH_B) {
-            rhs = -deta * __ldg(a.in + o);
-        } else if (MODE == TH_T) {
-            rhs = a.in[o];
-        } else if (MODE == TH_SUPD) {
-            const T sv = a.r[o] - alpha * a.v[o];
-            a.vec[o] = sv;
-            rhs = -deta * sv;
-        } else {
-            const T pv = a.r[o] + beta * (a.vec[o] - omega * a.v[o]);
-            a.vec[o] = pv;
-            rhs = -deta * pv;
+    for (int k0 = 0; k0 < a.nz; k0 += D) {
+        const int cnt = min(D, a.nz - k0);
+        T u0[D], u1[D], u2[D], pp[D], mm[D];
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            if (q < cnt) {
+                const long long o = col + pl * (k0 + q);
+                pp[q] = __ldg(P + o);
+                mm[q] = __ldg(M + o);
+                if (MODE == TH_B) {
+                    u0[q] = __ldg(a.in + o);
+                } else if (MODE == TH_T) {
+                    u0[q] = a.in[o];  // in place: in == out
+                } else if (MODE == TH_SUPD) {
+                    u0[q] = __ldg(a.r + o);
+                    u1[q] = __ldg(a.v + o);
+                } else {
+                    u0[q] = __ldg(a.r + o);
+                    u1[q] = a.vec[o];  // p is updated in place
+                    u2[q] = __ldg(a.v + o);
+                }
+            }
         }
-        y = rhs * __ldg(P + o) + __ldg(M + o) * y;
-        a.out[o] = y;
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            if (q < cnt) {
+                const long long o = col + pl * (k0 + q);
+                T rhs;
+                if (MODE == TH_B) {
+                    rhs = -deta * u0[q];
+                } else if (MODE == TH_T) {
+                    rhs = u0[q];
+                } else if (MODE == TH_SUPD) {
+                    const T sv = u0[q] - alpha * u1[q];
+                    a.vec[o] = sv;
+                    rhs = -deta * sv;
+                } else {
+                    const T pv = u0[q] + beta * (u1[q] - omega * u2[q]);
+                    a.vec[o] = pv;
+                    rhs = -deta * pv;
+                }
+                y = rhs * pp[q] + mm[q] * y;
+                a.out[o] = y;
+            }
+        }
     }
     T xs = y;
     if (a.post) {
-        const long long o = col + (long long)a.plane * (a.nz - 1);
+        const long long o = col + pl * (a.nz - 1);
         a.out[o] = xs * __ldg(a.post + o);
-#pragma unroll 4
-        for (int k = a.nz - 2; k >= 0; --k) {
-            const long long q = col + (long long)a.plane * k;
-            xs = a.out[q] + __ldg(Q + q) * xs;
-            a.out[q] = xs * __ldg(a.post + q);
-        }
-        return;
     }
-#pragma unroll 4
-    for (int k = a.nz - 2; k >= 0; --k) {
-        const long long o = col + (long long)a.plane * k;
-        xs = a.out[o] + __ldg(Q + o) * xs;
-        a.out[o] = xs;
+    for (int k1 = a.nz - 2; k1 >= 0; k1 -= D) {
+        const int cnt = min(D, k1 + 1);  // levels k1, k1 - 1, ..., k1 - cnt + 1
+        T yy[D], qq[D], ps[D];
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            if (q < cnt) {
+                const long long o = col + pl * (k1 - q);
+                yy[q] = a.out[o];
+                qq[q] = __ldg(Q + o);
+                if (a.post) ps[q] = __ldg(a.post + o);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            if (q < cnt) {
+                const long long o = col + pl * (k1 - q);
+                xs = yy[q] + qq[q] * xs;
+                a.out[o] = a.post ? xs * ps[q] : xs;
+            }
+        }
     }
 }
 
@@ -612,22 +653,39 @@ struct UpdateArgs {
 // directions instead (x += alpha M p + omega M s), which keeps x consistent
 // with the recursive residual when M is evaluated in FP32 and so is not
 // exactly linear; no final x <- M x is then needed.
-template <typename T, bool FLEX>
+// V consecutive elements per thread with 128-bit loads (n % V == 0).
+template <typename T, bool FLEX, int V>
 __global__ void __launch_bounds__(256) k_update(UpdateArgs<T> a) {
     if (krylov_done(a.scal)) return;
     const T alpha = (T)a.scal->alpha, omega = (T)a.scal->omega;
     double rr = 0.0, rr0 = 0.0;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.n;
-         i += (long long)gridDim.x * blockDim.x) {
-        const T sv = a.s[i];
-        if (FLEX)
-            a.x[i] = a.x[i] + (alpha * a.zp[i] + omega * a.zs[i]);
-        else
-            a.x[i] = a.x[i] + (alpha * a.p[i] + omega * sv);
-        const T rv = sv - omega * a.t[i];
-        a.r[i] = rv;
-        rr += (double)rv * (double)rv;
-        rr0 += (double)rv * (double)a.r0[i];
+    const long long nv = a.n / V;
+    for (long long iv = blockIdx.x * (long long)blockDim.x + threadIdx.x; iv < nv;
+         iv += (long long)gridDim.x * blockDim.x) {
+        const long long i = iv * V;
+        T x[V], s[V], t[V], r0[V], d1[V], d2[V];
+        load_vec<T, V>(a.s + i, s);
+        load_vec<T, V>(a.t + i, t);
+        load_vec<T, V>(a.r0 + i, r0);
+        load_vec<T, V>(FLEX ? a.zp + i : a.p + i, d1);
+        if (FLEX) load_vec<T, V>(a.zs + i, d2);
+        {
+            using VT = typename Vec<T, V>::type;
+            const VT xv = *reinterpret_cast<const VT *>(a.x + i);
+            const T *e = reinterpret_cast<const T *>(&xv);
+#pragma unroll
+            for (int q = 0; q < V; ++q) x[q] = e[q];
+        }
+        T rv[V];
+#pragma unroll
+        for (int q = 0; q < V; ++q) {
+            x[q] = x[q] + (alpha * d1[q] + omega * (FLEX ? d2[q] : s[q]));
+            rv[q] = s[q] - omega * t[q];
+            rr += (double)rv[q] * (double)rv[q];
+            rr0 += (double)rv[q] * (double)r0[q];
+        }
+        store_vec<T, V>(a.x + i, x);
+        store_vec<T, V>(a.r + i, rv);
     }
     double v[2] = {rr, rr0};
     reduce_finalize<2>(a.red, v);

@@ -398,10 +398,17 @@ static int bicgstab_iteration(pcf_handle *h, const Work<T> &w, const LoopCfg &c)
         ua.red = red(h, w.scal, FIN_RESID);
         ua.scal = w.scal;
         ProfScope ps(h, sizeof(T) == 4 ? PCF_PROF_UPDATE32 : PCF_PROF_UPDATE64, 7.0 * sizeof(T) * (double)h->d.n);
-        if (c.flex)
-            k_update<T, true><<<vec_grid(h->d.n), 256, 0, h->stream>>>(ua);
-        else
-            k_update<T, false><<<vec_grid(h->d.n), 256, 0, h->stream>>>(ua);
+        constexpr int VU = sizeof(T) == 4 ? 4 : 2;
+        const bool vec = h->d.n % VU == 0;
+        const long long units = vec ? h->d.n / VU : h->d.n;
+        const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>((units + 255) / 256, 16LL * num_sms()));
+        if (c.flex) {
+            if (vec) k_update<T, true, VU><<<grid, 256, 0, h->stream>>>(ua);
+            else k_update<T, true, 1><<<grid, 256, 0, h->stream>>>(ua);
+        } else {
+            if (vec) k_update<T, false, VU><<<grid, 256, 0, h->stream>>>(ua);
+            else k_update<T, false, 1><<<grid, 256, 0, h->stream>>>(ua);
+        }
         PCF_CUDA_TRY(cudaGetLastError());
     }
     if (c.reliable) return reliable_update(h);
