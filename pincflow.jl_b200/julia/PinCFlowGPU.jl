@@ -1,0 +1,155 @@
+# PinCFlowGPU.jl -- routes PinCFlow.jl's pressure Poisson solve to the sm_100a
+# library libpincflow_poisson.so (include/pincflow_poisson.h) through ccall.
+#
+# Usage (after `using PinCFlow`):
+#     include("PinCFlowGPU.jl"); using .PinCFlowGPU
+#     PinCFlowGPU.enable!()          # later solve_poisson! calls run on the GPU
+#
+# The method below replaces
+#     PinCFlow.PoissonSolver.solve_poisson!(state, dt, rayleigh_factor, tolref)
+# (src/PoissonSolver/solve_poisson!.jl:39-75) with the same signature and
+# return convention (errflag, niter); dt == 0 raises as in the reference, a
+# non-converged solve returns (true, niter) and leaves dpip untouched.
+# Single MPI rank only (npx = npy = npz = 1).
+module PinCFlowGPU
+
+using PinCFlow
+const PS = PinCFlow.PoissonSolver
+
+const LIB = get(ENV, "PINCFLOW_POISSON_LIB",
+                joinpath(@__DIR__, "..", "lib", "libpincflow_poisson.so"))
+
+struct PcfDims
+    nx::Cint; ny::Cint; nz::Cint
+    nbx::Cint; nby::Cint; nbz::Cint
+    model::Cint; device::Cint
+end
+
+mutable struct PcfParams
+    tolerance::Cdouble
+    poisson_iterations::Cint
+    preconditioner::Cint
+    dtau::Cdouble
+    preconditioner_iterations::Cint
+    tolerance_is_relative::Cint
+    damp_horizontal_wind_on_rhs::Cint
+    precision::Cint
+    residual::Cint
+    inner_tolerance::Cdouble
+    max_refinements::Cint
+    learned::Cint
+    check_interval::Cint
+    restart_interval::Cint
+end
+
+mutable struct PcfResult
+    errflag::Cint; niter::Cint; nrefine::Cint; status::Cint
+    residual::Cdouble; true_residual::Cdouble; b_norm::Cdouble
+    ms_upload::Cdouble; ms_assemble::Cdouble; ms_solve::Cdouble
+    ms_download::Cdouble; ms_total::Cdouble
+end
+PcfResult() = PcfResult(0, 0, 0, 0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+
+const MODEL = Dict(:Boussinesq => 0, :PseudoIncompressible => 1, :Compressible => 2)
+const PRECISION = Dict(:fp64 => 0, :mixed => 1)
+
+# one handle per State, created on first use (grid and background uploaded once)
+const HANDLES = IdDict{Any, Ptr{Cvoid}}()
+const SETTINGS = Ref((precision = :fp64, device = 0))
+
+check(rc, what) = rc == 0 || error("$what: " *
+    unsafe_string(ccall((:pcf_strerror, LIB), Cstring, (Cint,), rc)))
+
+function handle(state)
+    haskey(HANDLES, state) && return HANDLES[state]
+    (; nx, ny, nz) = state.domain
+    (; nbx, nby, nbz) = state.namelists.domain
+    model = MODEL[state.namelists.atmosphere.model]
+    dims = Ref(PcfDims(nx, ny, nz, nbx, nby, nbz, model, SETTINGS[].device))
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:pcf_create, LIB), Cint, (Ptr{Ptr{Cvoid}}, Ptr{PcfDims}), h, dims), "pcf_create")
+    (; dx, dy, dz, jac, met) = state.grid
+    (; pbar, rhobar, thetabar, n2) = state.atmosphere
+    # met[:, :, :, r, c] is a contiguous block of the 5-D column-major array
+    m13 = @view met[:, :, :, 1, 3]
+    m23 = @view met[:, :, :, 2, 3]
+    m33 = @view met[:, :, :, 3, 3]
+    GC.@preserve jac met begin
+        check(ccall((:pcf_set_grid, LIB), Cint,
+                    (Ptr{Cvoid}, Cdouble, Cdouble, Cdouble, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+                    h[], dx, dy, dz, jac, pointer(m13), pointer(m23), pointer(m33)), "pcf_set_grid")
+    end
+    GC.@preserve pbar rhobar thetabar n2 begin
+        check(ccall((:pcf_set_background, LIB), Cint,
+                    (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+                    h[], pbar, rhobar, thetabar, n2), "pcf_set_background")
+    end
+    HANDLES[state] = h[]
+    return h[]
+end
+
+"""
+    release!(state)
+
+Frees the device memory of the handle created for `state` (State is immutable,
+so this is explicit rather than a finalizer).
+"""
+function release!(state)
+    h = pop!(HANDLES, state, C_NULL)
+    h == C_NULL || ccall((:pcf_destroy, LIB), Cint, (Ptr{Cvoid},), h)
+    return nothing
+end
+
+function params(state)
+    (; tolerance, poisson_iterations, preconditioner, dtau, preconditioner_iterations,
+       tolerance_is_relative) = state.namelists.poisson
+    p = PcfParams(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
+    ccall((:pcf_params_default, LIB), Cint, (Ref{PcfParams},), p)
+    p.tolerance = tolerance
+    p.poisson_iterations = poisson_iterations
+    p.preconditioner = preconditioner
+    p.dtau = dtau
+    p.preconditioner_iterations = preconditioner_iterations
+    p.tolerance_is_relative = tolerance_is_relative
+    p.damp_horizontal_wind_on_rhs = state.namelists.sponge.damp_horizontal_wind_on_rhs
+    p.precision = PRECISION[SETTINGS[].precision]
+    return p
+end
+
+function solve_poisson_gpu!(state, dt::AbstractFloat, rayleigh_factor::AbstractFloat,
+                            tolref::AbstractFloat)
+    dt == 0.0 && error("Error in solve_poisson!: dt = 0.0!")
+    h = handle(state)
+    (; rhs) = state.poisson
+    (; rho, p) = state.variables.predictands
+    (; betar) = state.sponge
+    (; dpip) = state.variables.increments
+    pp = state.namelists.atmosphere.model == :Compressible ? p : C_NULL
+    prm = params(state)
+    res = PcfResult()
+    GC.@preserve rhs rho p betar dpip begin
+        rc = ccall((:pcf_solve, LIB), Cint,
+                   (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Cdouble, Cdouble,
+                    Cdouble, Ref{PcfParams}, Ptr{Cdouble}, Ref{PcfResult}),
+                   h, rhs, rho, betar, pp, dt, rayleigh_factor, tolref, prm, dpip, res)
+    end
+    check(rc, "pcf_solve")
+    return (res.errflag != 0, Int(res.niter))
+end
+
+"""
+    enable!(; precision = :fp64, device = 0)
+
+Make `PinCFlow.PoissonSolver.solve_poisson!` run on the GPU.  `precision = :mixed`
+selects the FP32-inner / FP64-refined solve (same FP64 tolerance).
+"""
+function enable!(; precision::Symbol = :fp64, device::Integer = 0)
+    SETTINGS[] = (precision = precision, device = device)
+    @eval PS function solve_poisson!(state::PinCFlow.State, dt::AbstractFloat,
+                                     rayleigh_factor::AbstractFloat, tolref::AbstractFloat)
+        return $(solve_poisson_gpu!)(state, dt, rayleigh_factor, tolref)
+    end
+    return nothing
+end
+
+end # module
