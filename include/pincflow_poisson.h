@@ -229,6 +229,21 @@ long long pcf_launch_count(const pcf_handle *h);
  * reference prints only the final value (apply_bicgstab!.jl:124-127).
  * Copies min(cap, *n) entries; *n receives the total count. */
 int pcf_residual_history(pcf_handle *h, double *out, int cap, int *n);
+
+/* Allocation-free global dot product.  No counterpart in the reference: it
+ * is the deterministic sum of pcf_global_dot for callers that cannot let the
+ * library allocate device memory -- a host model whose GPU memory belongs to
+ * its own pool allocator (such as Julia's CUDA.jl pool), or a time step being
+ * captured into a CUDA graph, where cudaMalloc/cudaFree are not allowed.
+ * a, b: device arrays of n doubles; *result: a device double, written
+ * asynchronously on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream).  No handle is needed and nothing is allocated: the scratch is a
+ * fixed 64 KB __device__ array that every GPU loading the library holds until
+ * the process exits.  n must not exceed 268,435,456 (PCF_ERANGE otherwise).
+ * The first call on a device looks up the scratch address; make that call
+ * before any stream capture.  All calls share the scratch, so calls that may
+ * overlap on the GPU (on different streams) race and must be serialised. */
+int pcf_global_dot_noalloc(const double *a, const double *b, long long n, double *result, void *stream);
 int pcf_profile_enable(pcf_handle *h, int on);  /* also clears the accumulators */
 int pcf_profile_read(const pcf_handle *h, int tag, double *ms, long long *count, double *bytes);
 
