@@ -106,7 +106,8 @@ struct ProfAcc {
     long long count;
     double bytes;
 };
-struct ProfState;  // defined in pcf_solver.cu
+struct ProfState;   // defined in pcf_solver.cu
+struct GraphCache;  // captured iteration batches, defined in pcf_solver.cu
 
 }  // namespace pcf
 
@@ -153,4 +154,6 @@ struct pcf_handle {
     int prof_iter;               // iteration index of the launches being issued
     pcf::ProfState *prof;
     pcf::ProfAcc prof_acc[PCF_PROF_NTAGS];
+    pcf::GraphCache *gcache;
+    long long graph_launches;    // kernels in the graph being replayed
 };

@@ -420,6 +420,59 @@ struct RunOut {
     double res, b_norm;
 };
 
+// A batch of BiCGSTAB iterations captured as a CUDA graph.  The kernels'
+// arguments are the handle's fixed buffers and the loop configuration, so one
+// graph per configuration serves every later solve on the handle.
+struct GraphKey {
+    int tsize, precond, pc_iters, flex, reliable, pi, batch;
+    double deta;
+    bool operator==(const GraphKey &o) const {
+        return tsize == o.tsize && precond == o.precond && pc_iters == o.pc_iters && flex == o.flex &&
+               reliable == o.reliable && pi == o.pi && batch == o.batch && deta == o.deta;
+    }
+};
+struct GraphEntry {
+    GraphKey key;
+    cudaGraphExec_t exec;
+    long long launches;
+};
+struct GraphCache {
+    std::vector<GraphEntry> entries;
+};
+
+template <typename T>
+static int batch_graph(pcf_handle *h, const Work<T> &w, const LoopCfg &c, const GraphKey &key,
+                       cudaGraphExec_t *out) {
+    if (!h->gcache) h->gcache = new GraphCache();
+    for (const GraphEntry &e : h->gcache->entries)
+        if (e.key == key) {
+            *out = e.exec;
+            h->graph_launches = e.launches;
+            return PCF_OK;
+        }
+    const long long l0 = h->launches;
+    PCF_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = PCF_OK;
+    for (int q = 0; q < key.batch && rc == PCF_OK; ++q) rc = bicgstab_iteration<T>(h, w, c);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(h->stream, &graph);
+    const long long nlaunch = h->launches - l0;
+    h->launches = l0;  // captured, not launched
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ec != cudaSuccess) return pcf_set_cuda_error(ec);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return pcf_set_cuda_error(ei);
+    h->gcache->entries.push_back({key, exec, nlaunch});
+    h->graph_launches = nlaunch;
+    *out = exec;
+    return PCF_OK;
+}
+
 // A complete BiCGSTAB run on A x = b (b in w.r on entry is not required: b
 // is the `b` argument), x0 = 0.  On convergence x <- M x as at
 // apply_bicgstab!.jl:132-135.  Result vector: *xout (x or a z buffer).
@@ -448,19 +501,56 @@ static int bicgstab_run(pcf_handle *h, const Work<T> &w, const T *b, double tol,
     k_init<T><<<vec_grid(h->d.n), 256, 0, h->stream>>>(b, w.x, w.r, w.r0, w.p, h->d.n, red(h, w.scal, FIN_INIT));
     PCF_CUDA_TRY(cudaGetLastError());
     if (check_interval < 1) check_interval = 16;
-    int launched = 0;
-    for (;;) {
-        const int nb = std::min(check_interval, maxit - launched);
-        for (int q = 0; q < nb; ++q) {
-            h->prof_iter = launched + q;
-            int rc = bicgstab_iteration<T>(h, w, c);
-            if (rc) return rc;
-        }
-        launched += nb;
-        PCF_CUDA_TRY(cudaMemcpyAsync(h->h_scal, w.scal, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, h->stream));
-        PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
-        if (h->h_scal->done || launched >= maxit) break;
+    // Iterations are issued in batches of check_interval; a batch is a CUDA
+    // graph (captured once per handle and loop configuration) unless per-launch
+    // profiling is on.  The status word of batch b is read back while batch
+    // b + 1 is already queued, so the GPU never drains between batches; the
+    // batch queued after convergence returns at once.
+    GraphKey key{(int)sizeof(T), c.precond, c.pc_iters, c.flex, c.reliable, w.post != nullptr, check_interval,
+                 c.deta};
+    cudaGraphExec_t gexec = nullptr;
+    if (!h->prof_on) {
+        int rc = batch_graph<T>(h, w, c, key, &gexec);
+        if (rc) return rc;
     }
+    int launched = 0, inflight = 0, slot = 0;
+    int done_seen = 0;
+    KrylovScalars last;
+    std::memset(&last, 0, sizeof(last));
+    while (!done_seen) {
+        if (launched < maxit) {
+            const int nb = std::min(check_interval, maxit - launched);
+            if (gexec && nb == check_interval) {
+                h->launches += h->graph_launches;
+                PCF_CUDA_TRY(cudaGraphLaunch(gexec, h->stream));
+            } else {
+                for (int q = 0; q < nb; ++q) {
+                    h->prof_iter = launched + q;
+                    int rc = bicgstab_iteration<T>(h, w, c);
+                    if (rc) return rc;
+                }
+            }
+            launched += nb;
+            PCF_CUDA_TRY(cudaMemcpyAsync(h->h_scal + slot, w.scal, sizeof(KrylovScalars), cudaMemcpyDeviceToHost,
+                                         h->stream));
+            PCF_CUDA_TRY(cudaEventRecord(h->ev[5 + slot], h->stream));
+            slot ^= 1;
+            inflight += 1;
+        }
+        if (inflight == 0) break;
+        // wait for the older of the (at most two) batches in flight
+        if (inflight == 2 || launched >= maxit) {
+            const int old = (inflight == 2) ? slot : slot ^ 1;
+            PCF_CUDA_TRY(cudaEventSynchronize(h->ev[5 + old]));
+            last = h->h_scal[old];
+            inflight -= 1;
+            if (last.done) done_seen = 1;
+            if (launched >= maxit && inflight == 0) break;
+        }
+    }
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    // the latest status (a batch issued after convergence leaves it unchanged)
+    PCF_CUDA_TRY(cudaMemcpy(h->h_scal, w.scal, sizeof(KrylovScalars), cudaMemcpyDeviceToHost));
     const KrylovScalars s = *h->h_scal;
     h->prof_iter = -1;
     prof_flush(h, s.iter);
@@ -587,6 +677,10 @@ int pcf_destroy(pcf_handle *h) {
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (h->h_scal) cudaFreeHost(h->h_scal);
+    if (h->gcache) {
+        for (const GraphEntry &e : h->gcache->entries) cudaGraphExecDestroy(e.exec);
+        delete h->gcache;
+    }
     if (h->prof) {
         for (cudaEvent_t e : h->prof->pool) cudaEventDestroy(e);
         delete h->prof;
@@ -662,7 +756,7 @@ int pcf_create(pcf_handle **out, const pcf_dims *dims) {
     if ((rc = dalloc(h, (void **)&h->scal32, sizeof(KrylovScalars)))) return fail(rc);
     if ((rc = dalloc(h, (void **)&h->dot_out, sizeof(double) * 4))) return fail(rc);
     if ((rc = dalloc(h, (void **)&h->hist, sizeof(double) * kHistCap))) return fail(rc);
-    if (cudaMallocHost((void **)&h->h_scal, sizeof(KrylovScalars)) != cudaSuccess) return fail(PCF_ENOMEM);
+    if (cudaMallocHost((void **)&h->h_scal, 2 * sizeof(KrylovScalars)) != cudaSuccess) return fail(PCF_ENOMEM);
     if (cudaMemsetAsync(h->ticket, 0, sizeof(unsigned int) * 4, h->stream) != cudaSuccess) return fail(PCF_ECUDA);
     // fields a caller may legitimately leave unset read as zero
     if (cudaMemsetAsync(h->thetabar, 0, nh8, h->stream) != cudaSuccess) return fail(PCF_ECUDA);
