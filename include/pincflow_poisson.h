@@ -230,6 +230,48 @@ long long pcf_launch_count(const pcf_handle *h);
  * Copies min(cap, *n) entries; *n receives the total count. */
 int pcf_residual_history(pcf_handle *h, double *out, int cap, int *n);
 
+/* Test entry point of the learned part's tensor-core GEMM (no reference
+ * counterpart): D[M][N] = sum_k A(m,k) B(n,k), BF16 inputs as uint16 bit
+ * patterns with A(m,k) = A[m*a_rs + k*a_ks] (one of the two strides 1), FP32
+ * output, optional split-K.  Host arrays, current device.  N <= 256. */
+int pcf_gemm_bf16(const unsigned short *A, long long a_len, long long a_rs, long long a_ks,
+                  const unsigned short *B, long long b_len, long long b_rs, long long b_ks, int M, int N, int K,
+                  int ksplit, float *D);
+
+/* ---- learned warm start / preconditioner (no reference counterpart) ------
+ * A per-column network: the column of a field is resampled to 64 levels,
+ * then h1 = relu(W1 x + b1), h1 += dwconv3x3(h1), h2 = relu(W2 h1 + b2),
+ * h2 += dwconv3x3(h2), y = W3 h2 + b3 (64 -> 256 -> 256 -> 64, depthwise 3x3
+ * horizontal convolutions, periodic), resampled back.  BF16 weights and
+ * activations, FP32 accumulation on the tensor cores; FP32 master weights
+ * trained with Adam on the residual-weighted loss sum (N(b) - x)^2 / sum x^2.
+ * Parameter order: W1[256][64], b1[256], K1[256][9], W2[256][256], b2[256],
+ * K2[256][9], W3[64][256], b3[64] (tap = (dj+1)*3 + (di+1)). */
+typedef struct pcf_net pcf_net;
+int pcf_net_num_params(void);
+int pcf_net_create(pcf_net **net, int device, long long max_columns, unsigned seed);
+int pcf_net_destroy(pcf_net *net);
+int pcf_net_get_params(pcf_net *net, float *params);
+int pcf_net_set_params(pcf_net *net, const float *params);
+int pcf_net_save(pcf_net *net, const char *path);
+int pcf_net_load(pcf_net *net, const char *path);
+/* out = N(in) for host arrays of nz*ny*nx doubles */
+int pcf_net_forward(pcf_net *net, const double *in, int nx, int ny, int nz, double *out);
+/* out = beta * out + scale_out * N(scale_in * in) on device fields (doubles if fp64, else
+ * floats), on `stream` (a cudaStream_t, NULL: the network's own stream) */
+int pcf_net_apply_device(pcf_net *net, const void *in, int nx, int ny, int nz, double scale_in,
+                         double scale_out, double beta, void *out, int fp64, void *stream);
+/* one step on device FP32 fields b, x (normalised): loss before the step, gradients
+ * (nullable host buffer), Adam update when lr > 0 */
+int pcf_net_train_step(pcf_net *net, const float *b, const float *x, int nx, int ny, int nz, double lr,
+                       double *loss, float *grad);
+/* loss and gradients for host arrays, no update (gradient check) */
+int pcf_net_gradients(pcf_net *net, const double *b, const double *x, int nx, int ny, int nz, double *loss,
+                      float *grad);
+/* Attach a trained network to a solver: with prm->learned = 1 the mixed-precision
+ * solve starts from x0 = RMS(b) N(b / RMS(b)) instead of 0.  NULL detaches. */
+int pcf_set_network(pcf_handle *h, pcf_net *net);
+
 /* Allocation-free global dot product.  No counterpart in the reference: it
  * is the deterministic sum of pcf_global_dot for callers that cannot let the
  * library allocate device memory -- a host model whose GPU memory belongs to

@@ -156,4 +156,5 @@ struct pcf_handle {
     pcf::ProfAcc prof_acc[PCF_PROF_NTAGS];
     pcf::GraphCache *gcache;
     long long graph_launches;    // kernels in the graph being replayed
+    pcf_net *net;                // learned warm start (not owned)
 };

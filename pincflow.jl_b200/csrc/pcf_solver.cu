@@ -1010,6 +1010,14 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
     if ((rc = true_residual(h, h->b64, h->x64, &rnorm))) return rc;
     const double b_norm = rnorm;
     res->b_norm = b_norm;
+    if (prm->learned && h->net && b_norm > 0 && std::isfinite(b_norm)) {
+        // learned warm start: x0 = RMS(b) N(b / RMS(b)), then the FP64 residual of x0
+        h->launches += 6;
+        rc = pcf_net_apply_device(h->net, h->b64, h->d.nx, h->d.ny, h->d.nz, 1.0 / b_norm, b_norm, 0.0, h->x64, 1,
+                                  h->stream);
+        if (rc) return rc;
+        if ((rc = true_residual(h, h->b64, h->x64, &rnorm))) return rc;
+    }
     res->niter = 0;
     res->nrefine = 0;
     res->status = PCF_OK;
@@ -1034,7 +1042,7 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
     LoopCfg cm = c;
     cm.flex = 1;
     cm.reliable = 1;
-    double rel = 1.0;
+    double rel = rnorm / b_norm;
     int restarts = 0;
     for (;;) {
         k_to_float<<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->w64, w.s, h->d.n, 1.0 / b_norm);
@@ -1196,6 +1204,12 @@ int pcf_bicgstab(pcf_handle *h, const double *rhs, double tolref, const pcf_para
 }
 
 long long pcf_launch_count(const pcf_handle *h) { return h ? h->launches : 0; }
+
+int pcf_set_network(pcf_handle *h, pcf_net *net) {
+    if (!h) return PCF_EINVAL;
+    h->net = net;
+    return PCF_OK;
+}
 
 int pcf_residual_history(pcf_handle *h, double *out, int cap, int *n) {
     if (!h || !n || (cap > 0 && !out)) return PCF_EINVAL;

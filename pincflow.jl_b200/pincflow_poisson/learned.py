@@ -1,0 +1,173 @@
+"""Learned warm start for the Poisson solve (no reference counterpart).
+
+The network (pcf_net in include/pincflow_poisson.h) maps the right-hand side
+b of the scaled Poisson system A s = b to an estimate of s, column by column
+(64 -> 256 -> 256 -> 64 with depthwise 3x3 horizontal convolutions between
+the layers).  It is trained on the GPU by the library's own forward,
+backward and Adam kernels, on (right-hand side, solution) pairs that the
+plain FP64 solver itself produces on the training configuration (random
+Gaussian-hill terrain, 128 x 128 x 64; pincflow_poisson.configs.c3).
+Attached to a solver (PoissonSolver.attach_network) it provides the initial
+guess of the mixed-precision solve when PoissonNamelist.learned is set; the
+FP64 true residual still decides convergence.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from . import configs as C
+from .solver import PoissonNamelist, PoissonSolver
+
+NPARAM = 103_488
+
+
+def _bind(lib):
+    if getattr(lib, "_net_bound", False):
+        return lib
+    P = ctypes.POINTER
+    vp, dp, fp = ctypes.c_void_p, P(ctypes.c_double), P(ctypes.c_float)
+    lib.pcf_net_num_params.restype = ctypes.c_int
+    lib.pcf_net_create.argtypes = [P(vp), ctypes.c_int, ctypes.c_longlong, ctypes.c_uint]
+    lib.pcf_net_destroy.argtypes = [vp]
+    lib.pcf_net_get_params.argtypes = [vp, fp]
+    lib.pcf_net_set_params.argtypes = [vp, fp]
+    lib.pcf_net_save.argtypes = [vp, ctypes.c_char_p]
+    lib.pcf_net_load.argtypes = [vp, ctypes.c_char_p]
+    lib.pcf_net_forward.argtypes = [vp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
+    lib.pcf_net_train_step.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                       dp, fp]
+    lib.pcf_net_gradients.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, fp]
+    lib.pcf_set_network.argtypes = [vp, vp]
+    for name in ("pcf_net_create", "pcf_net_destroy", "pcf_net_get_params", "pcf_net_set_params", "pcf_net_save",
+                 "pcf_net_load", "pcf_net_forward", "pcf_net_train_step", "pcf_net_gradients", "pcf_set_network"):
+        getattr(lib, name).restype = ctypes.c_int
+    lib._net_bound = True
+    return lib
+
+
+class LearnedNet:
+    """Owns one pcf_net on a device."""
+
+    def __init__(self, device: int = 0, max_columns: int = 512 * 512, seed: int = 0):
+        self.lib = _bind(_lib.load())
+        assert self.lib.pcf_net_num_params() == NPARAM
+        self._h = ctypes.c_void_p()
+        _lib.check(self.lib.pcf_net_create(ctypes.byref(self._h), device, max_columns, seed), "pcf_net_create")
+
+    def close(self):
+        if self._h:
+            self.lib.pcf_net_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(NPARAM, dtype=np.float32)
+        _lib.check(self.lib.pcf_net_get_params(self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+                   "pcf_net_get_params")
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == NPARAM
+        _lib.check(self.lib.pcf_net_set_params(self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+                   "pcf_net_set_params")
+
+    def save(self, path: str):
+        _lib.check(self.lib.pcf_net_save(self._h, path.encode()), "pcf_net_save")
+
+    def load(self, path: str):
+        _lib.check(self.lib.pcf_net_load(self._h, path.encode()), "pcf_net_load")
+
+    def forward(self, field: np.ndarray) -> np.ndarray:
+        """N(field) for a host array of shape (nz, ny, nx)."""
+        f = np.ascontiguousarray(field, dtype=np.float64)
+        nz, ny, nx = f.shape
+        out = np.zeros_like(f)
+        _lib.check(self.lib.pcf_net_forward(self._h, _lib.dptr(f), nx, ny, nz, _lib.dptr(out)), "pcf_net_forward")
+        return out
+
+    def gradients(self, b: np.ndarray, x: np.ndarray):
+        """(loss, gradient vector) for one sample, host arrays (nz, ny, nx)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        nz, ny, nx = b.shape
+        loss = ctypes.c_double()
+        g = np.zeros(NPARAM, dtype=np.float32)
+        _lib.check(self.lib.pcf_net_gradients(self._h, _lib.dptr(b), _lib.dptr(x), nx, ny, nz, ctypes.byref(loss),
+                                              g.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), "pcf_net_gradients")
+        return loss.value, g
+
+    def train_step(self, d_b: int, d_x: int, shape, lr: float) -> float:
+        """One Adam step on device FP32 fields (raw pointers), returns the loss."""
+        nz, ny, nx = shape
+        loss = ctypes.c_double()
+        _lib.check(self.lib.pcf_net_train_step(self._h, ctypes.c_void_p(d_b), ctypes.c_void_p(d_x), nx, ny, nz, lr,
+                                               ctypes.byref(loss), None), "pcf_net_train_step")
+        return loss.value
+
+
+def attach(solver: PoissonSolver, net: LearnedNet | None):
+    lib = _bind(_lib.load())
+    _lib.check(lib.pcf_set_network(solver._h, net.handle if net else None), "pcf_set_network")
+    solver._net = net
+
+
+def training_pairs(indices, nx=128, ny=128, nz=64, tolerance=1e-8, device=0):
+    """(b / RMS(b), s / RMS(b)) FP32 pairs from plain FP64 solves of the training
+    configuration (configs.c3 with seeds `indices`)."""
+    out = []
+    solver = None
+    for i in indices:
+        cfg = C.c3(int(i), nx=nx, ny=ny, nz=nz)
+        if solver is None:
+            solver = PoissonSolver(cfg["dom"], cfg["model"], device=device)
+        solver.set_grid(cfg["fields"])
+        solver.set_background(cfg["fields"])
+        solver.compute_operator(cfg["rho"], cfg["betar"], cfg["dt"], cfg["rayleigh_factor"], return_coef=False)
+        nl = PoissonNamelist(tolerance=tolerance, tolerance_is_relative=True, poisson_iterations=5000)
+        s, info = solver.apply_bicgstab(cfg["rhs"], 1.0, nl)
+        if info.errflag:
+            continue
+        rms = float(np.sqrt(np.mean(cfg["rhs"] ** 2)))
+        out.append(((cfg["rhs"] / rms).astype(np.float32), (s / rms).astype(np.float32)))
+    if solver is not None:
+        solver.close()
+    return out
+
+
+def train(net: LearnedNet, pairs, epochs: int = 4, lr: float = 1e-3, device: int = 0, log=None):
+    """Adam over the pairs (one sample per step), on device.  Returns the
+    per-step losses."""
+    import torch
+    dev = torch.device("cuda", device)
+    data = [(torch.from_numpy(b).to(dev), torch.from_numpy(x).to(dev)) for b, x in pairs]
+    torch.cuda.synchronize()
+    losses = []
+    t0 = time.time()
+    for ep in range(epochs):
+        order = np.random.default_rng(ep).permutation(len(data))
+        for k in order:
+            b, x = data[k]
+            losses.append(net.train_step(b.data_ptr(), x.data_ptr(), tuple(b.shape), lr))
+        if log:
+            log(f"epoch {ep}: mean loss {np.mean(losses[-len(data):]):.4f} ({time.time() - t0:.1f} s)")
+    return losses

@@ -127,6 +127,12 @@ class PoissonSolver:
     def profile(self, on: bool = True):
         _lib.check(self.lib.pcf_profile_enable(self._h, int(bool(on))), "pcf_profile_enable")
 
+    def attach_network(self, net):
+        """Use a trained LearnedNet as the warm start of mixed-precision solves
+        with PoissonNamelist(learned=True); None detaches."""
+        from .learned import attach
+        attach(self, net)
+
     def residual_history(self) -> np.ndarray:
         """Relative recursive residual after each iteration of the last solve."""
         n = ctypes.c_int()

@@ -214,3 +214,24 @@ def test_c2_fixture_is_converged():
     with open(os.path.join(HERE, "golden", "c2_fp64_oracle.json")) as fh:
         d = json.load(fh)
     assert not d["errflag"] and d["true_residual"] <= 1e-10 and 300 < d["niter"] < 700
+
+
+def test_network_oracle_gradient_matches_finite_differences():
+    """Pins the network oracle: its analytic gradient (exact float64 network)
+    against central differences along random directions."""
+    from oracle import net_oracle as NO
+    rng = np.random.default_rng(0)
+    d = {}
+    for name, shape in NO.SIZES:
+        d[name] = rng.standard_normal(shape) * (0.2 if name.startswith("W") else 0.05)
+    p = NO.pack(d)
+    b = rng.standard_normal((64, 4, 5))
+    x = rng.standard_normal((64, 4, 5))
+    _, g = NO.loss_and_grad(p, b, x, bf=False)
+    for k in range(3):
+        v = rng.standard_normal(p.size)
+        eps = 1e-6
+        lp, _ = NO.loss_and_grad(p + eps * v, b, x, bf=False)
+        lm, _ = NO.loss_and_grad(p - eps * v, b, x, bf=False)
+        fd = (lp - lm) / (2 * eps)
+        assert abs(fd - g @ v) <= 1e-5 * max(1.0, abs(fd)), (fd, g @ v)
