@@ -2,7 +2,7 @@
 Poisson solve (PinCFlow.jl PoissonSolver) on B200.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config c2|c5|c1] [--method mixed|fp64]
+                  [--config c2|c5|c1] [--method mg|mixed|fp64]
 
 A step is one complete solve_poisson! (operator assembly, preconditioned
 BiCGSTAB to FP64 true relative residual 1e-10, unscaling into dpip) of the
@@ -44,6 +44,15 @@ WORKLOADS = {
           "isothermal 250 K, RHS N(0,1) seed 12345",
     "c5": "512x512x192 pseudo-incompressible, 20 Gaussian ridges <= 2 km, wave-packet RHS",
     "c1": "periodic hill 40x1x40 Boussinesq (one of its 200 solves)",
+}
+
+
+METHODS = {
+    "mg": "flexible FP32 BiCGSTAB inside FP64 iterative refinement (reliable updates on the FP64 true residual), "
+          "preconditioned by a horizontal aggregation multigrid V-cycle whose smoother is the reference "
+          "line relaxation",
+    "mixed": "flexible FP32 BiCGSTAB inside FP64 iterative refinement, reference preconditioner",
+    "fp64": "plain FP64 BiCGSTAB, reference preconditioner",
 }
 
 
@@ -222,7 +231,8 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
 
     nl_fast = pcf.PoissonNamelist(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000,
-                                  precision=args.method, residual="true")
+                                  precision="fp64" if args.method == "fp64" else "mixed", residual="true",
+                                  multigrid=args.method == "mg", mg_dtau=args.mg_dtau)
     nl_plain = pcf.PoissonNamelist(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000,
                                    precision="fp64", residual="true")
 
@@ -306,7 +316,8 @@ def run_ours(args, rank, world, local_rank):
 
     # --- roofline of the dominant kernel (FP32 Total apply) ---------------
     peak, peak_kind = load_peaks()
-    a32 = prof["apply32"] if args.method == "mixed" else prof["apply64"]
+    f32 = args.method != "fp64"
+    a32 = prof["apply32"] if f32 else prof["apply64"]
     kernel_ms = a32["ms"] / max(a32["count"], 1)
     bytes_per_launch = a32["bytes"] / max(a32["count"], 1)
     achieved = bytes_per_launch / (kernel_ms * 1e-3) / 1e9 if kernel_ms > 0 else 0.0
@@ -320,10 +331,9 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+f64" if args.method == "mixed" else "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32+f64" if f32 else "f64", "data": "synthetic",
         "config": {"workload": f"{args.config}: {WORKLOADS[args.config]}",
-                   "method": ("FP32 BiCGSTAB sweeps inside FP64 iterative refinement, reference preconditioner"
-                              if args.method == "mixed" else "plain FP64 BiCGSTAB"),
+                   "method": METHODS[args.method],
                    "convergence": "FP64 true residual RMS(b-Ax)/RMS(b) <= 1e-10",
                    "l2": "inputs larger than L2 (operator 3.4 GB FP64 + 0.8 GB FP32), no flush",
                    "parallelism": f"replicas x{world}"},
@@ -335,7 +345,7 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": launches,
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "wall_s": statistics.mean(e2e_wall)},
-        "roofline": {"bound": "hbm", "kernel": "k_stencil Total apply FP32 (fused dot)" if args.method == "mixed"
+        "roofline": {"bound": "hbm", "kernel": "k_stencil Total apply FP32 (fused dot / residual)" if f32
                      else "k_stencil Total apply FP64", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": ncu_traffic(args.config),
                      "algorithmic_bytes_per_launch": bytes_per_launch, "ms_per_launch": kernel_ms},
@@ -365,7 +375,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--size", default=None, help="c2 only: NXxNYxNZ instead of 256x256x128 (profiling captures)")
-    ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--method", default="mg", choices=sorted(METHODS))
+    ap.add_argument("--mg-dtau", type=float, default=2.0)
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--ref-sample-iters", type=int, default=3)
     ap.add_argument("--ref-iterations", type=int, default=450)

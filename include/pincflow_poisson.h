@@ -122,6 +122,11 @@ typedef struct {
     int learned;                   /* 0: off; 1: learned warm start + flexible BiCGSTAB */
     int check_interval;            /* iterations between host checks of the status word (16) */
     int restart_interval;          /* mixed: restart the Krylov recurrences at every n-th reliable update (1; 0: never) */
+    int multigrid;                 /* mixed: 0: the reference preconditioner; 1: horizontal aggregation multigrid
+                                      V-cycle with the reference line relaxation as smoother on every level (0) */
+    double mg_dtau;                /* multigrid: pseudo-time step of the smoother, all levels (1.0) */
+    int mg_coarse_iterations;      /* multigrid: smoothing steps on the coarsest level (4) */
+    int mg_min_columns;            /* multigrid: a level with at most this many columns is the coarsest (16) */
 } pcf_params;
 
 typedef struct {
@@ -193,6 +198,18 @@ int pcf_apply_operator(pcf_handle *h, const double *sin_, double *ls, int mode, 
 int pcf_apply_preconditioner(pcf_handle *h, const double *sin_, double *sout,
                              const pcf_params *prm, int precision);
 
+/* Horizontal aggregation multigrid preconditioner of the mixed solve (no
+ * reference counterpart; it wraps the reference line relaxation of
+ * apply_preconditioner!.jl:40-124 as the smoother of every level).
+ * pcf_multigrid_levels builds the hierarchy for the current operator with
+ * prm's mg_* settings and returns the level count and (nx, ny, nz) per level
+ * (up to cap levels); pcf_multigrid_operator copies the 25 planes of a level
+ * (level 0: the assembled FP64 operator); pcf_apply_multigrid applies one
+ * V-cycle z = MG(sin) in FP32 (host FP64 arrays, nx*ny*nz). */
+int pcf_multigrid_levels(pcf_handle *h, const pcf_params *prm, int cap, int *nlevels, int *dims);
+int pcf_multigrid_operator(pcf_handle *h, int level, double *coef);
+int pcf_apply_multigrid(pcf_handle *h, const double *sin, double *sout, const pcf_params *prm);
+
 /* apply_bicgstab!: solves A s = rhs with the handle's current operator;
  * interior arrays. */
 int pcf_bicgstab(pcf_handle *h, const double *rhs, double tolref, const pcf_params *prm,
@@ -221,7 +238,8 @@ enum pcf_prof_tag {
     PCF_PROF_UPDATE64 = 7,
     PCF_PROF_ASSEMBLE = 8,  /* operator assembly + factors */
     PCF_PROF_RELIABLE = 9,  /* FP64 true-residual applies of reliable updates (mostly skipped launches) */
-    PCF_PROF_NTAGS = 10
+    PCF_PROF_MG = 10,       /* multigrid coarse levels and grid transfers, FP32 */
+    PCF_PROF_NTAGS = 11
 };
 long long pcf_launch_count(const pcf_handle *h);
 /* Relative recursive residual after each BiCGSTAB iteration of the last

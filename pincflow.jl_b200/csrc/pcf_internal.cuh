@@ -108,6 +108,7 @@ struct ProfAcc {
 };
 struct ProfState;   // defined in pcf_solver.cu
 struct GraphCache;  // captured iteration batches, defined in pcf_solver.cu
+struct MgState;     // multigrid hierarchy, defined in pcf_solver.cu
 
 }  // namespace pcf
 
@@ -157,4 +158,6 @@ struct pcf_handle {
     pcf::GraphCache *gcache;
     long long graph_launches;    // kernels in the graph being replayed
     pcf_net *net;                // learned warm start (not owned)
+    pcf::MgState *mg;            // multigrid hierarchy (allocated on first use)
+    long long op_version;        // incremented whenever the operator changes
 };

@@ -279,7 +279,8 @@ enum Epi : int {
     EPI_DOT1 = 1,     // out = A s;  sum out*w1                      (<v, r0>)
     EPI_DOT2 = 2,     // out = A s;  sum out*w1, sum out*out         (<t, s>, <t, t>)
     EPI_PSEUDO = 3,   // out = s + d_eta (L_h s - b)                 (pseudo-time step)
-    EPI_RESID = 4     // out = b - A s;  sum out*out                 (true residual)
+    EPI_RESID = 4,    // out = b - A s;  sum out*out                 (true residual)
+    EPI_RESNR = 5     // out = b - A s                               (multigrid residual)
 };
 
 template <typename T>
@@ -409,7 +410,7 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
             // (measured 4.18 -> 4.50 TB/s); the dot-product operand is loaded after
             // the sum, which keeps those variants at 140 registers (5.31 vs 5.06 TB/s)
             T wv[V];
-            if (EPI == EPI_PSEUDO || EPI == EPI_RESID) load_vec<T, V>(a.w1 + base, wv);
+            if (EPI == EPI_PSEUDO || EPI == EPI_RESID || EPI == EPI_RESNR) load_vec<T, V>(a.w1 + base, wv);
             const T *sm2 = sm[(k + 10) % R::NS], *sm1 = sm[(k + 11) % R::NS], *s0 = sm[(k + 12) % R::NS],
                     *sp1 = sm[(k + 13) % R::NS], *sp2 = sm[(k + 14) % R::NS];
             T res[V];
@@ -501,6 +502,10 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
                     res[e] = wv[e] - res[e];
                     d0 += (double)res[e] * (double)res[e];
                 }
+                store_vec<T, V>(a.out + base, res);
+            } else if (EPI == EPI_RESNR) {
+#pragma unroll
+                for (int e = 0; e < V; ++e) res[e] = wv[e] - res[e];
                 store_vec<T, V>(a.out + base, res);
             }
         }

@@ -1,0 +1,281 @@
+// pcf_mg.cuh -- device kernels of the horizontal aggregation multigrid
+// preconditioner of the mixed-precision solve (no reference counterpart; the
+// reference preconditioner, apply_preconditioner!.jl:40-124, is its smoother).
+//
+// Hierarchy.  Level l+1 aggregates cx x cy columns of level l (cx, cy in
+// {1, 2}); levels keep every vertical level, so each column stays a line of
+// the smoother's tridiagonal solves.  With piecewise-constant prolongation
+// the Galerkin product of the 25-point operator has the same 25 offsets
+// (no xy diagonals arise), so every level runs the same stencil and Thomas
+// kernels as the finest one.
+//
+// Coarse operator.  The assembled operator is symmetrically scaled,
+// A = F^-1 A0 F^-1 with F = diag(fcscal) and A0 the unscaled operator whose
+// rows sum to (about) zero.  Level l+1 is
+//     A_c = Fc^-1 [ (1 / (cx cy)) R A0_l P ]_h Fc^-1,
+// R = P^T the aggregate sum, Fc the RMS of fcscal over an aggregate, and
+// [.]_h scales every coupling that crosses an aggregate boundary in x by
+// 1/cx (in y by 1/cy), moving the removed weight to the (0, 0, dz) entry of
+// the same row so that row sums, and with them the null space, are kept.
+// The 1/cx factor turns the Galerkin face couplings (cy fine faces per
+// coarse face) into those of a re-discretisation on the coarse grid, which
+// the pseudo-time smoother is tuned for.  Restriction and prolongation act
+// on fcscal-weighted values: b_c = sum(f r) / (cx cy f_c), s += f_c e / f.
+#pragma once
+
+#include "pcf_kernels.cuh"
+
+namespace pcf {
+
+// index of offset (dx, dy, dz) in the Tensor order of enum pcf_coef
+__host__ __device__ constexpr int coef_index(int dx, int dy, int dz) {
+    return dz == 0   ? (dx == -1 ? PCF_AL : dx == 1 ? PCF_AR : dy == -1 ? PCF_AB : dy == 1 ? PCF_AF : PCF_AC)
+           : dz == -1 ? (dx == -1 ? PCF_ALD : dx == 1 ? PCF_ARD : dy == -1 ? PCF_ABD : dy == 1 ? PCF_AFD : PCF_AD)
+           : dz == 1  ? (dx == -1 ? PCF_ALU : dx == 1 ? PCF_ARU : dy == -1 ? PCF_ABU : dy == 1 ? PCF_AFU : PCF_AU)
+           : dz == -2 ? (dx == -1 ? PCF_ALDD : dx == 1 ? PCF_ARDD : dy == -1 ? PCF_ABDD : dy == 1 ? PCF_AFDD : PCF_ADD)
+                      : (dx == -1 ? PCF_ALUU : dx == 1 ? PCF_ARUU : dy == -1 ? PCF_ABUU : dy == 1 ? PCF_AFUU : PCF_AUU);
+}
+
+__host__ __device__ constexpr int off_x(int p) {
+    return (p == PCF_AL || p == PCF_ALD || p == PCF_ALU || p == PCF_ALDD || p == PCF_ALUU)   ? -1
+           : (p == PCF_AR || p == PCF_ARD || p == PCF_ARU || p == PCF_ARDD || p == PCF_ARUU) ? 1
+                                                                                               : 0;
+}
+__host__ __device__ constexpr int off_y(int p) {
+    return (p == PCF_AB || p == PCF_ABD || p == PCF_ABU || p == PCF_ABDD || p == PCF_ABUU)   ? -1
+           : (p == PCF_AF || p == PCF_AFD || p == PCF_AFU || p == PCF_AFDD || p == PCF_AFUU) ? 1
+                                                                                               : 0;
+}
+__host__ __device__ constexpr int off_z(int p) {
+    return (p == PCF_AD || p == PCF_ALD || p == PCF_ARD || p == PCF_ABD || p == PCF_AFD)       ? -1
+           : (p == PCF_AU || p == PCF_ALU || p == PCF_ARU || p == PCF_ABU || p == PCF_AFU)     ? 1
+           : (p == PCF_ADD || p == PCF_ALDD || p == PCF_ARDD || p == PCF_ABDD || p == PCF_AFDD) ? -2
+           : (p == PCF_AUU || p == PCF_ALUU || p == PCF_ARUU || p == PCF_ABUU || p == PCF_AFUU) ? 2
+                                                                                                 : 0;
+}
+
+// floor((a + d) / c) for c in {1, 2} and a + d in [-1, 2]
+__host__ __device__ constexpr int agg_off(int a, int d, int c) { return c == 1 ? d : (a + d < 0 ? -1 : (a + d) / 2); }
+
+// fc_c = sqrt(mean over the aggregate of fc^2)
+template <typename TF, int CX, int CY>
+__global__ void __launch_bounds__(256) k_mg_fc(const TF *__restrict__ fc, int nx, int ny, int nz,
+                                                float *__restrict__ fcc) {
+    const int NX = nx / CX, NY = ny / CY;
+    const long long nc = (long long)NX * NY * nz;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nc; q += (long long)gridDim.x * blockDim.x) {
+        const int I = (int)(q % NX), J = (int)((q / NX) % NY), k = (int)(q / ((long long)NX * NY));
+        double acc = 0.0;
+#pragma unroll
+        for (int b = 0; b < CY; ++b)
+#pragma unroll
+            for (int a = 0; a < CX; ++a) {
+                const double f = (double)fc[(CX * I + a) + (long long)nx * ((CY * J + b) + (long long)ny * k)];
+                acc += f * f;
+            }
+        fcc[q] = (float)sqrt(acc / (CX * CY));
+    }
+}
+
+// Coarse operator of level l+1 from level l (see the file header).  One
+// thread per coarse cell; TI is the type of the finer level's planes and
+// fcscal (double on the finest level, float below).
+template <typename TI, int CX, int CY>
+__global__ void __launch_bounds__(128) k_mg_coarsen(const TI *__restrict__ coef, const TI *__restrict__ fc, int nx,
+                                                    int ny, int nz, const float *__restrict__ fcc,
+                                                    float *__restrict__ out) {
+    const int NX = nx / CX, NY = ny / CY;
+    const long long n = (long long)nx * ny * nz, nc = (long long)NX * NY * nz;
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nc) return;
+    const int I = (int)(q % NX), J = (int)((q / NX) % NY), k = (int)(q / ((long long)NX * NY));
+    double acc[PCF_NCOEF];
+#pragma unroll
+    for (int p = 0; p < PCF_NCOEF; ++p) acc[p] = 0.0;
+#pragma unroll
+    for (int b = 0; b < CY; ++b)
+#pragma unroll
+        for (int a = 0; a < CX; ++a) {
+            const int i = CX * I + a, j = CY * J + b;
+            const long long c = i + (long long)nx * (j + (long long)ny * k);
+            const double fcv = (double)fc[c];
+#pragma unroll
+            for (int p = 0; p < PCF_NCOEF; ++p) {
+                const int dz = off_z(p);
+                if (k + dz < 0 || k + dz >= nz) continue;  // multiplies a zero z-ghost
+                const int dx = off_x(p), dy = off_y(p);
+                const long long t = wrap(i + dx, nx) + (long long)nx * (wrap(j + dy, ny) + (long long)ny * (k + dz));
+                const double a0 = fcv * (double)coef[(long long)p * n + c] * (double)fc[t];
+                acc[coef_index(agg_off(a, dx, CX), agg_off(b, dy, CY), dz)] += a0;
+            }
+        }
+    // re-discretisation scaling of the couplings across aggregate faces
+#pragma unroll
+    for (int p = 0; p < PCF_NCOEF; ++p) {
+        const int dx = off_x(p), dy = off_y(p);
+        if (dx == 0 && dy == 0) continue;
+        const double keep = dx != 0 ? 1.0 / CX : 1.0 / CY;
+        const double moved = (1.0 - keep) * acc[p];
+        acc[p] -= moved;
+        acc[coef_index(0, 0, off_z(p))] += moved;
+    }
+    const double fcI = (double)fcc[q];
+#pragma unroll
+    for (int p = 0; p < PCF_NCOEF; ++p) {
+        const int dz = off_z(p);
+        double v = 0.0;
+        if (k + dz >= 0 && k + dz < nz) {
+            const long long t = wrap(I + off_x(p), NX) + (long long)NX * (wrap(J + off_y(p), NY) + (long long)NY * (k + dz));
+            v = acc[p] / ((double)(CX * CY) * fcI * (double)fcc[t]);
+        }
+        out[(long long)p * nc + q] = (float)v;
+    }
+}
+
+// Thomas pivots P, M, Q of a level (as k_factors, from FP32 planes).
+__global__ void __launch_bounds__(128) k_mg_factors(int plane, int nz, long long n, double deta,
+                                                    const float *__restrict__ coef, float *__restrict__ fac) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= plane) return;
+    const float *ac = coef + (long long)PCF_AC * n, *ad = coef + (long long)PCF_AD * n,
+                *au = coef + (long long)PCF_AU * n;
+    double qprev = 0.0;
+    for (int k = 0; k < nz; ++k) {
+        const long long o = col + (long long)plane * k;
+        const double piv = k == 0 ? 1.0 / (1.0 - deta * ac[o]) : 1.0 / (1.0 - deta * ac[o] - deta * ad[o] * qprev);
+        const double m = k == 0 ? 0.0 : deta * ad[o] * piv;
+        const double qv = deta * au[o] * piv;
+        fac[o] = (float)piv;
+        fac[n + o] = (float)m;
+        fac[2 * n + o] = (float)qv;
+        qprev = qv;
+    }
+}
+
+// b_c = sum over the aggregate of (f r) / (cx cy f_c)
+template <typename TF, int CX, int CY>
+__global__ void __launch_bounds__(256) k_mg_restrict(const float *__restrict__ r, const TF *__restrict__ fc, int nx,
+                                                      int ny, int nz, const float *__restrict__ fcc,
+                                                      float *__restrict__ bc, const KrylovScalars *guard) {
+    if (krylov_done(guard)) return;
+    const int NX = nx / CX, NY = ny / CY;
+    const long long nc = (long long)NX * NY * nz;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nc; q += (long long)gridDim.x * blockDim.x) {
+        const int I = (int)(q % NX), J = (int)((q / NX) % NY), k = (int)(q / ((long long)NX * NY));
+        float acc = 0.0f;
+#pragma unroll
+        for (int b = 0; b < CY; ++b)
+#pragma unroll
+            for (int a = 0; a < CX; ++a) {
+                const long long c = (CX * I + a) + (long long)nx * ((CY * J + b) + (long long)ny * k);
+                acc += (float)fc[c] * r[c];
+            }
+        bc[q] = acc / ((float)(CX * CY) * fcc[q]);
+    }
+}
+
+// s += f_c e / f (piecewise-constant prolongation of the coarse correction)
+template <typename TF, int CX, int CY>
+__global__ void __launch_bounds__(256) k_mg_prolong(const float *__restrict__ e, const float *__restrict__ fcc,
+                                                     const TF *__restrict__ fc, int nx, int ny, int nz, float *s,
+                                                     const KrylovScalars *guard) {
+    if (krylov_done(guard)) return;
+    const int NX = nx / CX, NY = ny / CY;
+    const long long n = (long long)nx * ny * nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+        const long long q = i / CX + (long long)NX * (j / CY + (long long)NY * k);
+        s[c] += fcc[q] * e[q] / (float)fc[c];
+    }
+}
+
+// The smoother's column solve on the coarse levels, one warp per column.
+// Both sweeps are first-order linear recurrences (y_k = rhs_k P_k + M_k y_k-1
+// up, x_k = y_k + Q_k x_k+1 down), so each lane composes the affine maps of
+// its own run of levels and a warp scan of the composites gives every run its
+// entry value: the column costs a few dependent steps instead of nz, which
+// is what matters on levels with few columns.  MODE is TH_B (rhs = -deta b)
+// or TH_T (rhs = t, in place allowed).  nz <= 32 * kLevelsPerLane.
+constexpr int kLevelsPerLane = 8;
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_thomas_warp(ThomasArgs<float> a) {
+    if (krylov_done(a.scal)) return;
+    const int col = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (col >= a.plane) return;  // uniform per warp
+    const float *P = a.fac, *M = a.fac + a.n, *Q = a.fac + 2 * a.n;
+    const long long pl = a.plane;
+    const int per = (a.nz + 31) >> 5;
+    const int kb = lane * per;
+    const float deta = (float)a.deta;
+    float rhs[kLevelsPerLane], mm[kLevelsPerLane], qq[kLevelsPerLane];
+    // forward: affine composite (A, B) of the lane's levels, y_out = A + B y_in
+    float A = 0.0f, B = 1.0f;
+#pragma unroll
+    for (int q = 0; q < kLevelsPerLane; ++q) {
+        const int k = kb + q;
+        if (q < per && k < a.nz) {
+            const long long o = col + pl * k;
+            const float in = a.in[o];
+            const float p = __ldg(P + o);
+            mm[q] = __ldg(M + o);
+            qq[q] = __ldg(Q + o);
+            rhs[q] = (MODE == TH_B ? -deta * in : in) * p;
+            A = fmaf(mm[q], A, rhs[q]);
+            B = mm[q] * B;
+        }
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const float Ao = __shfl_up_sync(0xffffffffu, A, o), Bo = __shfl_up_sync(0xffffffffu, B, o);
+        if (lane >= o) {
+            A = fmaf(B, Ao, A);
+            B = B * Bo;
+        }
+    }
+    float y = __shfl_up_sync(0xffffffffu, A, 1);
+    if (lane == 0) y = 0.0f;
+    float yv[kLevelsPerLane];
+#pragma unroll
+    for (int q = 0; q < kLevelsPerLane; ++q) {
+        const int k = kb + q;
+        if (q < per && k < a.nz) {
+            y = fmaf(mm[q], y, rhs[q]);
+            yv[q] = y;
+        }
+    }
+    // backward: x_k = y_k + Q_k x_k+1 with x_nz = 0; composite over the lane's
+    // levels from the top down, then a suffix scan across lanes
+    float C = 0.0f, D = 1.0f;  // x_kb = C + D x_(kb+per)
+#pragma unroll
+    for (int q = kLevelsPerLane - 1; q >= 0; --q) {
+        const int k = kb + q;
+        if (q < per && k < a.nz) {
+            const float qk = (k == a.nz - 1) ? 0.0f : qq[q];
+            C = fmaf(qk, C, yv[q]);
+            D = qk * D;
+        }
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const float Co = __shfl_down_sync(0xffffffffu, C, o), Do = __shfl_down_sync(0xffffffffu, D, o);
+        if (lane + o < 32) {
+            C = fmaf(D, Co, C);
+            D = D * Do;
+        }
+    }
+    float x = __shfl_down_sync(0xffffffffu, C, 1);
+    if (lane == 31) x = 0.0f;
+#pragma unroll
+    for (int q = kLevelsPerLane - 1; q >= 0; --q) {
+        const int k = kb + q;
+        if (q < per && k < a.nz) {
+            const float qk = (k == a.nz - 1) ? 0.0f : qq[q];
+            x = fmaf(qk, x, yv[q]);
+            a.out[col + pl * k] = x;
+        }
+    }
+}
+
+}  // namespace pcf

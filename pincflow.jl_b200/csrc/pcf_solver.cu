@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "pcf_kernels.cuh"
+#include "pcf_mg.cuh"
 
 namespace {
 thread_local cudaError_t g_last_cuda = cudaSuccess;
@@ -116,21 +117,23 @@ static ReduceCtx red(pcf_handle *h, KrylovScalars *scal, int op, double *out = n
     return c;
 }
 
-// Levels per block: enough z-chunks for ~8 blocks per SM, at least 8 levels
-// per chunk (each chunk re-reads 4 halo planes), at most kMaxPartials blocks.
+// Levels per block: enough z-chunks for ~8 blocks per SM, at most
+// kMaxPartials blocks.  Each chunk re-reads 4 halo planes of s, so chunks
+// are kept at 4 levels or more (only grids too small to fill the GPU, such
+// as coarse multigrid levels, get that short).
 static int pick_kc(long long xyblocks, int nz) {
     const long long want = 8LL * num_sms();
     long long chunks = (want + xyblocks - 1) / xyblocks;
     if (chunks < 1) chunks = 1;
     long long kc = (nz + chunks - 1) / chunks;
-    if (kc < 8) kc = 8;
+    if (kc < 4) kc = 4;
     if (kc > nz) kc = nz;
     while (kc < nz && xyblocks * ((nz + kc - 1) / kc) > kMaxPartials) kc = std::min<long long>(2 * kc, nz);
     return (int)kc;
 }
 
 template <typename T, int V, int TX, bool HORIZ, int EPI, bool DIFF>
-static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a) {
+static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_override) {
     constexpr int TY = 128 / TX;
     constexpr int W = TX * V;
     const long long gx = (a.nx + W - 1) / W, gy = (a.ny + TY - 1) / TY;
@@ -141,30 +144,37 @@ static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a) {
     const dim3 block(TX, TY, 1);
     // algorithmic words per cell: coefficient planes + input + output (+ second operand)
     const int words = (HORIZ ? 22 : 25) + 2 + (EPI == EPI_STORE ? 0 : 1);
-    const int tag = a.guard_update ? PCF_PROF_RELIABLE
-                    : HORIZ        ? (sizeof(T) == 4 ? PCF_PROF_PSEUDO32 : PCF_PROF_PSEUDO64)
-                                   : (sizeof(T) == 4 ? PCF_PROF_APPLY32 : PCF_PROF_APPLY64);
+    const int tag = tag_override >= 0 ? tag_override
+                    : a.guard_update ? PCF_PROF_RELIABLE
+                    : HORIZ          ? (sizeof(T) == 4 ? PCF_PROF_PSEUDO32 : PCF_PROF_PSEUDO64)
+                                     : (sizeof(T) == 4 ? PCF_PROF_APPLY32 : PCF_PROF_APPLY64);
     ProfScope ps(h, tag, (double)words * sizeof(T) * (double)a.n);
     k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF><<<grid, block, 0, h->stream>>>(a, kc);
     PCF_CUDA_TRY(cudaGetLastError());
     return PCF_OK;
 }
 
+// Stencil apply on a grid of dimensions d (the handle's grid or a multigrid level).
 template <typename T, bool HORIZ, int EPI, bool DIFF = false>
-static int launch_stencil(pcf_handle *h, StencilArgs<T> a) {
-    a.nx = h->d.nx;
-    a.ny = h->d.ny;
-    a.nz = h->d.nz;
-    a.n = h->d.n;
+static int launch_stencil_dims(pcf_handle *h, StencilArgs<T> a, const Dims &d, int tag = -1) {
+    a.nx = d.nx;
+    a.ny = d.ny;
+    a.nz = d.nz;
+    a.n = d.n;
     constexpr int VMAX = sizeof(T) == 4 ? 4 : 2;
     const bool vec = (a.nx % VMAX) == 0;
     const int wide = vec ? 32 * VMAX : 32;
     if (a.nx >= wide) {
-        if (vec) return launch_stencil_cfg<T, VMAX, 32, HORIZ, EPI, DIFF>(h, a);
-        return launch_stencil_cfg<T, 1, 32, HORIZ, EPI, DIFF>(h, a);
+        if (vec) return launch_stencil_cfg<T, VMAX, 32, HORIZ, EPI, DIFF>(h, a, tag);
+        return launch_stencil_cfg<T, 1, 32, HORIZ, EPI, DIFF>(h, a, tag);
     }
-    if (vec) return launch_stencil_cfg<T, VMAX, 8, HORIZ, EPI, DIFF>(h, a);
-    return launch_stencil_cfg<T, 1, 8, HORIZ, EPI, DIFF>(h, a);
+    if (vec) return launch_stencil_cfg<T, VMAX, 8, HORIZ, EPI, DIFF>(h, a, tag);
+    return launch_stencil_cfg<T, 1, 8, HORIZ, EPI, DIFF>(h, a, tag);
+}
+
+template <typename T, bool HORIZ, int EPI, bool DIFF = false>
+static int launch_stencil(pcf_handle *h, StencilArgs<T> a) {
+    return launch_stencil_dims<T, HORIZ, EPI, DIFF>(h, a, h->d);
 }
 
 // Total apply of the Krylov loop: plain form, or the FP32 difference form.
@@ -177,11 +187,12 @@ static int apply_total(pcf_handle *h, const StencilArgs<T> &a, bool diff) {
 }
 
 template <typename T, int MODE>
-static int launch_thomas(pcf_handle *h, const ThomasArgs<T> &a) {
+static int launch_thomas(pcf_handle *h, const ThomasArgs<T> &a, int tag = -1) {
     const int bs = 128;
     // input forming + P, M (forward) + y write, y read, Q, solution write
     const int words = (MODE == TH_B || MODE == TH_T ? 1 : (MODE == TH_SUPD ? 3 : 4)) + 6;
-    ProfScope ps(h, sizeof(T) == 4 ? PCF_PROF_THOMAS32 : PCF_PROF_THOMAS64, (double)words * sizeof(T) * (double)a.n);
+    ProfScope ps(h, tag >= 0 ? tag : sizeof(T) == 4 ? PCF_PROF_THOMAS32 : PCF_PROF_THOMAS64,
+                 (double)words * sizeof(T) * (double)a.n);
     k_thomas<T, MODE><<<(a.plane + bs - 1) / bs, bs, 0, h->stream>>>(a);
     PCF_CUDA_TRY(cudaGetLastError());
     return PCF_OK;
@@ -297,11 +308,302 @@ static int precond_apply(pcf_handle *h, const Work<T> &w, T *bvec, int iters, do
     return PCF_OK;
 }
 
+// ------------------------------------------------------------ multigrid --
+// Horizontal aggregation multigrid V-cycle (pcf_mg.cuh) around the
+// reference line relaxation, FP32, used as the right preconditioner of the
+// mixed-precision solve.  One cycle on level l with right-hand side b:
+//   s = S(b)              one pseudo-time step from zero (vertical Thomas)
+//   r = b - A s           restricted to level l+1 and cycled there
+//   s += P e              coarse correction
+//   s = S(b; s)           one pseudo-time step from s
+// and mg_coarse_iterations pseudo-time steps on the coarsest level.
+
+struct MgLevel {
+    Dims d;
+    int cx = 1, cy = 1;  // aggregation from the finer level (levels >= 1)
+    double dx = 0, dy = 0, deta = 0;
+    float *coef = nullptr, *fac = nullptr, *fc = nullptr, *b = nullptr, *s = nullptr, *t = nullptr;
+};
+struct MgState {
+    std::vector<MgLevel> lv;  // lv[0] is the handle's grid (its planes are the handle's)
+    std::vector<void *> allocs;
+    int min_columns = -1;
+    int coarse_iters = 0;
+    long long version = -1;  // operator version the coarse operators were built from
+    double dtau = 0;
+};
+
+__global__ void k_to_float(const double *__restrict__ a, float *__restrict__ b, long long n, double scale);
+
+// Columns per level up to which the coarse-level column solves use a warp per column.
+constexpr int kWarpThomasColumns = 16384;
+
+template <int MODE>
+static int mg_thomas(pcf_handle *h, const MgLevel &L, const ThomasArgs<float> &a, int tag) {
+    if (L.d.nz <= 32 * kLevelsPerLane && L.d.plane <= kWarpThomasColumns && (MODE == TH_B || MODE == TH_T) &&
+        a.post == nullptr) {
+        ProfScope ps(h, tag, 7.0 * 4 * (double)a.n);
+        const long long threads = 32LL * L.d.plane;
+        k_thomas_warp<MODE><<<(unsigned)((threads + 127) / 128), 128, 0, h->stream>>>(a);
+        PCF_CUDA_TRY(cudaGetLastError());
+        return PCF_OK;
+    }
+    return launch_thomas<float, MODE>(h, a, tag);
+}
+
+static ThomasArgs<float> mg_targs(const MgLevel &L, const float *fac, const float *in, float *out,
+                                  const KrylovScalars *guard) {
+    ThomasArgs<float> ta;
+    ta.fac = fac;
+    ta.in = in;
+    ta.r = nullptr;
+    ta.v = nullptr;
+    ta.vec = nullptr;
+    ta.out = out;
+    ta.post = nullptr;
+    ta.plane = L.d.plane;
+    ta.nz = L.d.nz;
+    ta.n = L.d.n;
+    ta.deta = L.deta;
+    ta.scal = guard;
+    return ta;
+}
+
+// b_{l+1} = R r_l
+static int mg_restrict(pcf_handle *h, int l, const float *r, const KrylovScalars *guard) {
+    const MgLevel &F = h->mg->lv[l], &Cl = h->mg->lv[l + 1];
+    ProfScope ps(h, PCF_PROF_MG, (2.0 + 2.0 / (Cl.cx * Cl.cy)) * 4 * (double)F.d.n);
+    const unsigned g = vec_grid(Cl.d.n);
+    if (Cl.cx == 2 && Cl.cy == 2)
+        k_mg_restrict<float, 2, 2><<<g, 256, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
+    else if (Cl.cx == 2)
+        k_mg_restrict<float, 2, 1><<<g, 256, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
+    else
+        k_mg_restrict<float, 1, 2><<<g, 256, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
+    PCF_CUDA_TRY(cudaGetLastError());
+    return PCF_OK;
+}
+
+// s_l += P e_{l+1}
+static int mg_prolong(pcf_handle *h, int l, const float *e, float *s, const KrylovScalars *guard) {
+    const MgLevel &F = h->mg->lv[l], &Cl = h->mg->lv[l + 1];
+    ProfScope ps(h, PCF_PROF_MG, (3.0 + 2.0 / (Cl.cx * Cl.cy)) * 4 * (double)F.d.n);
+    const unsigned g = vec_grid(F.d.n);
+    if (Cl.cx == 2 && Cl.cy == 2)
+        k_mg_prolong<float, 2, 2><<<g, 256, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
+    else if (Cl.cx == 2)
+        k_mg_prolong<float, 2, 1><<<g, 256, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
+    else
+        k_mg_prolong<float, 1, 2><<<g, 256, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
+    PCF_CUDA_TRY(cudaGetLastError());
+    return PCF_OK;
+}
+
+// One pseudo-time step from s on level L: out = s + deta (L_h s - b), then the column solve in place.
+static int mg_pseudo_step(pcf_handle *h, const MgLevel &L, const float *coef, const float *fac, const float *s,
+                          float *out, const float *b, const KrylovScalars *guard, const float *post, int tag) {
+    StencilArgs<float> sa;
+    sa.coef = coef;
+    sa.s = s;
+    sa.out = out;
+    sa.w1 = b;
+    sa.deta = L.deta;
+    sa.guard = guard;
+    int rc = launch_stencil_dims<float, true, EPI_PSEUDO>(h, sa, L.d, tag);
+    if (rc) return rc;
+    ThomasArgs<float> ta = mg_targs(L, fac, out, out, guard);
+    ta.post = post;
+    return tag == PCF_PROF_MG ? mg_thomas<TH_T>(h, L, ta, tag) : launch_thomas<float, TH_T>(h, ta);
+}
+
+// Cycle on a coarse level l >= 1 with right-hand side lv[l].b; *result is lv[l].s or lv[l].t.
+static int mg_cycle(pcf_handle *h, int l, const KrylovScalars *guard, float **result) {
+    MgState &m = *h->mg;
+    const MgLevel &L = m.lv[l];
+    int rc = mg_thomas<TH_B>(h, L, mg_targs(L, L.fac, L.b, L.s, guard), PCF_PROF_MG);
+    if (rc) return rc;
+    if (l + 1 == (int)m.lv.size()) {
+        float *cur = L.s, *oth = L.t;
+        for (int q = 1; q < m.coarse_iters; ++q) {
+            if ((rc = mg_pseudo_step(h, L, L.coef, L.fac, cur, oth, L.b, guard, nullptr, PCF_PROF_MG))) return rc;
+            std::swap(cur, oth);
+        }
+        *result = cur;
+        return PCF_OK;
+    }
+    StencilArgs<float> sa;
+    sa.coef = L.coef;
+    sa.s = L.s;
+    sa.out = L.t;
+    sa.w1 = L.b;
+    sa.deta = 0;
+    sa.guard = guard;
+    if ((rc = launch_stencil_dims<float, false, EPI_RESNR>(h, sa, L.d, PCF_PROF_MG))) return rc;
+    if ((rc = mg_restrict(h, l, L.t, guard))) return rc;
+    float *e = nullptr;
+    if ((rc = mg_cycle(h, l + 1, guard, &e))) return rc;
+    if ((rc = mg_prolong(h, l, e, L.s, guard))) return rc;
+    if ((rc = mg_pseudo_step(h, L, L.coef, L.fac, L.s, L.t, L.b, guard, nullptr, PCF_PROF_MG))) return rc;
+    *result = L.t;
+    return PCF_OK;
+}
+
+// The V-cycle on the handle's grid as the right preconditioner of the FP32
+// iteration: the first smoothing step forms its input by MODE (b itself, or
+// the BiCGSTAB p / s update written back to bvec, as precond_apply), and the
+// result (in o2) is multiplied by post (1 / fcscal) when post is set.
+template <int MODE>
+static int mg_precond(pcf_handle *h, const Work<float> &w, float *bvec, const KrylovScalars *guard, float **result,
+                      float *o1, float *o2, const float *post) {
+    MgState &m = *h->mg;
+    const MgLevel &L = m.lv[0];
+    ThomasArgs<float> ta = mg_targs(L, w.fac, bvec, o1, guard);
+    ta.r = w.r;
+    ta.v = w.v;
+    ta.vec = bvec;
+    const bool single = m.lv.size() == 1;
+    if (single && m.coarse_iters <= 1) ta.post = post;
+    int rc = launch_thomas<float, MODE>(h, ta);
+    if (rc) return rc;
+    if (single) {
+        // no coarser level: the coarsest-level smoothing on this grid
+        float *cur = o1, *oth = o2;
+        for (int q = 1; q < m.coarse_iters; ++q) {
+            if ((rc = mg_pseudo_step(h, L, w.coef, w.fac, cur, oth, bvec, guard,
+                                     q + 1 == m.coarse_iters ? post : nullptr, -1)))
+                return rc;
+            std::swap(cur, oth);
+        }
+        *result = cur;
+        return PCF_OK;
+    }
+    StencilArgs<float> sa;
+    sa.coef = w.coef;
+    sa.s = o1;
+    sa.out = o2;
+    sa.w1 = bvec;
+    sa.deta = 0;
+    sa.guard = guard;
+    if ((rc = launch_stencil<float, false, EPI_RESNR>(h, sa))) return rc;
+    if ((rc = mg_restrict(h, 0, o2, guard))) return rc;
+    float *e = nullptr;
+    if ((rc = mg_cycle(h, 1, guard, &e))) return rc;
+    if ((rc = mg_prolong(h, 0, e, o1, guard))) return rc;
+    if ((rc = mg_pseudo_step(h, L, w.coef, w.fac, o1, o2, bvec, guard, post, -1))) return rc;
+    *result = o2;
+    return PCF_OK;
+}
+
+static void mg_free(pcf_handle *h) {
+    if (!h->mg) return;
+    for (void *q : h->mg->allocs) cudaFree(q);
+    h->mg->allocs.clear();
+    h->mg->lv.clear();
+}
+
+static void clear_graphs(pcf_handle *h);
+
+// Builds (on the first call or when the level layout changes) and refreshes
+// (when the operator or the smoother's step changed) the hierarchy.
+static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
+    if (!(prm->mg_dtau > 0) || prm->mg_coarse_iterations < 1 || prm->mg_min_columns < 1) return PCF_EINVAL;
+    if (!h->mg) h->mg = new MgState();
+    MgState &m = *h->mg;
+    if (m.min_columns != prm->mg_min_columns || m.lv.empty()) {
+        cudaStreamSynchronize(h->stream);
+        clear_graphs(h);  // captured kernels hold the old level buffers
+        mg_free(h);
+        MgLevel L0;
+        L0.d = h->d;
+        L0.dx = h->dx;
+        L0.dy = h->dy;
+        m.lv.push_back(L0);
+        for (;;) {
+            const MgLevel &F = m.lv.back();
+            const int cx = (F.d.nx % 2 == 0 && F.d.nx >= 4) ? 2 : 1;
+            const int cy = (F.d.ny % 2 == 0 && F.d.ny >= 4) ? 2 : 1;
+            if (cx * cy == 1 || F.d.plane <= prm->mg_min_columns) break;
+            MgLevel C;
+            C.d.nx = F.d.nx / cx;
+            C.d.ny = F.d.ny / cy;
+            C.d.nz = F.d.nz;
+            C.d.plane = C.d.nx * C.d.ny;
+            C.d.n = (long long)C.d.plane * C.d.nz;
+            C.cx = cx;
+            C.cy = cy;
+            C.dx = F.dx * cx;
+            C.dy = F.dy * cy;
+            m.lv.push_back(C);
+        }
+        auto alloc = [&](float **p, long long count) -> int {
+            cudaError_t e = cudaMalloc((void **)p, sizeof(float) * (size_t)count);
+            if (e != cudaSuccess) return pcf_set_cuda_error(e);
+            m.allocs.push_back(*p);
+            h->bytes += (long long)sizeof(float) * count;
+            return PCF_OK;
+        };
+        int rc;
+        if ((rc = alloc(&m.lv[0].fc, h->d.n))) return rc;
+        for (size_t l = 1; l < m.lv.size(); ++l) {
+            MgLevel &C = m.lv[l];
+            if ((rc = alloc(&C.coef, C.d.n * PCF_NCOEF)) || (rc = alloc(&C.fac, C.d.n * 3)) ||
+                (rc = alloc(&C.fc, C.d.n)) || (rc = alloc(&C.b, C.d.n)) || (rc = alloc(&C.s, C.d.n)) ||
+                (rc = alloc(&C.t, C.d.n)))
+                return rc;
+        }
+        m.min_columns = prm->mg_min_columns;
+        m.version = -1;
+    }
+    m.coarse_iters = prm->mg_coarse_iterations;
+    for (MgLevel &L : m.lv) L.deta = prm->mg_dtau / (2 * (1 / (L.dx * L.dx) + 1 / (L.dy * L.dy)));
+    // the finest level's pivots are the handle's (shared with the reference preconditioner)
+    int rc = ensure_factors(h, m.lv[0].deta);
+    if (rc) return rc;
+    if (m.version == h->op_version && m.dtau == prm->mg_dtau) return PCF_OK;
+    // finest level: fcscal in FP32
+    {
+        ProfScope ps(h, PCF_PROF_ASSEMBLE, 12.0 * (double)h->d.n);
+        k_to_float<<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->fc64, m.lv[0].fc, h->d.n, 1.0);
+        PCF_CUDA_TRY(cudaGetLastError());
+    }
+    for (size_t l = 1; l < m.lv.size(); ++l) {
+        const MgLevel &F = m.lv[l - 1];
+        MgLevel &C = m.lv[l];
+        ProfScope ps(h, PCF_PROF_ASSEMBLE, (26.0 * (l == 1 ? 8 : 4) + 32.0 / (C.cx * C.cy)) * (double)F.d.n);
+        const unsigned gf = vec_grid(C.d.n), gc = (unsigned)((C.d.n + 127) / 128);
+#define PCF_MG_BUILD(CX, CY)                                                                                          \
+    do {                                                                                                              \
+        k_mg_fc<float, CX, CY><<<gf, 256, 0, h->stream>>>(F.fc, F.d.nx, F.d.ny, F.d.nz, C.fc);                        \
+        if (l == 1)                                                                                                   \
+            k_mg_coarsen<double, CX, CY><<<gc, 128, 0, h->stream>>>(h->coef64, h->fc64, F.d.nx, F.d.ny, F.d.nz, C.fc, \
+                                                                    C.coef);                                          \
+        else                                                                                                          \
+            k_mg_coarsen<float, CX, CY><<<gc, 128, 0, h->stream>>>(F.coef, F.fc, F.d.nx, F.d.ny, F.d.nz, C.fc,       \
+                                                                   C.coef);                                           \
+    } while (0)
+        if (C.cx == 2 && C.cy == 2)
+            PCF_MG_BUILD(2, 2);
+        else if (C.cx == 2)
+            PCF_MG_BUILD(2, 1);
+        else
+            PCF_MG_BUILD(1, 2);
+#undef PCF_MG_BUILD
+        PCF_CUDA_TRY(cudaGetLastError());
+        k_mg_factors<<<(C.d.plane + 127) / 128, 128, 0, h->stream>>>(C.d.plane, C.d.nz, C.d.n, C.deta, C.coef, C.fac);
+        PCF_CUDA_TRY(cudaGetLastError());
+        h->launches += 2;
+    }
+    m.version = h->op_version;
+    m.dtau = prm->mg_dtau;
+    return PCF_OK;
+}
+
 struct LoopCfg {
     int precond, pc_iters;
     double deta;
     int flex;      // accumulate x from the preconditioned directions (FP32 inner loop)
     int reliable;  // fold into the FP64 solution and restart r from the true residual
+    int mg = 0;    // multigrid V-cycle as the preconditioner (FP32 loop only)
 };
 
 // Reliable update (mixed precision): x64 += bnorm64 x32, r64 = b - A64 x64
@@ -336,7 +638,14 @@ static int bicgstab_iteration(pcf_handle *h, const Work<T> &w, const LoopCfg &c)
     T *z = nullptr, *zp = nullptr;
     // p = r + beta (p - omega v); z = M p
     if (c.precond) {
-        rc = precond_apply<T, TH_PUPD>(h, w, w.p, c.pc_iters, c.deta, w.scal, &z, nullptr, nullptr, w.post);
+        if constexpr (sizeof(T) == 4) {
+            if (c.mg)
+                rc = mg_precond<TH_PUPD>(h, w, w.p, w.scal, &z, w.za, w.zb, w.post);
+            else
+                rc = precond_apply<T, TH_PUPD>(h, w, w.p, c.pc_iters, c.deta, w.scal, &z, nullptr, nullptr, w.post);
+        } else {
+            rc = precond_apply<T, TH_PUPD>(h, w, w.p, c.pc_iters, c.deta, w.scal, &z, nullptr, nullptr, w.post);
+        }
         zp = z;
     } else {
         h->launches += 1;
@@ -361,8 +670,16 @@ static int bicgstab_iteration(pcf_handle *h, const Work<T> &w, const LoopCfg &c)
     }
     // s = r - alpha v; z = M s
     if (c.precond) {
-        rc = precond_apply<T, TH_SUPD>(h, w, w.s, c.pc_iters, c.deta, w.scal, &z, c.flex ? w.zc : w.za,
-                                       c.flex ? w.zd : w.zb, w.post);
+        bool done = false;
+        if constexpr (sizeof(T) == 4) {
+            if (c.mg) {
+                rc = mg_precond<TH_SUPD>(h, w, w.s, w.scal, &z, w.zc, w.zd, w.post);
+                done = true;
+            }
+        }
+        if (!done)
+            rc = precond_apply<T, TH_SUPD>(h, w, w.s, c.pc_iters, c.deta, w.scal, &z, c.flex ? w.zc : w.za,
+                                           c.flex ? w.zd : w.zb, w.post);
     } else {
         h->launches += 1;
         k_axpy_noprec<T, TH_SUPD><<<vec_grid(h->d.n), 256, 0, h->stream>>>(w.r, w.v, w.s, h->d.n, w.scal);
@@ -426,9 +743,11 @@ struct RunOut {
 struct GraphKey {
     int tsize, precond, pc_iters, flex, reliable, pi, batch;
     double deta;
+    int mg, mg_levels, mg_coarse_iters;
     bool operator==(const GraphKey &o) const {
         return tsize == o.tsize && precond == o.precond && pc_iters == o.pc_iters && flex == o.flex &&
-               reliable == o.reliable && pi == o.pi && batch == o.batch && deta == o.deta;
+               reliable == o.reliable && pi == o.pi && batch == o.batch && deta == o.deta && mg == o.mg &&
+               mg_levels == o.mg_levels && mg_coarse_iters == o.mg_coarse_iters;
     }
 };
 struct GraphEntry {
@@ -473,6 +792,12 @@ static int batch_graph(pcf_handle *h, const Work<T> &w, const LoopCfg &c, const 
     return PCF_OK;
 }
 
+static void clear_graphs(pcf_handle *h) {
+    if (!h->gcache) return;
+    for (const GraphEntry &e : h->gcache->entries) cudaGraphExecDestroy(e.exec);
+    h->gcache->entries.clear();
+}
+
 // A complete BiCGSTAB run on A x = b (b in w.r on entry is not required: b
 // is the `b` argument), x0 = 0.  On convergence x <- M x as at
 // apply_bicgstab!.jl:132-135.  Result vector: *xout (x or a z buffer).
@@ -507,7 +832,7 @@ static int bicgstab_run(pcf_handle *h, const Work<T> &w, const T *b, double tol,
     // b + 1 is already queued, so the GPU never drains between batches; the
     // batch queued after convergence returns at once.
     GraphKey key{(int)sizeof(T), c.precond, c.pc_iters, c.flex, c.reliable, w.post != nullptr, check_interval,
-                 c.deta};
+                 c.deta, c.mg, c.mg && h->mg ? (int)h->mg->lv.size() : 0, c.mg && h->mg ? h->mg->coarse_iters : 0};
     cudaGraphExec_t gexec = nullptr;
     if (!h->prof_on) {
         int rc = batch_graph<T>(h, w, c, key, &gexec);
@@ -653,6 +978,10 @@ int pcf_params_default(pcf_params *p) {
     p->learned = 0;
     p->check_interval = 16;
     p->restart_interval = 1;
+    p->multigrid = 0;
+    p->mg_dtau = 1.0;
+    p->mg_coarse_iterations = 4;
+    p->mg_min_columns = 16;
     return PCF_OK;
 }
 
@@ -680,6 +1009,10 @@ int pcf_destroy(pcf_handle *h) {
     if (h->gcache) {
         for (const GraphEntry &e : h->gcache->entries) cudaGraphExecDestroy(e.exec);
         delete h->gcache;
+    }
+    if (h->mg) {
+        mg_free(h);
+        delete h->mg;
     }
     if (h->prof) {
         for (cudaEvent_t e : h->prof->pool) cudaEventDestroy(e);
@@ -810,6 +1143,7 @@ static int assemble_device(pcf_handle *h, double dt, double rf, int damp_h) {
         if (rc) return rc;
     }
     h->operator_set = 1;
+    h->op_version += 1;
     return build_diff(h, 1);
 }
 
@@ -841,6 +1175,7 @@ int pcf_set_operator(pcf_handle *h, const double *coef) {
     h->launches += 1;
     PCF_CUDA_TRY(cudaGetLastError());
     h->operator_set = 1;
+    h->op_version += 1;
     h->fac_deta = std::nan("");
     int rc = build_diff(h, h->background_set);
     if (rc) return rc;
@@ -938,6 +1273,57 @@ int pcf_apply_preconditioner(pcf_handle *h, const double *sin_, double *sout, co
     return PCF_OK;
 }
 
+int pcf_multigrid_levels(pcf_handle *h, const pcf_params *prm, int cap, int *nlevels, int *dims) {
+    if (!h || !prm || !nlevels || cap < 0 || (cap > 0 && !dims)) return PCF_EINVAL;
+    if (!h->operator_set) return PCF_ENOTREADY;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    int rc = mg_prepare(h, prm);
+    if (rc) return rc;
+    const int nl = (int)h->mg->lv.size();
+    *nlevels = nl;
+    for (int l = 0; l < nl && l < cap; ++l) {
+        dims[3 * l] = h->mg->lv[l].d.nx;
+        dims[3 * l + 1] = h->mg->lv[l].d.ny;
+        dims[3 * l + 2] = h->mg->lv[l].d.nz;
+    }
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
+}
+
+int pcf_multigrid_operator(pcf_handle *h, int level, double *coef) {
+    if (!h || !coef || !h->mg || level < 0 || level >= (int)h->mg->lv.size()) return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    const MgLevel &L = h->mg->lv[level];
+    const long long m = L.d.n * PCF_NCOEF;
+    if (level == 0) {
+        PCF_CUDA_TRY(cudaMemcpyAsync(coef, h->coef64, sizeof(double) * m, cudaMemcpyDeviceToHost, h->stream));
+        PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        return PCF_OK;
+    }
+    std::vector<float> tmp((size_t)m);
+    PCF_CUDA_TRY(cudaMemcpyAsync(tmp.data(), L.coef, sizeof(float) * m, cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (long long q = 0; q < m; ++q) coef[q] = (double)tmp[(size_t)q];
+    return PCF_OK;
+}
+
+int pcf_apply_multigrid(pcf_handle *h, const double *sin_, double *sout, const pcf_params *prm) {
+    if (!h || !sin_ || !sout || !prm) return PCF_EINVAL;
+    if (!h->operator_set) return PCF_ENOTREADY;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    int rc = mg_prepare(h, prm);
+    if (rc) return rc;
+    if ((rc = upload_vec(h, sin_, h->b64, h->s32))) return rc;
+    float *z = nullptr;
+    rc = mg_precond<TH_B>(h, work32(h), h->s32, nullptr, &z, h->za32, h->zb32, nullptr);
+    if (rc) return rc;
+    k_to_double<<<vec_grid(h->d.n), 256, 0, h->stream>>>(z, h->w64, h->d.n);
+    PCF_CUDA_TRY(cudaGetLastError());
+    PCF_CUDA_TRY(cudaMemcpyAsync(sout, h->w64, sizeof(double) * h->d.n, cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
+}
+
 int pcf_global_dot(pcf_handle *h, const double *a, const double *b, double *out) {
     if (!h || !a || !b || !out) return PCF_EINVAL;
     PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
@@ -980,6 +1366,8 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
     c.flex = 0;
     c.reliable = 0;
     if (c.precond && c.pc_iters < 1) return PCF_EINVAL;
+    // the multigrid preconditioner runs in the FP32 loop of the mixed solve only
+    if (prm->multigrid && (prm->precision != PCF_PRECISION_MIXED || !c.precond)) return PCF_EINVAL;
     int rc;
     if (c.precond && (rc = ensure_factors(h, c.deta))) return rc;
     const int maxit = prm->poisson_iterations;
@@ -1042,6 +1430,11 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
     LoopCfg cm = c;
     cm.flex = 1;
     cm.reliable = 1;
+    if (prm->multigrid) {
+        if ((rc = mg_prepare(h, prm))) return rc;
+        cm.mg = 1;
+        cm.deta = h->mg->lv[0].deta;
+    }
     double rel = rnorm / b_norm;
     int restarts = 0;
     for (;;) {

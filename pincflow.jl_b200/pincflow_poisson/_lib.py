@@ -36,10 +36,10 @@ EXPORTS = [
     "pcf_set_background", "pcf_solve", "pcf_solve_device", "pcf_compute_operator",
     "pcf_set_operator", "pcf_apply_operator", "pcf_apply_preconditioner", "pcf_bicgstab",
     "pcf_global_dot", "pcf_device_bytes", "pcf_launch_count", "pcf_profile_enable", "pcf_profile_read",
-    "pcf_residual_history",
+    "pcf_residual_history", "pcf_multigrid_levels", "pcf_multigrid_operator", "pcf_apply_multigrid",
 ]
 PROF_TAGS = ["apply32", "apply64", "pseudo32", "pseudo64", "thomas32", "thomas64", "update32", "update64",
-             "assemble", "reliable64"]
+             "assemble", "reliable64", "mg"]
 
 
 class PcfDims(ctypes.Structure):
@@ -56,7 +56,9 @@ class PcfParams(ctypes.Structure):
                 ("damp_horizontal_wind_on_rhs", ctypes.c_int), ("precision", ctypes.c_int),
                 ("residual", ctypes.c_int), ("inner_tolerance", ctypes.c_double),
                 ("max_refinements", ctypes.c_int), ("learned", ctypes.c_int),
-                ("check_interval", ctypes.c_int), ("restart_interval", ctypes.c_int)]
+                ("check_interval", ctypes.c_int), ("restart_interval", ctypes.c_int),
+                ("multigrid", ctypes.c_int), ("mg_dtau", ctypes.c_double),
+                ("mg_coarse_iterations", ctypes.c_int), ("mg_min_columns", ctypes.c_int)]
 
 
 class PcfResult(ctypes.Structure):
@@ -117,6 +119,9 @@ def load(path: str | None = None):
     lib.pcf_profile_enable.argtypes = [vp, ctypes.c_int]
     lib.pcf_profile_read.argtypes = [vp, ctypes.c_int, dp, P(ctypes.c_longlong), dp]
     lib.pcf_residual_history.argtypes = [vp, dp, ctypes.c_int, P(ctypes.c_int)]
+    lib.pcf_multigrid_levels.argtypes = [vp, P(PcfParams), ctypes.c_int, P(ctypes.c_int), P(ctypes.c_int)]
+    lib.pcf_multigrid_operator.argtypes = [vp, ctypes.c_int, dp]
+    lib.pcf_apply_multigrid.argtypes = [vp, dp, dp, P(PcfParams)]
     for name in EXPORTS:
         getattr(lib, name).restype = getattr(lib, name).restype or ctypes.c_int
     lib.pcf_strerror.restype = ctypes.c_char_p

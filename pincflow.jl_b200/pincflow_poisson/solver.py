@@ -48,6 +48,10 @@ class PoissonNamelist:
     learned: bool = False
     check_interval: int = 16
     restart_interval: int = 1         # mixed: Krylov restart at every n-th reliable update (0: never)
+    multigrid: bool = False           # mixed: horizontal aggregation multigrid V-cycle as the preconditioner
+    mg_dtau: float = 1.0              # multigrid: pseudo-time step of the smoother on every level
+    mg_coarse_iterations: int = 4     # multigrid: smoothing steps on the coarsest level
+    mg_min_columns: int = 16          # multigrid: a level with at most this many columns is the coarsest
 
     def to_c(self) -> _lib.PcfParams:
         p = _lib.PcfParams()
@@ -66,6 +70,10 @@ class PoissonNamelist:
         p.learned = int(bool(self.learned))
         p.check_interval = int(self.check_interval)
         p.restart_interval = int(self.restart_interval)
+        p.multigrid = int(bool(self.multigrid))
+        p.mg_dtau = float(self.mg_dtau)
+        p.mg_coarse_iterations = int(self.mg_coarse_iterations)
+        p.mg_min_columns = int(self.mg_min_columns)
         return p
 
 
@@ -208,6 +216,31 @@ class PoissonSolver:
         _lib.check(self.lib.pcf_apply_preconditioner(self._h, _lib.dptr(_f64(sin)), _lib.dptr(out),
                                                      ctypes.byref(prm), _lib.PRECISION[precision]),
                    "pcf_apply_preconditioner")
+        return out
+
+    def multigrid_levels(self, namelist: PoissonNamelist) -> list:
+        """(nx, ny, nz) of every level of the multigrid hierarchy built for
+        the current operator (finest first)."""
+        prm = namelist.to_c()
+        n = ctypes.c_int()
+        dims = (ctypes.c_int * 96)()
+        _lib.check(self.lib.pcf_multigrid_levels(self._h, ctypes.byref(prm), 32, ctypes.byref(n), dims),
+                   "pcf_multigrid_levels")
+        return [(dims[3 * q], dims[3 * q + 1], dims[3 * q + 2]) for q in range(min(n.value, 32))]
+
+    def multigrid_operator(self, level: int, shape) -> np.ndarray:
+        """The 25 planes of a multigrid level, shape (25, nz, ny, nx)."""
+        nx, ny, nz = shape
+        out = np.zeros((_lib.NCOEF, nz, ny, nx))
+        _lib.check(self.lib.pcf_multigrid_operator(self._h, int(level), _lib.dptr(out)), "pcf_multigrid_operator")
+        return out
+
+    def apply_multigrid(self, sin, namelist: PoissonNamelist):
+        """One multigrid V-cycle z = MG(sin) (FP32 on the device)."""
+        out = np.zeros(self.dom.interior_shape)
+        prm = namelist.to_c()
+        _lib.check(self.lib.pcf_apply_multigrid(self._h, _lib.dptr(_f64(sin)), _lib.dptr(out), ctypes.byref(prm)),
+                   "pcf_apply_multigrid")
         return out
 
     def apply_bicgstab(self, rhs, tolref, namelist: PoissonNamelist):

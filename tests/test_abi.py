@@ -41,6 +41,7 @@ def _c_layout():
 int main(void) {
   printf("pcf_dims %zu\npcf_params %zu\npcf_result %zu\n", sizeof(pcf_dims), sizeof(pcf_params), sizeof(pcf_result));
   F(pcf_params, dtau) F(pcf_params, inner_tolerance) F(pcf_params, check_interval)
+  F(pcf_params, mg_dtau) F(pcf_params, mg_min_columns)
   F(pcf_result, residual) F(pcf_result, ms_total) F(pcf_dims, device)
   return 0;
 }
@@ -63,6 +64,8 @@ def test_struct_layouts_match_header(pcf):
     assert L.PcfParams.dtau.offset == c["pcf_params.dtau"]
     assert L.PcfParams.inner_tolerance.offset == c["pcf_params.inner_tolerance"]
     assert L.PcfParams.check_interval.offset == c["pcf_params.check_interval"]
+    assert L.PcfParams.mg_dtau.offset == c["pcf_params.mg_dtau"]
+    assert L.PcfParams.mg_min_columns.offset == c["pcf_params.mg_min_columns"]
     assert L.PcfResult.residual.offset == c["pcf_result.residual"]
     assert L.PcfResult.ms_total.offset == c["pcf_result.ms_total"]
     assert L.PcfDims.device.offset == c["pcf_dims.device"]
@@ -75,6 +78,7 @@ def test_params_default_mirror_poisson_namelist(pcf):
     assert p.tolerance == 1e-8 and p.poisson_iterations == 1000 and p.preconditioner == 1
     assert p.dtau == 1.0 and p.preconditioner_iterations == 2 and p.tolerance_is_relative == 0
     assert p.damp_horizontal_wind_on_rhs == 0 and p.precision == 0 and p.residual == 0 and p.learned == 0
+    assert p.multigrid == 0
     nl = pcf.PoissonNamelist().to_c()
     for name, _ in pcf._lib.PcfParams._fields_:
         assert getattr(nl, name) == getattr(p, name), name

@@ -1,0 +1,127 @@
+"""GPU: the multigrid preconditioner of the mixed solve against its oracle
+(oracle/mg_oracle.py) and the plain FP64 solve.
+
+Tolerances (relative to the largest magnitude of the oracle result):
+  coarse operators      2e-5   (FP32 planes; levels >= 2 are built from FP32 inputs)
+  one V-cycle           1e-4   (FP32 arithmetic through every level)
+  solve                 FP64 true residual <= 1e-10; pressure within 1e-6 of
+                        the oracle's plain FP64 solution (null space removed)
+"""
+import numpy as np
+import pytest
+
+from _cases import CASES, case, consistent_rhs, null_weights, oracle_operator, rel_err
+from pincflow_poisson import fields as F
+
+pytestmark = pytest.mark.gpu
+
+MG = dict(multigrid=True, mg_dtau=2.0, mg_coarse_iterations=4, mg_min_columns=16)
+
+
+@pytest.fixture(scope="module")
+def solvers(pcf):
+    cache = {}
+
+    def get(name):
+        if name not in cache:
+            cfg = case(name)
+            s = pcf.PoissonSolver(cfg["dom"], cfg["model"])
+            s.set_grid(cfg["fields"])
+            s.set_background(cfg["fields"])
+            cache[name] = (cfg, s)
+        return cache[name]
+
+    yield get
+    for _, s in cache.values():
+        s.close()
+
+
+def _drop_null(cfg, x):
+    dom = cfg["dom"]
+    nv = null_weights(cfg) / dom.interior(cfg["fields"]["jac"])
+    return x - np.vdot(nv, x) / np.vdot(nv, nv) * nv
+
+
+def _oracle_mg(cfg, coef, **kw):
+    from oracle.mg_oracle import Multigrid
+    f = cfg["fields"]
+    return Multigrid(coef, F.fcscal(cfg["dom"], f), f["dx"], f["dy"], dtau=kw.get("mg_dtau", 2.0),
+                     coarse_iterations=kw.get("mg_coarse_iterations", 4), min_columns=kw.get("mg_min_columns", 16))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_hierarchy_and_coarse_operators(name, solvers, oracle, pcf):
+    cfg, s = solvers(name)
+    d, coef = oracle_operator(oracle, cfg)
+    s.set_operator(coef)
+    nl = pcf.PoissonNamelist(precision="mixed", **MG)
+    levels = s.multigrid_levels(nl)
+    mg = _oracle_mg(cfg, coef, **MG)
+    assert levels == [l[:3] for l in mg.dims]
+    for lv in range(1, min(4, len(levels))):
+        got = s.multigrid_operator(lv, levels[lv])
+        want = mg.levels[lv]["coef"]
+        assert rel_err(got, want) < 2e-5, (lv, rel_err(got, want))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_vcycle_matches_oracle(name, solvers, oracle, pcf):
+    cfg, s = solvers(name)
+    d, coef = oracle_operator(oracle, cfg)
+    s.set_operator(coef)
+    b = np.random.default_rng(17).standard_normal(cfg["dom"].interior_shape)
+    got = s.apply_multigrid(b, pcf.PoissonNamelist(precision="mixed", **MG))
+    want = _oracle_mg(cfg, coef, **MG).cycle(b)
+    assert rel_err(got, want) < 1e-4, rel_err(got, want)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_multigrid_solve_reaches_fp64_residual(name, solvers, oracle, pcf):
+    cfg, s = solvers(name)
+    d, coef = oracle_operator(oracle, cfg)
+    s.set_operator(coef)
+    rhs = consistent_rhs(oracle, cfg)
+    kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=4000, precision="mixed")
+    got, info = s.apply_bicgstab(rhs, 1.0, pcf.PoissonNamelist(**kw, **MG))
+    assert not info.errflag, info
+    assert info.true_residual <= 1e-10
+    r = rhs - oracle.apply_operator(d, coef, got)
+    assert np.sqrt((r ** 2).mean()) / np.sqrt((rhs ** 2).mean()) <= 1.5e-10
+    ref, _ = oracle.bicgstab(d, coef, cfg["fields"]["dx"], cfg["fields"]["dy"], rhs, tolerance=1e-12,
+                             tolerance_is_relative=True, poisson_iterations=4000)
+    if cfg["model"] == "Compressible":
+        assert rel_err(got, ref) < 1e-6
+    else:
+        assert rel_err(_drop_null(cfg, got), _drop_null(cfg, ref)) < 1e-6
+    _, plain = s.apply_bicgstab(rhs, 1.0, pcf.PoissonNamelist(**kw))
+    assert info.niter <= plain.niter, (info.niter, plain.niter)
+
+
+def test_multigrid_rejected_outside_the_mixed_solve(solvers, pcf):
+    cfg, s = solvers("mtn")
+    with pytest.raises(pcf.PoissonError) as e:
+        s.apply_bicgstab(cfg["rhs"], 1.0, pcf.PoissonNamelist(precision="fp64", **MG))
+    assert e.value.code == pcf._lib.PCF_EINVAL
+    with pytest.raises(pcf.PoissonError) as e:
+        s.apply_bicgstab(cfg["rhs"], 1.0, pcf.PoissonNamelist(precision="mixed", **dict(MG, mg_dtau=0.0)))
+    assert e.value.code == pcf._lib.PCF_EINVAL
+
+
+def test_multigrid_iteration_count_at_scale(pcf):
+    """Stretched 128 x 96 x 48 mountain grid: the multigrid-preconditioned
+    mixed solve reaches the FP64 true residual 1e-10 in at most a fifth of the
+    plain FP64 iteration count."""
+    from pincflow_poisson import configs as C
+    cfg = C.c2(nx=128, ny=96, nz=48)
+    with pcf.PoissonSolver(cfg["dom"], cfg["model"]) as s:
+        s.set_grid(cfg["fields"])
+        s.set_background(cfg["fields"])
+        s.compute_operator(cfg["rho"], cfg["betar"], cfg["dt"], cfg["rayleigh_factor"], return_coef=False)
+        kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=5000, residual="true")
+        _, i64 = s.apply_bicgstab(cfg["rhs"], 1.0, pcf.PoissonNamelist(precision="fp64", **kw))
+        _, img = s.apply_bicgstab(cfg["rhs"], 1.0, pcf.PoissonNamelist(precision="mixed", **kw, **MG))
+        hist = s.residual_history()
+    assert not i64.errflag and not img.errflag, (i64, img)
+    assert img.true_residual <= 1e-10
+    assert 5 * img.niter <= i64.niter, (img.niter, i64.niter)
+    assert len(hist) == img.niter and hist[-1] <= 1e-10
