@@ -44,6 +44,8 @@ WORKLOADS = {
           "isothermal 250 K, RHS N(0,1) seed 12345",
     "c5": "512x512x192 pseudo-incompressible, 20 Gaussian ridges <= 2 km, wave-packet RHS",
     "c1": "periodic hill 40x1x40 Boussinesq (one of its 200 solves)",
+    "c4": "32-member uneven ensemble, nx = ny in {64, 96, 128, 192}, nz = nx/2, random Gaussian hills and "
+          "stratification, RHS N(0,1) per member",
 }
 
 
@@ -201,6 +203,180 @@ def run_reference(args, rank, world):
             "cpu_baseline": {"value": value, "unit": "s", "cores": used, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------- ensemble (c4) --
+
+def run_ensemble(args, rank, world, local_rank):
+    """C4: all members solved together (one graph launch per iteration batch
+    for all members, tile shapes from the autotuner), against the same
+    members solved one after another by the plain FP64 solver."""
+    import torch
+
+    import pincflow_poisson as pcf
+    from pincflow_poisson import configs as C
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    sizes = C.c4_sizes(seed=4 + rank)
+    members = []
+    for q, nx in enumerate(sizes):
+        cfg = C.c4(1000 * rank + q, nx)
+        s = pcf.PoissonSolver(cfg["dom"], cfg["model"], device=local_rank)
+        s.set_grid(cfg["fields"])
+        s.set_background(cfg["fields"])
+        d = {k: torch.from_numpy(np.ascontiguousarray(cfg[k])).to(dev) for k in ("rhs", "rho", "betar")}
+        d["dpip"] = torch.zeros(cfg["dom"].halo_shape, dtype=torch.float64, device=dev)
+        members.append((cfg, s, d))
+    torch.cuda.synchronize()
+    kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000, residual="true")
+    nl_ens = pcf.PoissonNamelist(**kw, precision="mixed", multigrid=True, mg_dtau=args.mg_dtau, autotune=True)
+    nl_plain = pcf.PoissonNamelist(**kw, precision="fp64")
+    ens = pcf.Ensemble([m[1] for m in members])
+    cols = lambda key: [m[2][key].data_ptr() for m in members]
+    scal = lambda key: [m[0][key] for m in members]
+
+    def solve_all():
+        infos = ens.solve_poisson_device(cols("rhs"), cols("rho"), cols("betar"), scal("dt"),
+                                         scal("rayleigh_factor"), scal("tolref"), nl_ens, cols("dpip"))
+        bad = [q for q, i in enumerate(infos) if i.errflag]
+        if bad:
+            raise RuntimeError(f"members {bad} did not converge")
+        return infos
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        solve_all()
+    barrier()
+    l0 = ens.launch_count
+    with ClockSampler(local_rank) as clk:
+        runs = [solve_all() for _ in range(args.steps)]
+        barrier()
+    launches = ens.launch_count - l0
+    ms = max_over_ranks(statistics.mean(r[0].timings_ms["total"] for r in runs))
+    n = len(members)
+    value = world * n / (ms / 1e3)
+
+    # the same members one after another: plain FP64, and the single-handle multigrid solve
+    nl_single = pcf.PoissonNamelist(**kw, precision="mixed", multigrid=True, mg_dtau=args.mg_dtau, autotune=True)
+
+    def sequential(nl):
+        tot, iters = 0.0, []
+        for cfg, s, d in members:
+            i = s.solve_poisson_device(d["rhs"].data_ptr(), d["rho"].data_ptr(), d["betar"].data_ptr(), cfg["dt"],
+                                       cfg["rayleigh_factor"], cfg["tolref"], nl, d["dpip"].data_ptr())
+            if i.errflag:
+                raise RuntimeError(f"sequential solve did not converge: {i}")
+            tot += i.timings_ms["total"]
+            iters.append(i.niter)
+        return tot, iters
+
+    sequential(nl_single)  # graphs captured for every member
+    barrier()
+    plain_ms, plain_iters = sequential(nl_plain)
+    single_ms, single_iters = sequential(nl_single)
+    plain_ms = max_over_ranks(plain_ms)
+    single_ms = max_over_ranks(single_ms)
+
+    # end to end: member inputs from pinned host memory, results back to the host
+    hosts = [{k: torch.from_numpy(np.ascontiguousarray(m[0][k])).pin_memory() for k in ("rhs", "rho", "betar")}
+             for m in members]
+    outs = [torch.zeros(m[0]["dom"].halo_shape, dtype=torch.float64).pin_memory() for m in members]
+    h2d = sum(int(h[k].numel()) * 8 for h in hosts for k in h)
+    d2h = sum(int(o.numel()) * 8 for o in outs)
+    barrier()
+    e2e = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for h, (_, _, d) in zip(hosts, members):
+            for k in ("rhs", "rho", "betar"):
+                d[k].copy_(h[k], non_blocking=True)
+        torch.cuda.synchronize()
+        solve_all()
+        for o, (_, _, d) in zip(outs, members):
+            o.copy_(d["dpip"], non_blocking=True)
+        torch.cuda.synchronize()
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(statistics.mean(e2e))
+
+    if rank != 0:
+        ens.close()
+        for m in members:
+            m[1].close()
+        return
+    # roofline: the FP32 Krylov Total apply of the largest member, per-launch events
+    big = max(range(n), key=lambda q: sizes[q])
+    cfg, s, d = members[big]
+    s.profile(True)
+    s.solve_poisson_device(d["rhs"].data_ptr(), d["rho"].data_ptr(), d["betar"].data_ptr(), cfg["dt"],
+                           cfg["rayleigh_factor"], cfg["tolref"], nl_single, d["dpip"].data_ptr())
+    prof = s.profile_read()
+    s.profile(False)
+    a32 = prof["apply32"]
+    kernel_ms = a32["ms"] / max(a32["count"], 1)
+    bpl = a32["bytes"] / max(a32["count"], 1)
+    peak, peak_kind = load_peaks()
+    achieved = bpl / (kernel_ms * 1e-3) / 1e9 if kernel_ms > 0 else 0.0
+    cells = sum(m[0]["dom"].nx * m[0]["dom"].ny * m[0]["dom"].nz for m in members)
+    it = [i.niter for i in runs[-1]]
+    line = {
+        "metric": "ensemble solves/s to FP64 true rel. residual 1e-10 (32 uneven members), 1 B200",
+        "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": f"c4: {WORKLOADS['c4']}", "members": sizes, "cells": cells,
+                   "method": METHODS["mg"] + "; all members advanced together, one CUDA graph launch per "
+                             "batch of iterations, stencil tiles from the autotuner",
+                   "l2": "members total far above L2 (126 MB), no flush", "parallelism": f"replicas x{world}"},
+        "iterations": it, "plain_fp64_iterations": plain_iters,
+        "sequential_plain_fp64_solves_per_s": n / (plain_ms / 1e3),
+        "sequential_single_mg_solves_per_s": n / (single_ms / 1e3),
+        "speedup_vs_sequential_plain_fp64": plain_ms / ms,
+        "speedup_vs_sequential_single_mg": single_ms / ms,
+        "cell_updates_per_s": world * sum(m[0]["dom"].nx * m[0]["dom"].ny * m[0]["dom"].nz * 2 * i.niter
+                                          for m, i in zip(members, runs[-1])) / (ms / 1e3),
+        "gpu_launches": launches,
+        "e2e": {"value": world * n / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "kernel": f"k_stencil Total apply FP32 of the {sizes[big]}^2 member",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": bpl,
+                     "ms_per_launch": kernel_ms},
+        "autotune": [{k: e[k] for k in ("kernel", "nx", "nz", "tile_x", "levels", "ms_best", "ms_default")}
+                     for e in pcf.autotune_entries() if e["kernel"] == "total32_diff"],
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        # oracle assembly + 1 iteration per size class, scaled by each member's plain FP64 iteration count
+        per_class = {}
+        total = 0.0
+        for (cfg, _, _), niter in zip(members, plain_iters):
+            nx = cfg["dom"].nx
+            if nx not in per_class:
+                per_class[nx] = oracle_sample(cfg, 1, os.cpu_count())
+            t_asm, t_it, used = per_class[nx]
+            total += t_asm + t_it * niter
+        line["cpu_baseline"] = {"value": n / total, "unit": "solves/s", "cores": used, "kind": "port",
+                                "sample": "oracle FP64 assembly + 1 BiCGSTAB iteration per size class, scaled by "
+                                          "each member's GPU FP64 iteration count and summed over the members"}
+    print(json.dumps(line), flush=True)
+    ens.close()
+    for m in members:
+        m[1].close()
 
 
 # ----------------------------------------------------------------- GPU arm --
@@ -400,7 +576,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.config == "c4":
+            run_ensemble(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

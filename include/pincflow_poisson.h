@@ -127,6 +127,8 @@ typedef struct {
     double mg_dtau;                /* multigrid: pseudo-time step of the smoother, all levels (1.0) */
     int mg_coarse_iterations;      /* multigrid: smoothing steps on the coarsest level (4) */
     int mg_min_columns;            /* multigrid: a level with at most this many columns is the coarsest (16) */
+    int autotune;                  /* 1: time the stencil tile shapes of every new grid size on first use and keep
+                                      the fastest (process-wide table, pcf_autotune_entries); 0: fixed heuristic (0) */
 } pcf_params;
 
 typedef struct {
@@ -209,6 +211,46 @@ int pcf_apply_preconditioner(pcf_handle *h, const double *sin_, double *sout,
 int pcf_multigrid_levels(pcf_handle *h, const pcf_params *prm, int cap, int *nlevels, int *dims);
 int pcf_multigrid_operator(pcf_handle *h, int level, double *coef);
 int pcf_apply_multigrid(pcf_handle *h, const double *sin, double *sout, const pcf_params *prm);
+
+/* Stencil tile autotuner (no reference counterpart).  One entry per device,
+ * kernel family and grid size that a solve with pcf_params.autotune = 1 has
+ * tuned: the chosen tile (tile_x threads along x, 128 threads per block, vec
+ * values per thread) and z-levels per block, with the measured time per
+ * launch of the chosen and of the heuristic shape. */
+enum {
+    PCF_TUNE_TOTAL32 = 0,       /* Total apply, FP32, plain form (multigrid residuals) */
+    PCF_TUNE_TOTAL32_DIFF = 1,  /* Total apply, FP32, difference form (Krylov loop) */
+    PCF_TUNE_HORIZ32 = 2,       /* Horizontal apply + pseudo-time step, FP32 */
+    PCF_TUNE_TOTAL64 = 3,
+    PCF_TUNE_HORIZ64 = 4
+};
+typedef struct {
+    int kernel, nx, ny, nz;
+    int tile_x, vec, levels;
+    double ms_best, ms_default;
+} pcf_tune_entry;
+int pcf_autotune_entries(pcf_tune_entry *out, int cap, int *count);
+int pcf_autotune_clear(void);
+
+/* Ensemble of solver handles (no reference counterpart; the reference runs
+ * ensemble members as separate MPI sub-communicators, src/ensemble.jl:40-43).
+ * Members are handles on one device with grid and background set; their
+ * sizes may differ.  pcf_ensemble_solve_device runs solve_poisson! for every
+ * member (arrays of per-member device pointers and scalars, as
+ * pcf_solve_device) with the mixed-precision iteration only: after each
+ * member's setup on its own stream, every batch of check_interval
+ * iterations of all members is one CUDA graph launch.  res has one entry
+ * per member.  A handle may belong to one ensemble at a time and must not be
+ * used by another thread while the ensemble solves. */
+typedef struct pcf_ensemble pcf_ensemble;
+int pcf_ensemble_create(pcf_ensemble **e, pcf_handle *const *members, int count);
+int pcf_ensemble_destroy(pcf_ensemble *e);
+int pcf_ensemble_solve_device(pcf_ensemble *e, const double *const *d_rhs, const double *const *d_rho,
+                              const double *const *d_betar, const double *const *d_p, const double *dt,
+                              const double *rayleigh_factor, const double *tolref, const pcf_params *prm,
+                              double *const *d_dpip, pcf_result *res);
+long long pcf_ensemble_launch_count(const pcf_ensemble *e);
+
 
 /* apply_bicgstab!: solves A s = rhs with the handle's current operator;
  * interior arrays. */

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "pcf_kernels.cuh"
@@ -133,11 +134,12 @@ static int pick_kc(long long xyblocks, int nz) {
 }
 
 template <typename T, int V, int TX, bool HORIZ, int EPI, bool DIFF>
-static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_override) {
+static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_override, int kc) {
     constexpr int TY = 128 / TX;
     constexpr int W = TX * V;
     const long long gx = (a.nx + W - 1) / W, gy = (a.ny + TY - 1) / TY;
-    const int kc = pick_kc(gx * gy, a.nz);
+    if (kc <= 0) kc = pick_kc(gx * gy, a.nz);
+    kc = std::min(kc, a.nz);
     // one partial sum per block: the grid must fit the partials buffer
     if (gx * gy * ((a.nz + kc - 1) / kc) > kMaxPartials || gy > 65535) return PCF_ERANGE;
     const dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)((a.nz + kc - 1) / kc));
@@ -154,6 +156,62 @@ static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_ov
     return PCF_OK;
 }
 
+// ------------------------------------------------------------ autotuner --
+// Tile shapes of k_stencil: 128 threads as TX x (128 / TX), each thread
+// holding V consecutive x values (V = 4 in FP32, 2 in FP64 when nx allows),
+// and kc z-levels per block.  The heuristic picks TX = 32 for wide grids and
+// TX = 8 otherwise, with pick_kc; with pcf_params.autotune the first solve on
+// a grid size times every tile shape at several kc around pick_kc's and keeps
+// the fastest for that size class in a process-wide table (per device and
+// kernel family), which later launches of any handle consult.
+constexpr int kTileX[3] = {32, 16, 8};
+
+static int tune_family(int tsize, bool horiz, bool diff) {
+    if (tsize == 8) return horiz ? PCF_TUNE_HORIZ64 : PCF_TUNE_TOTAL64;
+    return horiz ? PCF_TUNE_HORIZ32 : diff ? PCF_TUNE_TOTAL32_DIFF : PCF_TUNE_TOTAL32;
+}
+
+struct TuneRec {
+    int device;
+    pcf_tune_entry e;
+    int tile;
+};
+static std::mutex g_tune_mu;
+static std::vector<TuneRec> g_tune;
+
+static bool tune_lookup(int family, int device, const Dims &d, int *tile, int *kc) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const TuneRec &r : g_tune)
+        if (r.device == device && r.e.kernel == family && r.e.nx == d.nx && r.e.ny == d.ny && r.e.nz == d.nz) {
+            *tile = r.tile;
+            *kc = r.e.levels;
+            return true;
+        }
+    return false;
+}
+
+static int default_tile(int nx, int vmax) {
+    const bool vec = nx % vmax == 0;
+    return nx >= (vec ? 32 * vmax : 32) ? 0 : 2;
+}
+
+template <typename T, bool HORIZ, int EPI, bool DIFF>
+static int launch_tile(pcf_handle *h, const StencilArgs<T> &a, int tile, int kc, int tag) {
+    constexpr int VMAX = sizeof(T) == 4 ? 4 : 2;
+    const bool vec = (a.nx % VMAX) == 0;
+    switch (tile) {
+        case 0:
+            return vec ? launch_stencil_cfg<T, VMAX, 32, HORIZ, EPI, DIFF>(h, a, tag, kc)
+                       : launch_stencil_cfg<T, 1, 32, HORIZ, EPI, DIFF>(h, a, tag, kc);
+        case 1:
+            return vec ? launch_stencil_cfg<T, VMAX, 16, HORIZ, EPI, DIFF>(h, a, tag, kc)
+                       : launch_stencil_cfg<T, 1, 16, HORIZ, EPI, DIFF>(h, a, tag, kc);
+        default:
+            return vec ? launch_stencil_cfg<T, VMAX, 8, HORIZ, EPI, DIFF>(h, a, tag, kc)
+                       : launch_stencil_cfg<T, 1, 8, HORIZ, EPI, DIFF>(h, a, tag, kc);
+    }
+}
+
 // Stencil apply on a grid of dimensions d (the handle's grid or a multigrid level).
 template <typename T, bool HORIZ, int EPI, bool DIFF = false>
 static int launch_stencil_dims(pcf_handle *h, StencilArgs<T> a, const Dims &d, int tag = -1) {
@@ -162,14 +220,101 @@ static int launch_stencil_dims(pcf_handle *h, StencilArgs<T> a, const Dims &d, i
     a.nz = d.nz;
     a.n = d.n;
     constexpr int VMAX = sizeof(T) == 4 ? 4 : 2;
-    const bool vec = (a.nx % VMAX) == 0;
-    const int wide = vec ? 32 * VMAX : 32;
-    if (a.nx >= wide) {
-        if (vec) return launch_stencil_cfg<T, VMAX, 32, HORIZ, EPI, DIFF>(h, a, tag);
-        return launch_stencil_cfg<T, 1, 32, HORIZ, EPI, DIFF>(h, a, tag);
+    int tile = 0, kc = 0;
+    if (!tune_lookup(tune_family(sizeof(T), HORIZ, DIFF), h->dims.device, d, &tile, &kc)) {
+        tile = default_tile(a.nx, VMAX);
+        kc = 0;
     }
-    if (vec) return launch_stencil_cfg<T, VMAX, 8, HORIZ, EPI, DIFF>(h, a, tag);
-    return launch_stencil_cfg<T, 1, 8, HORIZ, EPI, DIFF>(h, a, tag);
+    return launch_tile<T, HORIZ, EPI, DIFF>(h, a, tile, kc, tag);
+}
+
+// Times the candidate tile shapes of one kernel family on grid d (once per
+// size class and device) with the given operator and scratch vectors.
+template <typename T, bool HORIZ, bool DIFF>
+static int tune_stencil(pcf_handle *h, const Dims &d, const T *coef, const T *sv, T *out, const T *b) {
+    const int family = tune_family(sizeof(T), HORIZ, DIFF);
+    int t0, k0;
+    if (tune_lookup(family, h->dims.device, d, &t0, &k0)) return PCF_OK;
+    constexpr int VMAX = sizeof(T) == 4 ? 4 : 2;
+    constexpr int EPI = HORIZ ? EPI_PSEUDO : EPI_STORE;
+    StencilArgs<T> a;
+    a.coef = coef;
+    a.s = sv;
+    a.out = out;
+    a.w1 = b;
+    a.deta = 0.1;
+    a.nx = d.nx;
+    a.ny = d.ny;
+    a.nz = d.nz;
+    a.n = d.n;
+    const int vmax_ok = d.nx % VMAX == 0 ? VMAX : 1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PCF_CUDA_TRY(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return PCF_ECUDA;
+    }
+    const int saved_prof = h->prof_on;
+    h->prof_on = 0;
+    auto time_cfg = [&](int tile, int kc, double *ms) -> int {
+        int rc = launch_tile<T, HORIZ, EPI, DIFF>(h, a, tile, kc, -1);
+        if (rc) return rc;
+        PCF_CUDA_TRY(cudaEventRecord(e0, h->stream));
+        for (int q = 0; q < 3; ++q)
+            if ((rc = launch_tile<T, HORIZ, EPI, DIFF>(h, a, tile, kc, -1))) return rc;
+        PCF_CUDA_TRY(cudaEventRecord(e1, h->stream));
+        PCF_CUDA_TRY(cudaEventSynchronize(e1));
+        float f = 0;
+        PCF_CUDA_TRY(cudaEventElapsedTime(&f, e0, e1));
+        *ms = f / 3.0;
+        return PCF_OK;
+    };
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    const int tdef = default_tile(d.nx, VMAX);
+    int best_tile = tdef, best_kc = 0;
+    double best = 1e300, def_ms = 0;
+    int rc = PCF_OK;
+    for (int tile = 0; tile < 3 && rc == PCF_OK; ++tile) {
+        const int W = kTileX[tile] * vmax_ok, TY = 128 / kTileX[tile];
+        const long long xyb = (long long)((d.nx + W - 1) / W) * ((d.ny + TY - 1) / TY);
+        const int kd = pick_kc(xyb, d.nz);
+        const int cands[4] = {kd, kd / 2, 2 * kd, 4 * kd};
+        for (int q = 0; q < 4 && rc == PCF_OK; ++q) {
+            const int kc = std::min(cands[q], d.nz);
+            if (kc < 2 || xyb * ((d.nz + kc - 1) / kc) > kMaxPartials) continue;
+            bool seen = false;
+            for (int r = 0; r < q; ++r) seen |= std::min(cands[r], d.nz) == kc;
+            if (seen) continue;
+            double ms = 0;
+            rc = time_cfg(tile, kc, &ms);
+            if (rc) break;
+            if (tile == tdef && q == 0) def_ms = ms;
+            if (ms < best) {
+                best = ms;
+                best_tile = tile;
+                best_kc = kc;
+            }
+        }
+    }
+    h->prof_on = saved_prof;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    TuneRec r;
+    r.device = h->dims.device;
+    r.tile = best_tile;
+    r.e.kernel = family;
+    r.e.nx = d.nx;
+    r.e.ny = d.ny;
+    r.e.nz = d.nz;
+    r.e.tile_x = kTileX[best_tile];
+    r.e.vec = vmax_ok;
+    r.e.levels = best_kc;
+    r.e.ms_best = best;
+    r.e.ms_default = def_ms;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.push_back(r);
+    return PCF_OK;
 }
 
 template <typename T, bool HORIZ, int EPI, bool DIFF = false>
@@ -598,6 +743,31 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
     return PCF_OK;
 }
 
+// Tunes the stencil families that a solve with these settings launches
+// (before its iteration batches are captured).
+static int autotune_handle(pcf_handle *h, const pcf_params *prm) {
+    int rc;
+    if (prm->precision == PCF_PRECISION_MIXED) {
+        if ((rc = tune_stencil<float, false, true>(h, h->d, h->coefB32, h->za32, h->zb32, h->s32))) return rc;
+        if (prm->preconditioner && !prm->multigrid &&
+            (rc = tune_stencil<float, true, false>(h, h->d, h->coef32, h->za32, h->zb32, h->s32)))
+            return rc;
+        if (prm->multigrid && h->mg) {
+            if ((rc = tune_stencil<float, true, false>(h, h->d, h->coef32, h->za32, h->zb32, h->s32))) return rc;
+            if ((rc = tune_stencil<float, false, false>(h, h->d, h->coef32, h->za32, h->zb32, h->s32))) return rc;
+            for (size_t l = 1; l < h->mg->lv.size(); ++l) {
+                const MgLevel &L = h->mg->lv[l];
+                if ((rc = tune_stencil<float, false, false>(h, L.d, L.coef, L.s, L.t, L.b))) return rc;
+                if ((rc = tune_stencil<float, true, false>(h, L.d, L.coef, L.s, L.t, L.b))) return rc;
+            }
+        }
+    } else if (prm->preconditioner) {
+        if ((rc = tune_stencil<double, true, false>(h, h->d, h->coef64, h->za64, h->zb64, h->s64))) return rc;
+    }
+    // FP64 applies: the reference loop and the true residual of the mixed solve
+    return tune_stencil<double, false, false>(h, h->d, h->coef64, h->za64, h->zb64, h->s64);
+}
+
 struct LoopCfg {
     int precond, pc_iters;
     double deta;
@@ -801,12 +971,11 @@ static void clear_graphs(pcf_handle *h) {
 // A complete BiCGSTAB run on A x = b (b in w.r on entry is not required: b
 // is the `b` argument), x0 = 0.  On convergence x <- M x as at
 // apply_bicgstab!.jl:132-135.  Result vector: *xout (x or a z buffer).
+// The part of a run before its iterations: the scalar block and
+// r0 = r = p = b, x = 0 (apply_bicgstab!.jl:44-67).
 template <typename T>
-static int bicgstab_run(pcf_handle *h, const Work<T> &w, const T *b, double tol, int maxit, const LoopCfg &c,
-                        int check_interval, bool precondition_unconverged, T **xout, RunOut *out,
-                        int hist_off = 0, double hist_scale = 1.0, double bnorm64 = 0.0, double ru_delta = 0.0,
-                        int restart_every = 0) {
-    // scalar block
+static int run_start(pcf_handle *h, const Work<T> &w, const T *b, double tol, int maxit, const LoopCfg &c,
+                     int hist_off, double hist_scale, double bnorm64, double ru_delta, int restart_every) {
     KrylovScalars init;
     std::memset(&init, 0, sizeof(init));
     init.tol = tol;
@@ -825,14 +994,59 @@ static int bicgstab_run(pcf_handle *h, const Work<T> &w, const T *b, double tol,
     h->launches += 1;
     k_init<T><<<vec_grid(h->d.n), 256, 0, h->stream>>>(b, w.x, w.r, w.r0, w.p, h->d.n, red(h, w.scal, FIN_INIT));
     PCF_CUDA_TRY(cudaGetLastError());
+    return PCF_OK;
+}
+
+// The part of a run after its iterations (the stream is drained here): the
+// outcome, the residual history and, for the reference form, x <- M x
+// (apply_bicgstab!.jl:132-135).
+template <typename T>
+static int run_finish(pcf_handle *h, const Work<T> &w, const LoopCfg &c, bool precondition_unconverged,
+                      int hist_off, T **xout, RunOut *out) {
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    // the latest status (a batch issued after convergence leaves it unchanged)
+    PCF_CUDA_TRY(cudaMemcpy(h->h_scal, w.scal, sizeof(KrylovScalars), cudaMemcpyDeviceToHost));
+    const KrylovScalars s = *h->h_scal;
+    h->prof_iter = -1;
+    prof_flush(h, s.iter);
+    h->hist_len = std::min(hist_off + s.iter, kHistCap);
+    out->iters = s.iter;
+    out->converged = s.converged;
+    out->status = s.status;
+    out->res = c.reliable ? s.res_true : (s.b_norm > 0 ? s.res / s.b_norm : 0.0);
+    out->b_norm = s.b_norm;
+    out->nupdates = s.nupdates;
+    *xout = w.x;
+    const bool finish = s.converged || (precondition_unconverged && s.status == PCF_OK);
+    if (finish && s.iter > 0 && c.precond && !c.flex) {
+        T *z = nullptr;
+        int rc = precond_apply<T, TH_B>(h, w, w.x, c.pc_iters, c.deta, nullptr, &z);
+        if (rc) return rc;
+        *xout = z;
+    }
+    return PCF_OK;
+}
+
+static GraphKey graph_key(const pcf_handle *h, int tsize, const LoopCfg &c, bool pi, int check_interval) {
+    return GraphKey{tsize, c.precond, c.pc_iters, c.flex, c.reliable, pi, check_interval, c.deta, c.mg,
+                    c.mg && h->mg ? (int)h->mg->lv.size() : 0, c.mg && h->mg ? h->mg->coarse_iters : 0};
+}
+
+// A complete BiCGSTAB run: run_start, the iteration batches, run_finish.
+template <typename T>
+static int bicgstab_run(pcf_handle *h, const Work<T> &w, const T *b, double tol, int maxit, const LoopCfg &c,
+                        int check_interval, bool precondition_unconverged, T **xout, RunOut *out,
+                        int hist_off = 0, double hist_scale = 1.0, double bnorm64 = 0.0, double ru_delta = 0.0,
+                        int restart_every = 0) {
+    int rc0 = run_start<T>(h, w, b, tol, maxit, c, hist_off, hist_scale, bnorm64, ru_delta, restart_every);
+    if (rc0) return rc0;
     if (check_interval < 1) check_interval = 16;
     // Iterations are issued in batches of check_interval; a batch is a CUDA
     // graph (captured once per handle and loop configuration) unless per-launch
     // profiling is on.  The status word of batch b is read back while batch
     // b + 1 is already queued, so the GPU never drains between batches; the
     // batch queued after convergence returns at once.
-    GraphKey key{(int)sizeof(T), c.precond, c.pc_iters, c.flex, c.reliable, w.post != nullptr, check_interval,
-                 c.deta, c.mg, c.mg && h->mg ? (int)h->mg->lv.size() : 0, c.mg && h->mg ? h->mg->coarse_iters : 0};
+    const GraphKey key = graph_key(h, (int)sizeof(T), c, w.post != nullptr, check_interval);
     cudaGraphExec_t gexec = nullptr;
     if (!h->prof_on) {
         int rc = batch_graph<T>(h, w, c, key, &gexec);
@@ -873,28 +1087,7 @@ static int bicgstab_run(pcf_handle *h, const Work<T> &w, const T *b, double tol,
             if (launched >= maxit && inflight == 0) break;
         }
     }
-    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
-    // the latest status (a batch issued after convergence leaves it unchanged)
-    PCF_CUDA_TRY(cudaMemcpy(h->h_scal, w.scal, sizeof(KrylovScalars), cudaMemcpyDeviceToHost));
-    const KrylovScalars s = *h->h_scal;
-    h->prof_iter = -1;
-    prof_flush(h, s.iter);
-    h->hist_len = std::min(hist_off + s.iter, kHistCap);
-    out->iters = s.iter;
-    out->converged = s.converged;
-    out->status = s.status;
-    out->res = c.reliable ? s.res_true : (s.b_norm > 0 ? s.res / s.b_norm : 0.0);
-    out->b_norm = s.b_norm;
-    out->nupdates = s.nupdates;
-    *xout = w.x;
-    const bool finish = s.converged || (precondition_unconverged && s.status == PCF_OK);
-    if (finish && s.iter > 0 && c.precond && !c.flex) {
-        T *z = nullptr;
-        int rc = precond_apply<T, TH_B>(h, w, w.x, c.pc_iters, c.deta, nullptr, &z);
-        if (rc) return rc;
-        *xout = z;
-    }
-    return PCF_OK;
+    return run_finish<T>(h, w, c, precondition_unconverged, hist_off, xout, out);
 }
 
 // ------------------------------------------------------- small kernels --
@@ -979,9 +1172,10 @@ int pcf_params_default(pcf_params *p) {
     p->check_interval = 16;
     p->restart_interval = 1;
     p->multigrid = 0;
-    p->mg_dtau = 1.0;
+    p->mg_dtau = 2.0;
     p->mg_coarse_iterations = 4;
     p->mg_min_columns = 16;
+    p->autotune = 0;
     return PCF_OK;
 }
 
@@ -1324,6 +1518,20 @@ int pcf_apply_multigrid(pcf_handle *h, const double *sin_, double *sout, const p
     return PCF_OK;
 }
 
+int pcf_autotune_entries(pcf_tune_entry *out, int cap, int *count) {
+    if (!count || cap < 0 || (cap > 0 && !out)) return PCF_EINVAL;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    *count = (int)g_tune.size();
+    for (int q = 0; q < cap && q < (int)g_tune.size(); ++q) out[q] = g_tune[q].e;
+    return PCF_OK;
+}
+
+int pcf_autotune_clear(void) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.clear();
+    return PCF_OK;
+}
+
 int pcf_global_dot(pcf_handle *h, const double *a, const double *b, double *out) {
     if (!h || !a || !b || !out) return PCF_EINVAL;
     PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
@@ -1373,6 +1581,7 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
     const int maxit = prm->poisson_iterations;
 
     if (prm->precision != PCF_PRECISION_MIXED) {
+        if (prm->autotune && (rc = autotune_handle(h, prm))) return rc;
         double *x = nullptr;
         RunOut ro;
         rc = bicgstab_run<double>(h, work64(h), h->b64, tol, maxit, c, prm->check_interval, false, &x, &ro);
@@ -1435,6 +1644,7 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
         cm.mg = 1;
         cm.deta = h->mg->lv[0].deta;
     }
+    if (prm->autotune && (rc = autotune_handle(h, prm))) return rc;
     double rel = rnorm / b_norm;
     int restarts = 0;
     for (;;) {
@@ -1629,6 +1839,323 @@ int pcf_profile_read(const pcf_handle *h, int tag, double *ms, long long *count,
     if (ms) *ms = h->prof_acc[tag].ms;
     if (count) *count = h->prof_acc[tag].count;
     if (bytes) *bytes = h->prof_acc[tag].bytes;
+    return PCF_OK;
+}
+
+
+// ============================================================== ensemble ==
+// Mixed-precision solves of several handles (ensemble members, possibly of
+// different grid sizes) advanced together: each member's setup runs on its
+// own stream, then every batch of check_interval iterations of all members
+// is ONE CUDA graph launch (captured once per ensemble and configuration:
+// the members' iteration chains are parallel branches forked from and joined
+// to the ensemble's stream), and one status read-back per batch serves all
+// members.  Members that converge early keep returning at once from their
+// kernels (device-side done flag) until the last one finishes.
+
+struct pcf_ensemble {
+    std::vector<pcf_handle *> m;
+    int device = 0;
+    cudaStream_t origin = nullptr;
+    cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr, t2 = nullptr, done = nullptr;
+    cudaEvent_t slot_ev[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t exec = nullptr;
+    long long graph_launches = 0;
+    long long launches = 0;
+    bool key_valid = false;
+    int key_ci = 0, key_precond = 0, key_pc_iters = 0, key_mg = 0, key_mg_ci = 0, key_mg_min = 0;
+    double key_dtau = 0, key_mg_dtau = 0;
+    KrylovScalars *h_status = nullptr;  // pinned, 2 slots x members
+    double *h_norm = nullptr;           // pinned, members
+};
+
+static LoopCfg ensemble_loop_cfg(pcf_handle *h, const pcf_params *prm) {
+    LoopCfg c;
+    c.precond = prm->preconditioner;
+    c.pc_iters = prm->preconditioner_iterations;
+    c.deta = deta_of(h, prm->dtau);
+    c.flex = 1;
+    c.reliable = 1;
+    c.mg = prm->multigrid ? 1 : 0;
+    if (c.mg) c.deta = h->mg->lv[0].deta;
+    return c;
+}
+
+static int ensemble_capture(pcf_ensemble *e, const pcf_params *prm, int ci) {
+    if (e->exec) {
+        cudaGraphExecDestroy(e->exec);
+        e->exec = nullptr;
+    }
+    std::vector<long long> l0(e->m.size());
+    for (size_t q = 0; q < e->m.size(); ++q) l0[q] = e->m[q]->launches;
+    PCF_CUDA_TRY(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal));
+    int rc = PCF_OK;
+    cudaError_t ce = cudaEventRecord(e->fork, e->origin);
+    for (size_t q = 0; q < e->m.size() && rc == PCF_OK && ce == cudaSuccess; ++q) {
+        pcf_handle *h = e->m[q];
+        ce = cudaStreamWaitEvent(h->stream, e->fork, 0);
+        if (ce != cudaSuccess) break;
+        const LoopCfg c = ensemble_loop_cfg(h, prm);
+        const Work<float> w = work32_pi(h);
+        for (int it = 0; it < ci && rc == PCF_OK; ++it) rc = bicgstab_iteration<float>(h, w, c);
+        if (rc) break;
+        ce = cudaEventRecord(e->join[q], h->stream);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->origin, e->join[q], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(e->origin, &graph);
+    long long nl = 0;
+    for (size_t q = 0; q < e->m.size(); ++q) {
+        nl += e->m[q]->launches - l0[q];
+        e->m[q]->launches = l0[q];  // captured, not launched
+    }
+    if (rc || ce != cudaSuccess || ee != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (rc) return rc;
+        return pcf_set_cuda_error(ce != cudaSuccess ? ce : ee);
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&e->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return pcf_set_cuda_error(ei);
+    e->graph_launches = nl;
+    e->key_valid = true;
+    e->key_ci = ci;
+    e->key_precond = prm->preconditioner;
+    e->key_pc_iters = prm->preconditioner_iterations;
+    e->key_dtau = prm->dtau;
+    e->key_mg = prm->multigrid;
+    e->key_mg_ci = prm->mg_coarse_iterations;
+    e->key_mg_min = prm->mg_min_columns;
+    e->key_mg_dtau = prm->mg_dtau;
+    return PCF_OK;
+}
+
+int pcf_ensemble_destroy(pcf_ensemble *e) {
+    if (!e) return PCF_OK;
+    cudaSetDevice(e->device);
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    cudaEvent_t evs[] = {e->fork, e->t0, e->t1, e->t2, e->done, e->slot_ev[0], e->slot_ev[1]};
+    for (cudaEvent_t x : evs)
+        if (x) cudaEventDestroy(x);
+    for (cudaEvent_t x : e->join)
+        if (x) cudaEventDestroy(x);
+    if (e->h_status) cudaFreeHost(e->h_status);
+    if (e->h_norm) cudaFreeHost(e->h_norm);
+    if (e->origin) cudaStreamDestroy(e->origin);
+    delete e;
+    return PCF_OK;
+}
+
+int pcf_ensemble_create(pcf_ensemble **out, pcf_handle *const *members, int count) {
+    if (!out || !members || count < 1) return PCF_EINVAL;
+    *out = nullptr;
+    for (int q = 0; q < count; ++q) {
+        if (!members[q] || members[q]->dims.device != members[0]->dims.device) return PCF_EINVAL;
+        for (int r = 0; r < q; ++r)
+            if (members[r] == members[q]) return PCF_EINVAL;  // each member owns its buffers
+    }
+    PCF_CUDA_TRY(cudaSetDevice(members[0]->dims.device));
+    pcf_ensemble *e = new pcf_ensemble();
+    e->m.assign(members, members + count);
+    e->device = members[0]->dims.device;
+    e->join.assign(count, nullptr);
+    auto fail = [&](int code) {
+        pcf_ensemble_destroy(e);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&e->origin, cudaStreamNonBlocking) != cudaSuccess) return fail(PCF_ECUDA);
+    cudaEvent_t *evs[] = {&e->fork, &e->t0, &e->t1, &e->t2, &e->done, &e->slot_ev[0], &e->slot_ev[1]};
+    for (cudaEvent_t *x : evs)
+        if (cudaEventCreate(x) != cudaSuccess) return fail(PCF_ECUDA);
+    for (cudaEvent_t &x : e->join)
+        if (cudaEventCreateWithFlags(&x, cudaEventDisableTiming) != cudaSuccess) return fail(PCF_ECUDA);
+    if (cudaMallocHost((void **)&e->h_status, 2 * sizeof(KrylovScalars) * count) != cudaSuccess) return fail(PCF_ENOMEM);
+    if (cudaMallocHost((void **)&e->h_norm, sizeof(double) * count) != cudaSuccess) return fail(PCF_ENOMEM);
+    *out = e;
+    return PCF_OK;
+}
+
+long long pcf_ensemble_launch_count(const pcf_ensemble *e) { return e ? e->launches : 0; }
+
+int pcf_ensemble_solve_device(pcf_ensemble *e, const double *const *d_rhs, const double *const *d_rho,
+                              const double *const *d_betar, const double *const *d_p, const double *dt,
+                              const double *rayleigh_factor, const double *tolref, const pcf_params *prm,
+                              double *const *d_dpip, pcf_result *res) {
+    if (!e || !d_rhs || !d_rho || !d_betar || !dt || !rayleigh_factor || !tolref || !prm || !d_dpip || !res)
+        return PCF_EINVAL;
+    const int n = (int)e->m.size();
+    for (int q = 0; q < n; ++q) {
+        pcf_handle *h = e->m[q];
+        if (!d_rhs[q] || !d_rho[q] || !d_betar[q] || !d_dpip[q] || dt[q] == 0.0) return PCF_EINVAL;
+        if (h->dims.model == PCF_MODEL_COMPRESSIBLE && (!d_p || !d_p[q])) return PCF_EINVAL;
+        if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
+    }
+    // the ensemble advances the mixed-precision iteration only
+    if (prm->precision != PCF_PRECISION_MIXED || prm->learned || (prm->preconditioner && prm->preconditioner_iterations < 1) ||
+        (prm->multigrid && !prm->preconditioner))
+        return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(e->device));
+    const int ci = prm->check_interval < 1 ? 16 : prm->check_interval;
+    const int maxit = prm->poisson_iterations;
+    int rc;
+    PCF_CUDA_TRY(cudaEventRecord(e->t0, e->origin));
+    // setup on every member's stream: inputs, assembly, pivots, multigrid
+    // hierarchy, r = b - A 0 in FP64 with its norm read back asynchronously
+    for (int q = 0; q < n; ++q) {
+        pcf_handle *h = e->m[q];
+        std::memset(&res[q], 0, sizeof(pcf_result));
+        const size_t hb = sizeof(double) * (size_t)h->nh;
+        PCF_CUDA_TRY(cudaStreamWaitEvent(h->stream, e->t0, 0));
+        PCF_CUDA_TRY(cudaEventRecord(h->ev[0], h->stream));
+        PCF_CUDA_TRY(cudaMemcpyAsync(h->rho, d_rho[q], hb, cudaMemcpyDeviceToDevice, h->stream));
+        PCF_CUDA_TRY(cudaMemcpyAsync(h->betar, d_betar[q], hb, cudaMemcpyDeviceToDevice, h->stream));
+        if (d_p && d_p[q]) PCF_CUDA_TRY(cudaMemcpyAsync(h->p, d_p[q], hb, cudaMemcpyDeviceToDevice, h->stream));
+        PCF_CUDA_TRY(cudaMemcpyAsync(h->b64, d_rhs[q], sizeof(double) * h->d.n, cudaMemcpyDeviceToDevice, h->stream));
+        PCF_CUDA_TRY(cudaEventRecord(h->ev[1], h->stream));
+        if ((rc = assemble_device(h, dt[q], rayleigh_factor[q], prm->damp_horizontal_wind_on_rhs))) return rc;
+        if (prm->preconditioner && (rc = ensure_factors(h, deta_of(h, prm->dtau)))) return rc;
+        if (prm->multigrid && (rc = mg_prepare(h, prm))) return rc;
+        if (prm->autotune && (rc = autotune_handle(h, prm))) return rc;
+        PCF_CUDA_TRY(cudaEventRecord(h->ev[2], h->stream));
+        PCF_CUDA_TRY(cudaMemsetAsync(h->x64, 0, sizeof(double) * h->d.n, h->stream));
+        StencilArgs<double> a;
+        a.coef = h->coef64;
+        a.s = h->x64;
+        a.out = h->w64;
+        a.w1 = h->b64;
+        a.deta = 0;
+        a.guard = nullptr;
+        a.red = red(h, nullptr, FIN_STORE, h->dot_out);
+        if ((rc = launch_stencil<double, false, EPI_RESID>(h, a))) return rc;
+        PCF_CUDA_TRY(cudaMemcpyAsync(e->h_norm + q, h->dot_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
+    for (int q = 0; q < n; ++q) PCF_CUDA_TRY(cudaStreamSynchronize(e->m[q]->stream));
+    // the iteration graph, captured with every stream idle
+    if (!e->exec || !e->key_valid || e->key_ci != ci || e->key_precond != prm->preconditioner ||
+        e->key_pc_iters != prm->preconditioner_iterations || e->key_dtau != prm->dtau || e->key_mg != prm->multigrid ||
+        e->key_mg_ci != prm->mg_coarse_iterations || e->key_mg_min != prm->mg_min_columns ||
+        e->key_mg_dtau != prm->mg_dtau) {
+        if ((rc = ensemble_capture(e, prm, ci))) return rc;
+    }
+    std::vector<double> bnorm(n), tol(n);
+    std::vector<char> active(n, 0);
+    int nactive = 0;
+    for (int q = 0; q < n; ++q) {
+        pcf_handle *h = e->m[q];
+        tol[q] = prm->tolerance_is_relative ? prm->tolerance : prm->tolerance / tolref[q];
+        bnorm[q] = std::sqrt(e->h_norm[q] / (double)h->d.n);
+        res[q].b_norm = bnorm[q];
+        if (!std::isfinite(bnorm[q])) {
+            res[q].status = PCF_ENONFINITE;
+            res[q].errflag = 1;
+        } else if (bnorm[q] > 0.0 && 1.0 > tol[q]) {
+            active[q] = 1;
+            nactive += 1;
+        }
+        if (!active[q]) {
+            // the member's kernels in the graph must return at once
+            KrylovScalars idle;
+            std::memset(&idle, 0, sizeof(idle));
+            idle.done = 1;
+            PCF_CUDA_TRY(cudaMemcpyAsync(h->scal32, &idle, sizeof(idle), cudaMemcpyHostToDevice, h->stream));
+            continue;
+        }
+        const LoopCfg c = ensemble_loop_cfg(h, prm);
+        const Work<float> w = work32_pi(h);
+        k_to_float<<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->w64, w.s, h->d.n, 1.0 / bnorm[q]);
+        h->launches += 1;
+        PCF_CUDA_TRY(cudaGetLastError());
+        if ((rc = run_start<float>(h, w, w.s, tol[q], maxit, c, 0, 1.0, bnorm[q], prm->inner_tolerance,
+                                   prm->restart_interval)))
+            return rc;
+    }
+    for (int q = 0; q < n; ++q) {
+        PCF_CUDA_TRY(cudaEventRecord(e->join[q], e->m[q]->stream));
+        PCF_CUDA_TRY(cudaStreamWaitEvent(e->origin, e->join[q], 0));
+    }
+    PCF_CUDA_TRY(cudaEventRecord(e->t1, e->origin));
+    // batches: one graph launch for all members, status of batch b read while b + 1 runs
+    int launched = 0, inflight = 0, slot = 0;
+    bool all_done = nactive == 0;
+    while (!all_done) {
+        if (launched < maxit) {
+            PCF_CUDA_TRY(cudaGraphLaunch(e->exec, e->origin));
+            e->launches += e->graph_launches;
+            launched += ci;
+            for (int q = 0; q < n; ++q)
+                if (active[q])
+                    PCF_CUDA_TRY(cudaMemcpyAsync(e->h_status + slot * n + q, e->m[q]->scal32, sizeof(KrylovScalars),
+                                                 cudaMemcpyDeviceToHost, e->origin));
+            PCF_CUDA_TRY(cudaEventRecord(e->slot_ev[slot], e->origin));
+            slot ^= 1;
+            inflight += 1;
+        }
+        if (inflight == 0) break;
+        if (inflight == 2 || launched >= maxit) {
+            const int old = (inflight == 2) ? slot : slot ^ 1;
+            PCF_CUDA_TRY(cudaEventSynchronize(e->slot_ev[old]));
+            inflight -= 1;
+            bool all = true;
+            for (int q = 0; q < n; ++q)
+                if (active[q] && !e->h_status[old * n + q].done) all = false;
+            all_done = all;
+            if (launched >= maxit && inflight == 0) break;
+        }
+    }
+    PCF_CUDA_TRY(cudaEventRecord(e->done, e->origin));
+    // outcomes; a member whose FP32 iteration broke down is solved again by
+    // the single-handle solver (with its restarts after a breakdown)
+    for (int q = 0; q < n; ++q) {
+        pcf_handle *h = e->m[q];
+        PCF_CUDA_TRY(cudaStreamWaitEvent(h->stream, e->done, 0));
+        const double *x = h->x64;
+        if (active[q]) {
+            const LoopCfg c = ensemble_loop_cfg(h, prm);
+            const Work<float> w = work32_pi(h);
+            float *xe = nullptr;
+            RunOut ro;
+            if ((rc = run_finish<float>(h, w, c, false, 0, &xe, &ro))) return rc;
+            res[q].niter = ro.iters;
+            res[q].nrefine = ro.nupdates;
+            res[q].status = ro.status;
+            res[q].residual = res[q].true_residual = ro.nupdates > 0 ? ro.res : 1.0;
+            res[q].errflag = ro.converged ? 0 : 1;
+            if (!ro.converged && ro.status == PCF_EBREAKDOWN) {
+                pcf_result r2;
+                std::memset(&r2, 0, sizeof(r2));
+                if ((rc = krylov_solve(h, tolref[q], prm, &x, &r2))) return rc;
+                r2.niter += res[q].niter;
+                r2.nrefine += res[q].nrefine;
+                res[q] = r2;
+            }
+        } else if (res[q].status == PCF_OK) {
+            res[q].residual = res[q].true_residual = 0.0;
+        }
+        PCF_CUDA_TRY(cudaEventRecord(h->ev[3], h->stream));
+        if (!res[q].errflag) {
+            k_unscale<<<vec_grid(h->d.n), 256, 0, h->stream>>>(x, h->pbar, h->rhobar, 1.0 / dt[q], h->d.nx, h->d.ny,
+                                                               h->d.nz, h->dims.nbx, h->dims.nby, h->dims.nbz, h->nxx,
+                                                               h->nyy, d_dpip[q], h->dims.nbx, h->dims.nby,
+                                                               h->dims.nbz, h->nxx, h->nyy);
+            h->launches += 1;
+            PCF_CUDA_TRY(cudaGetLastError());
+        }
+        PCF_CUDA_TRY(cudaEventRecord(h->ev[4], h->stream));
+        PCF_CUDA_TRY(cudaEventRecord(e->join[q], h->stream));
+        PCF_CUDA_TRY(cudaStreamWaitEvent(e->origin, e->join[q], 0));
+    }
+    PCF_CUDA_TRY(cudaEventRecord(e->t2, e->origin));
+    PCF_CUDA_TRY(cudaEventSynchronize(e->t2));
+    const float total = elapsed(e->t0, e->t2), loop = elapsed(e->t1, e->done);
+    for (int q = 0; q < n; ++q) {
+        pcf_handle *h = e->m[q];
+        res[q].ms_upload = elapsed(h->ev[0], h->ev[1]);
+        res[q].ms_assemble = elapsed(h->ev[1], h->ev[2]);
+        res[q].ms_solve = loop;
+        res[q].ms_download = elapsed(h->ev[3], h->ev[4]);
+        res[q].ms_total = total;
+    }
     return PCF_OK;
 }
 

@@ -7,6 +7,8 @@ plus the caller-side construction of the grid, background and workloads.
 """
 from . import configs, fields
 from ._lib import PoissonError, load
-from .solver import PoissonNamelist, PoissonSolver, SolveInfo
+from .ensemble import Ensemble
+from .solver import PoissonNamelist, PoissonSolver, SolveInfo, autotune_clear, autotune_entries
 
-__all__ = ["PoissonNamelist", "PoissonSolver", "SolveInfo", "PoissonError", "load", "fields", "configs"]
+__all__ = ["PoissonNamelist", "PoissonSolver", "SolveInfo", "PoissonError", "load", "fields", "configs",
+           "autotune_entries", "autotune_clear", "Ensemble"]

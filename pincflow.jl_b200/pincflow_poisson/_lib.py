@@ -37,7 +37,10 @@ EXPORTS = [
     "pcf_set_operator", "pcf_apply_operator", "pcf_apply_preconditioner", "pcf_bicgstab",
     "pcf_global_dot", "pcf_device_bytes", "pcf_launch_count", "pcf_profile_enable", "pcf_profile_read",
     "pcf_residual_history", "pcf_multigrid_levels", "pcf_multigrid_operator", "pcf_apply_multigrid",
+    "pcf_autotune_entries", "pcf_autotune_clear", "pcf_ensemble_create", "pcf_ensemble_destroy",
+    "pcf_ensemble_solve_device", "pcf_ensemble_launch_count",
 ]
+TUNE_KERNELS = ["total32", "total32_diff", "horiz32", "total64", "horiz64"]
 PROF_TAGS = ["apply32", "apply64", "pseudo32", "pseudo64", "thomas32", "thomas64", "update32", "update64",
              "assemble", "reliable64", "mg"]
 
@@ -58,7 +61,14 @@ class PcfParams(ctypes.Structure):
                 ("max_refinements", ctypes.c_int), ("learned", ctypes.c_int),
                 ("check_interval", ctypes.c_int), ("restart_interval", ctypes.c_int),
                 ("multigrid", ctypes.c_int), ("mg_dtau", ctypes.c_double),
-                ("mg_coarse_iterations", ctypes.c_int), ("mg_min_columns", ctypes.c_int)]
+                ("mg_coarse_iterations", ctypes.c_int), ("mg_min_columns", ctypes.c_int),
+                ("autotune", ctypes.c_int)]
+
+
+class PcfTuneEntry(ctypes.Structure):
+    _fields_ = [("kernel", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("tile_x", ctypes.c_int), ("vec", ctypes.c_int), ("levels", ctypes.c_int),
+                ("ms_best", ctypes.c_double), ("ms_default", ctypes.c_double)]
 
 
 class PcfResult(ctypes.Structure):
@@ -122,6 +132,8 @@ def load(path: str | None = None):
     lib.pcf_multigrid_levels.argtypes = [vp, P(PcfParams), ctypes.c_int, P(ctypes.c_int), P(ctypes.c_int)]
     lib.pcf_multigrid_operator.argtypes = [vp, ctypes.c_int, dp]
     lib.pcf_apply_multigrid.argtypes = [vp, dp, dp, P(PcfParams)]
+    lib.pcf_autotune_entries.argtypes = [P(PcfTuneEntry), ctypes.c_int, P(ctypes.c_int)]
+    lib.pcf_autotune_clear.argtypes = []
     for name in EXPORTS:
         getattr(lib, name).restype = getattr(lib, name).restype or ctypes.c_int
     lib.pcf_strerror.restype = ctypes.c_char_p

@@ -49,9 +49,10 @@ class PoissonNamelist:
     check_interval: int = 16
     restart_interval: int = 1         # mixed: Krylov restart at every n-th reliable update (0: never)
     multigrid: bool = False           # mixed: horizontal aggregation multigrid V-cycle as the preconditioner
-    mg_dtau: float = 1.0              # multigrid: pseudo-time step of the smoother on every level
+    mg_dtau: float = 2.0              # multigrid: pseudo-time step of the smoother on every level
     mg_coarse_iterations: int = 4     # multigrid: smoothing steps on the coarsest level
     mg_min_columns: int = 16          # multigrid: a level with at most this many columns is the coarsest
+    autotune: bool = False            # time the stencil tile shapes of each new grid size on first use
 
     def to_c(self) -> _lib.PcfParams:
         p = _lib.PcfParams()
@@ -74,6 +75,7 @@ class PoissonNamelist:
         p.mg_dtau = float(self.mg_dtau)
         p.mg_coarse_iterations = int(self.mg_coarse_iterations)
         p.mg_min_columns = int(self.mg_min_columns)
+        p.autotune = int(bool(self.autotune))
         return p
 
 
@@ -269,6 +271,25 @@ class PoissonSolver:
                                              ctypes.c_void_p(d_dpip), ctypes.byref(res)),
                    "pcf_solve_device")
         return _info(res)
+
+
+def autotune_entries() -> list:
+    """The stencil tile choices the autotuner has made in this process."""
+    lib = _lib.load()
+    n = ctypes.c_int()
+    _lib.check(lib.pcf_autotune_entries(None, 0, ctypes.byref(n)), "pcf_autotune_entries")
+    arr = (_lib.PcfTuneEntry * max(n.value, 1))()
+    _lib.check(lib.pcf_autotune_entries(arr, n.value, ctypes.byref(n)), "pcf_autotune_entries")
+    out = []
+    for e in arr[:n.value]:
+        d = {name: getattr(e, name) for name, _ in e._fields_}
+        d["kernel"] = _lib.TUNE_KERNELS[e.kernel]
+        out.append(d)
+    return out
+
+
+def autotune_clear():
+    _lib.check(_lib.load().pcf_autotune_clear(), "pcf_autotune_clear")
 
 
 def _info(res: _lib.PcfResult) -> SolveInfo:
