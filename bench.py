@@ -2,7 +2,7 @@
 Poisson solve (PinCFlow.jl PoissonSolver) on B200.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config c2|c5|c1] [--method mg|mixed|fp64]
+                  [--config c2|c5|c1|c4] [--method mg|mixed|fp64]
 
 A step is one complete solve_poisson! (operator assembly, preconditioned
 BiCGSTAB to FP64 true relative residual 1e-10, unscaling into dpip) of the
@@ -43,7 +43,7 @@ WORKLOADS = {
     "c2": "256x256x128 pseudo-incompressible, stretched terrain-following grid, Gaussian mountain 1 km, "
           "isothermal 250 K, RHS N(0,1) seed 12345",
     "c5": "512x512x192 pseudo-incompressible, 20 Gaussian ridges <= 2 km, wave-packet RHS",
-    "c1": "periodic hill 40x1x40 Boussinesq (one of its 200 solves)",
+    "c1": "periodic hill 40x1x40 Boussinesq, the 200 pressure solves of 100 time steps (rayleigh_factor 1, 2)",
     "c4": "32-member uneven ensemble, nx = ny in {64, 96, 128, 192}, nz = nx/2, random Gaussian hills and "
           "stratification, RHS N(0,1) per member",
 }
@@ -70,6 +70,18 @@ def make_workload(name, seed_offset=0, size=None):
     if name == "c1":
         return configs.c1(seed=seed_offset, step=0)
     raise SystemExit(f"unknown config {name}")
+
+
+def max_over_ranks_of(x, device):
+    """The maximum of x over the ranks of the default process group (x itself
+    without one): every multi-GPU time is the slowest rank's."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def load_peaks():
@@ -179,8 +191,69 @@ def oracle_iterations(config):
     return None, None
 
 
+def run_reference_c1(args, world):
+    """The 200 periodic-hill solves on the oracle, all host threads."""
+    from oracle import oracle as O
+    from pincflow_poisson import configs as C
+    O.build()
+    O.set_threads(os.cpu_count())
+    cfgs = [C.c1(seed=0, step=k) for k in range(200)]
+    dom = cfgs[0]["dom"]
+    d = O.dims(dom.nx, dom.ny, dom.nz, dom.nbx)
+    times = []
+    for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        for c in cfgs:
+            O.solve_poisson(d, O.MODELS[c["model"]], c["fields"], c["rho"], c["betar"], c["rhs"], c["dt"],
+                            c["rayleigh_factor"], tolerance=1e-10, tolerance_is_relative=True,
+                            poisson_iterations=20000)
+        if step >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    value = statistics.mean(times)
+    return value, "s", False, O.get_threads(), "per step: all 200 solves, oracle FP64 (assembly + BiCGSTAB)"
+
+
+def run_reference_c4(args, world):
+    """The 32 ensemble members on the oracle: assembly + a few iterations per
+    size class, scaled by the oracle's full-solve iteration count of that
+    class (tests/golden/c4_fp64_oracle.json) and summed over the members."""
+    from pincflow_poisson import configs as C
+    p = os.path.join(REPO, "tests", "golden", "c4_fp64_oracle.json")
+    with open(p) as fh:
+        counts = {int(k): v["niter"] for k, v in json.load(fh)["classes"].items()}
+    sizes = C.c4_sizes()
+    times = []
+    for step in range(args.warmup + args.steps):
+        per = {}
+        for nx in sorted(set(sizes)):
+            t_asm, t_it, used = oracle_sample(C.c4(sizes.index(nx), nx), args.ref_sample_iters, os.cpu_count())
+            per[nx] = t_asm + t_it * counts[nx]
+        if step >= args.warmup:
+            times.append(sum(per[nx] for nx in sizes))
+    value = len(sizes) / statistics.mean(times)
+    return value, "solves/s", True, used, (f"per step: oracle FP64 assembly + {args.ref_sample_iters} BiCGSTAB "
+                                           "iterations per size class, scaled by the oracle's full-solve count "
+                                           "of that class and summed over the 32 members")
+
+
 def run_reference(args, rank, world):
     if rank != 0:
+        return
+    if args.config in ("c1", "c4"):
+        value, unit, hib, used, sample = (run_reference_c1 if args.config == "c1" else run_reference_c4)(args, world)
+        metric = ("time for the 200 pressure solves of 100 steps to FP64 true rel. residual 1e-10, 1 B200"
+                  if args.config == "c1" else
+                  "ensemble solves/s to FP64 true rel. residual 1e-10 (32 uneven members), 1 B200")
+        line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": (value if unit == "s" else 32 / value) * 1e3,
+                "higher_is_better": hib, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": f"{args.config}: {WORKLOADS[args.config]}",
+                           "method": "plain FP64 BiCGSTAB with the reference preconditioner (CPU restatement "
+                                     "of the Julia code)"},
+                "cpu_baseline": {"value": value, "unit": unit, "cores": used, "kind": "port", "sample": sample},
+                "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
         return
     cfg = make_workload(args.config, size=args.size)
     niter, src = oracle_iterations(args.config)
@@ -203,6 +276,100 @@ def run_reference(args, rank, world):
             "cpu_baseline": {"value": value, "unit": "s", "cores": used, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------ periodic hill (c1) --
+
+def run_c1(args, rank, world, local_rank):
+    """C1: one step = the 200 pressure solves of 100 time steps of the periodic
+    hill (2 per step, rayleigh_factor 1 and 2), each with its own seeded
+    right-hand side, through one solver handle."""
+    import torch
+
+    import pincflow_poisson as pcf
+    from pincflow_poisson import configs as C
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    cfgs = [C.c1(seed=rank, step=k) for k in range(200)]
+    dom, f = cfgs[0]["dom"], cfgs[0]["fields"]
+    s = pcf.PoissonSolver(dom, cfgs[0]["model"], device=local_rank)
+    s.set_grid(f)
+    s.set_background(f)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    ins = [(t(c["rhs"]), t(c["rho"]), t(c["betar"])) for c in cfgs]
+    d_dpip = torch.zeros(dom.halo_shape, dtype=torch.float64, device=dev)
+    kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000, residual="true")
+    nl_fast = pcf.PoissonNamelist(**kw, precision="fp64" if args.method == "fp64" else "mixed",
+                                  multigrid=args.method == "mg", mg_dtau=args.mg_dtau)
+    nl_plain = pcf.PoissonNamelist(**kw, precision="fp64")
+
+    def all_solves(nl):
+        ms, it = 0.0, []
+        for c, (r, rho, b) in zip(cfgs, ins):
+            i = s.solve_poisson_device(r.data_ptr(), rho.data_ptr(), b.data_ptr(), c["dt"], c["rayleigh_factor"],
+                                       c["tolref"], nl, d_dpip.data_ptr())
+            if i.errflag:
+                raise RuntimeError(f"solve did not converge: {i}")
+            ms += i.timings_ms["total"]
+            it.append(i.niter)
+        return ms, it
+
+    for _ in range(args.warmup):
+        all_solves(nl_fast)
+    torch.cuda.synchronize()
+    l0 = s.launch_count
+    with ClockSampler(local_rank) as clk:
+        t0 = time.perf_counter()
+        runs = [all_solves(nl_fast) for _ in range(args.steps)]
+        wall = (time.perf_counter() - t0) / args.steps
+    launches = s.launch_count - l0
+    ms = statistics.mean(r[0] for r in runs)
+    plain_ms, plain_it = all_solves(nl_plain)
+    # end to end through the host-array entry point
+    h = [(np.ascontiguousarray(c["rhs"]), np.ascontiguousarray(c["rho"]), np.ascontiguousarray(c["betar"]))
+         for c in cfgs]
+    hd = np.zeros(dom.halo_shape)
+    t0 = time.perf_counter()
+    for c, (r, rho, b) in zip(cfgs, h):
+        s.solve_poisson(r, rho, b, c["dt"], c["rayleigh_factor"], c["tolref"], nl_fast, hd)
+    e2e_s = time.perf_counter() - t0
+    n = dom.nx * dom.ny * dom.nz
+    if rank != 0:
+        s.close()
+        return
+    line = {
+        "metric": "time for the 200 pressure solves of 100 steps to FP64 true rel. residual 1e-10, 1 B200",
+        "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.method == "fp64" else "f32+f64", "data": "synthetic",
+        "config": {"workload": f"c1: {WORKLOADS['c1']}", "method": METHODS[args.method],
+                   "l2": "1600-cell grid: L2-resident by design (latency-bound workload)",
+                   "parallelism": f"replicas x{world}"},
+        "wall_s_per_step": wall, "plain_fp64_s": plain_ms / 1e3, "speedup_vs_plain_fp64": plain_ms / ms,
+        "iterations_mean": statistics.mean(runs[-1][1]), "plain_fp64_iterations_mean": statistics.mean(plain_it),
+        "solves_per_s": world * 200 / (ms / 1e3), "gpu_launches": launches,
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 200 * 8 * (n + 2 * int(np.prod(dom.halo_shape))),
+                "d2h_bytes_per_step": 200 * 8 * n},
+        "roofline": {"bound": "latency", "note": "40x1x40 cells: each kernel moves a few tens of KB, so the solve "
+                     "is bound by launch and dependency latency, not by HBM", "achieved": None, "peak": None,
+                     "unit": "GB/s", "frac": None, "traffic": None},
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        O.build()
+        O.set_threads(1)
+        d = O.dims(dom.nx, dom.ny, dom.nz, dom.nbx)
+        t0 = time.perf_counter()
+        for c in cfgs:
+            O.solve_poisson(d, O.MODELS[c["model"]], c["fields"], c["rho"], c["betar"], c["rhs"], c["dt"],
+                            c["rayleigh_factor"], tolerance=1e-10, tolerance_is_relative=True,
+                            poisson_iterations=20000)
+        line["cpu_baseline"] = {"value": time.perf_counter() - t0, "unit": "s", "cores": 1, "kind": "port",
+                                "sample": "all 200 solves, oracle FP64 (assembly + BiCGSTAB), 1 thread"}
+    print(json.dumps(line), flush=True)
+    s.close()
 
 
 # ---------------------------------------------------------- ensemble (c4) --
@@ -252,12 +419,7 @@ def run_ensemble(args, rank, world, local_rank):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(x, dev)
 
     for _ in range(args.warmup):
         solve_all()
@@ -426,11 +588,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(x, dev)
 
     for _ in range(args.warmup):
         solve_dev(nl_fast)
@@ -459,9 +617,14 @@ def run_ours(args, rank, world, local_rank):
     profiled_ms = statistics.mean(i.timings_ms["total"] for i in prof_infos)
 
     # --- plain FP64 BiCGSTAB on the same inputs ---------------------------
+    fast_dpip = dom.interior(d_dpip.cpu().numpy()).copy()
     barrier()
     plain = [solve_dev(nl_plain) for _ in range(args.plain_steps)]
     barrier()
+    plain_dpip = dom.interior(d_dpip.cpu().numpy()).copy()
+    # both solves leave the constant (null-space) component of dpip free
+    diff = fast_dpip - plain_dpip
+    dev_max = float(np.abs(diff - diff.mean()).max() / np.abs(plain_dpip - plain_dpip.mean()).max())
     plain_s = max_over_ranks(statistics.mean(i.timings_ms["total"] for i in plain)) / 1e3
 
     # --- end to end through the host-array entry point --------------------
@@ -511,11 +674,13 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": f"{args.config}: {WORKLOADS[args.config]}",
                    "method": METHODS[args.method],
                    "convergence": "FP64 true residual RMS(b-Ax)/RMS(b) <= 1e-10",
-                   "l2": "inputs larger than L2 (operator 3.4 GB FP64 + 0.8 GB FP32), no flush",
+                   "l2": f"inputs larger than L2 (operator {25 * n * 8 / 1e9:.1f} GB FP64 + "
+                         f"{25 * n * 4 / 1e9:.1f} GB FP32 x 2 forms vs 126 MB L2), no flush",
                    "parallelism": f"replicas x{world}"},
         "plain_fp64_s": plain_s, "speedup_vs_plain_fp64": plain_s / value,
         "iterations": last.niter, "refinements": last.nrefine, "true_residual": last.true_residual,
         "plain_fp64_iterations": plain[-1].niter,
+        "max_pointwise_dev_vs_plain_fp64": dev_max,
         "solves_per_s": world / value,
         "cell_updates_per_s": world * n * (2 * last.niter) / value,
         "gpu_launches": launches,
@@ -578,6 +743,8 @@ def main():
     try:
         if args.config == "c4":
             run_ensemble(args, rank, world, local_rank)
+        elif args.config == "c1":
+            run_c1(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

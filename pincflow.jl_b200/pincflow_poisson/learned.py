@@ -171,3 +171,68 @@ def train(net: LearnedNet, pairs, epochs: int = 4, lr: float = 1e-3, device: int
         if log:
             log(f"epoch {ep}: mean loss {np.mean(losses[-len(data):]):.4f} ({time.time() - t0:.1f} s)")
     return losses
+
+
+def evaluate(net: LearnedNet, indices, nx=128, ny=128, nz=64, device=0, **namelist):
+    """Iterations and solve times with and without the learned warm start on
+    configs.c3(index) problems: [(index, niter_without, niter_with, ms_without, ms_with)]."""
+    out = []
+    for i in indices:
+        cfg = C.c3(int(i), nx=nx, ny=ny, nz=nz)
+        with PoissonSolver(cfg["dom"], cfg["model"], device=device) as s:
+            s.set_grid(cfg["fields"])
+            s.set_background(cfg["fields"])
+            dpip = np.zeros(cfg["dom"].halo_shape)
+            args = (cfg["rhs"], cfg["rho"], cfg["betar"], cfg["dt"], cfg["rayleigh_factor"], cfg["tolref"])
+            kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=5000, precision="mixed",
+                      residual="true", **namelist)
+            s.solve_poisson(*args, PoissonNamelist(**kw), dpip)  # warm-up (graph capture)
+            a = s.solve_poisson(*args, PoissonNamelist(**kw), dpip)
+            s.attach_network(net)
+            s.solve_poisson(*args, PoissonNamelist(**kw, learned=True), dpip)
+            b = s.solve_poisson(*args, PoissonNamelist(**kw, learned=True), dpip)
+            s.attach_network(None)
+        out.append((int(i), a.niter, b.niter, a.timings_ms["solve"], b.timings_ms["solve"]))
+    return out
+
+
+def main(argv=None):
+    """Training run of the learned warm start on the training configuration
+    (configs.c3): generates the (rhs, solution) pairs with the plain FP64
+    solver, trains with Adam on the GPU, evaluates the warm start on held-out
+    problems, and writes the weights file."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--pairs", type=int, default=512)
+    ap.add_argument("--epochs", type=int, default=4)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--size", default="128x128x64")
+    ap.add_argument("--eval", type=int, default=8, help="held-out problems (configs.c3 indices from 100000)")
+    ap.add_argument("--out", default=None, help="weights file to write")
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    nx, ny, nz = (int(v) for v in a.size.lower().split("x"))
+    t0 = time.time()
+    pairs = training_pairs(range(a.pairs), nx=nx, ny=ny, nz=nz, device=a.device)
+    t1 = time.time()
+    net = LearnedNet(device=a.device, max_columns=nx * ny, seed=0)
+    losses = train(net, pairs, epochs=a.epochs, lr=a.lr, device=a.device,
+                   log=lambda m: print(m, flush=True))
+    t2 = time.time()
+    if a.out:
+        net.save(a.out)
+    held = range(100000, 100000 + a.eval)
+    ev_ref = evaluate(net, held, nx, ny, nz, a.device)
+    ev_mg = evaluate(net, held, nx, ny, nz, a.device, multigrid=True)
+    summary = dict(pairs=len(pairs), size=[nx, ny, nz], generation_s=t1 - t0, training_s=t2 - t1,
+                   steps=len(losses), loss_first_epoch=float(np.mean(losses[:len(pairs)])),
+                   loss_last_epoch=float(np.mean(losses[-len(pairs):])),
+                   warm_start_reference_preconditioner=ev_ref, warm_start_multigrid=ev_mg)
+    print(json.dumps(summary), flush=True)
+    net.close()
+    return summary
+
+
+if __name__ == "__main__":
+    main()
