@@ -717,7 +717,7 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--size", default=None, help="c2 only: NXxNYxNZ instead of 256x256x128 (profiling captures)")
     ap.add_argument("--method", default="mg", choices=sorted(METHODS))
-    ap.add_argument("--mg-dtau", type=float, default=2.0)
+    ap.add_argument("--mg-dtau", type=float, default=2.5)
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--ref-sample-iters", type=int, default=3)
     ap.add_argument("--ref-iterations", type=int, default=450)

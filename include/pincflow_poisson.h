@@ -120,11 +120,11 @@ typedef struct {
     double inner_tolerance;        /* mixed: FP64 reliable update each time the FP32 residual fell by this factor (1e-2) */
     int max_refinements;           /* mixed: cap on restarts of the FP32 iteration after a breakdown (5) */
     int learned;                   /* 0: off; 1: learned warm start + flexible BiCGSTAB */
-    int check_interval;            /* iterations between host checks of the status word (16) */
+    int check_interval;            /* iterations per graph batch between host checks of the status word (4) */
     int restart_interval;          /* mixed: restart the Krylov recurrences at every n-th reliable update (1; 0: never) */
     int multigrid;                 /* mixed: 0: the reference preconditioner; 1: horizontal aggregation multigrid
                                       V-cycle with the reference line relaxation as smoother on every level (0) */
-    double mg_dtau;                /* multigrid: pseudo-time step of the smoother, all levels (1.0) */
+    double mg_dtau;                /* multigrid: pseudo-time step of the smoother, all levels (2.5) */
     int mg_coarse_iterations;      /* multigrid: smoothing steps on the coarsest level (4) */
     int mg_min_columns;            /* multigrid: a level with at most this many columns is the coarsest (16) */
     int autotune;                  /* 1: time the stencil tile shapes of every new grid size on first use and keep

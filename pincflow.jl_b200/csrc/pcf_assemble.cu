@@ -32,8 +32,11 @@ struct AssembleArgs {
     int nx, ny, nz, nxx, nyy, nbx, nby, nbz;
     int z_size, ko, model, damp_h;
     double dx, dy, dz, dt, rf;
+    double rdx, rdy, rdz;  // 1 / dx, 1 / dy, 1 / dz
     double gamma, kappa, rsp, pref;
     const double *jac, *met13, *met23, *met33, *pbar, *rhobar, *thetabar, *n2, *rho, *betar, *p;
+    const double *fch;   // fcscal = sqrt(pbar^2 / rhobar) on the haloed grid (computed with the background)
+    const double *rfch;  // 1 / fcscal, same grid
     double *coef64;
     float *coef32;
 };
@@ -82,16 +85,16 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
     auto M23 = [&](int di, int dj, int dk) { return __ldg(a.met23 + h + di * sx + dj * sy + dk * sz); };
     auto M33 = [&](int di, int dj, int dk) { return __ldg(a.met33 + h + di * sx + dj * sy + dk * sz); };
     auto N2 = [&](int dk) { return __ldg(a.n2 + h + dk * sz); };
-    auto FC = [&](int di, int dj, int dk) {  // fcscal = sqrt(pbar^2 / rhobar)
-        const double pb = PB(di, dj, dk);
-        return sqrt(pb * pb / RB(di, dj, dk));
-    };
+    auto RFC = [&](int di, int dj, int dk) { return __ldg(a.rfch + h + di * sx + dj * sy + dk * sz); };
     // Jacobian-weighted value at the w-level between dk and dk + up (up = +-1):
-    // (J(dk+up) X(dk) + J(dk) X(dk+up)) / (J(dk) + J(dk+up))
-    auto zint = [&](double xk, double xn, double jk, double jn) { return (jn * xk + jk * xn) / (jk + jn); };
+    // (J(dk+up) X(dk) + J(dk) X(dk+up)) / (J(dk) + J(dk+up)); rj = 1 / (J(dk) + J(dk+up)).
+    // Divisions are the kernel's main cost in FP64, so every repeated
+    // denominator is inverted once.
+    auto zint = [&](double xk, double xn, double jk, double jn, double rj) { return (jn * xk + jk * xn) * rj; };
 
     const double dt2 = a.dt * a.dt;
     const double jc = J(0, 0, 0), ju = J(0, 0, 1), jd = J(0, 0, -1);
+    const double rju = 1.0 / (jc + ju), rjd = 1.0 / (jc + jd);
     const double jacinv = 1.0 / jc;
     const double pc = PB(0, 0, 0);
     const double jpc = jc * pc;
@@ -109,16 +112,16 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
     const double fwu = fw(0), fwd = fw(-1);
 
     // vertical face quantities
-    const double pudiv = jc * ju * (pc + PB(0, 0, 1)) / (jc + ju);
-    const double pddiv = jc * jd * (pc + PB(0, 0, -1)) / (jc + jd);
-    const double n2u = zint(N2(0), N2(1), jc, ju), n2d = zint(N2(0), N2(-1), jc, jd);
-    const double facu = 1.0 + a.dt * zint(BR(0, 0, 0), BR(0, 0, 1), jc, ju) * a.rf;
-    const double facd = 1.0 + a.dt * zint(BR(0, 0, 0), BR(0, 0, -1), jc, jd) * a.rf;
+    const double pudiv = jc * ju * (pc + PB(0, 0, 1)) * rju;
+    const double pddiv = jc * jd * (pc + PB(0, 0, -1)) * rjd;
+    const double n2u = zint(N2(0), N2(1), jc, ju, rju), n2d = zint(N2(0), N2(-1), jc, jd, rjd);
+    const double facu = 1.0 + a.dt * zint(BR(0, 0, 0), BR(0, 0, 1), jc, ju, rju) * a.rf;
+    const double facd = 1.0 + a.dt * zint(BR(0, 0, 0), BR(0, 0, -1), jc, jd, rjd) * a.rf;
     const double impu = 1.0 / (facu + fwu * n2u * dt2);
     const double impd = 1.0 / (facd + fwd * n2d * dt2);
     // buoyancy-coupling factors shared by every horizontal face
-    const double cu = jacinv / a.dz * pudiv * impu * fwu * n2u * dt2 * 0.5;
-    const double cd = jacinv / a.dz * pddiv * impd * fwd * n2d * dt2 * 0.5;
+    const double cu = jacinv * a.rdz * pudiv * impu * fwu * n2u * dt2 * 0.5;
+    const double cd = jacinv * a.rdz * pddiv * impd * fwd * n2d * dt2 * 0.5;
 
     const int kg = a.ko + k;
     const bool bot = kg == a.nbz, top = kg == a.z_size + a.nbz - 1;
@@ -155,7 +158,7 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
         const int dj = dir == 2 ? 1 : (dir == 3 ? -1 : 0);
         const int cn = dir == 0 ? CR : (dir == 1 ? CL : (dir == 2 ? CF : CB));
         const double sgn = (dir == 0 || dir == 2) ? 1.0 : -1.0;  // outward normal
-        const double dh = dir < 2 ? a.dx : a.dy;
+        const double rdh = dir < 2 ? a.rdx : a.rdy;
         const double *met = dir < 2 ? a.met13 : a.met23;
         auto MH = [&](int dk) { return __ldg(met + h + dk * sz); };
         auto MHn = [&](int dk) { return __ldg(met + h + di * sx + dj * sy + dk * sz); };
@@ -166,69 +169,73 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
             const double pgra = 0.5 * (PB(0, 0, dl) + PB(di, dj, dl));
             const double rho_e = 0.5 * (RO(0, 0, dl) + RO(di, dj, dl) + RB(0, 0, dl) + RB(di, dj, dl));
             const double fac = a.damp_h ? 1.0 + a.dt * 0.5 * (BR(0, 0, dl) + BR(di, dj, dl)) * a.rf : 1.0;
-            const double imp_over_rho = (1.0 / fac) / rho_e;
+            const double imp_over_rho = 1.0 / (fac * rho_e);
             double g;
             if (dl == 0) {
                 // gedge{r,l,f,b} (:426-639): horizontal gradient plus the two vertical couplings
                 const double pdiv = 0.5 * (jpc + J(di, dj, 0) * PB(di, dj, 0));
-                g = sgn * jacinv / dh * pdiv;
-                if (!top) g += cu * MH(0) * ju / (jc + ju);
-                if (!bot) g -= cd * MH(0) * jd / (jc + jd);
+                g = sgn * jacinv * rdh * pdiv;
+                if (!top) g += cu * MH(0) * ju * rju;
+                if (!bot) g -= cd * MH(0) * jd * rjd;
                 g *= imp_over_rho;
             } else if (dl == 1) {
                 // guedge{r,l,f,b} (:656-722)
-                g = cu * MH(1) * jc / (jc + ju) * imp_over_rho;
+                g = cu * MH(1) * jc * rju * imp_over_rho;
             } else {
                 // gdedge{r,l,f,b} (:725-791)
-                g = -cd * MH(-1) * jc / (jc + jd) * imp_over_rho;
+                g = -cd * MH(-1) * jc * rjd * imp_over_rho;
             }
             const double flux = g * pgra;
             const double metf = 0.5 * (MH(dl) + MHn(dl));
             // horizontal difference (s_hi - s_lo)/dh, hi = neighbour for r/f, cell for l/b
-            const double wh = flux / dh;
+            const double wh = flux * rdh;
             A[cn][dl + 2] += sgn * wh;
             A[CC][dl + 2] -= sgn * wh;
-            add_vz(CC, cn, dl, flux * metf / a.dz);
+            add_vz(CC, cn, dl, flux * metf * a.rdz);
         }
     }
 
     // ---- the 2 vertical faces ------------------------------------------------
     if (!top) {  // G(k + 1/2) (:642-646)
-        const double rho_u = zint(RO(0, 0, 0), RO(0, 0, 1), jc, ju) + zint(RB(0, 0, 0), RB(0, 0, 1), jc, ju);
-        const double g = jacinv / a.dz * pudiv * impu / rho_u;
-        const double flux = g * zint(pc, PB(0, 0, 1), jc, ju);
-        const double w33 = flux * zint(M33(0, 0, 0), M33(0, 0, 1), jc, ju) / a.dz;
+        const double rho_u =
+            zint(RO(0, 0, 0), RO(0, 0, 1), jc, ju, rju) + zint(RB(0, 0, 0), RB(0, 0, 1), jc, ju, rju);
+        const double g = jacinv * a.rdz * pudiv * impu / rho_u;
+        const double flux = g * zint(pc, PB(0, 0, 1), jc, ju, rju);
+        const double w33 = flux * zint(M33(0, 0, 0), M33(0, 0, 1), jc, ju, rju) * a.rdz;
         A[CC][3] += w33;
         A[CC][2] -= w33;
-        const double w13 = flux * zint(M13(0, 0, 0), M13(0, 0, 1), jc, ju) * 0.5 / a.dx;
-        const double w23 = flux * zint(M23(0, 0, 0), M23(0, 0, 1), jc, ju) * 0.5 / a.dy;
+        const double w13 = flux * zint(M13(0, 0, 0), M13(0, 0, 1), jc, ju, rju) * 0.5 * a.rdx;
+        const double w23 = flux * zint(M23(0, 0, 0), M23(0, 0, 1), jc, ju, rju) * 0.5 * a.rdy;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int di = q == 0 ? 1 : (q == 1 ? -1 : 0), dj = q == 2 ? 1 : (q == 3 ? -1 : 0);
             const int cn = q == 0 ? CR : (q == 1 ? CL : (q == 2 ? CF : CB));
             const double w = (q < 2 ? w13 : w23) * ((q == 0 || q == 2) ? 1.0 : -1.0);
             const double j0 = J(di, dj, 0), j1 = J(di, dj, 1);
-            A[cn][2] += w * j1 / (j0 + j1);
-            A[cn][3] += w * j0 / (j0 + j1);
+            const double r01 = w / (j0 + j1);
+            A[cn][2] += j1 * r01;
+            A[cn][3] += j0 * r01;
         }
     }
     if (!bot) {  // G(k - 1/2) (:649-653)
-        const double rho_d = zint(RO(0, 0, 0), RO(0, 0, -1), jc, jd) + zint(RB(0, 0, 0), RB(0, 0, -1), jc, jd);
-        const double g = -jacinv / a.dz * pddiv * impd / rho_d;
-        const double flux = g * zint(pc, PB(0, 0, -1), jc, jd);
-        const double w33 = flux * zint(M33(0, 0, 0), M33(0, 0, -1), jc, jd) / a.dz;
+        const double rho_d =
+            zint(RO(0, 0, 0), RO(0, 0, -1), jc, jd, rjd) + zint(RB(0, 0, 0), RB(0, 0, -1), jc, jd, rjd);
+        const double g = -jacinv * a.rdz * pddiv * impd / rho_d;
+        const double flux = g * zint(pc, PB(0, 0, -1), jc, jd, rjd);
+        const double w33 = flux * zint(M33(0, 0, 0), M33(0, 0, -1), jc, jd, rjd) * a.rdz;
         A[CC][2] += w33;
         A[CC][1] -= w33;
-        const double w13 = flux * zint(M13(0, 0, 0), M13(0, 0, -1), jc, jd) * 0.5 / a.dx;
-        const double w23 = flux * zint(M23(0, 0, 0), M23(0, 0, -1), jc, jd) * 0.5 / a.dy;
+        const double w13 = flux * zint(M13(0, 0, 0), M13(0, 0, -1), jc, jd, rjd) * 0.5 * a.rdx;
+        const double w23 = flux * zint(M23(0, 0, 0), M23(0, 0, -1), jc, jd, rjd) * 0.5 * a.rdy;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int di = q == 0 ? 1 : (q == 1 ? -1 : 0), dj = q == 2 ? 1 : (q == 3 ? -1 : 0);
             const int cn = q == 0 ? CR : (q == 1 ? CL : (q == 2 ? CF : CB));
             const double w = (q < 2 ? w13 : w23) * ((q == 0 || q == 2) ? 1.0 : -1.0);
             const double j0 = J(di, dj, 0), j1 = J(di, dj, -1);
-            A[cn][2] += w * j1 / (j0 + j1);
-            A[cn][1] += w * j0 / (j0 + j1);
+            const double r01 = w / (j0 + j1);
+            A[cn][2] += j1 * r01;
+            A[cn][1] += j0 * r01;
         }
     }
 
@@ -240,14 +247,14 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
     (void)case_k;
 
     // ---- scaling by 1 / (fcscal fcscal_neighbour) and store ----------------
-    const double fcc = FC(0, 0, 0);
+    const double rfcc = RFC(0, 0, 0);
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
         const int di = c == CR ? 1 : (c == CL ? -1 : 0);
         const int dj = c == CF ? 1 : (c == CB ? -1 : 0);
 #pragma unroll
         for (int z = 0; z < 5; ++z) {
-            const double v = A[c][z] / fcc / FC(di, dj, z - 2);
+            const double v = A[c][z] * rfcc * RFC(di, dj, z - 2);
             const long long o = (long long)kPlane[c][z] * n + cell;
             a.coef64[o] = v;
             a.coef32[o] = (float)v;
@@ -297,6 +304,9 @@ int pcf_launch_assemble(pcf_handle *h, double dt, double rf, int damp_h) {
     a.jac = h->jac; a.met13 = h->met13; a.met23 = h->met23; a.met33 = h->met33;
     a.pbar = h->pbar; a.rhobar = h->rhobar; a.thetabar = h->thetabar; a.n2 = h->n2;
     a.rho = h->rho; a.betar = h->betar; a.p = h->p;
+    a.fch = h->fch;
+    a.rfch = h->rfch;
+    a.rdx = 1.0 / h->dx; a.rdy = 1.0 / h->dy; a.rdz = 1.0 / h->dz;
     a.coef64 = h->coef64; a.coef32 = h->coef32;
     const long long n = h->d.n;
     const int bs = 128;

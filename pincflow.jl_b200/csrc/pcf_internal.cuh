@@ -134,6 +134,7 @@ struct pcf_handle {
     // difference form of the FP32 operator for pi = s / fcscal (k_build_diff)
     float *coefB32;
     double *fc64, *fch;  // fcscal on the interior and on the haloed grid
+    double *rfch;        // 1 / fcscal on the haloed grid
     float *rfc32;        // 1 / fcscal on the interior
     double fac_deta;  // d_eta the factors were built with (NaN: none)
     // FP64 Krylov vectors

@@ -772,11 +772,16 @@ __global__ void __launch_bounds__(128) k_build_diff(const double *__restrict__ A
     rfc32[c] = (float)(1.0 / fch[h]);
 }
 
-// fcscal = sqrt(pbar^2 / rhobar) on the haloed grid, or 1 where no background is set.
+// fcscal = sqrt(pbar^2 / rhobar) and its reciprocal on the haloed grid, or 1
+// where no background is set.
 __global__ void k_fcscal_halo(const double *__restrict__ pbar, const double *__restrict__ rhobar, double *out,
-                              long long nh, int have_background) {
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nh; q += (long long)gridDim.x * blockDim.x)
-        out[q] = have_background ? sqrt(pbar[q] * pbar[q] / rhobar[q]) : 1.0;
+                              double *rout, long long nh, int have_background) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nh;
+         q += (long long)gridDim.x * blockDim.x) {
+        const double f = have_background ? sqrt(pbar[q] * pbar[q] / rhobar[q]) : 1.0;
+        out[q] = f;
+        rout[q] = 1.0 / f;
+    }
 }
 
 // Reliable update, step 3 (after r64 = b - A x64 in FP64): r32 = r64 / bnorm64

@@ -384,10 +384,23 @@ static double deta_of(const pcf_handle *h, double dtau) {
 
 // Difference-form FP32 operator (k_build_diff) from the FP64 operator; the
 // variable is pi = s / fcscal, with fcscal = 1 when no background is set.
-static int build_diff(pcf_handle *h, int have_background) {
-    h->launches += 2;
-    k_fcscal_halo<<<vec_grid(h->nh), 256, 0, h->stream>>>(h->pbar, h->rhobar, h->fch, h->nh, have_background);
+// fcscal on the haloed grid from the background (or 1 without one); the
+// assembly and the difference form read it.
+static int fcscal_halo(pcf_handle *h, int have_background) {
+    h->launches += 1;
+    k_fcscal_halo<<<vec_grid(h->nh), 256, 0, h->stream>>>(h->pbar, h->rhobar, h->fch, h->rfch, h->nh,
+                                                           have_background);
     PCF_CUDA_TRY(cudaGetLastError());
+    return PCF_OK;
+}
+
+static int build_diff(pcf_handle *h, int have_background) {
+    // with a background, fch was computed when it was set
+    if (!have_background) {
+        int rc = fcscal_halo(h, 0);
+        if (rc) return rc;
+    }
+    h->launches += 1;
     k_build_diff<<<(unsigned)((h->d.n + 127) / 128), 128, 0, h->stream>>>(
         h->coef64, h->fch, h->d.nx, h->d.ny, h->d.nz, h->dims.nbx, h->dims.nby, h->dims.nbz, h->nxx, h->nyy,
         h->coefB32, h->fc64, h->rfc32);
@@ -1169,10 +1182,10 @@ int pcf_params_default(pcf_params *p) {
     p->inner_tolerance = 1.0e-2;
     p->max_refinements = 5;
     p->learned = 0;
-    p->check_interval = 16;
+    p->check_interval = 4;
     p->restart_interval = 1;
     p->multigrid = 0;
-    p->mg_dtau = 2.0;
+    p->mg_dtau = 2.5;
     p->mg_coarse_iterations = 4;
     p->mg_min_columns = 16;
     p->autotune = 0;
@@ -1191,7 +1204,7 @@ int pcf_destroy(pcf_handle *h) {
     int dev = h->dims.device;
     cudaSetDevice(dev);
     void *ptrs[] = {h->jac, h->met13, h->met23, h->met33, h->pbar, h->rhobar, h->thetabar, h->n2, h->rho, h->betar,
-                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch,
+                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch,
                     h->x64, h->r64, h->r064, h->p64, h->v64, h->s64,
                     h->t64, h->za64, h->zb64, h->b64, h->w64, h->x32, h->r32, h->r032, h->p32, h->v32, h->s32,
                     h->t32, h->za32, h->zb32, h->zc32, h->zd32, h->partials, h->ticket, h->scal64, h->scal32,
@@ -1269,6 +1282,7 @@ int pcf_create(pcf_handle **out, const pcf_dims *dims) {
     if ((rc = dalloc(h, (void **)&h->fc64, n8))) return fail(rc);
     if ((rc = dalloc(h, (void **)&h->rfc32, n4))) return fail(rc);
     if ((rc = dalloc(h, (void **)&h->fch, nh8))) return fail(rc);
+    if ((rc = dalloc(h, (void **)&h->rfch, nh8))) return fail(rc);
     double **v64[] = {&h->x64, &h->r64, &h->r064, &h->p64, &h->v64, &h->s64, &h->t64, &h->za64, &h->zb64, &h->b64,
                       &h->w64};
     for (double **v : v64)
@@ -1323,6 +1337,8 @@ int pcf_set_background(pcf_handle *h, const double *pbar, const double *rhobar, 
     PCF_CUDA_TRY(cudaMemcpyAsync(h->rhobar, rhobar, b, cudaMemcpyHostToDevice, h->stream));
     PCF_CUDA_TRY(cudaMemcpyAsync(h->n2, n2, b, cudaMemcpyHostToDevice, h->stream));
     if (thetabar) PCF_CUDA_TRY(cudaMemcpyAsync(h->thetabar, thetabar, b, cudaMemcpyHostToDevice, h->stream));
+    int rc = fcscal_halo(h, 1);
+    if (rc) return rc;
     PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
     h->background_set = 1;
     return PCF_OK;

@@ -46,10 +46,10 @@ class PoissonNamelist:
     inner_tolerance: float = 1.0e-2   # mixed: residual drop between FP64 reliable updates
     max_refinements: int = 5          # mixed: restarts of the FP32 iteration after a breakdown
     learned: bool = False
-    check_interval: int = 16
+    check_interval: int = 4
     restart_interval: int = 1         # mixed: Krylov restart at every n-th reliable update (0: never)
     multigrid: bool = False           # mixed: horizontal aggregation multigrid V-cycle as the preconditioner
-    mg_dtau: float = 2.0              # multigrid: pseudo-time step of the smoother on every level
+    mg_dtau: float = 2.5              # multigrid: pseudo-time step of the smoother on every level
     mg_coarse_iterations: int = 4     # multigrid: smoothing steps on the coarsest level
     mg_min_columns: int = 16          # multigrid: a level with at most this many columns is the coarsest
     autotune: bool = False            # time the stencil tile shapes of each new grid size on first use

@@ -75,14 +75,15 @@ def test_vcycle_matches_oracle(name, solvers, oracle, pcf):
     assert rel_err(got, want) < 1e-4, rel_err(got, want)
 
 
+@pytest.mark.parametrize("dtau", [2.0, 2.5])
 @pytest.mark.parametrize("name", CASES)
-def test_multigrid_solve_reaches_fp64_residual(name, solvers, oracle, pcf):
+def test_multigrid_solve_reaches_fp64_residual(name, dtau, solvers, oracle, pcf):
     cfg, s = solvers(name)
     d, coef = oracle_operator(oracle, cfg)
     s.set_operator(coef)
     rhs = consistent_rhs(oracle, cfg)
     kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=4000, precision="mixed")
-    got, info = s.apply_bicgstab(rhs, 1.0, pcf.PoissonNamelist(**kw, **MG))
+    got, info = s.apply_bicgstab(rhs, 1.0, pcf.PoissonNamelist(**kw, **dict(MG, mg_dtau=dtau)))
     assert not info.errflag, info
     assert info.true_residual <= 1e-10
     r = rhs - oracle.apply_operator(d, coef, got)
