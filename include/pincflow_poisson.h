@@ -197,6 +197,21 @@ int pcf_apply_operator(pcf_handle *h, const double *sin_, double *ls, int mode, 
 
 /* apply_preconditioner!: sout = M sin with prm->dtau and
  * prm->preconditioner_iterations; interior arrays. */
+/* compute_lhs! (src/PoissonSolver/compute_lhs!.jl:68-160 Boussinesq /
+ * PseudoIncompressible, :162-223 Compressible): rhs (interior, nx*ny*nz) =
+ * the scaled divergence of the staggered winds u, v, w (haloed arrays of the
+ * reference's predictands; mass fluxes in the Compressible model) and tolref
+ * = RMS(rhs) / RMS(bu, bv, bw).  heating (interior, or NULL for zero) is the
+ * Compressible model's compute_volume_force(state, i, j, k, P()); the other
+ * models ignore it.  A zero divergence gives tolref = 1.  Needs the grid and
+ * background.  Returns PCF_ENONFINITE where the reference raises (or on
+ * non-finite sums).  The _device variant takes device pointers (rhs may be
+ * the input of pcf_solve_device). */
+int pcf_compute_lhs(pcf_handle *h, const double *u, const double *v, const double *w,
+                    const double *heating, double *rhs, double *tolref);
+int pcf_compute_lhs_device(pcf_handle *h, const double *d_u, const double *d_v, const double *d_w,
+                           const double *d_heating, double *d_rhs, double *tolref);
+
 int pcf_apply_preconditioner(pcf_handle *h, const double *sin_, double *sout,
                              const pcf_params *prm, int precision);
 

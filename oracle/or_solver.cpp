@@ -373,4 +373,49 @@ double or_compute_lhs(const or_dims *d, double dx, double dy, double dz, double 
     return NAN;  // the reference raises here
 }
 
+double or_compute_lhs_compressible(const or_dims *d, double dx, double dy, double dz, double ma,
+                                   double kappa, const double *jac, const double *pbar,
+                                   const double *rhobar, const double *u, const double *v,
+                                   const double *w, const double *heating, double *rhs) {
+    const int nx = d->nx, ny = d->ny, nz = d->nz;
+    const int nxx = nx + 2 * d->nbx, nyy = ny + 2 * d->nby;
+    const long vol = (long)nx * ny * nz;
+    std::vector<double> norm2(vol);
+    auto H = [&](int a, int b, int c) {
+        return (size_t)a + (size_t)nxx * ((size_t)b + (size_t)nyy * (size_t)c);
+    };
+    // compute_lhs!.jl:177-203
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = d->nbz; k < d->nbz + nz; ++k)
+        for (int j = d->nby; j < d->nby + ny; ++j)
+            for (int i = d->nbx; i < d->nbx + nx; ++i) {
+                const double fcscal = std::sqrt(std::pow(pbar[H(i, j, k)], 2.0) / rhobar[H(i, j, k)]);
+                const double ur = u[H(i, j, k)], ul = u[H(i - 1, j, k)];
+                const double vf = v[H(i, j, k)], vb = v[H(i, j - 1, k)];
+                const double wu = w[H(i, j, k)], wd = w[H(i, j, k - 1)];
+                const size_t n = (size_t)(i - d->nbx) +
+                                 (size_t)nx * ((size_t)(j - d->nby) + (size_t)ny * (k - d->nbz));
+                const double ma2 = std::pow(ma, 2.0);
+                double heat = (heating ? heating[n] : 0.0) * ma2 * kappa;
+                double bu = (ur - ul) / dx / jac[H(i, j, k)] * ma2 * kappa;
+                double bv = (vf - vb) / dy / jac[H(i, j, k)] * ma2 * kappa;
+                double bw = (wu - wd) / dz / jac[H(i, j, k)] * ma2 * kappa;
+                bu /= fcscal;
+                bv /= fcscal;
+                bw /= fcscal;
+                heat /= fcscal;
+                rhs[n] = bu + bv + bw - heat;
+                norm2[n] = bu * bu + bv * bv + bw * bw + heat * heat;
+            }
+    // :205-222
+    const double nn = (double)nx * ny * d->z_size;
+    double divl2 = global_sum(vol, [&](long i) { return rhs[i] * rhs[i]; });
+    divl2 = std::sqrt(divl2 / nn);
+    double divl2_norm = global_sum(vol, [&](long i) { return norm2[i]; });
+    divl2_norm = std::sqrt(divl2_norm / nn);
+    if (divl2_norm != 0.0) return divl2 / divl2_norm;
+    if (divl2 == 0.0) return 1.0;
+    return NAN;  // the reference raises here
+}
+
 }  // extern "C"

@@ -50,6 +50,7 @@ def lib():
         d = ctypes.POINTER(ctypes.c_double)
         _lib.or_dot.restype = ctypes.c_double
         _lib.or_compute_lhs.restype = ctypes.c_double
+        _lib.or_compute_lhs_compressible.restype = ctypes.c_double
         _lib.or_grid.restype = ctypes.c_int
         _lib.or_solve_poisson.restype = ctypes.c_int
         del d
@@ -185,14 +186,18 @@ def solve_poisson(d: Dims, model, f: dict, rho, betar, rhs, dt, rayleigh_factor,
     return dpip, dict(errflag=bool(out[0]), niter=int(out[1]), residual=out[2], b_norm=out[3])
 
 
-def compute_lhs(d: Dims, f: dict, u, v, w):
+def compute_lhs(d: Dims, f: dict, u, v, w, model="PseudoIncompressible", heating=None):
+    """compute_lhs!: (rhs, tolref); Compressible takes the heating field (interior, None: 0)."""
     c = constants()
     rhs = np.zeros(interior_shape(d))
-    tolref = lib().or_compute_lhs(ctypes.byref(d), ctypes.c_double(f["dx"]),
-                                  ctypes.c_double(f["dy"]), ctypes.c_double(f["dz"]),
-                                  ctypes.c_double(c["ma"]), ctypes.c_double(c["kappa"]),
-                                  _p(f["jac"]), _p(f["pbar"]), _p(f["rhobar"]), _p(u), _p(v),
-                                  _p(w), _p(rhs))
+    args = [ctypes.byref(d), ctypes.c_double(f["dx"]), ctypes.c_double(f["dy"]), ctypes.c_double(f["dz"]),
+            ctypes.c_double(c["ma"]), ctypes.c_double(c["kappa"]), _p(f["jac"]), _p(f["pbar"]),
+            _p(f["rhobar"]), _p(u), _p(v), _p(w)]
+    if model == "Compressible":
+        h = None if heating is None else np.ascontiguousarray(heating, dtype=np.float64)
+        tolref = lib().or_compute_lhs_compressible(*args, _pn(h), _p(rhs))
+    else:
+        tolref = lib().or_compute_lhs(*args, _p(rhs))
     return rhs, tolref
 
 

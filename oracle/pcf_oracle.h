@@ -136,6 +136,15 @@ double or_compute_lhs(const or_dims *d, double dx, double dy, double dz, double 
                       const double *rhobar, const double *u, const double *v,
                       const double *w, double *rhs);
 
+/* compute_lhs! (Compressible), src/PoissonSolver/compute_lhs!.jl:162-223.
+ * u, v, w are the staggered mass fluxes; heating (interior, may be NULL for
+ * zero) is compute_volume_force(state, i, j, k, P()), which the caller
+ * supplies.  Returns tolref as or_compute_lhs. */
+double or_compute_lhs_compressible(const or_dims *d, double dx, double dy, double dz, double ma,
+                                   double kappa, const double *jac, const double *pbar,
+                                   const double *rhobar, const double *u, const double *v,
+                                   const double *w, const double *heating, double *rhs);
+
 /* Helpers for tests and the CPU baseline. */
 double or_dot(long n, const double *a, const double *b); /* pairwise FP64 sum */
 void or_set_threads(int n);

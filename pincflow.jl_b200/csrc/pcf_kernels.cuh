@@ -803,6 +803,58 @@ __global__ void __launch_bounds__(256) k_ru_convert(const double *__restrict__ r
     reduce_finalize<1>(red, s);
 }
 
+// compute_lhs! (src/PoissonSolver/compute_lhs!.jl:68-223): the scaled
+// divergence of the staggered winds (Boussinesq / PseudoIncompressible: of
+// J P u on the cell faces; Compressible: of the mass fluxes, minus the
+// caller's heating), with the sums of b^2 and of bu^2 + bv^2 + bw^2 (+ heat^2)
+// that make tolref, reduced deterministically into red.out[0..1].
+struct LhsArgs {
+    int nx, ny, nz, nxx, nyy, nbx, nby, nbz, compressible;
+    double rdx, rdy, rdz, c;  // c = Ma^2 kappa
+    const double *jac, *pbar, *rfch, *u, *v, *w, *heating;
+    double *rhs;
+    ReduceCtx red;
+};
+
+__global__ void __launch_bounds__(256) k_compute_lhs(LhsArgs a) {
+    const long long n = (long long)a.nx * a.ny * a.nz;
+    const long long sy = a.nxx, sz = (long long)a.nxx * a.nyy;
+    double s0 = 0.0, s1 = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % a.nx), j = (int)((q / a.nx) % a.ny), k = (int)(q / ((long long)a.nx * a.ny));
+        const long long h = (i + a.nbx) + sy * (j + a.nby) + sz * (k + a.nbz);
+        const double jc = a.jac[h];
+        const double sc = a.c / jc * a.rfch[h];  // Ma^2 kappa / (J fcscal)
+        const double ur = a.u[h], ul = a.u[h - 1], vf = a.v[h], vb = a.v[h - sy], wu = a.w[h], wd = a.w[h - sz];
+        double bu, bv, bw, heat = 0.0;
+        if (a.compressible) {
+            bu = (ur - ul) * a.rdx * sc;
+            bv = (vf - vb) * a.rdy * sc;
+            bw = (wu - wd) * a.rdz * sc;
+            if (a.heating) heat = a.heating[q] * a.c * a.rfch[h];
+        } else {
+            const double jp = jc * a.pbar[h];
+            const double pr = 0.5 * (jp + a.jac[h + 1] * a.pbar[h + 1]);
+            const double pl = 0.5 * (jp + a.jac[h - 1] * a.pbar[h - 1]);
+            const double pf = 0.5 * (jp + a.jac[h + sy] * a.pbar[h + sy]);
+            const double pb = 0.5 * (jp + a.jac[h - sy] * a.pbar[h - sy]);
+            const double ju = a.jac[h + sz], jd = a.jac[h - sz];
+            const double pu = jc * ju * (a.pbar[h] + a.pbar[h + sz]) / (jc + ju);
+            const double pd = jc * jd * (a.pbar[h] + a.pbar[h - sz]) / (jc + jd);
+            bu = (pr * ur - pl * ul) * a.rdx * sc;
+            bv = (pf * vf - pb * vb) * a.rdy * sc;
+            bw = (pu * wu - pd * wd) * a.rdz * sc;
+        }
+        const double b = bu + bv + bw - heat;
+        a.rhs[q] = b;
+        s0 += b * b;
+        s1 += bu * bu + bv * bv + bw * bw + heat * heat;
+    }
+    double v[2] = {s0, s1};
+    reduce_finalize<2>(a.red, v);
+}
+
 // Without preconditioner: s = r - alpha v or p = r + beta (p - omega v).
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) k_axpy_noprec(const T *r, const T *v, T *vec, long long n,

@@ -1204,7 +1204,7 @@ int pcf_destroy(pcf_handle *h) {
     int dev = h->dims.device;
     cudaSetDevice(dev);
     void *ptrs[] = {h->jac, h->met13, h->met23, h->met33, h->pbar, h->rhobar, h->thetabar, h->n2, h->rho, h->betar,
-                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch,
+                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch, h->wind,
                     h->x64, h->r64, h->r064, h->p64, h->v64, h->s64,
                     h->t64, h->za64, h->zb64, h->b64, h->w64, h->x32, h->r32, h->r032, h->p32, h->v32, h->s32,
                     h->t32, h->za32, h->zb32, h->zc32, h->zd32, h->partials, h->ticket, h->scal64, h->scal32,
@@ -1545,6 +1545,86 @@ int pcf_autotune_entries(pcf_tune_entry *out, int cap, int *count) {
 int pcf_autotune_clear(void) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune.clear();
+    return PCF_OK;
+}
+
+// compute_lhs! on device arrays; d_rhs may be the handle's own b64.
+static int compute_lhs_device(pcf_handle *h, const double *d_u, const double *d_v, const double *d_w,
+                              const double *d_heat, double *d_rhs, double *tolref) {
+    if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
+    LhsArgs a;
+    a.nx = h->d.nx;
+    a.ny = h->d.ny;
+    a.nz = h->d.nz;
+    a.nxx = h->nxx;
+    a.nyy = h->nyy;
+    a.nbx = h->dims.nbx;
+    a.nby = h->dims.nby;
+    a.nbz = h->dims.nbz;
+    a.compressible = h->dims.model == PCF_MODEL_COMPRESSIBLE;
+    a.rdx = 1.0 / h->dx;
+    a.rdy = 1.0 / h->dy;
+    a.rdz = 1.0 / h->dz;
+    // Ma^2 kappa: Ma = uref / aref = 1 (Constants.jl:124, :149), kappa = (gamma - 1) / gamma (:115)
+    a.c = 1.0 * 1.0 * ((1.4 - 1.0) / 1.4);
+    a.jac = h->jac;
+    a.pbar = h->pbar;
+    a.rfch = h->rfch;
+    a.u = d_u;
+    a.v = d_v;
+    a.w = d_w;
+    a.heating = d_heat;
+    a.rhs = d_rhs;
+    a.red = red(h, nullptr, FIN_STORE, h->dot_out);
+    {
+        ProfScope ps(h, PCF_PROF_ASSEMBLE, (a.compressible ? 10.0 : 14.0) * 8 * (double)h->d.n);
+        k_compute_lhs<<<vec_grid(h->d.n), 256, 0, h->stream>>>(a);
+        PCF_CUDA_TRY(cudaGetLastError());
+    }
+    double sums[2] = {0, 0};
+    PCF_CUDA_TRY(cudaMemcpyAsync(sums, h->dot_out, sizeof(sums), cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    // compute_lhs!.jl:138-157 (one rank: x_size y_size z_size = nx ny nz)
+    const double nn = (double)h->d.n;
+    const double divl2 = std::sqrt(sums[0] / nn), norm = std::sqrt(sums[1] / nn);
+    if (!std::isfinite(divl2) || !std::isfinite(norm)) return PCF_ENONFINITE;
+    if (norm != 0.0)
+        *tolref = divl2 / norm;
+    else if (divl2 == 0.0)
+        *tolref = 1.0;
+    else
+        return PCF_ENONFINITE;  // the reference raises "divl2_norm = 0 while divl2 != 0"
+    return PCF_OK;
+}
+
+int pcf_compute_lhs_device(pcf_handle *h, const double *d_u, const double *d_v, const double *d_w,
+                           const double *d_heating, double *d_rhs, double *tolref) {
+    if (!h || !d_u || !d_v || !d_w || !d_rhs || !tolref) return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    return compute_lhs_device(h, d_u, d_v, d_w, d_heating, d_rhs, tolref);
+}
+
+int pcf_compute_lhs(pcf_handle *h, const double *u, const double *v, const double *w, const double *heating,
+                    double *rhs, double *tolref) {
+    if (!h || !u || !v || !w || !rhs || !tolref) return PCF_EINVAL;
+    if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    if (!h->wind) {
+        // three haloed staging arrays, allocated on the first host-array call
+        int rc = dalloc(h, (void **)&h->wind, 3 * sizeof(double) * (size_t)h->nh);
+        if (rc) return rc;
+    }
+    const size_t hb = sizeof(double) * (size_t)h->nh;
+    double *du = h->wind, *dv = h->wind + h->nh, *dw = h->wind + 2 * h->nh;
+    PCF_CUDA_TRY(cudaMemcpyAsync(du, u, hb, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(dv, v, hb, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(dw, w, hb, cudaMemcpyHostToDevice, h->stream));
+    if (heating)
+        PCF_CUDA_TRY(cudaMemcpyAsync(h->t64, heating, sizeof(double) * h->d.n, cudaMemcpyHostToDevice, h->stream));
+    int rc = compute_lhs_device(h, du, dv, dw, heating ? h->t64 : nullptr, h->s64, tolref);
+    if (rc) return rc;
+    PCF_CUDA_TRY(cudaMemcpyAsync(rhs, h->s64, sizeof(double) * h->d.n, cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
     return PCF_OK;
 }
 

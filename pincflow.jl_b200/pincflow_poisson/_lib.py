@@ -38,7 +38,7 @@ EXPORTS = [
     "pcf_global_dot", "pcf_device_bytes", "pcf_launch_count", "pcf_profile_enable", "pcf_profile_read",
     "pcf_residual_history", "pcf_multigrid_levels", "pcf_multigrid_operator", "pcf_apply_multigrid",
     "pcf_autotune_entries", "pcf_autotune_clear", "pcf_ensemble_create", "pcf_ensemble_destroy",
-    "pcf_ensemble_solve_device", "pcf_ensemble_launch_count",
+    "pcf_ensemble_solve_device", "pcf_ensemble_launch_count", "pcf_compute_lhs", "pcf_compute_lhs_device",
 ]
 TUNE_KERNELS = ["total32", "total32_diff", "horiz32", "total64", "horiz64"]
 PROF_TAGS = ["apply32", "apply64", "pseudo32", "pseudo64", "thomas32", "thomas64", "update32", "update64",
@@ -134,6 +134,8 @@ def load(path: str | None = None):
     lib.pcf_apply_multigrid.argtypes = [vp, dp, dp, P(PcfParams)]
     lib.pcf_autotune_entries.argtypes = [P(PcfTuneEntry), ctypes.c_int, P(ctypes.c_int)]
     lib.pcf_autotune_clear.argtypes = []
+    lib.pcf_compute_lhs.argtypes = [vp, dp, dp, dp, dp, dp, dp]
+    lib.pcf_compute_lhs_device.argtypes = [vp, vp, vp, vp, vp, vp, dp]
     for name in EXPORTS:
         getattr(lib, name).restype = getattr(lib, name).restype or ctypes.c_int
     lib.pcf_strerror.restype = ctypes.c_char_p

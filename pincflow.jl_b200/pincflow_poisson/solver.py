@@ -191,6 +191,26 @@ class PoissonSolver:
                                       _lib.dptr(dpip), ctypes.byref(res)), "pcf_solve")
         return _info(res)
 
+    def compute_lhs(self, u, v, w, heating=None):
+        """compute_lhs!: (rhs, tolref) from the haloed staggered winds (mass
+        fluxes in the Compressible model, with the heating field)."""
+        rhs = np.zeros(self.dom.interior_shape)
+        tol = ctypes.c_double()
+        h = None if heating is None else _f64(heating)
+        _lib.check(self.lib.pcf_compute_lhs(self._h, _lib.dptr(_f64(u)), _lib.dptr(_f64(v)), _lib.dptr(_f64(w)),
+                                            _lib.dptr(h), _lib.dptr(rhs), ctypes.byref(tol)), "pcf_compute_lhs")
+        return rhs, tol.value
+
+    def compute_lhs_device(self, d_u: int, d_v: int, d_w: int, d_rhs: int, d_heating: int | None = None) -> float:
+        """compute_lhs! on device arrays (raw pointers); returns tolref."""
+        tol = ctypes.c_double()
+        _lib.check(self.lib.pcf_compute_lhs_device(self._h, ctypes.c_void_p(d_u), ctypes.c_void_p(d_v),
+                                                   ctypes.c_void_p(d_w),
+                                                   None if d_heating is None else ctypes.c_void_p(d_heating),
+                                                   ctypes.c_void_p(d_rhs), ctypes.byref(tol)),
+                   "pcf_compute_lhs_device")
+        return tol.value
+
     def compute_operator(self, rho, betar, dt, rayleigh_factor, damp_horizontal_wind_on_rhs=False,
                          p=None, return_coef=True):
         coef = np.zeros((_lib.NCOEF,) + self.dom.interior_shape) if return_coef else None

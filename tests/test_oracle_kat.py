@@ -235,3 +235,30 @@ def test_network_oracle_gradient_matches_finite_differences():
         lm, _ = NO.loss_and_grad(p - eps * v, b, x, bf=False)
         fd = (lp - lm) / (2 * eps)
         assert abs(fd - g @ v) <= 1e-5 * max(1.0, abs(fd)), (fd, g @ v)
+
+
+def test_compute_lhs_compressible_is_a_flux_divergence(oracle):
+    """Compressible compute_lhs! (compute_lhs!.jl:162-223): with periodic mass
+    fluxes and W = 0 at the walls, sum(J fcscal b) = -kappa sum(J heating)
+    (Ma = 1), i.e. 0 without heating; zero fluxes and heating give b = 0,
+    tolref = 1."""
+    cfg = C.c2(nx=16, ny=12, nz=8)
+    dom, f = cfg["dom"], cfg["fields"]
+    d = oracle.dims(dom.nx, dom.ny, dom.nz, dom.nbx)
+    rng = np.random.default_rng(8)
+    u, v, w = (rng.standard_normal(dom.halo_shape) for _ in range(3))
+    for a in (u, v, w):
+        F._periodic_xy(dom, a)
+    w[:dom.nbz] = 0.0
+    w[dom.nbz + dom.nz - 1:] = 0.0
+    wt = dom.interior(f["jac"]) * F.fcscal(dom, f)
+    kappa = oracle.constants()["kappa"]
+    rhs, tolref = oracle.compute_lhs(d, f, u, v, w, model="Compressible")
+    assert abs(np.sum(wt * rhs)) <= 1e-13 * np.sum(np.abs(wt * rhs)) and 0 < tolref < 10
+    heat = np.full(dom.interior_shape, 0.3)
+    rhs_h, _ = oracle.compute_lhs(d, f, u, v, w, model="Compressible", heating=heat)
+    want = -kappa * 0.3 * np.sum(dom.interior(f["jac"]))
+    assert abs(np.sum(wt * rhs_h) - want) <= 1e-12 * abs(want)
+    z = np.zeros(dom.halo_shape)
+    rhs0, t0 = oracle.compute_lhs(d, f, z, z, z, model="Compressible")
+    assert not rhs0.any() and t0 == 1.0
