@@ -212,6 +212,25 @@ int pcf_compute_lhs(pcf_handle *h, const double *u, const double *v, const doubl
 int pcf_compute_lhs_device(pcf_handle *h, const double *d_u, const double *d_v, const double *d_w,
                            const double *d_heating, double *d_rhs, double *tolref);
 
+/* The corrector after the solve (apply_corrector!.jl:58-61): fills the halo
+ * of dpip (periodic x/y, mirrored z: set_*_boundaries_of_field!) and applies
+ * correct!(state, dt, rayleigh_factor) (correct!.jl:164-385, with
+ * compute_pressure_gradient.jl:108-297): u, v, w, rhop corrected in place,
+ * pip += dpip on the interior and one ghost layer.  All arrays haloed; rho,
+ * betar and p are those of the handle's last solve.  The _device variant
+ * takes device pointers.  pcf_apply_corrector_device runs the whole
+ * apply_corrector!(state, dt, rayleigh_factor) (:44-61) on device arrays:
+ * compute_lhs!, solve_poisson! (into d_dpip), then the corrector; like the
+ * reference it leaves the fields uncorrected when res->errflag is set. */
+int pcf_correct(pcf_handle *h, double dt, double rayleigh_factor, int damp_horizontal_wind_on_rhs, double *dpip,
+                double *u, double *v, double *w, double *rhop, double *pip);
+int pcf_correct_device(pcf_handle *h, double dt, double rayleigh_factor, int damp_horizontal_wind_on_rhs,
+                       double *d_dpip, double *d_u, double *d_v, double *d_w, double *d_rhop, double *d_pip);
+int pcf_apply_corrector_device(pcf_handle *h, double *d_u, double *d_v, double *d_w, const double *d_rho,
+                               double *d_rhop, const double *d_betar, const double *d_p, double *d_pip,
+                               const double *d_heating, double dt, double rayleigh_factor, const pcf_params *prm,
+                               double *d_dpip, pcf_result *res);
+
 int pcf_apply_preconditioner(pcf_handle *h, const double *sin_, double *sout,
                              const pcf_params *prm, int precision);
 

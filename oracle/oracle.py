@@ -201,6 +201,21 @@ def compute_lhs(d: Dims, f: dict, u, v, w, model="PseudoIncompressible", heating
     return rhs, tolref
 
 
+def correct(d: Dims, model, f: dict, rho, betar, dt, rayleigh_factor, dpip, u, v, w, rhop, pip,
+            damp_horizontal_wind_on_rhs=False, p=None):
+    """apply_corrector!.jl:58-61 after the solve: fills dpip's halos and
+    corrects u, v, w, rhop, pip; returns copies (dpip, u, v, w, rhop, pip)."""
+    c = constants()
+    out = [np.array(x, dtype=np.float64, copy=True) for x in (dpip, u, v, w, rhop, pip)]
+    lib().or_correct(ctypes.byref(d), int(model), ctypes.c_double(f["dx"]), ctypes.c_double(f["dy"]),
+                     ctypes.c_double(f["dz"]), _p(f["jac"]), _p(f["met13"]), _p(f["met23"]), _p(f["met33"]),
+                     _p(f["rhobar"]), _p(f["pbar"]), _pn(f.get("thetabar")), _p(f["n2"]), _p(betar), _p(rho),
+                     _pn(p), ctypes.c_double(dt), ctypes.c_double(rayleigh_factor),
+                     int(bool(damp_horizontal_wind_on_rhs)), ctypes.c_double(1.0 / c["kappa"]),
+                     ctypes.c_double(1.0 / c["ma"] ** 2), ctypes.c_double(c["g_ndim"]), *[_p(x) for x in out])
+    return tuple(out)
+
+
 def dot(a, b) -> float:
     a = np.ascontiguousarray(a, dtype=np.float64).ravel()
     b = np.ascontiguousarray(b, dtype=np.float64).ravel()

@@ -145,6 +145,20 @@ double or_compute_lhs_compressible(const or_dims *d, double dx, double dy, doubl
                                    const double *rhobar, const double *u, const double *v,
                                    const double *w, const double *heating, double *rhs);
 
+/* The corrector after the solve (apply_corrector!.jl:58-61): dpip's halo
+ * fill (periodic x/y, mirrored z; in place) then correct!.jl:164-385
+ * (u, v, w, rhop corrected in place, pip += dpip on one ghost layer
+ * around the interior).  All arrays haloed; model 0/1/2 as
+ * or_compute_operator; kappainv = 1/kappa, mainv2 = 1/Ma^2, g_ndim the
+ * non-dimensional gravity (Constants.jl:116, :131, :150). */
+void or_fill_dpip(const or_dims *d, double *dpip);
+void or_correct(const or_dims *d, int model, double dx, double dy, double dz, const double *jac,
+                const double *met13, const double *met23, const double *met33, const double *rhobar,
+                const double *pbar, const double *thetabar, const double *n2, const double *betar,
+                const double *rho, const double *p, double dt, double rayleigh_factor, int damp_h,
+                double kappainv, double mainv2, double g_ndim, double *dpip, double *u, double *v,
+                double *w, double *rhop, double *pip);
+
 /* Helpers for tests and the CPU baseline. */
 double or_dot(long n, const double *a, const double *b); /* pairwise FP64 sum */
 void or_set_threads(int n);

@@ -135,7 +135,8 @@ struct pcf_handle {
     float *coefB32;
     double *fc64, *fch;  // fcscal on the interior and on the haloed grid
     double *rfch;        // 1 / fcscal on the haloed grid
-    double *wind;        // u, v, w staging of pcf_compute_lhs (3 haloed arrays, on first use)
+    double *stage;       // 6 haloed staging arrays of the host-array wind entry points (on first use)
+    double *corr;        // corx, cory of the corrector (2 haloed arrays, on first use)
     float *rfc32;        // 1 / fcscal on the interior
     double fac_deta;  // d_eta the factors were built with (NaN: none)
     // FP64 Krylov vectors

@@ -29,6 +29,8 @@ int pcf_set_cuda_error(cudaError_t e) {
 
 int pcf_launch_assemble(pcf_handle *h, double dt, double rf, int damp_h);
 int pcf_launch_factors(pcf_handle *h, double deta);
+int pcf_launch_correct(pcf_handle *h, double dt, double rf, int damp_h, double *dpip, double *u, double *v,
+                       double *w, double *rhop, double *pip, double *corx, double *cory);
 
 namespace pcf {
 
@@ -1204,7 +1206,7 @@ int pcf_destroy(pcf_handle *h) {
     int dev = h->dims.device;
     cudaSetDevice(dev);
     void *ptrs[] = {h->jac, h->met13, h->met23, h->met33, h->pbar, h->rhobar, h->thetabar, h->n2, h->rho, h->betar,
-                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch, h->wind,
+                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch, h->stage, h->corr,
                     h->x64, h->r64, h->r064, h->p64, h->v64, h->s64,
                     h->t64, h->za64, h->zb64, h->b64, h->w64, h->x32, h->r32, h->r032, h->p32, h->v32, h->s32,
                     h->t32, h->za32, h->zb32, h->zc32, h->zd32, h->partials, h->ticket, h->scal64, h->scal32,
@@ -1548,7 +1550,13 @@ int pcf_autotune_clear(void) {
     return PCF_OK;
 }
 
-// compute_lhs! on device arrays; d_rhs may be the handle's own b64.
+// Staging for the host-array entry points of the winds (allocated once).
+static int ensure_stage(pcf_handle *h) {
+    if (h->stage) return PCF_OK;
+    return dalloc(h, (void **)&h->stage, 6 * sizeof(double) * (size_t)h->nh);
+}
+
+// compute_lhs! on device arrays.
 static int compute_lhs_device(pcf_handle *h, const double *d_u, const double *d_v, const double *d_w,
                               const double *d_heat, double *d_rhs, double *tolref) {
     if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
@@ -1609,13 +1617,10 @@ int pcf_compute_lhs(pcf_handle *h, const double *u, const double *v, const doubl
     if (!h || !u || !v || !w || !rhs || !tolref) return PCF_EINVAL;
     if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
     PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
-    if (!h->wind) {
-        // three haloed staging arrays, allocated on the first host-array call
-        int rc = dalloc(h, (void **)&h->wind, 3 * sizeof(double) * (size_t)h->nh);
-        if (rc) return rc;
-    }
+    int rc0 = ensure_stage(h);
+    if (rc0) return rc0;
     const size_t hb = sizeof(double) * (size_t)h->nh;
-    double *du = h->wind, *dv = h->wind + h->nh, *dw = h->wind + 2 * h->nh;
+    double *du = h->stage, *dv = h->stage + h->nh, *dw = h->stage + 2 * h->nh;
     PCF_CUDA_TRY(cudaMemcpyAsync(du, u, hb, cudaMemcpyHostToDevice, h->stream));
     PCF_CUDA_TRY(cudaMemcpyAsync(dv, v, hb, cudaMemcpyHostToDevice, h->stream));
     PCF_CUDA_TRY(cudaMemcpyAsync(dw, w, hb, cudaMemcpyHostToDevice, h->stream));
@@ -1626,6 +1631,62 @@ int pcf_compute_lhs(pcf_handle *h, const double *u, const double *v, const doubl
     PCF_CUDA_TRY(cudaMemcpyAsync(rhs, h->s64, sizeof(double) * h->d.n, cudaMemcpyDeviceToHost, h->stream));
     PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
     return PCF_OK;
+}
+
+int pcf_correct_device(pcf_handle *h, double dt, double rayleigh_factor, int damp_horizontal_wind_on_rhs,
+                       double *d_dpip, double *d_u, double *d_v, double *d_w, double *d_rhop, double *d_pip) {
+    if (!h || !d_dpip || !d_u || !d_v || !d_w || !d_rhop || !d_pip) return PCF_EINVAL;
+    if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    if (!h->corr) {
+        int rc = dalloc(h, (void **)&h->corr, 2 * sizeof(double) * (size_t)h->nh);
+        if (rc) return rc;
+    }
+    int rc = pcf_launch_correct(h, dt, rayleigh_factor, damp_horizontal_wind_on_rhs, d_dpip, d_u, d_v, d_w, d_rhop,
+                                d_pip, h->corr, h->corr + h->nh);
+    if (rc) return rc;
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
+}
+
+int pcf_correct(pcf_handle *h, double dt, double rayleigh_factor, int damp_horizontal_wind_on_rhs, double *dpip,
+                double *u, double *v, double *w, double *rhop, double *pip) {
+    if (!h || !dpip || !u || !v || !w || !rhop || !pip) return PCF_EINVAL;
+    if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    int rc = ensure_stage(h);
+    if (rc) return rc;
+    double *host[6] = {dpip, u, v, w, rhop, pip};
+    const size_t hb = sizeof(double) * (size_t)h->nh;
+    for (int q = 0; q < 6; ++q)
+        PCF_CUDA_TRY(cudaMemcpyAsync(h->stage + q * h->nh, host[q], hb, cudaMemcpyHostToDevice, h->stream));
+    double *s = h->stage;
+    const long long nh = h->nh;
+    if ((rc = pcf_correct_device(h, dt, rayleigh_factor, damp_horizontal_wind_on_rhs, s, s + nh, s + 2 * nh,
+                                 s + 3 * nh, s + 4 * nh, s + 5 * nh)))
+        return rc;
+    for (int q = 0; q < 6; ++q)
+        PCF_CUDA_TRY(cudaMemcpyAsync(host[q], h->stage + q * h->nh, hb, cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
+}
+
+int pcf_apply_corrector_device(pcf_handle *h, double *d_u, double *d_v, double *d_w, const double *d_rho,
+                               double *d_rhop, const double *d_betar, const double *d_p, double *d_pip,
+                               const double *d_heating, double dt, double rayleigh_factor, const pcf_params *prm,
+                               double *d_dpip, pcf_result *res) {
+    if (!h || !d_u || !d_v || !d_w || !d_rho || !d_rhop || !d_betar || !d_pip || !prm || !d_dpip || !res)
+        return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    // apply_corrector!.jl:44-61: compute_lhs!, solve_poisson!, dpip halos, correct!
+    double tolref = 0;
+    int rc = compute_lhs_device(h, d_u, d_v, d_w, d_heating, h->s64, &tolref);
+    if (rc) return rc;
+    if ((rc = pcf_solve_device(h, h->s64, d_rho, d_betar, d_p, dt, rayleigh_factor, tolref, prm, d_dpip, res)))
+        return rc;
+    if (res->errflag) return PCF_OK;  // the reference returns (errflag, niter) uncorrected
+    return pcf_correct_device(h, dt, rayleigh_factor, prm->damp_horizontal_wind_on_rhs, d_dpip, d_u, d_v, d_w,
+                              d_rhop, d_pip);
 }
 
 int pcf_global_dot(pcf_handle *h, const double *a, const double *b, double *out) {

@@ -39,6 +39,7 @@ EXPORTS = [
     "pcf_residual_history", "pcf_multigrid_levels", "pcf_multigrid_operator", "pcf_apply_multigrid",
     "pcf_autotune_entries", "pcf_autotune_clear", "pcf_ensemble_create", "pcf_ensemble_destroy",
     "pcf_ensemble_solve_device", "pcf_ensemble_launch_count", "pcf_compute_lhs", "pcf_compute_lhs_device",
+    "pcf_correct", "pcf_correct_device", "pcf_apply_corrector_device",
 ]
 TUNE_KERNELS = ["total32", "total32_diff", "horiz32", "total64", "horiz64"]
 PROF_TAGS = ["apply32", "apply64", "pseudo32", "pseudo64", "thomas32", "thomas64", "update32", "update64",
@@ -136,6 +137,10 @@ def load(path: str | None = None):
     lib.pcf_autotune_clear.argtypes = []
     lib.pcf_compute_lhs.argtypes = [vp, dp, dp, dp, dp, dp, dp]
     lib.pcf_compute_lhs_device.argtypes = [vp, vp, vp, vp, vp, vp, dp]
+    lib.pcf_correct.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, dp, dp]
+    lib.pcf_correct_device.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, vp, vp, vp, vp, vp, vp]
+    lib.pcf_apply_corrector_device.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_double,
+                                               ctypes.c_double, P(PcfParams), vp, P(PcfResult)]
     for name in EXPORTS:
         getattr(lib, name).restype = getattr(lib, name).restype or ctypes.c_int
     lib.pcf_strerror.restype = ctypes.c_char_p

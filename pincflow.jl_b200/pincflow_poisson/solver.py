@@ -211,6 +211,40 @@ class PoissonSolver:
                    "pcf_compute_lhs_device")
         return tol.value
 
+    def correct(self, dt, rayleigh_factor, dpip, u, v, w, rhop, pip, damp_horizontal_wind_on_rhs=False):
+        """The corrector after solve_poisson (apply_corrector!.jl:58-61): fills
+        dpip's halo and corrects u, v, w, rhop, pip, all haloed float64 arrays
+        modified in place (rho, betar, p of the last solve)."""
+        arrs = [dpip, u, v, w, rhop, pip]
+        for a in arrs:
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]):
+                raise TypeError("correct: arrays must be C-contiguous float64")
+        _lib.check(self.lib.pcf_correct(self._h, float(dt), float(rayleigh_factor),
+                                        int(bool(damp_horizontal_wind_on_rhs)), *[_lib.dptr(a) for a in arrs]),
+                   "pcf_correct")
+
+    def correct_device(self, dt, rayleigh_factor, d_dpip, d_u, d_v, d_w, d_rhop, d_pip,
+                       damp_horizontal_wind_on_rhs=False):
+        """correct on device arrays (raw pointers), in place."""
+        ptrs = [ctypes.c_void_p(x) for x in (d_dpip, d_u, d_v, d_w, d_rhop, d_pip)]
+        _lib.check(self.lib.pcf_correct_device(self._h, float(dt), float(rayleigh_factor),
+                                               int(bool(damp_horizontal_wind_on_rhs)), *ptrs), "pcf_correct_device")
+
+    def apply_corrector_device(self, d_u, d_v, d_w, d_rho, d_rhop, d_betar, d_pip, dt, rayleigh_factor,
+                               namelist: PoissonNamelist, d_dpip, d_p=None, d_heating=None) -> SolveInfo:
+        """apply_corrector!(state, dt, rayleigh_factor) on device arrays:
+        compute_lhs!, solve_poisson!, dpip halos, correct!.  Returns the solve's
+        SolveInfo; the fields stay uncorrected when info.errflag is set."""
+        res = _lib.PcfResult()
+        prm = namelist.to_c()
+        vp = ctypes.c_void_p
+        opt = lambda x: None if x is None else vp(x)  # noqa: E731
+        _lib.check(self.lib.pcf_apply_corrector_device(self._h, vp(d_u), vp(d_v), vp(d_w), vp(d_rho), vp(d_rhop),
+                                                       vp(d_betar), opt(d_p), vp(d_pip), opt(d_heating), float(dt),
+                                                       float(rayleigh_factor), ctypes.byref(prm), vp(d_dpip),
+                                                       ctypes.byref(res)), "pcf_apply_corrector_device")
+        return _info(res)
+
     def compute_operator(self, rho, betar, dt, rayleigh_factor, damp_horizontal_wind_on_rhs=False,
                          p=None, return_coef=True):
         coef = np.zeros((_lib.NCOEF,) + self.dom.interior_shape) if return_coef else None

@@ -262,3 +262,32 @@ def test_compute_lhs_compressible_is_a_flux_divergence(oracle):
     z = np.zeros(dom.halo_shape)
     rhs0, t0 = oracle.compute_lhs(d, f, z, z, z, model="Compressible")
     assert not rhs0.any() and t0 == 1.0
+
+
+@pytest.mark.parametrize("name", ["mtn", "hill", "odd"])
+def test_corrector_removes_the_divergence(name, oracle):
+    """The reference's projection: compute_lhs! -> solve_poisson! -> correct!
+    leaves winds whose compute_lhs! vanishes (to the solver tolerance), which
+    ties the restatements of the operator, compute_lhs! and correct! (with
+    compute_pressure_gradient and the dpip halo fill) to one another."""
+    from _cases import case
+    cfg = case(name)
+    dom, f = cfg["dom"], cfg["fields"]
+    d = oracle.dims(dom.nx, dom.ny, dom.nz, dom.nbx)
+    rng = np.random.default_rng(3)
+    u, v, w = (rng.standard_normal(dom.halo_shape) for _ in range(3))
+    for a in (u, v, w):
+        F._periodic_xy(dom, a)
+    w[:dom.nbz] = 0.0
+    w[dom.nbz + dom.nz - 1:] = 0.0
+    model = oracle.MODELS[cfg["model"]]
+    rhs, tolref = oracle.compute_lhs(d, f, u, v, w, model=cfg["model"])
+    dpip, info = oracle.solve_poisson(d, model, f, cfg["rho"], cfg["betar"], rhs, cfg["dt"], cfg["rayleigh_factor"],
+                                      tolref=tolref, tolerance=1e-13, tolerance_is_relative=True,
+                                      poisson_iterations=5000)
+    assert not info["errflag"]
+    z = np.zeros(dom.halo_shape)
+    _, u2, v2, w2, _, _ = oracle.correct(d, model, f, cfg["rho"], cfg["betar"], cfg["dt"], cfg["rayleigh_factor"],
+                                         dpip, u, v, w, z, z)
+    rhs2, _ = oracle.compute_lhs(d, f, u2, v2, w2, model=cfg["model"])
+    assert np.sqrt(np.mean(rhs2 ** 2)) <= 1e-11 * np.sqrt(np.mean(rhs ** 2))
