@@ -5,11 +5,14 @@
 #     include("PinCFlowGPU.jl"); using .PinCFlowGPU
 #     PinCFlowGPU.enable!()          # later solve_poisson! calls run on the GPU
 #
-# The method below replaces
+# The methods below replace
 #     PinCFlow.PoissonSolver.solve_poisson!(state, dt, rayleigh_factor, tolref)
-# (src/PoissonSolver/solve_poisson!.jl:39-75) with the same signature and
-# return convention (errflag, niter); dt == 0 raises as in the reference, a
-# non-converged solve returns (true, niter) and leaves dpip untouched.
+# (src/PoissonSolver/solve_poisson!.jl:39-75) and, with enable!(corrector = true),
+#     PinCFlow.PoissonSolver.apply_corrector!(state, dt, rayleigh_factor)
+# (src/PoissonSolver/apply_corrector!.jl:44-61: compute_lhs!, the solve, the
+# dpip halo fill and correct!) with the same signatures and return convention
+# (errflag, niter); dt == 0 raises as in the reference, a non-converged solve
+# returns (true, niter) and leaves dpip and the fields untouched.
 # Single MPI rank only (npx = npy = npz = 1).
 module PinCFlowGPU
 
@@ -40,6 +43,11 @@ mutable struct PcfParams
     learned::Cint
     check_interval::Cint
     restart_interval::Cint
+    multigrid::Cint
+    mg_dtau::Cdouble
+    mg_coarse_iterations::Cint
+    mg_min_columns::Cint
+    autotune::Cint
 end
 
 mutable struct PcfResult
@@ -55,7 +63,7 @@ const PRECISION = Dict(:fp64 => 0, :mixed => 1)
 
 # one handle per State, created on first use (grid and background uploaded once)
 const HANDLES = IdDict{Any, Ptr{Cvoid}}()
-const SETTINGS = Ref((precision = :fp64, device = 0))
+const SETTINGS = Ref((precision = :fp64, multigrid = false, device = 0))
 
 check(rc, what) = rc == 0 || error("$what: " *
     unsafe_string(ccall((:pcf_strerror, LIB), Cstring, (Cint,), rc)))
@@ -103,7 +111,7 @@ end
 function params(state)
     (; tolerance, poisson_iterations, preconditioner, dtau, preconditioner_iterations,
        tolerance_is_relative) = state.namelists.poisson
-    p = PcfParams(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
+    p = PcfParams(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
     ccall((:pcf_params_default, LIB), Cint, (Ref{PcfParams},), p)
     p.tolerance = tolerance
     p.poisson_iterations = poisson_iterations
@@ -113,6 +121,8 @@ function params(state)
     p.tolerance_is_relative = tolerance_is_relative
     p.damp_horizontal_wind_on_rhs = state.namelists.sponge.damp_horizontal_wind_on_rhs
     p.precision = PRECISION[SETTINGS[].precision]
+    p.multigrid = SETTINGS[].multigrid
+    p.autotune = 1
     return p
 end
 
@@ -137,17 +147,59 @@ function solve_poisson_gpu!(state, dt::AbstractFloat, rayleigh_factor::AbstractF
     return (res.errflag != 0, Int(res.niter))
 end
 
+# apply_corrector!.jl:44-61 through the library: compute_lhs! (with the
+# Compressible model's heating from the reference's own compute_volume_force),
+# the solve, then the dpip halo fill and correct!.
+function apply_corrector_gpu!(state, dt::AbstractFloat, rayleigh_factor::AbstractFloat)
+    h = handle(state)
+    (; u, v, w, rhop, pip) = state.variables.predictands
+    (; dpip) = state.variables.increments
+    (; rhs) = state.poisson
+    heating = C_NULL
+    if state.namelists.atmosphere.model == :Compressible
+        (; i0, i1, j0, j1, k0, k1) = state.domain
+        heating = [PinCFlow.Update.compute_volume_force(state, i, j, k, PinCFlow.P())
+                   for i in i0:i1, j in j0:j1, k in k0:k1]
+    end
+    tolref = Ref{Cdouble}(0.0)
+    GC.@preserve u v w heating rhs begin
+        check(ccall((:pcf_compute_lhs, LIB), Cint,
+                    (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ref{Cdouble}),
+                    h, u, v, w, heating, rhs, tolref), "pcf_compute_lhs")
+    end
+    (errflag, niter) = solve_poisson_gpu!(state, dt, rayleigh_factor, tolref[])
+    errflag && return (errflag, niter)
+    damp = state.namelists.sponge.damp_horizontal_wind_on_rhs
+    GC.@preserve dpip u v w rhop pip begin
+        check(ccall((:pcf_correct, LIB), Cint,
+                    (Ptr{Cvoid}, Cdouble, Cdouble, Cint, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
+                     Ptr{Cdouble}, Ptr{Cdouble}),
+                    h, dt, rayleigh_factor, damp, dpip, u, v, w, rhop, pip), "pcf_correct")
+    end
+    return (errflag, niter)
+end
+
 """
-    enable!(; precision = :fp64, device = 0)
+    enable!(; precision = :fp64, multigrid = false, corrector = false, device = 0)
 
 Make `PinCFlow.PoissonSolver.solve_poisson!` run on the GPU.  `precision = :mixed`
-selects the FP32-inner / FP64-refined solve (same FP64 tolerance).
+selects the FP32-inner / FP64-refined solve (same FP64 tolerance), and
+`multigrid = true` (with `:mixed`) its multigrid preconditioner.
+`corrector = true` also replaces `apply_corrector!` (compute_lhs!, the solve and
+correct! all on the GPU).
 """
-function enable!(; precision::Symbol = :fp64, device::Integer = 0)
-    SETTINGS[] = (precision = precision, device = device)
+function enable!(; precision::Symbol = :fp64, multigrid::Bool = false, corrector::Bool = false,
+                 device::Integer = 0)
+    SETTINGS[] = (precision = precision, multigrid = multigrid, device = device)
     @eval PS function solve_poisson!(state::PinCFlow.State, dt::AbstractFloat,
                                      rayleigh_factor::AbstractFloat, tolref::AbstractFloat)
         return $(solve_poisson_gpu!)(state, dt, rayleigh_factor, tolref)
+    end
+    if corrector
+        @eval PS function apply_corrector!(state::PinCFlow.State, dt::AbstractFloat,
+                                           rayleigh_factor::AbstractFloat)
+            return $(apply_corrector_gpu!)(state, dt, rayleigh_factor)
+        end
     end
     return nothing
 end

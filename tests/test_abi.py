@@ -115,3 +115,33 @@ def test_no_device_is_an_error_not_a_fallback(pcf):
     with pytest.raises(pcf.PoissonError) as e:
         pcf.PoissonSolver(pcf.fields.Domain(8, 8, 8))
     assert e.value.code == pcf._lib.PCF_ENODEVICE
+
+
+def _c_struct_fields(name):
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    body = re.search(r"typedef struct \{([^{}]*)\}\s*" + name + r";", src).group(1)
+    fields = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        typ, names = decl.split(None, 1)
+        fields += [(n.strip(), typ) for n in names.split(",")]
+    return fields
+
+
+def _julia_struct_fields(name):
+    src = open(os.path.join(REPO, "pincflow.jl_b200", "julia", "PinCFlowGPU.jl")).read()
+    body = re.search(r"(?:mutable )?struct " + name + r"\n(.*?)\nend", src, flags=re.S).group(1)
+    return [(n, t) for n, t in re.findall(r"(\w+)::(\w+)", body)]
+
+
+@pytest.mark.parametrize("c_name, jl_name", [("pcf_params", "PcfParams"), ("pcf_result", "PcfResult"),
+                                             ("pcf_dims", "PcfDims")])
+def test_julia_binding_structs_match_the_header(c_name, jl_name):
+    """The ccall binding's struct mirrors have the header's fields, in order
+    and with matching C types (a missing field would let pcf_params_default
+    write past the Julia object)."""
+    ctype = {"int": "Cint", "double": "Cdouble"}
+    c = [(n, ctype[t]) for n, t in _c_struct_fields(c_name)]
+    assert _julia_struct_fields(jl_name) == c
