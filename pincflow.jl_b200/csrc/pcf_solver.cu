@@ -17,6 +17,7 @@
 
 #include "pcf_kernels.cuh"
 #include "pcf_mg.cuh"
+#include "pcf_tiny.cuh"
 
 namespace {
 thread_local cudaError_t g_last_cuda = cudaSuccess;
@@ -495,8 +496,11 @@ struct MgState {
 
 __global__ void k_to_float(const double *__restrict__ a, float *__restrict__ b, long long n, double scale);
 
-// Columns per level up to which the coarse-level column solves use a warp per column.
-constexpr int kWarpThomasColumns = 16384;
+// Columns per level up to which the coarse-level column solves use a warp per
+// column.  Above it the column-per-thread sweep has enough columns in flight
+// to stream at bandwidth, while the warp form's per-lane level loads touch a
+// sector per lane (measured 27 us against about 10 us at 128 x 128 x 128).
+constexpr int kWarpThomasColumns = 4096;
 
 template <int MODE>
 static int mg_thomas(pcf_handle *h, const MgLevel &L, const ThomasArgs<float> &a, int tag) {
@@ -1720,6 +1724,68 @@ static int true_residual(pcf_handle *h, const double *b, const double *x, double
     return PCF_OK;
 }
 
+// Grids of at most kTinyMaxCells cells: the reference FP64 BiCGSTAB in one
+// thread block (pcf_tiny.cuh), whatever the precision and multigrid settings
+// (on such grids the solve is bound by launch latency, so neither reduced
+// precision nor the multigrid hierarchy pays off).  Convergence is tested on
+// the recursive residual as in the reference; the FP64 true residual is
+// reported and, for the mixed precision or true-residual settings, decides
+// errflag.
+static int tiny_solve(pcf_handle *h, double tol, const pcf_params *prm, const double **xres, pcf_result *res) {
+    const double deta = deta_of(h, prm->dtau);
+    int rc;
+    if (prm->preconditioner && (rc = ensure_factors(h, deta))) return rc;
+    static int attr_device = -1;
+    const size_t smem = sizeof(double) * kTinyVectors * (size_t)h->d.n;
+    if (attr_device != h->dims.device) {
+        PCF_CUDA_TRY(cudaFuncSetAttribute(k_tiny_bicgstab, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)(sizeof(double) * kTinyVectors * kTinyMaxCells)));
+        attr_device = h->dims.device;
+    }
+    TinyArgs a;
+    a.nx = h->d.nx;
+    a.ny = h->d.ny;
+    a.nz = h->d.nz;
+    a.n = (int)h->d.n;
+    a.plane = h->d.plane;
+    a.coef = h->coef64;
+    a.fac = h->fac64;
+    a.b = h->b64;
+    a.x = h->x64;
+    a.tol = tol;
+    a.maxit = prm->poisson_iterations;
+    a.precond = prm->preconditioner;
+    a.pc_iters = prm->preconditioner_iterations;
+    a.deta = deta;
+    a.scal = h->scal64;
+    a.hist = h->hist;
+    a.hist_cap = kHistCap;
+    {
+        ProfScope ps(h, PCF_PROF_APPLY64, 0.0);
+        k_tiny_bicgstab<<<1, kTinyThreads, smem, h->stream>>>(a);
+        PCF_CUDA_TRY(cudaGetLastError());
+    }
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->h_scal, h->scal64, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    const KrylovScalars ks = *h->h_scal;
+    prof_flush(h, 0);
+    h->hist_len = std::min(ks.iter, kHistCap);
+    res->niter = ks.iter;
+    res->nrefine = 0;
+    res->status = ks.status;
+    res->errflag = ks.converged ? 0 : 1;
+    res->b_norm = ks.b_norm;
+    res->residual = ks.b_norm > 0 ? ks.res / ks.b_norm : 0.0;
+    *xres = h->x64;
+    double tr = 0;
+    if ((rc = true_residual(h, h->b64, h->x64, &tr))) return rc;
+    res->true_residual = ks.b_norm > 0 ? tr / ks.b_norm : 0.0;
+    const bool true_test = prm->residual == PCF_RESIDUAL_TRUE || prm->precision == PCF_PRECISION_MIXED;
+    if (prm->precision == PCF_PRECISION_MIXED) res->residual = res->true_residual;
+    if (true_test && !res->errflag && res->true_residual > tol) res->errflag = 1;
+    return PCF_OK;
+}
+
 // Solves A x = b64 (device) according to prm; the solution ends in *xres
 // (a device FP64 buffer owned by the handle).
 static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, const double **xres, pcf_result *res) {
@@ -1733,6 +1799,7 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
     if (c.precond && c.pc_iters < 1) return PCF_EINVAL;
     // the multigrid preconditioner runs in the FP32 loop of the mixed solve only
     if (prm->multigrid && (prm->precision != PCF_PRECISION_MIXED || !c.precond)) return PCF_EINVAL;
+    if (h->d.n <= kTinyMaxCells) return tiny_solve(h, tol, prm, xres, res);
     int rc;
     if (c.precond && (rc = ensure_factors(h, c.deta))) return rc;
     const int maxit = prm->poisson_iterations;

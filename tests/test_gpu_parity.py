@@ -268,3 +268,28 @@ def test_mixed_precision_iteration_count_at_scale(pcf):
     assert imx.true_residual <= 1e-10
     assert imx.niter <= 1.25 * i64.niter + 5, (imx.niter, i64.niter)
     assert len(hist) == imx.niter and hist[-1] <= 1e-10
+
+
+def test_tiny_grid_solves_in_one_block(solvers, oracle, pcf):
+    """Grids of at most 2048 cells (the 40 x 1 x 40 periodic hill) run the
+    reference FP64 BiCGSTAB in one thread block: a solve is a handful of
+    launches (assembly, factors, the solve, the true residual), and its
+    iteration count and solution match the oracle's as the multi-kernel path
+    does; the mixed-precision setting gets the same FP64 solve."""
+    cfg, s = solvers("hill")
+    d, coef = oracle_operator(oracle, cfg)
+    s.set_operator(coef)
+    rhs = consistent_rhs(oracle, cfg)
+    ref, ri = oracle.bicgstab(d, coef, cfg["fields"]["dx"], cfg["fields"]["dy"], rhs, tolerance=1e-10,
+                              tolerance_is_relative=True, poisson_iterations=4000)
+    for prec in ("fp64", "mixed"):
+        l0 = s.launch_count
+        got, info = s.apply_bicgstab(rhs, 1.0, pcf.PoissonNamelist(tolerance=1e-10, tolerance_is_relative=True,
+                                                                   poisson_iterations=4000, precision=prec,
+                                                                   multigrid=prec == "mixed"))
+        assert s.launch_count - l0 <= 6, s.launch_count - l0
+        assert not info.errflag and iterations_agree(info.niter, ri["niter"]), (info.niter, ri["niter"])
+        assert info.true_residual <= 1.01e-10
+        assert rel_err(_drop_null(cfg, got), _drop_null(cfg, ref)) < 1e-6
+        hist = s.residual_history()
+        assert len(hist) == info.niter and hist[-1] <= 1e-10
