@@ -119,7 +119,7 @@ typedef struct {
     int residual;                  /* PCF_RESIDUAL_RECURSIVE */
     double inner_tolerance;        /* mixed: FP64 reliable update each time the FP32 residual fell by this factor (1e-2) */
     int max_refinements;           /* mixed: cap on restarts of the FP32 iteration after a breakdown (5) */
-    int learned;                   /* 0: off; 1: learned warm start + flexible BiCGSTAB */
+    int learned;                   /* mixed, bit set: 1 learned warm start, 2 learned preconditioner stage (0) */
     int check_interval;            /* iterations per graph batch between host checks of the status word (4) */
     int restart_interval;          /* mixed: restart the Krylov recurrences at every n-th reliable update (1; 0: never) */
     int multigrid;                 /* mixed: 0: the reference preconditioner; 1: horizontal aggregation multigrid
@@ -318,7 +318,8 @@ enum pcf_prof_tag {
     PCF_PROF_ASSEMBLE = 8,  /* operator assembly + factors */
     PCF_PROF_RELIABLE = 9,  /* FP64 true-residual applies of reliable updates (mostly skipped launches) */
     PCF_PROF_MG = 10,       /* multigrid coarse levels and grid transfers, FP32 */
-    PCF_PROF_NTAGS = 11
+    PCF_PROF_LEARNED = 11,  /* learned preconditioner stage: residual, network, combination */
+    PCF_PROF_NTAGS = 12
 };
 long long pcf_launch_count(const pcf_handle *h);
 /* Relative recursive residual after each BiCGSTAB iteration of the last
@@ -365,8 +366,15 @@ int pcf_net_train_step(pcf_net *net, const float *b, const float *x, int nx, int
 /* loss and gradients for host arrays, no update (gradient check) */
 int pcf_net_gradients(pcf_net *net, const double *b, const double *x, int nx, int ny, int nz, double *loss,
                       float *grad);
-/* Attach a trained network to a solver: with prm->learned = 1 the mixed-precision
- * solve starts from x0 = RMS(b) N(b / RMS(b)) instead of 0.  NULL detaches. */
+/* Hold the biases at zero (zeroed now, skipped by Adam): the network is then
+ * positively homogeneous, N(a x) = a N(x) for a > 0, and applies to a
+ * residual of any size without normalisation (the preconditioner stage). */
+int pcf_net_set_bias_free(pcf_net *net, int on);
+/* Attach a trained network to a solver for the mixed-precision solve.
+ * prm->learned is a bit set: 1, warm start x0 = RMS(b) N(b / RMS(b)) instead
+ * of 0; 2, a learned stage in the right preconditioner of the flexible FP32
+ * BiCGSTAB, z = M(r) + N(r - A M(r)) with M the reference or multigrid
+ * preconditioner (for a bias-free network).  NULL detaches. */
 int pcf_set_network(pcf_handle *h, pcf_net *net);
 
 /* Allocation-free global dot product.  No counterpart in the reference: it

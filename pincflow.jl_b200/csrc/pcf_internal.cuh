@@ -162,5 +162,6 @@ struct pcf_handle {
     long long graph_launches;    // kernels in the graph being replayed
     pcf_net *net;                // learned warm start (not owned)
     pcf::MgState *mg;            // multigrid hierarchy (allocated on first use)
+    float *lr32;                 // learned preconditioner stage: residual and correction (2 n, on first use)
     long long op_version;        // incremented whenever the operator changes
 };

@@ -855,6 +855,16 @@ __global__ void __launch_bounds__(256) k_compute_lhs(LhsArgs a) {
     reduce_finalize<2>(a.red, v);
 }
 
+// Learned preconditioner stage, last step: z = (z_s + c) / fcscal (the FP32
+// loop's variable is pi = s / fcscal).
+__global__ void __launch_bounds__(256) k_learned_combine(float *z, const float *__restrict__ c,
+                                                         const float *__restrict__ rfc, long long n,
+                                                         const KrylovScalars *guard) {
+    if (krylov_done(guard)) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        z[i] = (z[i] + c[i]) * rfc[i];
+}
+
 // Without preconditioner: s = r - alpha v or p = r + beta (p - omega v).
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) k_axpy_noprec(const T *r, const T *v, T *vec, long long n,

@@ -78,6 +78,7 @@ struct Net {
     double *scal;  // [0] loss numerator, [1] sum T^2, [2] loss
     int *err;
     int step;
+    int no_bias;  // biases held at zero: N is then positively homogeneous, N(a x) = a N(x) for a > 0
 };
 
 // level position of output level l when resampling n_in levels to n_out
@@ -237,11 +238,16 @@ __global__ void k_colsum_part(const float *__restrict__ a, long long C, int F, f
 }
 
 // Adam (FP32 master weights), then refresh the BF16 copies of W1, W2, W3
+__device__ __forceinline__ bool is_bias(int i) {
+    return (i >= OFF_B1 && i < OFF_B1 + HID) || (i >= OFF_B2 && i < OFF_B2 + HID) || (i >= OFF_B3 && i < OFF_B3 + L);
+}
+
 __global__ void k_adam(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
                        float *__restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2,
-                       bf16 *__restrict__ w1b, bf16 *__restrict__ w2b, bf16 *__restrict__ w3b) {
+                       bf16 *__restrict__ w1b, bf16 *__restrict__ w2b, bf16 *__restrict__ w3b, int no_bias) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (no_bias && is_bias(i)) return;  // held at zero
     const float gi = g[i];
     const float mi = b1 * m[i] + (1.f - b1) * gi;
     const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
@@ -607,6 +613,22 @@ int pcf_net_apply_device(pcf_net *w, const void *in, int nx, int ny, int nz, dou
     return rc;
 }
 
+int pcf_net_set_bias_free(pcf_net *w, int on) {
+    if (!w) return PCF_EINVAL;
+    using namespace pcf::net;
+    Net &n = w->n;
+    PCF_CUDA_TRY(cudaSetDevice(n.device));
+    n.no_bias = on ? 1 : 0;
+    if (on) {
+        const int offs[3] = {OFF_B1, OFF_B2, OFF_B3}, lens[3] = {HID, HID, L};
+        for (int q = 0; q < 3; ++q)
+            for (float *a : {n.param, n.m, n.v})
+                PCF_CUDA_TRY(cudaMemsetAsync(a + offs[q], 0, sizeof(float) * lens[q], n.stream));
+        PCF_CUDA_TRY(cudaStreamSynchronize(n.stream));
+    }
+    return PCF_OK;
+}
+
 // Host-array forward (tests): out = N(in), both nz x ny x nx doubles.
 int pcf_net_forward(pcf_net *w, const double *in, int nx, int ny, int nz, double *out) {
     if (!w || !in || !out) return PCF_EINVAL;
@@ -646,7 +668,7 @@ int pcf_net_train_step(pcf_net *w, const float *b, const float *x, int nx, int n
         const float b1 = 0.9f, b2 = 0.999f;
         const float c1 = 1.f - std::pow(b1, (float)n.step), c2 = 1.f - std::pow(b2, (float)n.step);
         k_adam<<<(NPARAM + 255) / 256, 256, 0, n.stream>>>(n.param, n.grad, n.m, n.v, NPARAM, (float)lr, b1, b2,
-                                                           1e-8f, c1, c2, n.w1b, n.w2b, n.w3b);
+                                                           1e-8f, c1, c2, n.w1b, n.w2b, n.w3b, n.no_bias);
         PCF_CUDA_TRY(cudaGetLastError());
     }
     double s[3];

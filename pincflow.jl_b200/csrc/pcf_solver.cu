@@ -793,7 +793,34 @@ struct LoopCfg {
     int flex;      // accumulate x from the preconditioned directions (FP32 inner loop)
     int reliable;  // fold into the FP64 solution and restart r from the true residual
     int mg = 0;    // multigrid V-cycle as the preconditioner (FP32 loop only)
+    int learned_pc = 0;  // learned stage after the preconditioner (FP32 loop only)
 };
+
+// The learned preconditioner stage on the preconditioner's s-space output z
+// (in place): r2 = bvec - A z, c = N(r2), z = (z + c) / fcscal.  The network
+// is bias-free, hence N(a r2) = a N(r2), and needs no normalisation of r2.
+static int learned_stage(pcf_handle *h, const Work<float> &w, const float *bvec, float *z, const KrylovScalars *guard) {
+    float *r2 = h->lr32, *cc = h->lr32 + h->d.n;
+    StencilArgs<float> sa;
+    sa.coef = w.coef;
+    sa.s = z;
+    sa.out = r2;
+    sa.w1 = bvec;
+    sa.deta = 0;
+    sa.guard = guard;
+    int rc = launch_stencil<float, false, EPI_RESNR>(h, sa);
+    if (rc) return rc;
+    {
+        ProfScope ps(h, PCF_PROF_LEARNED, 8.0 * h->d.n);
+        h->launches += 6;  // gather, 3 GEMMs, 2 convolutions (the scope counts the scatter)
+        if ((rc = pcf_net_apply_device(h->net, r2, h->d.nx, h->d.ny, h->d.nz, 1.0, 1.0, 0.0, cc, 0, h->stream)))
+            return rc;
+    }
+    h->launches += 1;
+    k_learned_combine<<<vec_grid(h->d.n), 256, 0, h->stream>>>(z, cc, w.post, h->d.n, guard);
+    PCF_CUDA_TRY(cudaGetLastError());
+    return PCF_OK;
+}
 
 // Reliable update (mixed precision): x64 += bnorm64 x32, r64 = b - A64 x64
 // with the FP64 convergence test, r32 = r64 / bnorm64, <r32, r0>.  The three
@@ -828,10 +855,12 @@ static int bicgstab_iteration(pcf_handle *h, const Work<T> &w, const LoopCfg &c)
     // p = r + beta (p - omega v); z = M p
     if (c.precond) {
         if constexpr (sizeof(T) == 4) {
+            const float *post = c.learned_pc ? nullptr : w.post;
             if (c.mg)
-                rc = mg_precond<TH_PUPD>(h, w, w.p, w.scal, &z, w.za, w.zb, w.post);
+                rc = mg_precond<TH_PUPD>(h, w, w.p, w.scal, &z, w.za, w.zb, post);
             else
-                rc = precond_apply<T, TH_PUPD>(h, w, w.p, c.pc_iters, c.deta, w.scal, &z, nullptr, nullptr, w.post);
+                rc = precond_apply<T, TH_PUPD>(h, w, w.p, c.pc_iters, c.deta, w.scal, &z, nullptr, nullptr, post);
+            if (!rc && c.learned_pc) rc = learned_stage(h, w, w.p, z, w.scal);
         } else {
             rc = precond_apply<T, TH_PUPD>(h, w, w.p, c.pc_iters, c.deta, w.scal, &z, nullptr, nullptr, w.post);
         }
@@ -860,15 +889,20 @@ static int bicgstab_iteration(pcf_handle *h, const Work<T> &w, const LoopCfg &c)
     // s = r - alpha v; z = M s
     if (c.precond) {
         bool done = false;
+        const T *post = w.post;
         if constexpr (sizeof(T) == 4) {
+            if (c.learned_pc) post = nullptr;
             if (c.mg) {
-                rc = mg_precond<TH_SUPD>(h, w, w.s, w.scal, &z, w.zc, w.zd, w.post);
+                rc = mg_precond<TH_SUPD>(h, w, w.s, w.scal, &z, w.zc, w.zd, post);
                 done = true;
             }
         }
         if (!done)
             rc = precond_apply<T, TH_SUPD>(h, w, w.s, c.pc_iters, c.deta, w.scal, &z, c.flex ? w.zc : w.za,
-                                           c.flex ? w.zd : w.zb, w.post);
+                                           c.flex ? w.zd : w.zb, post);
+        if constexpr (sizeof(T) == 4) {
+            if (!rc && c.learned_pc) rc = learned_stage(h, w, w.s, z, w.scal);
+        }
     } else {
         h->launches += 1;
         k_axpy_noprec<T, TH_SUPD><<<vec_grid(h->d.n), 256, 0, h->stream>>>(w.r, w.v, w.s, h->d.n, w.scal);
@@ -933,10 +967,11 @@ struct GraphKey {
     int tsize, precond, pc_iters, flex, reliable, pi, batch;
     double deta;
     int mg, mg_levels, mg_coarse_iters;
+    const void *net;  // the learned stage's network (null: no stage)
     bool operator==(const GraphKey &o) const {
         return tsize == o.tsize && precond == o.precond && pc_iters == o.pc_iters && flex == o.flex &&
                reliable == o.reliable && pi == o.pi && batch == o.batch && deta == o.deta && mg == o.mg &&
-               mg_levels == o.mg_levels && mg_coarse_iters == o.mg_coarse_iters;
+               mg_levels == o.mg_levels && mg_coarse_iters == o.mg_coarse_iters && net == o.net;
     }
 };
 struct GraphEntry {
@@ -1048,7 +1083,8 @@ static int run_finish(pcf_handle *h, const Work<T> &w, const LoopCfg &c, bool pr
 
 static GraphKey graph_key(const pcf_handle *h, int tsize, const LoopCfg &c, bool pi, int check_interval) {
     return GraphKey{tsize, c.precond, c.pc_iters, c.flex, c.reliable, pi, check_interval, c.deta, c.mg,
-                    c.mg && h->mg ? (int)h->mg->lv.size() : 0, c.mg && h->mg ? h->mg->coarse_iters : 0};
+                    c.mg && h->mg ? (int)h->mg->lv.size() : 0, c.mg && h->mg ? h->mg->coarse_iters : 0,
+                    c.learned_pc ? (const void *)h->net : nullptr};
 }
 
 // A complete BiCGSTAB run: run_start, the iteration batches, run_finish.
@@ -1210,7 +1246,7 @@ int pcf_destroy(pcf_handle *h) {
     int dev = h->dims.device;
     cudaSetDevice(dev);
     void *ptrs[] = {h->jac, h->met13, h->met23, h->met33, h->pbar, h->rhobar, h->thetabar, h->n2, h->rho, h->betar,
-                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch, h->stage, h->corr,
+                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch, h->stage, h->corr, h->lr32,
                     h->x64, h->r64, h->r064, h->p64, h->v64, h->s64,
                     h->t64, h->za64, h->zb64, h->b64, h->w64, h->x32, h->r32, h->r032, h->p32, h->v32, h->s32,
                     h->t32, h->za32, h->zb32, h->zc32, h->zd32, h->partials, h->ticket, h->scal64, h->scal32,
@@ -1831,7 +1867,7 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
     if ((rc = true_residual(h, h->b64, h->x64, &rnorm))) return rc;
     const double b_norm = rnorm;
     res->b_norm = b_norm;
-    if (prm->learned && h->net && b_norm > 0 && std::isfinite(b_norm)) {
+    if ((prm->learned & 1) && h->net && b_norm > 0 && std::isfinite(b_norm)) {
         // learned warm start: x0 = RMS(b) N(b / RMS(b)), then the FP64 residual of x0
         h->launches += 6;
         rc = pcf_net_apply_device(h->net, h->b64, h->d.nx, h->d.ny, h->d.nz, 1.0 / b_norm, b_norm, 0.0, h->x64, 1,
@@ -1869,6 +1905,15 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
         cm.deta = h->mg->lv[0].deta;
     }
     if (prm->autotune && (rc = autotune_handle(h, prm))) return rc;
+    if ((prm->learned & 2) && h->net && c.precond) {
+        if (!h->lr32 && (rc = dalloc(h, (void **)&h->lr32, 2 * sizeof(float) * (size_t)h->d.n))) return rc;
+        // one forward outside any graph capture (the GEMM's first launch sets its attributes)
+        PCF_CUDA_TRY(cudaMemsetAsync(h->lr32, 0, 2 * sizeof(float) * (size_t)h->d.n, h->stream));
+        if ((rc = pcf_net_apply_device(h->net, h->lr32, h->d.nx, h->d.ny, h->d.nz, 1.0, 1.0, 0.0,
+                                       h->lr32 + h->d.n, 0, h->stream)))
+            return rc;
+        cm.learned_pc = 1;
+    }
     double rel = rnorm / b_norm;
     int restarts = 0;
     for (;;) {

@@ -42,8 +42,10 @@ def _bind(lib):
                                        dp, fp]
     lib.pcf_net_gradients.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, fp]
     lib.pcf_set_network.argtypes = [vp, vp]
+    lib.pcf_net_set_bias_free.argtypes = [vp, ctypes.c_int]
     for name in ("pcf_net_create", "pcf_net_destroy", "pcf_net_get_params", "pcf_net_set_params", "pcf_net_save",
-                 "pcf_net_load", "pcf_net_forward", "pcf_net_train_step", "pcf_net_gradients", "pcf_set_network"):
+                 "pcf_net_load", "pcf_net_forward", "pcf_net_train_step", "pcf_net_gradients", "pcf_set_network",
+                 "pcf_net_set_bias_free"):
         getattr(lib, name).restype = ctypes.c_int
     lib._net_bound = True
     return lib
@@ -96,6 +98,10 @@ class LearnedNet:
 
     def load(self, path: str):
         _lib.check(self.lib.pcf_net_load(self._h, path.encode()), "pcf_net_load")
+
+    def set_bias_free(self, on: bool = True):
+        """Hold the biases at zero: N(a x) = a N(x) for a > 0 (the preconditioner stage)."""
+        _lib.check(self.lib.pcf_net_set_bias_free(self._h, int(bool(on))), "pcf_net_set_bias_free")
 
     def forward(self, field: np.ndarray) -> np.ndarray:
         """N(field) for a host array of shape (nz, ny, nx)."""
@@ -154,6 +160,35 @@ def training_pairs(indices, nx=128, ny=128, nz=64, tolerance=1e-8, device=0):
     return out
 
 
+def preconditioner_pairs(indices, nx=128, ny=128, nz=64, tolerance=1e-8, device=0, **mg):
+    """(r2 / RMS(r2), e / RMS(r2)) FP32 pairs for the learned preconditioner
+    stage: for a training right-hand side b with plain FP64 solution s*, the
+    multigrid V-cycle's output z = M(b) leaves the residual r2 = b - A z and
+    the error e = s* - z, which the stage N(r2) should approximate."""
+    out = []
+    solver = None
+    nl_mg = PoissonNamelist(precision="mixed", multigrid=True, **mg)
+    for i in indices:
+        cfg = C.c3(int(i), nx=nx, ny=ny, nz=nz)
+        if solver is None:
+            solver = PoissonSolver(cfg["dom"], cfg["model"], device=device)
+        solver.set_grid(cfg["fields"])
+        solver.set_background(cfg["fields"])
+        solver.compute_operator(cfg["rho"], cfg["betar"], cfg["dt"], cfg["rayleigh_factor"], return_coef=False)
+        nl = PoissonNamelist(tolerance=tolerance, tolerance_is_relative=True, poisson_iterations=5000)
+        s, info = solver.apply_bicgstab(cfg["rhs"], 1.0, nl)
+        if info.errflag:
+            continue
+        z = solver.apply_multigrid(cfg["rhs"], nl_mg)
+        r2 = cfg["rhs"] - solver.apply_operator(z)
+        e = s - z
+        sc = float(np.sqrt(np.mean(r2 ** 2)))
+        out.append(((r2 / sc).astype(np.float32), (e / sc).astype(np.float32)))
+    if solver is not None:
+        solver.close()
+    return out
+
+
 def train(net: LearnedNet, pairs, epochs: int = 4, lr: float = 1e-3, device: int = 0, log=None):
     """Adam over the pairs (one sample per step), on device.  Returns the
     per-step losses."""
@@ -196,11 +231,37 @@ def evaluate(net: LearnedNet, indices, nx=128, ny=128, nz=64, device=0, **nameli
     return out
 
 
+def evaluate_stage(net: LearnedNet, indices, nx=128, ny=128, nz=64, device=0):
+    """Multigrid mixed solves with and without the learned preconditioner
+    stage on configs.c3(index) problems:
+    [(index, niter_without, niter_with, ms_without, ms_with)]."""
+    out = []
+    for i in indices:
+        cfg = C.c3(int(i), nx=nx, ny=ny, nz=nz)
+        with PoissonSolver(cfg["dom"], cfg["model"], device=device) as s:
+            s.set_grid(cfg["fields"])
+            s.set_background(cfg["fields"])
+            dpip = np.zeros(cfg["dom"].halo_shape)
+            args = (cfg["rhs"], cfg["rho"], cfg["betar"], cfg["dt"], cfg["rayleigh_factor"], cfg["tolref"])
+            kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=5000, precision="mixed",
+                      residual="true", multigrid=True)
+            s.solve_poisson(*args, PoissonNamelist(**kw), dpip)
+            a = s.solve_poisson(*args, PoissonNamelist(**kw), dpip)
+            s.attach_network(net)
+            s.solve_poisson(*args, PoissonNamelist(**kw, learned=2), dpip)
+            b = s.solve_poisson(*args, PoissonNamelist(**kw, learned=2), dpip)
+            s.attach_network(None)
+        out.append((int(i), a.niter, b.niter, a.timings_ms["solve"], b.timings_ms["solve"]))
+    return out
+
+
 def main(argv=None):
-    """Training run of the learned warm start on the training configuration
-    (configs.c3): generates the (rhs, solution) pairs with the plain FP64
-    solver, trains with Adam on the GPU, evaluates the warm start on held-out
-    problems, and writes the weights file."""
+    """Training run of the learned part on the training configuration
+    (configs.c3): generates the training pairs with the plain FP64 solver,
+    trains with Adam on the GPU, evaluates on held-out problems, and writes
+    the weights file.  --stage trains the bias-free preconditioner stage on
+    the multigrid V-cycle's (residual, error) pairs instead of the warm
+    start on (rhs, solution) pairs."""
     import argparse
     import json
     ap = argparse.ArgumentParser(description=main.__doc__)
@@ -211,24 +272,31 @@ def main(argv=None):
     ap.add_argument("--eval", type=int, default=8, help="held-out problems (configs.c3 indices from 100000)")
     ap.add_argument("--out", default=None, help="weights file to write")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--stage", action="store_true", help="train the preconditioner stage (bias-free)")
     a = ap.parse_args(argv)
     nx, ny, nz = (int(v) for v in a.size.lower().split("x"))
     t0 = time.time()
-    pairs = training_pairs(range(a.pairs), nx=nx, ny=ny, nz=nz, device=a.device)
+    make = preconditioner_pairs if a.stage else training_pairs
+    pairs = make(range(a.pairs), nx=nx, ny=ny, nz=nz, device=a.device)
     t1 = time.time()
     net = LearnedNet(device=a.device, max_columns=nx * ny, seed=0)
+    if a.stage:
+        net.set_bias_free(True)
     losses = train(net, pairs, epochs=a.epochs, lr=a.lr, device=a.device,
                    log=lambda m: print(m, flush=True))
     t2 = time.time()
     if a.out:
         net.save(a.out)
     held = range(100000, 100000 + a.eval)
-    ev_ref = evaluate(net, held, nx, ny, nz, a.device)
-    ev_mg = evaluate(net, held, nx, ny, nz, a.device, multigrid=True)
-    summary = dict(pairs=len(pairs), size=[nx, ny, nz], generation_s=t1 - t0, training_s=t2 - t1,
-                   steps=len(losses), loss_first_epoch=float(np.mean(losses[:len(pairs)])),
-                   loss_last_epoch=float(np.mean(losses[-len(pairs):])),
-                   warm_start_reference_preconditioner=ev_ref, warm_start_multigrid=ev_mg)
+    summary = dict(role="preconditioner stage" if a.stage else "warm start", pairs=len(pairs), size=[nx, ny, nz],
+                   generation_s=t1 - t0, training_s=t2 - t1, steps=len(losses),
+                   loss_first_epoch=float(np.mean(losses[:len(pairs)])),
+                   loss_last_epoch=float(np.mean(losses[-len(pairs):])))
+    if a.stage:
+        summary["stage_multigrid"] = evaluate_stage(net, held, nx, ny, nz, a.device)
+    else:
+        summary["warm_start_reference_preconditioner"] = evaluate(net, held, nx, ny, nz, a.device)
+        summary["warm_start_multigrid"] = evaluate(net, held, nx, ny, nz, a.device, multigrid=True)
     print(json.dumps(summary), flush=True)
     net.close()
     return summary

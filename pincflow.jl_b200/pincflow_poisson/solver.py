@@ -45,7 +45,7 @@ class PoissonNamelist:
     residual: str = "recursive"      # "recursive" | "true"
     inner_tolerance: float = 1.0e-2   # mixed: residual drop between FP64 reliable updates
     max_refinements: int = 5          # mixed: restarts of the FP32 iteration after a breakdown
-    learned: bool = False
+    learned: int = 0                  # mixed, bit set: 1 learned warm start, 2 learned preconditioner stage
     check_interval: int = 4
     restart_interval: int = 1         # mixed: Krylov restart at every n-th reliable update (0: never)
     multigrid: bool = False           # mixed: horizontal aggregation multigrid V-cycle as the preconditioner
@@ -68,7 +68,7 @@ class PoissonNamelist:
         p.residual = _lib.RESIDUAL[self.residual]
         p.inner_tolerance = float(self.inner_tolerance)
         p.max_refinements = int(self.max_refinements)
-        p.learned = int(bool(self.learned))
+        p.learned = int(self.learned)
         p.check_interval = int(self.check_interval)
         p.restart_interval = int(self.restart_interval)
         p.multigrid = int(bool(self.multigrid))

@@ -113,3 +113,52 @@ def test_training_reduces_loss_and_warm_start_gains(netmod):
                 h_on = s.residual_history()
                 gains.append((off.niter, on.niter))
         print("iterations without / with the learned warm start:", gains)
+
+
+def test_bias_free_network_is_positively_homogeneous(netmod):
+    learned, NO = netmod
+    p = _random_params(NO, 6)
+    b = np.random.default_rng(7).standard_normal((64, 8, 8))
+    with learned.LearnedNet(max_columns=64) as net:
+        net.set_params(p)
+        net.set_bias_free(True)
+        q = NO.unpack(net.get_params())
+        assert not q["b1"].any() and not q["b2"].any() and not q["b3"].any()
+        y1, y2 = net.forward(b), net.forward(3.0 * b)
+    assert _normwise(y2, 3.0 * y1) < 1e-2
+
+
+def test_learned_preconditioner_stage(netmod):
+    """The bias-free network trained on the multigrid V-cycle's (residual,
+    error) pairs serves as a stage of the flexible FP32 BiCGSTAB's right
+    preconditioner, z = M(r) + N(r - A M(r)): the solve still reaches the FP64
+    true residual 1e-10, and the iteration counts with and without the stage
+    are recorded."""
+    learned, _ = netmod
+    import pincflow_poisson as pcf
+    from pincflow_poisson import configs as C
+    pairs = learned.preconditioner_pairs(range(12), nx=32, ny=32, nz=64)
+    assert len(pairs) == 12
+    with learned.LearnedNet(max_columns=32 * 32, seed=2) as net:
+        net.set_bias_free(True)
+        losses = learned.train(net, pairs, epochs=25, lr=2e-3)
+        assert np.mean(losses[-12:]) < np.mean(losses[:12])
+        counts = []
+        for i in range(100, 104):
+            cfg = C.c3(i, nx=32, ny=32, nz=64)
+            with pcf.PoissonSolver(cfg["dom"], cfg["model"]) as s:
+                s.set_grid(cfg["fields"])
+                s.set_background(cfg["fields"])
+                s.compute_operator(cfg["rho"], cfg["betar"], cfg["dt"], cfg["rayleigh_factor"], return_coef=False)
+                s.attach_network(net)
+                kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=4000, precision="mixed",
+                          multigrid=True)
+                _, off = s.apply_bicgstab(cfg["rhs"], 1.0, pcf.PoissonNamelist(**kw))
+                x, on = s.apply_bicgstab(cfg["rhs"], 1.0, pcf.PoissonNamelist(learned=2, **kw))
+                assert not off.errflag and not on.errflag, (off, on)
+                assert on.true_residual <= 1e-10
+                r = cfg["rhs"] - s.apply_operator(x)
+                assert np.sqrt(np.mean(r ** 2)) / np.sqrt(np.mean(cfg["rhs"] ** 2)) <= 1.5e-10
+                counts.append((off.niter, on.niter))
+        print("multigrid iterations without / with the learned stage:", counts)
+        assert all(b <= 2 * a + 4 for a, b in counts), counts
