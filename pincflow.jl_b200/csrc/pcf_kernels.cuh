@@ -642,6 +642,84 @@ __global__ void __launch_bounds__(128) k_thomas(ThomasArgs<T> a) {
     }
 }
 
+// The column solve for the coarse multigrid levels (TH_B or TH_T, no
+// post-scaling), where few columns leave the column-per-thread sweep with too
+// little parallelism to hide its serial chain of loads: LPC threads per
+// column, each holding a run of at most CH = 8 consecutive levels.  Both
+// sweeps are first-order linear recurrences (y_k = rhs_k P_k + M_k y_k-1 up,
+// x_k = y_k + Q_k x_k+1 down), so each thread loads its whole run at once,
+// composes the run's affine maps, the composites of a column's runs are
+// chained through shared memory, and each run is then swept in registers.
+// Block (32, LPC): warp w holds run w of 32 adjacent columns, so every load
+// and store instruction covers a full 128-byte line.
+template <int MODE, int LPC>
+__global__ void __launch_bounds__(32 * LPC) k_thomas_split(ThomasArgs<float> a) {
+    constexpr int CH = 8;
+    if (krylov_done(a.scal)) return;
+    __shared__ float sa[LPC][32], sb[LPC][32];
+    const int lane = threadIdx.x, part = threadIdx.y;
+    const long long col = blockIdx.x * 32LL + lane;
+    const bool valid = col < a.plane;
+    const float *__restrict__ P = a.fac;
+    const float *__restrict__ M = a.fac + a.n;
+    const float *__restrict__ Q = a.fac + 2 * a.n;
+    const long long pl = a.plane;
+    const int per = (a.nz + LPC - 1) / LPC;  // <= CH (checked by the host)
+    const int kb = part * per;
+    // levels of this run inside the column; the others are identity maps in
+    // both sweeps (P = 0, M = 1 up; y = 0, Q = 1 down)
+    const int nv = valid ? max(0, min(per, a.nz - kb)) : 0;
+    const float deta = (float)a.deta;
+    float yv[CH], pp[CH], mm[CH], qq[CH];
+    // the run's loads, all issued before any use
+#pragma unroll
+    for (int q = 0; q < CH; ++q) {
+        const int k = kb + q;
+        const bool on = q < nv;
+        const long long o = col + pl * (on ? k : 0);
+        yv[q] = on ? a.in[o] : 0.f;
+        pp[q] = on ? __ldg(P + o) : 0.f;
+        mm[q] = on ? __ldg(M + o) : 1.f;
+        qq[q] = !on ? 1.f : (k != a.nz - 1 ? __ldg(Q + o) : 0.f);
+    }
+    // forward composite y_out = A + B y_in (identity maps past the run)
+    float A = 0.f, B = 1.f;
+#pragma unroll
+    for (int q = 0; q < CH; ++q) {
+        yv[q] = (MODE == TH_B ? -deta * yv[q] : yv[q]) * pp[q];
+        A = mm[q] * A + yv[q];
+        B = mm[q] * B;
+    }
+    sa[part][lane] = A;
+    sb[part][lane] = B;
+    __syncthreads();
+    float y = 0.f;
+    for (int w = 0; w < part; ++w) y = sb[w][lane] * y + sa[w][lane];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < CH; ++q) {
+        y = mm[q] * y + yv[q];
+        yv[q] = q < nv ? y : 0.f;
+    }
+    // backward composite x_kb = C + D x_(kb + per), x_nz = 0
+    float C = 0.f, D = 1.f;
+#pragma unroll
+    for (int q = CH - 1; q >= 0; --q) {
+        C = qq[q] * C + yv[q];
+        D = qq[q] * D;
+    }
+    sa[part][lane] = C;
+    sb[part][lane] = D;
+    __syncthreads();
+    float x = 0.f;
+    for (int w = LPC - 1; w > part; --w) x = sb[w][lane] * x + sa[w][lane];
+#pragma unroll
+    for (int q = CH - 1; q >= 0; --q) {
+        x = qq[q] * x + yv[q];
+        if (q < nv) a.out[col + pl * (kb + q)] = x;
+    }
+}
+
 // ------------------------------------------------------- vector updates --
 
 template <typename T>

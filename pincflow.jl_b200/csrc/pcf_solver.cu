@@ -496,23 +496,27 @@ struct MgState {
 
 __global__ void k_to_float(const double *__restrict__ a, float *__restrict__ b, long long n, double scale);
 
-// Columns per level up to which the coarse-level column solves use a warp per
-// column.  Above it the column-per-thread sweep has enough columns in flight
-// to stream at bandwidth, while the warp form's per-lane level loads touch a
-// sector per lane (measured 27 us against about 10 us at 128 x 128 x 128).
-constexpr int kWarpThomasColumns = 4096;
+// Coarse levels with few columns: k_thomas_split (runs of at most 8 levels,
+// up to 32 threads per column); otherwise the column-per-thread sweep.
+constexpr int kSplitThomasColumns = 16384;
 
 template <int MODE>
 static int mg_thomas(pcf_handle *h, const MgLevel &L, const ThomasArgs<float> &a, int tag) {
-    if (L.d.nz <= 32 * kLevelsPerLane && L.d.plane <= kWarpThomasColumns && (MODE == TH_B || MODE == TH_T) &&
-        a.post == nullptr) {
-        ProfScope ps(h, tag, 7.0 * 4 * (double)a.n);
-        const long long threads = 32LL * L.d.plane;
-        k_thomas_warp<MODE><<<(unsigned)((threads + 127) / 128), 128, 0, h->stream>>>(a);
-        PCF_CUDA_TRY(cudaGetLastError());
-        return PCF_OK;
+    int lpc = 1;
+    while (lpc < 32 && (a.nz + lpc - 1) / lpc > 8) lpc *= 2;
+    if (L.d.plane > kSplitThomasColumns || (a.nz + lpc - 1) / lpc > 8 || a.post != nullptr || lpc < 2)
+        return launch_thomas<float, MODE>(h, a, tag);
+    ProfScope ps(h, tag, 6.0 * 4 * (double)a.n);
+    const unsigned grid = (unsigned)((a.plane + 31) / 32);
+    switch (lpc) {
+        case 2: k_thomas_split<MODE, 2><<<grid, dim3(32, 2), 0, h->stream>>>(a); break;
+        case 4: k_thomas_split<MODE, 4><<<grid, dim3(32, 4), 0, h->stream>>>(a); break;
+        case 8: k_thomas_split<MODE, 8><<<grid, dim3(32, 8), 0, h->stream>>>(a); break;
+        case 16: k_thomas_split<MODE, 16><<<grid, dim3(32, 16), 0, h->stream>>>(a); break;
+        default: k_thomas_split<MODE, 32><<<grid, dim3(32, 32), 0, h->stream>>>(a); break;
     }
-    return launch_thomas<float, MODE>(h, a, tag);
+    PCF_CUDA_TRY(cudaGetLastError());
+    return PCF_OK;
 }
 
 static ThomasArgs<float> mg_targs(const MgLevel &L, const float *fac, const float *in, float *out,
