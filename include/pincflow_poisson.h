@@ -234,6 +234,57 @@ int pcf_apply_corrector_device(pcf_handle *h, double *d_u, double *d_v, double *
                                const double *d_heating, double dt, double rayleigh_factor, const pcf_params *prm,
                                double *d_dpip, pcf_result *res);
 
+/* The implicit half step around the solve (src/Integration/
+ * implicit_integration!.jl:49-77, one rank, no tracers).  All arrays are the
+ * reference's haloed FP64 predictands and need nz > nbz.
+ *
+ * pcf_set_predictand_boundaries_device replaces set_boundaries!(state,
+ * BoundaryPredictands()) (src/Boundaries/set_boundaries!.jl:46-60): x and y
+ * periodic; in z rho and rhop point-reflected, u, v, pip and p
+ * line-reflected, w zero on both walls and point-reflected
+ * (set_vertical_boundaries!.jl:185-240).  rho is filled for the
+ * PseudoIncompressible and Compressible models (NULL allowed for
+ * Boussinesq), p for Compressible (else NULL allowed).
+ *
+ * pcf_modify_compressible_wind_device replaces modify_compressible_wind!(
+ * state, *) (divide = 0) and (state, /) (divide = 1)
+ * (src/Integration/modify_compressible_wind!.jl:38-80); a no-op unless the
+ * model is Compressible.
+ *
+ * pcf_implicit_predictor_device replaces implicit_integration!.jl:53-63:
+ * save_backups!(state, :w) into d_wold (NULL: handle scratch), the implicit
+ * predictor update!(state, dt, U() / V() / W(), RHS(), Implicit(),
+ * rayleigh_factor) (src/Update/update!.jl:837-882, :988-1033, :1248-1336),
+ * set_boundaries!, update!(..., RhoP(), ...) (:632-728), set_boundaries!.
+ * d_dudt, d_dvdt are the WKB momentum tendencies (state.wkb.tendencies) of
+ * compute_volume_force.jl:159-206, or both NULL for wkb_mode = NoWKB.
+ *
+ * pcf_implicit_step_device runs the whole implicit_integration!.jl:49-77
+ * without output: modify_compressible_wind!(*), set_boundaries!, the
+ * predictor, apply_corrector! (as pcf_apply_corrector_device, d_heating as
+ * there), modify_compressible_wind!(/), set_boundaries!.  On res->errflag
+ * it returns PCF_OK with the predicted, uncorrected fields (where the
+ * reference writes output and raises).  dt == 0 returns PCF_EINVAL.
+ * pcf_implicit_step is the same with host arrays (heating interior, wold
+ * may be NULL; u, v, w, rho, rhop, pip, p, dpip and wold are written
+ * back). */
+int pcf_set_predictand_boundaries_device(pcf_handle *h, double *d_rho, double *d_rhop, double *d_u, double *d_v,
+                                         double *d_w, double *d_pip, double *d_p);
+int pcf_modify_compressible_wind_device(pcf_handle *h, const double *d_p, double *d_u, double *d_v, double *d_w,
+                                        int divide);
+int pcf_implicit_predictor_device(pcf_handle *h, double dt, double rayleigh_factor, int damp_horizontal_wind_on_rhs,
+                                  double *d_u, double *d_v, double *d_w, double *d_rho, double *d_rhop,
+                                  double *d_pip, double *d_p, const double *d_betar, const double *d_dudt,
+                                  const double *d_dvdt, double *d_wold);
+int pcf_implicit_step_device(pcf_handle *h, double dt, double rayleigh_factor, const pcf_params *prm, double *d_u,
+                             double *d_v, double *d_w, double *d_rho, double *d_rhop, double *d_pip, double *d_p,
+                             const double *d_betar, const double *d_dudt, const double *d_dvdt,
+                             const double *d_heating, double *d_wold, double *d_dpip, pcf_result *res);
+int pcf_implicit_step(pcf_handle *h, double dt, double rayleigh_factor, const pcf_params *prm, double *u, double *v,
+                      double *w, double *rho, double *rhop, double *pip, double *p, const double *betar,
+                      const double *dudt, const double *dvdt, const double *heating, double *wold, double *dpip,
+                      pcf_result *res);
+
 int pcf_apply_preconditioner(pcf_handle *h, const double *sin_, double *sout,
                              const pcf_params *prm, int precision);
 

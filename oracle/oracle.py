@@ -220,3 +220,68 @@ def dot(a, b) -> float:
     a = np.ascontiguousarray(a, dtype=np.float64).ravel()
     b = np.ascontiguousarray(b, dtype=np.float64).ravel()
     return lib().or_dot(ctypes.c_long(a.size), _p(a), _p(b))
+
+
+def set_predictand_boundaries(d: Dims, model, rho, rhop, u, v, w, pip, p=None):
+    """set_boundaries!(state, BoundaryPredictands()) in place (model: int)."""
+    pp = p if p is not None else np.zeros_like(rho)
+    lib().or_set_predictand_boundaries(ctypes.byref(d), int(model), _p(rho), _p(rhop), _p(u), _p(v), _p(w),
+                                       _p(pip), _p(pp))
+
+
+def modify_compressible_wind(d: Dims, model, f: dict, p, u, v, w, divide=False):
+    """modify_compressible_wind!(state, * or /) in place (Compressible only)."""
+    if int(model) != 2:
+        return
+    lib().or_modify_compressible_wind(ctypes.byref(d), int(model), _p(f["jac"]), _p(p), _p(u), _p(v), _p(w),
+                                      int(bool(divide)))
+
+
+def implicit_predictor(d: Dims, model, f: dict, betar, dt, rayleigh_factor, rho, rhop, u, v, w, pip, p=None,
+                       dudt=None, dvdt=None, damp_horizontal_wind_on_rhs=False):
+    """implicit_integration!.jl:53-63 on copies: returns
+    (rho, rhop, u, v, w, pip, p, wold) after save_backups!(:w), the implicit
+    U, V, W updates, set_boundaries!, the implicit RhoP update and
+    set_boundaries!.  model: int; dudt/dvdt None for NoWKB."""
+    c = constants()
+    out = [np.array(x, dtype=np.float64, copy=True) for x in (rho, rhop, u, v, w, pip)]
+    pp = np.array(p if p is not None else np.zeros_like(rho), dtype=np.float64, copy=True)
+    wold = np.zeros_like(out[4])
+    lib().or_implicit_predictor(
+        ctypes.byref(d), int(model), ctypes.c_double(f["dx"]), ctypes.c_double(f["dy"]), ctypes.c_double(f["dz"]),
+        _p(f["jac"]), _p(f["met13"]), _p(f["met23"]), _p(f["met33"]), _p(f["rhobar"]), _p(f["pbar"]),
+        _pn(f.get("thetabar")), _p(f["n2"]), _p(betar), _p(out[0]), _p(pp), ctypes.c_double(dt),
+        ctypes.c_double(rayleigh_factor), int(bool(damp_horizontal_wind_on_rhs)), ctypes.c_double(1.0 / c["kappa"]),
+        ctypes.c_double(1.0 / c["ma"] ** 2), ctypes.c_double(c["g_ndim"]), _pn(dudt), _pn(dvdt), _p(out[2]),
+        _p(out[3]), _p(out[4]), _p(out[1]), _p(out[5]), _p(wold))
+    return (*out, pp if p is not None else None, wold)
+
+
+def implicit_step(d: Dims, model_name, f: dict, betar, dt, rayleigh_factor, rho, rhop, u, v, w, pip, p=None,
+                  dudt=None, dvdt=None, heating=None, damp_horizontal_wind_on_rhs=False, **solver):
+    """implicit_integration!.jl:49-77 without output, on copies:
+    modify_compressible_wind!(*), set_boundaries!, the predictor (:53-63),
+    apply_corrector! (compute_lhs!, solve_poisson!, dpip halos, correct!),
+    modify_compressible_wind!(/), set_boundaries!.  Returns
+    (fields dict, info); on errflag the fields are those after the
+    predictor (the reference raises there)."""
+    model = MODELS[model_name]
+    rho, rhop, u, v, w, pip = [np.array(x, dtype=np.float64, copy=True) for x in (rho, rhop, u, v, w, pip)]
+    p = None if p is None else np.array(p, dtype=np.float64, copy=True)
+    modify_compressible_wind(d, model, f, p, u, v, w)
+    set_predictand_boundaries(d, model, rho, rhop, u, v, w, pip, p)
+    rho, rhop, u, v, w, pip, p, wold = implicit_predictor(
+        d, model, f, betar, dt, rayleigh_factor, rho, rhop, u, v, w, pip, p=p, dudt=dudt, dvdt=dvdt,
+        damp_horizontal_wind_on_rhs=damp_horizontal_wind_on_rhs)
+    rhs, tolref = compute_lhs(d, f, u, v, w, model=model_name, heating=heating)
+    dpip, info = solve_poisson(d, model, f, rho, betar, rhs, dt, rayleigh_factor, tolref=tolref,
+                               damp_horizontal_wind_on_rhs=damp_horizontal_wind_on_rhs, p=p, **solver)
+    out = dict(rho=rho, rhop=rhop, u=u, v=v, w=w, pip=pip, p=p, wold=wold, dpip=dpip, rhs=rhs)
+    if info["errflag"]:
+        return out, info
+    dpip, u, v, w, rhop, pip = correct(d, model, f, rho, betar, dt, rayleigh_factor, dpip, u, v, w, rhop, pip,
+                                       damp_horizontal_wind_on_rhs=damp_horizontal_wind_on_rhs, p=p)
+    modify_compressible_wind(d, model, f, p, u, v, w, divide=True)
+    set_predictand_boundaries(d, model, rho, rhop, u, v, w, pip, p)
+    out.update(rho=rho, rhop=rhop, u=u, v=v, w=w, pip=pip, p=p, dpip=dpip)
+    return out, info

@@ -159,6 +159,28 @@ void or_correct(const or_dims *d, int model, double dx, double dy, double dz, co
                 double kappainv, double mainv2, double g_ndim, double *dpip, double *u, double *v,
                 double *w, double *rhop, double *pip);
 
+/* The implicit half step around the corrector (implicit_integration!.jl:
+ * 49-77 without output), one rank, no tracers.
+ * or_set_predictand_boundaries: set_boundaries!(state, BoundaryPredictands())
+ * (periodic x/y; in z rho, rhop point-reflected, u, v, pip, p
+ * line-reflected, w zero on the walls and point-reflected); rho is filled
+ * for models 1 and 2, p for model 2.  or_modify_compressible_wind:
+ * modify_compressible_wind!(state, * or /) (Compressible only; divide = 1
+ * for /).  or_implicit_predictor: save_backups!(state, :w) into wold, then
+ * update!(U, V, W; Implicit()), set_boundaries!, update!(RhoP; Implicit()),
+ * set_boundaries! (:53-63); dudt, dvdt are the WKB momentum tendencies or
+ * NULL (NoWKB).  All arrays haloed. */
+void or_set_predictand_boundaries(const or_dims *d, int model, double *rho, double *rhop, double *u, double *v,
+                                  double *w, double *pip, double *p);
+void or_modify_compressible_wind(const or_dims *d, int model, const double *jac, const double *p, double *u,
+                                 double *v, double *w, int divide);
+void or_implicit_predictor(const or_dims *d, int model, double dx, double dy, double dz, const double *jac,
+                           const double *met13, const double *met23, const double *met33, const double *rhobar,
+                           const double *pbar, const double *thetabar, const double *n2, const double *betar,
+                           double *rho, double *p, double dt, double rayleigh_factor, int damp_h, double kappainv,
+                           double mainv2, double g_ndim, const double *dudt, const double *dvdt, double *u,
+                           double *v, double *w, double *rhop, double *pip, double *wold);
+
 /* Helpers for tests and the CPU baseline. */
 double or_dot(long n, const double *a, const double *b); /* pairwise FP64 sum */
 void or_set_threads(int n);

@@ -1,9 +1,14 @@
-// pcf_correct.cu -- the corrector after the Poisson solve (apply_corrector!.jl:
-// 58-61) on the device: the boundary fill of dpip, then correct!.jl:164-385
-// with compute_pressure_gradient.jl:108-297, compute_compressible_wind_factor
-// .jl:102-157 and compute_buoyancy_factor.jl:108-172.  FP64 throughout, one
-// thread per (staggered) cell; each kernel reads a few haloed fields and
-// writes one or two, so they are memory-bound and run once per solve.
+// pcf_correct.cu -- the implicit half step around the Poisson solve on the
+// device.  Before the solve (implicit_integration!.jl:49-63): the implicit
+// predictor update!(..., U/V/W/RhoP, RHS(), Implicit(), rf) (update!.jl:
+// 632-728, :837-882, :988-1033, :1248-1336), set_boundaries!(state,
+// BoundaryPredictands()) and modify_compressible_wind!.jl:38-80.  After it
+// (apply_corrector!.jl:58-61): the boundary fill of dpip, then
+// correct!.jl:164-385.  Both use compute_pressure_gradient.jl:108-297,
+// compute_compressible_wind_factor.jl:102-157 and compute_buoyancy_factor.jl:
+// 108-172.  FP64 throughout, one thread per (staggered) cell; each kernel
+// reads a few haloed fields and writes one or two, so they are memory-bound
+// and run once per solve.
 //
 // Index conventions as in pcf_assemble.cu: interior cell (ii, jj, kk) is the
 // haloed cell (ii + nbx, jj + nby, kk + nbz); one rank (ko = 0, z_size = nz).
@@ -17,6 +22,9 @@ struct CorrectArgs {
     double kappainv, mainv2, g_ndim;
     const double *jac, *met13, *met23, *met33, *rhobar, *pbar, *thetabar, *n2, *betar, *rho, *p;
     double *dpip, *u, *v, *w, *rhop, *pip, *corx, *cory;
+    // predictor only: WKB momentum tendencies (NULL: NoWKB) and the w backup
+    const double *dudt, *dvdt;
+    double *wold;
 };
 
 struct Ix {
@@ -44,15 +52,15 @@ __global__ void __launch_bounds__(256) k_fill_dpip(CorrectArgs a) {
     }
 }
 
-// compute_pressure_gradient for U (dir 0) or V (dir 1) at the face (i+1/2, j, k) or (i, j+1/2, k)
-__device__ double grad_h(const CorrectArgs &a, const Ix &at, int i, int j, int k, int dir) {
+// compute_pressure_gradient of the field P for U (dir 0) or V (dir 1) at the
+// face (i+1/2, j, k) or (i, j+1/2, k)
+__device__ double grad_h(const CorrectArgs &a, const double *P, const Ix &at, int i, int j, int k, int dir) {
     const long long c = at(i, j, k), o = dir == 0 ? 1 : at.sy, n = c + o;
     const double *met = dir == 0 ? a.met13 : a.met23;
     const double rh = dir == 0 ? a.rdx : a.rdy;
     const double rhoe = 0.5 * (a.rho[c] + a.rho[n]) + 0.5 * (a.rhobar[c] + a.rhobar[n]);
     const double pe = 0.5 * (a.pbar[c] + a.pbar[n]);
     const double mete = 0.5 * (met[c] + met[n]);
-    const double *P = a.dpip;
     const long long z = at.sz;
     double dz;
     if (k == a.nbz) {  // bottom: one-sided
@@ -69,10 +77,10 @@ __device__ double grad_h(const CorrectArgs &a, const Ix &at, int i, int j, int k
     return a.kappainv * a.mainv2 * pe / rhoe * ((P[n] - P[c]) * rh + mete * dz * 0.5 * a.rdz);
 }
 
-// compute_pressure_gradient for W at (i, j, k+1/2)
-__device__ double grad_w(const CorrectArgs &a, const Ix &at, int i, int j, int k) {
+// compute_pressure_gradient of the field P for W at (i, j, k+1/2)
+__device__ double grad_w(const CorrectArgs &a, const double *P, const Ix &at, int i, int j, int k) {
     const long long c = at(i, j, k), u = c + at.sz;
-    const double *J = a.jac, *P = a.dpip;
+    const double *J = a.jac;
     const double jk = J[c], jk1 = J[u], rj = 1.0 / (jk + jk1);
     const double rhoe = (jk1 * a.rho[c] + jk * a.rho[u]) * rj + (jk1 * a.rhobar[c] + jk * a.rhobar[u]) * rj;
     const double pe = (jk1 * a.pbar[c] + jk * a.pbar[u]) * rj;
@@ -100,7 +108,7 @@ __global__ void __launch_bounds__(256) k_correct_uv(CorrectArgs a) {
         if (y >= 1) {  // U at i + 1/2 for i in i0-1 .. i1
             double factor = 1.0;
             if (a.damp_h) factor += a.dt * 0.5 * (a.betar[c] + a.betar[c + 1]) * a.rf;
-            const double cor = a.dt / factor * grad_h(a, at, i, j, k, 0);
+            const double cor = a.dt / factor * grad_h(a, a.dpip, at, i, j, k, 0);
             a.corx[c] = cor;
             const double wf = a.model == PCF_MODEL_COMPRESSIBLE ? (a.jac[c] * a.p[c] + a.jac[c + 1] * a.p[c + 1]) / 2 : 1.0;
             a.u[c] -= wf * cor;
@@ -109,7 +117,7 @@ __global__ void __launch_bounds__(256) k_correct_uv(CorrectArgs a) {
             const long long n = c + at.sy;
             double factor = 1.0;
             if (a.damp_h) factor += a.dt * 0.5 * (a.betar[c] + a.betar[n]) * a.rf;
-            const double cor = a.dt / factor * grad_h(a, at, i, j, k, 1);
+            const double cor = a.dt / factor * grad_h(a, a.dpip, at, i, j, k, 1);
             a.cory[c] = cor;
             const double wf = a.model == PCF_MODEL_COMPRESSIBLE ? (a.jac[c] * a.p[c] + a.jac[n] * a.p[n]) / 2 : 1.0;
             a.v[c] -= wf * cor;
@@ -135,7 +143,7 @@ __global__ void __launch_bounds__(256) k_correct_w_rhop_pip(CorrectArgs a) {
         const double *J = a.jac;
         const long long u = c + at.sz, l = c - 1, b = c - at.sy;
         const bool top = k == a.nbz + a.nz - 1, bot = k == a.nbz;
-        const double gu = top ? 0.0 : grad_w(a, at, i, j, k);
+        const double gu = top ? 0.0 : grad_w(a, a.dpip, at, i, j, k);
         if (!top) {  // W at k + 1/2 for k in k0 .. k1-1
             const double rj = 1.0 / (J[c] + J[u]);
             const double factor = 1.0 + a.dt * (J[u] * a.betar[c] + J[c] * a.betar[u]) * rj * a.rf;
@@ -155,7 +163,7 @@ __global__ void __launch_bounds__(256) k_correct_w_rhop_pip(CorrectArgs a) {
             a.w[c] += -a.dt * inv * jp * gu - inv * fw * n2e * dt2 * jp * 0.5 * cross;
         }
         // rho'
-        const double gl = bot ? 0.0 : grad_w(a, at, i, j, k - 1);
+        const double gl = bot ? 0.0 : grad_w(a, a.dpip, at, i, j, k - 1);
         const double gradient = 0.5 * (gl + gu);
         const double factor = 1.0 + a.dt * a.betar[c] * a.rf;
         const double fb = a.model == PCF_MODEL_COMPRESSIBLE ? a.pbar[c] / a.thetabar[c] / (a.rho[c] + a.rhobar[c])
@@ -169,14 +177,239 @@ __global__ void __launch_bounds__(256) k_correct_w_rhop_pip(CorrectArgs a) {
     }
 }
 
+
+// ------------------------------------------------------------ predictor --
+
+// set_boundaries!(state, BoundaryPredictands()) on one rank: x and y
+// periodic (the zonal, then the meridional pass over the full haloed range),
+// then the wall conditions in z over the full horizontal range, mode + (line
+// reflection) or - (point reflection); the staggered w is zero on both walls
+// (the haloed level k0 - 1 and the interior level k1) and point-reflected
+// about them.  With nz > nbz every ghost value is a function of interior
+// values alone, so one pass over the haloed grid fills all fields without
+// ordering.
+constexpr int kMaxFillFields = 7;
+struct FillArgs {
+    int nx, ny, nz, nxx, nyy, nbx, nby, nbz, nf;
+    double *f[kMaxFillFields];
+    double sign[kMaxFillFields];
+    int staggered[kMaxFillFields];
+};
+
+__global__ void __launch_bounds__(256) k_fill_predictands(FillArgs a) {
+    const int nzz = a.nz + 2 * a.nbz;
+    const long long nh = (long long)a.nxx * a.nyy * nzz;
+    const long long sy = a.nxx, sz = (long long)a.nxx * a.nyy;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nh; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % a.nxx), j = (int)((q / a.nxx) % a.nyy), k = (int)(q / sz);
+        const int ii = i - a.nbx, jj = j - a.nby, kk = k - a.nbz;
+        const bool hin = ii >= 0 && ii < a.nx && jj >= 0 && jj < a.ny;
+        const bool zin = kk >= 0 && kk < a.nz;
+        int si = ii % a.nx;
+        if (si < 0) si += a.nx;
+        int sj = jj % a.ny;
+        if (sj < 0) sj += a.ny;
+        const long long col = (si + a.nbx) + sy * (sj + a.nby);
+        for (int m = 0; m < a.nf; ++m) {
+            double *f = a.f[m];
+            if (a.staggered[m]) {
+                if (kk == -1 || kk == a.nz - 1) {
+                    f[q] = 0.0;
+                } else if (kk < -1) {
+                    f[q] = a.sign[m] * f[col + sz * (-kk - 2 + a.nbz)];
+                } else if (kk >= a.nz) {
+                    f[q] = a.sign[m] * f[col + sz * (2 * (a.nz - 1) - kk + a.nbz)];
+                } else if (!hin) {
+                    f[q] = f[col + sz * k];
+                }
+            } else {
+                if (hin && zin) continue;
+                if (zin) f[q] = f[col + sz * k];
+                else if (kk < 0) f[q] = a.sign[m] * f[col + sz * (-kk - 1 + a.nbz)];
+                else f[q] = a.sign[m] * f[col + sz * (2 * a.nz - 1 - kk + a.nbz)];
+            }
+        }
+    }
+}
+
+// modify_compressible_wind!.jl:52-80 on the interior: u, v, w multiplied
+// (divide = 0) or divided (divide = 1) by the compressible wind factors.
+__global__ void __launch_bounds__(256) k_modify_wind(CorrectArgs a, int divide) {
+    const long long m = (long long)a.nx * a.ny * a.nz;
+    const Ix at{a.nxx, (long long)a.nxx * a.nyy};
+    const double *J = a.jac, *P = a.p;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < m; q += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(q % a.nx), y = (int)((q / a.nx) % a.ny), z = (int)(q / ((long long)a.nx * a.ny));
+        const long long c = at(x + a.nbx, y + a.nby, z + a.nbz), r = c + 1, f = c + at.sy, t = c + at.sz;
+        // explicitly rounded products and sums (no FMA contraction), so the
+        // factors and hence u, v, w round exactly as in the reference
+        const double jpc = __dmul_rn(J[c], P[c]);
+        const double fu = __dadd_rn(jpc, __dmul_rn(J[r], P[r])) / 2;
+        const double fv = __dadd_rn(jpc, __dmul_rn(J[f], P[f])) / 2;
+        const double fw = __dmul_rn(__dmul_rn(J[c], J[t]), __dadd_rn(P[c], P[t])) / __dadd_rn(J[c], J[t]);
+        if (divide) {
+            a.u[c] = a.u[c] / fu;
+            a.v[c] = a.v[c] / fv;
+            a.w[c] = a.w[c] / fw;
+        } else {
+            a.u[c] = __dmul_rn(a.u[c], fu);
+            a.v[c] = __dmul_rn(a.v[c], fv);
+            a.w[c] = __dmul_rn(a.w[c], fw);
+        }
+    }
+}
+
+__device__ __forceinline__ double wind_factor_u(const CorrectArgs &a, long long c, long long o) {
+    return a.model == PCF_MODEL_COMPRESSIBLE ? (a.jac[c] * a.p[c] + a.jac[c + o] * a.p[c + o]) / 2 : 1.0;
+}
+__device__ __forceinline__ double wind_factor_w(const CorrectArgs &a, long long c, long long sz) {
+    if (a.model != PCF_MODEL_COMPRESSIBLE) return 1.0;
+    const double jk = a.jac[c], jk1 = a.jac[c + sz];
+    return jk * jk1 * (a.p[c] + a.p[c + sz]) / (jk + jk1);
+}
+
+// compute_volume_force(state, i, j, k, W()) (compute_volume_force.jl:185-206)
+__device__ __forceinline__ double force_w(const CorrectArgs &a, long long c, long long sz) {
+    if (!a.dudt) return 0.0;
+    const double *J = a.jac;
+    const long long u = c + sz;
+    return (J[u] * (a.met13[c] * a.dudt[c] + a.met23[c] * a.dvdt[c]) +
+            J[c] * (a.met13[u] * a.dudt[u] + a.met23[u] * a.dvdt[u])) /
+           (J[c] + J[u]);
+}
+
+// update!(U / V, RHS(), Implicit()) (update!.jl:837-882, :988-1033) over the
+// (nx + 1) x (ny + 1) x nz staggered positions of k_correct_uv, and the
+// backup wold = w (save_backups!.jl:16-24) of the whole haloed array.
+__global__ void __launch_bounds__(256) k_predict_uv(CorrectArgs a) {
+    const long long m = (long long)(a.nx + 1) * (a.ny + 1) * a.nz;
+    const long long nh = (long long)a.nxx * a.nyy * (a.nz + 2 * a.nbz);
+    const Ix at{a.nxx, (long long)a.nxx * a.nyy};
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nh; q += (long long)gridDim.x * blockDim.x) {
+        a.wold[q] = a.w[q];
+        if (q >= m) continue;
+        const int x = (int)(q % (a.nx + 1)), y = (int)((q / (a.nx + 1)) % (a.ny + 1)),
+                  kk = (int)(q / ((long long)(a.nx + 1) * (a.ny + 1)));
+        const int i = a.nbx - 1 + x, j = a.nby - 1 + y, k = a.nbz + kk;
+        const long long c = at(i, j, k);
+        if (y >= 1) {  // U at i + 1/2 for i in i0-1 .. i1
+            const long long n = c + 1;
+            double rhoe = 0.5 * (a.rho[c] + a.rho[n]);
+            rhoe += 0.5 * (a.rhobar[c] + a.rhobar[n]);
+            const double gradient = grad_h(a, a.pip, at, i, j, k, 0);
+            const double force = a.dudt ? (a.dudt[c] + a.dudt[n]) / 2 : 0.0;
+            double factor = 1.0;
+            if (a.damp_h) factor += a.dt * 0.5 * (a.betar[c] + a.betar[n]) * a.rf;
+            const double jp = wind_factor_u(a, c, 1);
+            a.u[c] = 1.0 / factor * (a.u[c] + a.dt * (-gradient + force / rhoe) * jp);
+        }
+        if (x >= 1) {  // V at j + 1/2 for j in j0-1 .. j1
+            const long long n = c + at.sy;
+            double rhoe = 0.5 * (a.rho[c] + a.rho[n]);
+            rhoe += 0.5 * (a.rhobar[c] + a.rhobar[n]);
+            const double gradient = grad_h(a, a.pip, at, i, j, k, 1);
+            const double force = a.dvdt ? (a.dvdt[c] + a.dvdt[n]) / 2 : 0.0;
+            double factor = 1.0;
+            if (a.damp_h) factor += a.dt * 0.5 * (a.betar[c] + a.betar[n]) * a.rf;
+            const double jp = wind_factor_u(a, c, at.sy);
+            a.v[c] = 1.0 / factor * (a.v[c] + a.dt * (-gradient + force / rhoe) * jp);
+        }
+    }
+}
+
+// update!(W, RHS(), Implicit()) (update!.jl:1248-1336) for k in k0 .. k1-1,
+// with the u and v of k_predict_uv and the rho' before its own update.
+__global__ void __launch_bounds__(256) k_predict_w(CorrectArgs a) {
+    const long long m = (long long)a.nx * a.ny * (a.nz - 1);
+    const Ix at{a.nxx, (long long)a.nxx * a.nyy};
+    const double dt2 = a.dt * a.dt;
+    const double *J = a.jac;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < m; q += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(q % a.nx), y = (int)((q / a.nx) % a.ny), z = (int)(q / ((long long)a.nx * a.ny));
+        const int i = a.nbx + x, j = a.nby + y, k = a.nbz + z;
+        const long long c = at(i, j, k), u = c + at.sz, l = c - 1, b = c - at.sy;
+        const double rj = J[c] + J[u];
+        double rhoc = a.rho[c];
+        double rhou = a.rho[u];
+        double rhoedgeu = (J[u] * a.rho[c] + J[c] * a.rho[u]) / rj;
+        rhoc += a.rhobar[c];
+        rhou += a.rhobar[u];
+        rhoedgeu += (J[u] * a.rhobar[c] + J[c] * a.rhobar[u]) / rj;
+        const double gradient = grad_w(a, a.pip, at, i, j, k);
+        const double force = force_w(a, c, at.sz);
+        const double n2edgeu = (J[u] * a.n2[c] + J[c] * a.n2[u]) / rj;
+        double factor = 1.0;
+        factor += a.dt * (J[u] * a.betar[c] + J[c] * a.betar[u]) / rj * a.rf;
+        const double bb = -a.g_ndim * (J[u] * a.rhop[c] / rhoc / J[c] + J[c] * a.rhop[u] / rhou / J[u]) / rj;
+        const double uc = 0.5 * (a.u[c] / wind_factor_u(a, c, 1) + a.u[l] / wind_factor_u(a, l, 1));
+        const double uu = 0.5 * (a.u[u] / wind_factor_u(a, u, 1) + a.u[l + at.sz] / wind_factor_u(a, l + at.sz, 1));
+        const double vc = 0.5 * (a.v[c] / wind_factor_u(a, c, at.sy) + a.v[b] / wind_factor_u(a, b, at.sy));
+        const double vu =
+            0.5 * (a.v[u] / wind_factor_u(a, u, at.sy) + a.v[b + at.sz] / wind_factor_u(a, b + at.sz, at.sy));
+        const double jpedgeu = wind_factor_w(a, c, at.sz);
+        double fw;
+        const double den = J[u] * (a.rho[c] + a.rhobar[c]) + J[c] * (a.rho[u] + a.rhobar[u]);
+        if (a.model == PCF_MODEL_COMPRESSIBLE)
+            fw = (J[u] * a.pbar[c] / a.thetabar[c] + J[c] * a.pbar[u] / a.thetabar[u]) / den;
+        else
+            fw = (J[u] * a.rhobar[c] + J[c] * a.rhobar[u]) / den;
+        a.w[c] = 1.0 / (factor + fw * n2edgeu * dt2) *
+                 (a.w[c] - a.dt * gradient * jpedgeu + a.dt * bb * jpedgeu + a.dt * force / rhoedgeu * jpedgeu +
+                  jpedgeu * fw * n2edgeu * dt2 *
+                      (J[u] * (a.met13[c] * uc + a.met23[c] * vc) + J[c] * (a.met13[u] * uu + a.met23[u] * vu)) / rj);
+    }
+}
+
+// update!(RhoP, RHS(), Implicit()) (update!.jl:632-728) on the interior,
+// after the boundary fill of u, v, w.
+__global__ void __launch_bounds__(256) k_predict_rhop(CorrectArgs a) {
+    const long long m = (long long)a.nx * a.ny * a.nz;
+    const Ix at{a.nxx, (long long)a.nxx * a.nyy};
+    const double dt2 = a.dt * a.dt;
+    const double *J = a.jac;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < m; q += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(q % a.nx), y = (int)((q / a.nx) % a.ny), z = (int)(q / ((long long)a.nx * a.ny));
+        const int i = a.nbx + x, j = a.nby + y, k = a.nbz + z;
+        const long long c = at(i, j, k), u = c + at.sz, d = c - at.sz, l = c - 1, b = c - at.sy;
+        const double rhoc = a.rho[c] + a.rhobar[c];
+        double rhoedgeu = (J[u] * a.rho[c] + J[c] * a.rho[u]) / (J[c] + J[u]);
+        rhoedgeu += (J[u] * a.rhobar[c] + J[c] * a.rhobar[u]) / (J[c] + J[u]);
+        double rhoedged = (J[d] * a.rho[c] + J[c] * a.rho[d]) / (J[c] + J[d]);
+        rhoedged += (J[d] * a.rhobar[c] + J[c] * a.rhobar[d]) / (J[c] + J[d]);
+        const double wv = 0.5 * (a.wold[c] / wind_factor_w(a, c, at.sz) + a.wold[d] / wind_factor_w(a, d, at.sz));
+        const bool bot = z == 0, top = z == a.nz - 1 && !bot;
+        const double lower_gradient = bot ? 0.0 : grad_w(a, a.pip, at, i, j, k - 1);
+        const double lower_force = bot ? 0.0 : force_w(a, d, at.sz);
+        const double upper_gradient = top ? 0.0 : grad_w(a, a.pip, at, i, j, k);
+        const double upper_force = top ? 0.0 : force_w(a, c, at.sz);
+        const double gradient = 0.5 * (lower_gradient + upper_gradient);
+        const double force = 0.5 * (lower_force / rhoedged + upper_force / rhoedgeu) * rhoc;
+        double factor = 1.0;
+        factor += a.dt * a.betar[c] * a.rf;
+        double bb = -a.g_ndim * a.rhop[c] / (a.rho[c] + a.rhobar[c]);
+        const double fb = a.model == PCF_MODEL_COMPRESSIBLE ? a.pbar[c] / a.thetabar[c] / (a.rho[c] + a.rhobar[c])
+                                                            : a.rhobar[c] / (a.rho[c] + a.rhobar[c]);
+        const double n2c = a.n2[c], jc = J[c];
+        bb = 1.0 / (factor + fb * n2c * dt2) *
+             (-fb * n2c * a.dt * jc * (wv + a.dt * (-gradient + force / rhoc)) + factor * bb +
+              fb * n2c * a.dt * jc * factor * 0.5 *
+                  (a.met13[c] * (a.u[c] / wind_factor_u(a, c, 1) + a.u[l] / wind_factor_u(a, l, 1)) +
+                   a.met23[c] * (a.v[c] / wind_factor_u(a, c, at.sy) + a.v[b] / wind_factor_u(a, b, at.sy))));
+        a.rhop[c] = -bb * (a.rho[c] + a.rhobar[c]) / a.g_ndim;
+    }
+}
+
 }  // namespace pcf
 
-// dpip (haloed, interior from the solve) -> halo fill and the corrections of
-// u, v, w, rho', pip (haloed, in place); rho, betar, p are the handle's (the
-// last solve's inputs).  corx, cory: haloed scratch.
-int pcf_launch_correct(pcf_handle *h, double dt, double rf, int damp_h, double *dpip, double *u, double *v,
-                       double *w, double *rhop, double *pip, double *corx, double *cory) {
-    pcf::CorrectArgs a;
+static unsigned fill_grid(long long n) {
+    long long g2 = (n + 255) / 256;
+    return (unsigned)(g2 < 1 ? 1 : (g2 > 4096 ? 4096 : g2));
+}
+
+// The handle's grid, background and constants in a CorrectArgs; rho, p,
+// betar are the handle's copies of the last solve's inputs.
+static pcf::CorrectArgs correct_args(pcf_handle *h, double dt, double rf, int damp_h) {
+    pcf::CorrectArgs a{};
     a.nx = h->d.nx; a.ny = h->d.ny; a.nz = h->d.nz;
     a.nxx = h->nxx; a.nyy = h->nyy;
     a.nbx = h->dims.nbx; a.nby = h->dims.nby; a.nbz = h->dims.nbz;
@@ -192,15 +425,83 @@ int pcf_launch_correct(pcf_handle *h, double dt, double rf, int damp_h, double *
     a.jac = h->jac; a.met13 = h->met13; a.met23 = h->met23; a.met33 = h->met33;
     a.rhobar = h->rhobar; a.pbar = h->pbar; a.thetabar = h->thetabar; a.n2 = h->n2;
     a.betar = h->betar; a.rho = h->rho; a.p = h->p;
+    return a;
+}
+
+// dpip (haloed, interior from the solve) -> halo fill and the corrections of
+// u, v, w, rho', pip (haloed, in place); rho, betar, p are the handle's (the
+// last solve's inputs).  corx, cory: haloed scratch.
+int pcf_launch_correct(pcf_handle *h, double dt, double rf, int damp_h, double *dpip, double *u, double *v,
+                       double *w, double *rhop, double *pip, double *corx, double *cory) {
+    pcf::CorrectArgs a = correct_args(h, dt, rf, damp_h);
     a.dpip = dpip; a.u = u; a.v = v; a.w = w; a.rhop = rhop; a.pip = pip; a.corx = corx; a.cory = cory;
-    auto grid = [](long long n) {
-        long long g2 = (n + 255) / 256;
-        return (unsigned)(g2 < 1 ? 1 : (g2 > 4096 ? 4096 : g2));
-    };
+    auto grid = fill_grid;
     h->launches += 3;
     pcf::k_fill_dpip<<<grid(h->nh), 256, 0, h->stream>>>(a);
     pcf::k_correct_uv<<<grid((long long)(a.nx + 1) * (a.ny + 1) * a.nz), 256, 0, h->stream>>>(a);
     pcf::k_correct_w_rhop_pip<<<grid((long long)(a.nx + 2) * (a.ny + 2) * (a.nz + 2)), 256, 0, h->stream>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PCF_OK : pcf_set_cuda_error(e);
+}
+
+// set_boundaries!(state, BoundaryPredictands()): the model's predictands
+// (rhop, u, v, w, pip; rho for PseudoIncompressible and Compressible; p for
+// Compressible), haloed, in place.  Needs nz > nbz.
+int pcf_launch_fill_predictands(pcf_handle *h, double *rho, double *rhop, double *u, double *v, double *w,
+                                double *pip, double *p) {
+    pcf::FillArgs a{};
+    a.nx = h->d.nx; a.ny = h->d.ny; a.nz = h->d.nz;
+    a.nxx = h->nxx; a.nyy = h->nyy;
+    a.nbx = h->dims.nbx; a.nby = h->dims.nby; a.nbz = h->dims.nbz;
+    auto add = [&](double *f, double sign, int stag) {
+        a.f[a.nf] = f;
+        a.sign[a.nf] = sign;
+        a.staggered[a.nf] = stag;
+        ++a.nf;
+    };
+    const int model = h->dims.model;
+    if (model != PCF_MODEL_BOUSSINESQ) add(rho, -1.0, 0);
+    add(rhop, -1.0, 0);
+    add(u, 1.0, 0);
+    add(v, 1.0, 0);
+    add(w, -1.0, 1);
+    add(pip, 1.0, 0);
+    if (model == PCF_MODEL_COMPRESSIBLE) add(p, 1.0, 0);
+    h->launches += 1;
+    pcf::k_fill_predictands<<<fill_grid(h->nh), 256, 0, h->stream>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PCF_OK : pcf_set_cuda_error(e);
+}
+
+// modify_compressible_wind!(state, * or /) (Compressible only; no-op otherwise).
+int pcf_launch_modify_wind(pcf_handle *h, const double *p, double *u, double *v, double *w, int divide) {
+    if (h->dims.model != PCF_MODEL_COMPRESSIBLE) return PCF_OK;
+    pcf::CorrectArgs a = correct_args(h, 0.0, 0.0, 0);
+    a.p = p; a.u = u; a.v = v; a.w = w;
+    h->launches += 1;
+    pcf::k_modify_wind<<<fill_grid((long long)a.nx * a.ny * a.nz), 256, 0, h->stream>>>(a, divide);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PCF_OK : pcf_set_cuda_error(e);
+}
+
+// implicit_integration!.jl:53-63: wold = w, the implicit U, V, W updates,
+// the predictand boundaries, the implicit RhoP update, the boundaries again.
+// All arrays haloed device pointers of the caller (rho, p, betar: the
+// current state; p only read in the Compressible model; dudt, dvdt: NULL for
+// NoWKB).
+int pcf_launch_predictor(pcf_handle *h, double dt, double rf, int damp_h, double *u, double *v, double *w,
+                         double *rho, double *rhop, double *pip, double *p, const double *betar, const double *dudt,
+                         const double *dvdt, double *wold) {
+    pcf::CorrectArgs a = correct_args(h, dt, rf, damp_h);
+    a.u = u; a.v = v; a.w = w; a.rhop = rhop; a.pip = pip; a.rho = rho; a.p = p; a.betar = betar;
+    a.dudt = dudt; a.dvdt = dvdt; a.wold = wold;
+    h->launches += 3;
+    pcf::k_predict_uv<<<fill_grid(h->nh), 256, 0, h->stream>>>(a);
+    pcf::k_predict_w<<<fill_grid((long long)a.nx * a.ny * (a.nz - 1)), 256, 0, h->stream>>>(a);
+    int rc = pcf_launch_fill_predictands(h, rho, rhop, u, v, w, pip, p);
+    if (rc) return rc;
+    pcf::k_predict_rhop<<<fill_grid((long long)a.nx * a.ny * a.nz), 256, 0, h->stream>>>(a);
+    if ((rc = pcf_launch_fill_predictands(h, rho, rhop, u, v, w, pip, p))) return rc;
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PCF_OK : pcf_set_cuda_error(e);
 }

@@ -137,6 +137,7 @@ struct pcf_handle {
     double *rfch;        // 1 / fcscal on the haloed grid
     double *stage;       // 6 haloed staging arrays of the host-array wind entry points (on first use)
     double *corr;        // corx, cory of the corrector (2 haloed arrays, on first use)
+    double *istage;      // staging of pcf_implicit_step: 12 haloed arrays + 1 interior (on first use)
     float *rfc32;        // 1 / fcscal on the interior
     double fac_deta;  // d_eta the factors were built with (NaN: none)
     // FP64 Krylov vectors

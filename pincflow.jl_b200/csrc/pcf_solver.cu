@@ -32,6 +32,12 @@ int pcf_launch_assemble(pcf_handle *h, double dt, double rf, int damp_h);
 int pcf_launch_factors(pcf_handle *h, double deta);
 int pcf_launch_correct(pcf_handle *h, double dt, double rf, int damp_h, double *dpip, double *u, double *v,
                        double *w, double *rhop, double *pip, double *corx, double *cory);
+int pcf_launch_fill_predictands(pcf_handle *h, double *rho, double *rhop, double *u, double *v, double *w,
+                                double *pip, double *p);
+int pcf_launch_modify_wind(pcf_handle *h, const double *p, double *u, double *v, double *w, int divide);
+int pcf_launch_predictor(pcf_handle *h, double dt, double rf, int damp_h, double *u, double *v, double *w,
+                         double *rho, double *rhop, double *pip, double *p, const double *betar, const double *dudt,
+                         const double *dvdt, double *wold);
 
 namespace pcf {
 
@@ -1250,7 +1256,7 @@ int pcf_destroy(pcf_handle *h) {
     int dev = h->dims.device;
     cudaSetDevice(dev);
     void *ptrs[] = {h->jac, h->met13, h->met23, h->met33, h->pbar, h->rhobar, h->thetabar, h->n2, h->rho, h->betar,
-                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch, h->stage, h->corr, h->lr32,
+                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch, h->stage, h->corr, h->istage, h->lr32,
                     h->x64, h->r64, h->r064, h->p64, h->v64, h->s64,
                     h->t64, h->za64, h->zb64, h->b64, h->w64, h->x32, h->r32, h->r032, h->p32, h->v32, h->s32,
                     h->t32, h->za32, h->zb32, h->zc32, h->zd32, h->partials, h->ticket, h->scal64, h->scal32,
@@ -1731,6 +1737,132 @@ int pcf_apply_corrector_device(pcf_handle *h, double *d_u, double *d_v, double *
     if (res->errflag) return PCF_OK;  // the reference returns (errflag, niter) uncorrected
     return pcf_correct_device(h, dt, rayleigh_factor, prm->damp_horizontal_wind_on_rhs, d_dpip, d_u, d_v, d_w,
                               d_rhop, d_pip);
+}
+
+// ------------------------------------------------- implicit half step --
+
+static int predictor_ready(pcf_handle *h, const void *u, const void *v, const void *w, const void *rho,
+                           const void *rhop, const void *pip, const void *p, const void *betar, const void *dudt,
+                           const void *dvdt) {
+    if (!h || !u || !v || !w || !rho || !rhop || !pip || !betar) return PCF_EINVAL;
+    if ((dudt == nullptr) != (dvdt == nullptr)) return PCF_EINVAL;
+    if (h->dims.model == PCF_MODEL_COMPRESSIBLE && !p) return PCF_EINVAL;
+    if (h->d.nz <= h->dims.nbz) return PCF_EINVAL;  // the wall reflections read interior levels only
+    if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
+    return PCF_OK;
+}
+
+int pcf_set_predictand_boundaries_device(pcf_handle *h, double *d_rho, double *d_rhop, double *d_u, double *d_v,
+                                         double *d_w, double *d_pip, double *d_p) {
+    if (!h || !d_rhop || !d_u || !d_v || !d_w || !d_pip) return PCF_EINVAL;
+    if (h->dims.model != PCF_MODEL_BOUSSINESQ && !d_rho) return PCF_EINVAL;
+    if (h->dims.model == PCF_MODEL_COMPRESSIBLE && !d_p) return PCF_EINVAL;
+    if (h->d.nz <= h->dims.nbz) return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    int rc = pcf_launch_fill_predictands(h, d_rho, d_rhop, d_u, d_v, d_w, d_pip, d_p);
+    if (rc) return rc;
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
+}
+
+int pcf_modify_compressible_wind_device(pcf_handle *h, const double *d_p, double *d_u, double *d_v, double *d_w,
+                                        int divide) {
+    if (!h || !d_u || !d_v || !d_w) return PCF_EINVAL;
+    if (h->dims.model == PCF_MODEL_COMPRESSIBLE && !d_p) return PCF_EINVAL;
+    if (!h->grid_set) return PCF_ENOTREADY;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    int rc = pcf_launch_modify_wind(h, d_p, d_u, d_v, d_w, divide);
+    if (rc) return rc;
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
+}
+
+static double *wold_scratch(pcf_handle *h, double *d_wold, int *rc) {
+    *rc = PCF_OK;
+    if (d_wold) return d_wold;
+    if (!h->corr) *rc = dalloc(h, (void **)&h->corr, 2 * sizeof(double) * (size_t)h->nh);
+    return h->corr;  // consumed by the RhoP update before the corrector reuses it
+}
+
+int pcf_implicit_predictor_device(pcf_handle *h, double dt, double rayleigh_factor, int damp_horizontal_wind_on_rhs,
+                                  double *d_u, double *d_v, double *d_w, double *d_rho, double *d_rhop,
+                                  double *d_pip, double *d_p, const double *d_betar, const double *d_dudt,
+                                  const double *d_dvdt, double *d_wold) {
+    int rc = predictor_ready(h, d_u, d_v, d_w, d_rho, d_rhop, d_pip, d_p, d_betar, d_dudt, d_dvdt);
+    if (rc) return rc;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    double *wold = wold_scratch(h, d_wold, &rc);
+    if (rc) return rc;
+    if ((rc = pcf_launch_predictor(h, dt, rayleigh_factor, damp_horizontal_wind_on_rhs, d_u, d_v, d_w, d_rho, d_rhop,
+                                   d_pip, d_p, d_betar, d_dudt, d_dvdt, wold)))
+        return rc;
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
+}
+
+int pcf_implicit_step_device(pcf_handle *h, double dt, double rayleigh_factor, const pcf_params *prm, double *d_u,
+                             double *d_v, double *d_w, double *d_rho, double *d_rhop, double *d_pip, double *d_p,
+                             const double *d_betar, const double *d_dudt, const double *d_dvdt,
+                             const double *d_heating, double *d_wold, double *d_dpip, pcf_result *res) {
+    int rc = predictor_ready(h, d_u, d_v, d_w, d_rho, d_rhop, d_pip, d_p, d_betar, d_dudt, d_dvdt);
+    if (rc) return rc;
+    if (!prm || !d_dpip || !res) return PCF_EINVAL;
+    if (dt == 0.0) return PCF_EINVAL;  // solve_poisson!.jl:46-48 raises
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    double *wold = wold_scratch(h, d_wold, &rc);
+    if (rc) return rc;
+    const int damp = prm->damp_horizontal_wind_on_rhs;
+    // implicit_integration!.jl:49-63
+    if ((rc = pcf_launch_modify_wind(h, d_p, d_u, d_v, d_w, 0))) return rc;
+    if ((rc = pcf_launch_fill_predictands(h, d_rho, d_rhop, d_u, d_v, d_w, d_pip, d_p))) return rc;
+    if ((rc = pcf_launch_predictor(h, dt, rayleigh_factor, damp, d_u, d_v, d_w, d_rho, d_rhop, d_pip, d_p, d_betar,
+                                   d_dudt, d_dvdt, wold)))
+        return rc;
+    // :65-71: apply_corrector!; like the reference, an unconverged solve
+    // returns with the predicted (uncorrected) fields and errflag set
+    if ((rc = pcf_apply_corrector_device(h, d_u, d_v, d_w, d_rho, d_rhop, d_betar, d_p, d_pip, d_heating, dt,
+                                         rayleigh_factor, prm, d_dpip, res)))
+        return rc;
+    if (res->errflag) return PCF_OK;
+    // :75-77
+    if ((rc = pcf_launch_modify_wind(h, d_p, d_u, d_v, d_w, 1))) return rc;
+    if ((rc = pcf_launch_fill_predictands(h, d_rho, d_rhop, d_u, d_v, d_w, d_pip, d_p))) return rc;
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
+}
+
+int pcf_implicit_step(pcf_handle *h, double dt, double rayleigh_factor, const pcf_params *prm, double *u, double *v,
+                      double *w, double *rho, double *rhop, double *pip, double *p, const double *betar,
+                      const double *dudt, const double *dvdt, const double *heating, double *wold, double *dpip,
+                      pcf_result *res) {
+    int rc = predictor_ready(h, u, v, w, rho, rhop, pip, p, betar, dudt, dvdt);
+    if (rc) return rc;
+    if (!prm || !dpip || !res) return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    const size_t nh = (size_t)h->nh, n = (size_t)h->d.n;
+    if (!h->istage && (rc = dalloc(h, (void **)&h->istage, sizeof(double) * (12 * nh + n)))) return rc;
+    double *s = h->istage;
+    double *d[12];
+    for (int q = 0; q < 12; ++q) d[q] = s + q * nh;
+    double *d_heat = s + 12 * nh;
+    // u v w rho rhop pip p betar dudt dvdt wold dpip
+    const double *in[10] = {u, v, w, rho, rhop, pip, p, betar, dudt, dvdt};
+    const size_t hb = sizeof(double) * nh;
+    for (int q = 0; q < 10; ++q)
+        if (in[q]) PCF_CUDA_TRY(cudaMemcpyAsync(d[q], in[q], hb, cudaMemcpyHostToDevice, h->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(d[11], dpip, hb, cudaMemcpyHostToDevice, h->stream));
+    if (heating) PCF_CUDA_TRY(cudaMemcpyAsync(d_heat, heating, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    if ((rc = pcf_implicit_step_device(h, dt, rayleigh_factor, prm, d[0], d[1], d[2], d[3], d[4], d[5], p ? d[6] : nullptr,
+                                       d[7], dudt ? d[8] : nullptr, dvdt ? d[9] : nullptr, heating ? d_heat : nullptr,
+                                       d[10], d[11], res)))
+        return rc;
+    double *out[8] = {u, v, w, rho, rhop, pip, p, dpip};
+    const int idx[8] = {0, 1, 2, 3, 4, 5, 6, 11};
+    for (int q = 0; q < 8; ++q)
+        if (out[q]) PCF_CUDA_TRY(cudaMemcpyAsync(out[q], d[idx[q]], hb, cudaMemcpyDeviceToHost, h->stream));
+    if (wold) PCF_CUDA_TRY(cudaMemcpyAsync(wold, d[10], hb, cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return PCF_OK;
 }
 
 int pcf_global_dot(pcf_handle *h, const double *a, const double *b, double *out) {

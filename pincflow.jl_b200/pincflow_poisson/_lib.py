@@ -40,6 +40,8 @@ EXPORTS = [
     "pcf_autotune_entries", "pcf_autotune_clear", "pcf_ensemble_create", "pcf_ensemble_destroy",
     "pcf_ensemble_solve_device", "pcf_ensemble_launch_count", "pcf_compute_lhs", "pcf_compute_lhs_device",
     "pcf_correct", "pcf_correct_device", "pcf_apply_corrector_device",
+    "pcf_set_predictand_boundaries_device", "pcf_modify_compressible_wind_device",
+    "pcf_implicit_predictor_device", "pcf_implicit_step_device", "pcf_implicit_step",
 ]
 TUNE_KERNELS = ["total32", "total32_diff", "horiz32", "total64", "horiz64"]
 PROF_TAGS = ["apply32", "apply64", "pseudo32", "pseudo64", "thomas32", "thomas64", "update32", "update64",
@@ -141,6 +143,12 @@ def load(path: str | None = None):
     lib.pcf_correct_device.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, vp, vp, vp, vp, vp, vp]
     lib.pcf_apply_corrector_device.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_double,
                                                ctypes.c_double, P(PcfParams), vp, P(PcfResult)]
+    f64 = ctypes.c_double
+    lib.pcf_set_predictand_boundaries_device.argtypes = [vp] + [vp] * 7
+    lib.pcf_modify_compressible_wind_device.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int]
+    lib.pcf_implicit_predictor_device.argtypes = [vp, f64, f64, ctypes.c_int] + [vp] * 11
+    lib.pcf_implicit_step_device.argtypes = [vp, f64, f64, P(PcfParams)] + [vp] * 13 + [P(PcfResult)]
+    lib.pcf_implicit_step.argtypes = [vp, f64, f64, P(PcfParams)] + [dp] * 13 + [P(PcfResult)]
     for name in EXPORTS:
         getattr(lib, name).restype = getattr(lib, name).restype or ctypes.c_int
     lib.pcf_strerror.restype = ctypes.c_char_p

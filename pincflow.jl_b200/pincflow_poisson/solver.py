@@ -245,6 +245,71 @@ class PoissonSolver:
                                                        ctypes.byref(res)), "pcf_apply_corrector_device")
         return _info(res)
 
+    # ------------------------------------------------ implicit half step --
+
+    def set_predictand_boundaries_device(self, d_rho, d_rhop, d_u, d_v, d_w, d_pip, d_p=None):
+        """set_boundaries!(state, BoundaryPredictands()) on device arrays (raw
+        pointers of haloed float64 fields), in place."""
+        vp = ctypes.c_void_p
+        opt = lambda x: None if x is None else vp(x)  # noqa: E731
+        _lib.check(self.lib.pcf_set_predictand_boundaries_device(self._h, opt(d_rho), vp(d_rhop), vp(d_u), vp(d_v),
+                                                                 vp(d_w), vp(d_pip), opt(d_p)),
+                   "pcf_set_predictand_boundaries_device")
+
+    def modify_compressible_wind_device(self, d_p, d_u, d_v, d_w, divide=False):
+        """modify_compressible_wind!(state, * or /) on device arrays, in place."""
+        vp = ctypes.c_void_p
+        _lib.check(self.lib.pcf_modify_compressible_wind_device(self._h, None if d_p is None else vp(d_p), vp(d_u),
+                                                                vp(d_v), vp(d_w), int(bool(divide))),
+                   "pcf_modify_compressible_wind_device")
+
+    def implicit_predictor_device(self, dt, rayleigh_factor, d_u, d_v, d_w, d_rho, d_rhop, d_pip, d_betar, d_p=None,
+                                  d_dudt=None, d_dvdt=None, d_wold=None, damp_horizontal_wind_on_rhs=False):
+        """implicit_integration!.jl:53-63 on device arrays: wold = w, the
+        implicit U, V, W updates, set_boundaries!, the implicit RhoP update,
+        set_boundaries!.  d_dudt/d_dvdt: WKB tendencies or None (NoWKB)."""
+        vp = ctypes.c_void_p
+        opt = lambda x: None if x is None else vp(x)  # noqa: E731
+        _lib.check(self.lib.pcf_implicit_predictor_device(
+            self._h, float(dt), float(rayleigh_factor), int(bool(damp_horizontal_wind_on_rhs)), vp(d_u), vp(d_v),
+            vp(d_w), vp(d_rho), vp(d_rhop), vp(d_pip), opt(d_p), vp(d_betar), opt(d_dudt), opt(d_dvdt), opt(d_wold)),
+            "pcf_implicit_predictor_device")
+
+    def implicit_step_device(self, dt, rayleigh_factor, namelist: PoissonNamelist, d_u, d_v, d_w, d_rho, d_rhop,
+                             d_pip, d_betar, d_dpip, d_p=None, d_dudt=None, d_dvdt=None, d_heating=None,
+                             d_wold=None) -> SolveInfo:
+        """implicit_integration!.jl:49-77 without output on device arrays:
+        the predictor, apply_corrector! and the compressible wind factors.
+        Returns the solve's SolveInfo; on info.errflag the fields are the
+        predicted, uncorrected ones."""
+        res = _lib.PcfResult()
+        prm = namelist.to_c()
+        vp = ctypes.c_void_p
+        opt = lambda x: None if x is None else vp(x)  # noqa: E731
+        _lib.check(self.lib.pcf_implicit_step_device(
+            self._h, float(dt), float(rayleigh_factor), ctypes.byref(prm), vp(d_u), vp(d_v), vp(d_w), vp(d_rho),
+            vp(d_rhop), vp(d_pip), opt(d_p), vp(d_betar), opt(d_dudt), opt(d_dvdt), opt(d_heating), opt(d_wold),
+            vp(d_dpip), ctypes.byref(res)), "pcf_implicit_step_device")
+        return _info(res)
+
+    def implicit_step(self, dt, rayleigh_factor, namelist: PoissonNamelist, u, v, w, rho, rhop, pip, betar, dpip,
+                      p=None, dudt=None, dvdt=None, heating=None, wold=None) -> SolveInfo:
+        """implicit_step_device with host arrays: u, v, w, rho, rhop, pip, p,
+        dpip (and wold, if given) are C-contiguous float64 arrays updated in
+        place; heating is interior, the rest haloed."""
+        for a in (u, v, w, rho, rhop, pip, dpip, p, wold):
+            if a is not None and not (isinstance(a, np.ndarray) and a.dtype == np.float64
+                                      and a.flags["C_CONTIGUOUS"]):
+                raise TypeError("implicit_step: in-place arrays must be C-contiguous float64")
+        betar, dudt, dvdt, heating = (None if a is None else _f64(a) for a in (betar, dudt, dvdt, heating))
+        res = _lib.PcfResult()
+        prm = namelist.to_c()
+        args = [u, v, w, rho, rhop, pip, p, betar, dudt, dvdt, heating, wold, dpip]
+        _lib.check(self.lib.pcf_implicit_step(self._h, float(dt), float(rayleigh_factor), ctypes.byref(prm),
+                                              *[_lib.dptr(a) for a in args], ctypes.byref(res)),
+                   "pcf_implicit_step")
+        return _info(res)
+
     def compute_operator(self, rho, betar, dt, rayleigh_factor, damp_horizontal_wind_on_rhs=False,
                          p=None, return_coef=True):
         coef = np.zeros((_lib.NCOEF,) + self.dom.interior_shape) if return_coef else None
