@@ -2,7 +2,7 @@
 Poisson solve (PinCFlow.jl PoissonSolver) on B200.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config c2|c5|c1|c4] [--method mg|mixed|fp64]
+                  [--config c2|c5|c1|c4|step] [--method mg|mixed|fp64]
 
 A step is one complete solve_poisson! (operator assembly, preconditioned
 BiCGSTAB to FP64 true relative residual 1e-10, unscaling into dpip) of the
@@ -18,6 +18,9 @@ oracle, a C++ restatement of the Julia code; Julia is not available): each
 step runs the operator assembly plus a bounded number of BiCGSTAB
 iterations on the full workload, scaled to a complete solve by the
 oracle's own iteration count for that workload.
+--config step times the whole implicit half step around the solve
+(implicit_integration!.jl:49-77: predictor, compute_lhs!, solve, correct!)
+on the c2 grid, its roofline line the predictor kernels.
 Multi-GPU runs are independent replicas (the solve does not shard across
 GPUs in this build): weak scaling, one solve per rank per step.
 """
@@ -46,7 +49,11 @@ WORKLOADS = {
     "c1": "periodic hill 40x1x40 Boussinesq, the 200 pressure solves of 100 time steps (rayleigh_factor 1, 2)",
     "c4": "32-member uneven ensemble, nx = ny in {64, 96, 128, 192}, nz = nx/2, random Gaussian hills and "
           "stratification, RHS N(0,1) per member",
+    "step": "implicit half step (implicit_integration!.jl:49-77) on the c2 grid: implicit predictor, "
+            "compute_lhs!, solve to 1e-10, correct!; winds and pi' N(0,1), rho' 1e-3 N(0,1) rhobar, seed 777",
 }
+STEP_METRIC = "time per implicit half step (predictor + compute_lhs! + solve to FP64 true rel. residual 1e-10 + " \
+              "correct!), 1 B200"
 
 
 METHODS = {
@@ -70,6 +77,53 @@ def make_workload(name, seed_offset=0, size=None):
     if name == "c1":
         return configs.c1(seed=seed_offset, step=0)
     raise SystemExit(f"unknown config {name}")
+
+
+def step_state(cfg, seed):
+    """Seeded predictands of the implicit-step workload (haloed arrays)."""
+    dom = cfg["dom"]
+    rng = np.random.default_rng(seed)
+    u, v, w = (rng.standard_normal(dom.halo_shape) for _ in range(3))
+    rhop = 1e-3 * rng.standard_normal(dom.halo_shape) * cfg["fields"]["rhobar"]
+    pip = rng.standard_normal(dom.halo_shape)
+    return dict(u=u, v=v, w=w, rho=np.ascontiguousarray(cfg["rho"]), rhop=rhop, pip=pip)
+
+
+def oracle_step_parts(cfg, state):
+    """Seconds of the oracle's predictor, compute_lhs! and corrector on the
+    full workload (single-threaded loops), and the right-hand side."""
+    from oracle import oracle as O
+    O.build()
+    dom, f = cfg["dom"], cfg["fields"]
+    d = O.dims(dom.nx, dom.ny, dom.nz, dom.nbx)
+    model = O.MODELS[cfg["model"]]
+    t0 = time.perf_counter()
+    rho, rhop, u, v, w, pip, _, _ = O.implicit_predictor(d, model, f, cfg["betar"], cfg["dt"], cfg["rayleigh_factor"],
+                                                         state["rho"], state["rhop"], state["u"], state["v"],
+                                                         state["w"], state["pip"])
+    t1 = time.perf_counter()
+    rhs, _ = O.compute_lhs(d, f, u, v, w, model=cfg["model"])
+    t2 = time.perf_counter()
+    O.correct(d, model, f, rho, cfg["betar"], cfg["dt"], cfg["rayleigh_factor"], np.zeros(dom.halo_shape), u, v, w,
+              rhop, pip)
+    t3 = time.perf_counter()
+    return t1 - t0, t2 - t1, t3 - t2, rhs
+
+
+def reference_step_seconds(cfg, state, sample_iters):
+    """The oracle's implicit half step: predictor + compute_lhs! + assembly +
+    `sample_iters` BiCGSTAB iterations scaled to the c2 oracle's full-solve
+    iteration count + corrector.  Returns (seconds, threads, sample text)."""
+    t_pred, t_lhs, t_corr, rhs = oracle_step_parts(cfg, state)
+    c = dict(cfg)
+    c["rhs"] = rhs
+    niter, src = oracle_iterations("c2")
+    t_asm, t_it, used = oracle_sample(c, sample_iters, os.cpu_count())
+    total = t_pred + t_lhs + t_asm + t_it * (niter or 0) + t_corr
+    sample = (f"oracle FP64 implicit predictor {t_pred:.2f} s, compute_lhs! {t_lhs:.2f} s and correct! {t_corr:.2f} s "
+              f"(1 thread) + assembly {t_asm:.2f} s and {sample_iters} BiCGSTAB iterations on {used} threads scaled "
+              f"to {niter} iterations ({src}, the c2 grid)")
+    return total, used, sample
 
 
 def max_over_ranks_of(x, device):
@@ -241,11 +295,12 @@ def run_reference_c4(args, world):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    if args.config in ("c1", "c4"):
-        value, unit, hib, used, sample = (run_reference_c1 if args.config == "c1" else run_reference_c4)(args, world)
-        metric = ("time for the 200 pressure solves of 100 steps to FP64 true rel. residual 1e-10, 1 B200"
-                  if args.config == "c1" else
-                  "ensemble solves/s to FP64 true rel. residual 1e-10 (32 uneven members), 1 B200")
+    if args.config in ("c1", "c4", "step"):
+        runner = {"c1": run_reference_c1, "c4": run_reference_c4, "step": run_reference_step}[args.config]
+        value, unit, hib, used, sample = runner(args, world)
+        metric = {"c1": "time for the 200 pressure solves of 100 steps to FP64 true rel. residual 1e-10, 1 B200",
+                  "c4": "ensemble solves/s to FP64 true rel. residual 1e-10 (32 uneven members), 1 B200",
+                  "step": STEP_METRIC}[args.config]
         line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": (value if unit == "s" else 32 / value) * 1e3,
                 "higher_is_better": hib, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -278,6 +333,129 @@ def run_reference(args, rank, world):
             "cpu_baseline": {"value": value, "unit": "s", "cores": used, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------- implicit half step --
+
+def run_step(args, rank, world, local_rank):
+    """One step = implicit_integration!.jl:49-77 without output on device
+    arrays: the implicit predictor with its boundary fills, compute_lhs!, the
+    solve (--method) to FP64 true rel. residual 1e-10, the dpip fill and
+    correct!.  Every step starts from the same seeded state (restored by a
+    device copy outside the timed step)."""
+    import torch
+
+    import pincflow_poisson as pcf
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    cfg = make_workload("c2", seed_offset=rank, size=args.size)
+    dom, f = cfg["dom"], cfg["fields"]
+    state = step_state(cfg, 777 + rank)
+    s = pcf.PoissonSolver(dom, cfg["model"], device=local_rank)
+    s.set_grid(f)
+    s.set_background(f)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    pristine = {k: t(v) for k, v in state.items()}
+    work = {k: v.clone() for k, v in pristine.items()}
+    betar = t(cfg["betar"])
+    dpip = torch.zeros(dom.halo_shape, dtype=torch.float64, device=dev)
+    wold = torch.zeros(dom.halo_shape, dtype=torch.float64, device=dev)
+    kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000, residual="true")
+    nl_fast = pcf.PoissonNamelist(**kw, precision="fp64" if args.method == "fp64" else "mixed",
+                                  multigrid=args.method == "mg", mg_dtau=args.mg_dtau)
+    nl_plain = pcf.PoissonNamelist(**kw, precision="fp64")
+
+    def step(nl):
+        for k in work:
+            work[k].copy_(pristine[k])
+        torch.cuda.synchronize()
+        info = s.implicit_step_device(cfg["dt"], cfg["rayleigh_factor"], nl, *[work[k].data_ptr() for k in
+                                      ("u", "v", "w", "rho", "rhop", "pip")], betar.data_ptr(), dpip.data_ptr(),
+                                      d_wold=wold.data_ptr())
+        if info.errflag:
+            raise RuntimeError(f"step did not converge: {info}")
+        return info
+
+    for _ in range(args.warmup):
+        step(nl_fast)
+    l0 = s.launch_count
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        infos = [step(nl_fast) for _ in range(args.steps)]
+        torch.cuda.synchronize()
+    launches = s.launch_count - l0
+    ms_per_step = max_over_ranks_of(statistics.mean(i.timings_ms["total"] for i in infos), dev)
+    solve_ms = statistics.mean(i.timings_ms["solve"] + i.timings_ms["assemble"] for i in infos)
+
+    s.profile(True)
+    step(nl_fast)
+    prof = s.profile_read()
+    s.profile(False)
+    plain = step(nl_plain)
+    plain_s = max_over_ranks_of(plain.timings_ms["total"], dev) / 1e3
+
+    # end to end: the host-array entry point with its copies, from pinned memory
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    h_betar = pin(cfg["betar"])
+    e2e_s = []
+    for _ in range(args.steps):
+        h = {k: pin(v) for k, v in state.items()}
+        h_dpip = pin(np.zeros(dom.halo_shape))
+        t0 = time.perf_counter()
+        info = s.implicit_step(cfg["dt"], cfg["rayleigh_factor"], nl_fast, h["u"], h["v"], h["w"], h["rho"],
+                               h["rhop"], h["pip"], h_betar, h_dpip)
+        e2e_s.append(time.perf_counter() - t0)
+        if info.errflag:
+            raise RuntimeError(f"e2e step did not converge: {info}")
+    e2e = max_over_ranks_of(statistics.mean(e2e_s), dev)
+    nh = int(np.prod(dom.halo_shape))
+    if rank != 0:
+        s.close()
+        return
+    peak, peak_kind = load_peaks()
+    pr, co = prof["predict"], prof["correct"]
+    pr_ms = pr["ms"] / max(pr["count"], 1)
+    pr_bytes = pr["bytes"] / max(pr["count"], 1)
+    achieved = pr_bytes / (pr_ms * 1e-3) / 1e9 if pr_ms > 0 else 0.0
+    co_ms = co["ms"] / max(co["count"], 1)
+    co_gbs = co["bytes"] / max(co["count"], 1) / (co_ms * 1e-3) / 1e9 if co_ms > 0 else None
+    value = ms_per_step / 1e3
+    line = {
+        "metric": STEP_METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (predictor, corrector) + " + ("f64" if args.method == "fp64" else "f32+f64"),
+        "data": "synthetic",
+        "config": {"workload": f"step: {WORKLOADS['step']}", "method": METHODS[args.method],
+                   "l2": "fields of 73 MB each, ~20 of them per step: larger than L2, no flush",
+                   "parallelism": f"replicas x{world}"},
+        "solve_ms_in_step": solve_ms, "iterations": infos[-1].niter,
+        "plain_fp64_step_s": plain_s, "speedup_vs_plain_fp64_step": plain_s / value,
+        "gpu_launches": launches,
+        "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 8 * 8 * nh, "d2h_bytes_per_step": 8 * 7 * nh},
+        "roofline": {"bound": "hbm", "kernel": "implicit predictor: k_predict_uv, k_predict_w, k_predict_rhop and "
+                     "two k_fill_predictands", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": pr_bytes, "ms_per_launch": pr_ms},
+        "corrector": {"ms": co_ms, "gbs": co_gbs, "frac": co_gbs / peak if co_gbs else None},
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        total, used, sample = reference_step_seconds(cfg, state, args.ref_sample_iters)
+        line["cpu_baseline"] = {"value": total, "unit": "s", "cores": used, "kind": "port", "sample": sample}
+    print(json.dumps(line), flush=True)
+    s.close()
+
+
+def run_reference_step(args, world):
+    cfg = make_workload("c2", size=args.size)
+    state = step_state(cfg, 777)
+    times = []
+    for k in range(args.warmup + args.steps):
+        total, used, sample = reference_step_seconds(cfg, state, args.ref_sample_iters)
+        if k >= args.warmup:
+            times.append(total)
+    return statistics.mean(times), "s", False, used, "per step: " + sample
 
 
 # ------------------------------------------------------ periodic hill (c1) --
@@ -747,6 +925,8 @@ def main():
             run_ensemble(args, rank, world, local_rank)
         elif args.config == "c1":
             run_c1(args, rank, world, local_rank)
+        elif args.config == "step":
+            run_step(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

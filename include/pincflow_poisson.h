@@ -19,6 +19,15 @@
  *                             src/PoissonSolver/apply_bicgstab!.jl:24-150
  *   pcf_global_dot         <- compute_global_dot_product(a, b, state)
  *                             src/MPIOperations/compute_global_dot_product.jl:22-36
+ *   pcf_compute_lhs        <- compute_lhs!(state)
+ *                             src/PoissonSolver/compute_lhs!.jl:68-223
+ *   pcf_correct            <- correct!(state, dt, rayleigh_factor) after the dpip fill
+ *                             src/PoissonSolver/correct!.jl:164-385
+ *   pcf_implicit_predictor_device
+ *                          <- update!(state, dt, U/V/W/RhoP, RHS(), Implicit(), rf)
+ *                             src/Update/update!.jl:632-1336 (Implicit methods)
+ *   pcf_implicit_step      <- implicit_integration!(state, dtstage, ...) without output
+ *                             src/Integration/implicit_integration!.jl:40-80
  *   pcf_set_grid / pcf_set_background
  *                          <- the State fields these read: Grid.jac, Grid.met
  *                             (src/Types/FoundationalTypes/Grid.jl:243-313) and
@@ -265,6 +274,8 @@ int pcf_apply_corrector_device(pcf_handle *h, double *d_u, double *d_v, double *
  * there), modify_compressible_wind!(/), set_boundaries!.  On res->errflag
  * it returns PCF_OK with the predicted, uncorrected fields (where the
  * reference writes output and raises).  dt == 0 returns PCF_EINVAL.
+ * res->ms_total is the device time of the whole step (CUDA events on the
+ * handle's stream); the other timings are the solve's.
  * pcf_implicit_step is the same with host arrays (heating interior, wold
  * may be NULL; u, v, w, rho, rhop, pip, p, dpip and wold are written
  * back). */
@@ -370,7 +381,9 @@ enum pcf_prof_tag {
     PCF_PROF_RELIABLE = 9,  /* FP64 true-residual applies of reliable updates (mostly skipped launches) */
     PCF_PROF_MG = 10,       /* multigrid coarse levels and grid transfers, FP32 */
     PCF_PROF_LEARNED = 11,  /* learned preconditioner stage: residual, network, combination */
-    PCF_PROF_NTAGS = 12
+    PCF_PROF_PREDICT = 12,  /* implicit predictor with its predictand boundary fills (FP64) */
+    PCF_PROF_CORRECT = 13,  /* corrector: dpip boundary fill and correct! (FP64) */
+    PCF_PROF_NTAGS = 14
 };
 long long pcf_launch_count(const pcf_handle *h);
 /* Relative recursive residual after each BiCGSTAB iteration of the last

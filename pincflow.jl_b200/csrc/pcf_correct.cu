@@ -37,12 +37,13 @@ struct Ix {
 // value, so one pass over the haloed grid suffices.
 __global__ void __launch_bounds__(256) k_fill_dpip(CorrectArgs a) {
     const int nzz = a.nz + 2 * a.nbz;
-    const long long nh = (long long)a.nxx * a.nyy * nzz;
     const Ix at{a.nxx, (long long)a.nxx * a.nyy};
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nh; q += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(q % a.nxx), j = (int)((q / a.nxx) % a.nyy), k = (int)(q / ((long long)a.nxx * a.nyy));
+    {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+        if (i >= a.nxx || j >= a.nyy || k >= nzz) return;
+        const long long q = at(i, j, k);
         const int ii = i - a.nbx, jj = j - a.nby, kk = k - a.nbz;
-        if (ii >= 0 && ii < a.nx && jj >= 0 && jj < a.ny && kk >= 0 && kk < a.nz) continue;
+        if (ii >= 0 && ii < a.nx && jj >= 0 && jj < a.ny && kk >= 0 && kk < a.nz) return;
         int si = ii % a.nx;
         if (si < 0) si += a.nx;
         int sj = jj % a.ny;
@@ -78,8 +79,11 @@ __device__ double grad_h(const CorrectArgs &a, const double *P, const Ix &at, in
 }
 
 // compute_pressure_gradient of the field P for W at (i, j, k+1/2)
-__device__ double grad_w(const CorrectArgs &a, const double *P, const Ix &at, int i, int j, int k) {
-    const long long c = at(i, j, k), u = c + at.sz;
+// (compute_pressure_gradient.jl:212-297) for the point c at level k.  The
+// halo (nbx, nby >= 1, nbz >= 2) keeps the levels k0-1 and k1+1 in bounds.
+__device__ __forceinline__ double grad_w_at(const CorrectArgs &a, const double *P, long long c, long long sy,
+                                            long long sz) {
+    const long long u = c + sz;
     const double *J = a.jac;
     const double jk = J[c], jk1 = J[u], rj = 1.0 / (jk + jk1);
     const double rhoe = (jk1 * a.rho[c] + jk * a.rho[u]) * rj + (jk1 * a.rhobar[c] + jk * a.rhobar[u]) * rj;
@@ -87,22 +91,27 @@ __device__ double grad_w(const CorrectArgs &a, const double *P, const Ix &at, in
     const double m13 = (jk1 * a.met13[c] + jk * a.met13[u]) * rj;
     const double m23 = (jk1 * a.met23[c] + jk * a.met23[u]) * rj;
     const double m33 = (jk1 * a.met33[c] + jk * a.met33[u]) * rj;
-    auto edge = [&](long long q) {  // Jacobian-weighted dpip at the w-level of column q
-        return (J[q + at.sz] * P[q] + J[q] * P[q + at.sz]) / (J[q] + J[q + at.sz]);
+    auto edge = [&](long long q) {  // Jacobian-weighted P at the w-level of column q
+        return (J[q + sz] * P[q] + J[q] * P[q + sz]) / (J[q] + J[q + sz]);
     };
-    const double pr = edge(c + 1), pl = edge(c - 1), pf = edge(c + at.sy), pb = edge(c - at.sy);
+    const double pr = edge(c + 1), pl = edge(c - 1), pf = edge(c + sy), pb = edge(c - sy);
     return a.kappainv * a.mainv2 * pe / rhoe *
            (m13 * (pr - pl) * 0.5 * a.rdx + m23 * (pf - pb) * 0.5 * a.rdy + m33 * (P[u] - P[c]) * a.rdz);
 }
 
+// The pointwise kernels below are chains of dependent FP64 divisions and
+// products: they run at as many resident warps as 64 registers a thread
+// allow (4 blocks of 256 per SM), which hides those latencies better than
+// fewer threads with more loads in flight each.
+#define PCF_POINTWISE_BOUNDS __launch_bounds__(256, 4)
+
 // U and V corrections (correct!.jl:177-245) with corx, cory: thread (x, y, k)
 // over (nx + 1) x (ny + 1) x nz staggered positions; x = 0 is the face i0 - 1/2.
-__global__ void __launch_bounds__(256) k_correct_uv(CorrectArgs a) {
-    const long long m = (long long)(a.nx + 1) * (a.ny + 1) * a.nz;
+__global__ void PCF_POINTWISE_BOUNDS k_correct_uv(CorrectArgs a) {
     const Ix at{a.nxx, (long long)a.nxx * a.nyy};
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < m; q += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(q % (a.nx + 1)), y = (int)((q / (a.nx + 1)) % (a.ny + 1)),
-                  kk = (int)(q / ((long long)(a.nx + 1) * (a.ny + 1)));
+    {
+        const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, kk = blockIdx.z;
+        if (x > a.nx || y > a.ny) return;
         const int i = a.nbx - 1 + x, j = a.nby - 1 + y, k = a.nbz + kk;
         const long long c = at(i, j, k);
         if (y >= 1) {  // U at i + 1/2 for i in i0-1 .. i1
@@ -127,56 +136,55 @@ __global__ void __launch_bounds__(256) k_correct_uv(CorrectArgs a) {
 
 // W and rho' corrections (correct!.jl:247-360) on the interior, and
 // pip += dpip (:375-385) on the interior plus one ghost layer: thread per
-// cell of the (nx + 2) x (ny + 2) x (nz + 2) box.
-__global__ void __launch_bounds__(256) k_correct_w_rhop_pip(CorrectArgs a) {
+// cell of the (nx + 2) x (ny + 2) x (nz + 2) box.  COMP: the Compressible
+// model's wind and buoyancy factors (1 and rhobar / rho in the others).
+template <bool COMP>
+__global__ void PCF_POINTWISE_BOUNDS k_correct_w_rhop_pip(CorrectArgs a) {
     const int bx = a.nx + 2, by = a.ny + 2;
-    const long long m = (long long)bx * by * (a.nz + 2);
-    const Ix at{a.nxx, (long long)a.nxx * a.nyy};
+    const long long sy = a.nxx, sz = (long long)a.nxx * a.nyy;
     const double dt2 = a.dt * a.dt;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < m; q += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(q % bx), y = (int)((q / bx) % by), z = (int)(q / ((long long)bx * by));
-        const int i = a.nbx - 1 + x, j = a.nby - 1 + y, k = a.nbz - 1 + z;
-        const long long c = at(i, j, k);
-        a.pip[c] += a.dpip[c];
-        const bool interior = x >= 1 && x <= a.nx && y >= 1 && y <= a.ny && z >= 1 && z <= a.nz;
-        if (!interior) continue;
-        const double *J = a.jac;
-        const long long u = c + at.sz, l = c - 1, b = c - at.sy;
-        const bool top = k == a.nbz + a.nz - 1, bot = k == a.nbz;
-        const double gu = top ? 0.0 : grad_w(a, a.dpip, at, i, j, k);
-        if (!top) {  // W at k + 1/2 for k in k0 .. k1-1
-            const double rj = 1.0 / (J[c] + J[u]);
-            const double factor = 1.0 + a.dt * (J[u] * a.betar[c] + J[c] * a.betar[u]) * rj * a.rf;
-            const double n2e = (J[u] * a.n2[c] + J[c] * a.n2[u]) * rj;
-            double jp = 1.0, fw;
-            const double den = J[u] * (a.rho[c] + a.rhobar[c]) + J[c] * (a.rho[u] + a.rhobar[u]);
-            if (a.model == PCF_MODEL_COMPRESSIBLE) {
-                jp = J[c] * J[u] * (a.p[c] + a.p[u]) * rj;
-                fw = (J[u] * a.pbar[c] / a.thetabar[c] + J[c] * a.pbar[u] / a.thetabar[u]) / den;
-            } else {
-                fw = (J[u] * a.rhobar[c] + J[c] * a.rhobar[u]) / den;
-            }
-            const double inv = 1.0 / (factor + fw * n2e * dt2);
-            const double cross = (J[u] * (a.met13[c] * (a.corx[c] + a.corx[l]) + a.met23[c] * (a.cory[c] + a.cory[b])) +
-                                  J[c] * (a.met13[u] * (a.corx[u] + a.corx[l + at.sz]) +
-                                          a.met23[u] * (a.cory[u] + a.cory[b + at.sz]))) * rj;
-            a.w[c] += -a.dt * inv * jp * gu - inv * fw * n2e * dt2 * jp * 0.5 * cross;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    if (x >= bx || y >= by) return;
+    const int i = a.nbx - 1 + x, j = a.nby - 1 + y, k = a.nbz - 1 + z;
+    const long long c = i + sy * j + sz * k;
+    a.pip[c] += a.dpip[c];
+    const bool interior = x >= 1 && x <= a.nx && y >= 1 && y <= a.ny && z >= 1 && z <= a.nz;
+    if (!interior) return;
+    const double *J = a.jac;
+    const long long u = c + sz, l = c - 1, b = c - sy;
+    const bool top = k == a.nbz + a.nz - 1, bot = k == a.nbz;
+    const double gu = top ? 0.0 : grad_w_at(a, a.dpip, c, sy, sz);
+    if (!top) {  // W at k + 1/2 for k in k0 .. k1-1
+        const double rj = 1.0 / (J[c] + J[u]);
+        const double factor = 1.0 + a.dt * (J[u] * a.betar[c] + J[c] * a.betar[u]) * rj * a.rf;
+        const double n2e = (J[u] * a.n2[c] + J[c] * a.n2[u]) * rj;
+        double jp = 1.0, fw;
+        const double den = J[u] * (a.rho[c] + a.rhobar[c]) + J[c] * (a.rho[u] + a.rhobar[u]);
+        if (COMP) {
+            jp = J[c] * J[u] * (a.p[c] + a.p[u]) * rj;
+            fw = (J[u] * a.pbar[c] / a.thetabar[c] + J[c] * a.pbar[u] / a.thetabar[u]) / den;
+        } else {
+            fw = (J[u] * a.rhobar[c] + J[c] * a.rhobar[u]) / den;
         }
-        // rho'
-        const double gl = bot ? 0.0 : grad_w(a, a.dpip, at, i, j, k - 1);
-        const double gradient = 0.5 * (gl + gu);
-        const double factor = 1.0 + a.dt * a.betar[c] * a.rf;
-        const double fb = a.model == PCF_MODEL_COMPRESSIBLE ? a.pbar[c] / a.thetabar[c] / (a.rho[c] + a.rhobar[c])
-                                                            : a.rhobar[c] / (a.rho[c] + a.rhobar[c]);
-        const double n2c = a.n2[c];
-        const double db = -1.0 / (factor + fb * n2c * dt2) *
-                          (-fb * n2c * dt2 * J[c] * gradient +
-                           fb * n2c * a.dt * J[c] * factor * 0.5 *
-                               (a.met13[c] * (a.corx[c] + a.corx[l]) + a.met23[c] * (a.cory[c] + a.cory[b])));
-        a.rhop[c] -= (a.rho[c] + a.rhobar[c]) / a.g_ndim * db;
+        const double inv = 1.0 / (factor + fw * n2e * dt2);
+        const double cross = (J[u] * (a.met13[c] * (a.corx[c] + a.corx[l]) + a.met23[c] * (a.cory[c] + a.cory[b])) +
+                              J[c] * (a.met13[u] * (a.corx[u] + a.corx[l + sz]) +
+                                      a.met23[u] * (a.cory[u] + a.cory[b + sz]))) * rj;
+        a.w[c] += -a.dt * inv * jp * gu - inv * fw * n2e * dt2 * jp * 0.5 * cross;
     }
+    // rho'
+    const double gl = bot ? 0.0 : grad_w_at(a, a.dpip, c - sz, sy, sz);
+    const double gradient = 0.5 * (gl + gu);
+    const double factor = 1.0 + a.dt * a.betar[c] * a.rf;
+    const double fb = COMP ? a.pbar[c] / a.thetabar[c] / (a.rho[c] + a.rhobar[c])
+                           : a.rhobar[c] / (a.rho[c] + a.rhobar[c]);
+    const double n2c = a.n2[c];
+    const double db = -1.0 / (factor + fb * n2c * dt2) *
+                      (-fb * n2c * dt2 * J[c] * gradient +
+                       fb * n2c * a.dt * J[c] * factor * 0.5 *
+                           (a.met13[c] * (a.corx[c] + a.corx[l]) + a.met23[c] * (a.cory[c] + a.cory[b])));
+    a.rhop[c] -= (a.rho[c] + a.rhobar[c]) / a.g_ndim * db;
 }
-
 
 // ------------------------------------------------------------ predictor --
 
@@ -196,38 +204,70 @@ struct FillArgs {
     int staggered[kMaxFillFields];
 };
 
+// One thread per ghost cell (plus, for the staggered w, per interior cell
+// of the top level, which the wall condition zeroes), numbered as
+//   [0, 2 nbz P)            the z-ghost levels, P = nxx nyy cells each,
+//   [.., + nz R)            the x/y ghost ring of each interior level,
+//                           R = P - nx ny (nby full rows below, nby above,
+//                           then 2 nbx ghost cells per interior row),
+//   [.., + nx ny)           the interior of level k1 (w only).
 __global__ void __launch_bounds__(256) k_fill_predictands(FillArgs a) {
-    const int nzz = a.nz + 2 * a.nbz;
-    const long long nh = (long long)a.nxx * a.nyy * nzz;
+    const int P = a.nxx * a.nyy, R = P - a.nx * a.ny, S = a.nx * a.ny;
+    const int tA = 2 * a.nbz * P, tB = tA + a.nz * R, tC = tB + S;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tC) return;
+    int i, j, k;
+    bool top_interior = false;
+    if (t < tA) {
+        const int L = t / P, p = t - L * P;
+        k = L < a.nbz ? L : L + a.nz;
+        j = p / a.nxx;
+        i = p - j * a.nxx;
+    } else if (t < tB) {
+        const int kk = (t - tA) / R;
+        int r = (t - tA) - kk * R;
+        k = a.nbz + kk;
+        const int rows = a.nby * a.nxx;
+        if (r < rows) {
+            j = r / a.nxx;
+            i = r - j * a.nxx;
+        } else if (r < 2 * rows) {
+            r -= rows;
+            j = a.nby + a.ny + r / a.nxx;
+            i = r % a.nxx;
+        } else {
+            r -= 2 * rows;
+            const int w2 = 2 * a.nbx, row = r / w2, c = r - row * w2;
+            j = a.nby + row;
+            i = c < a.nbx ? c : a.nx + c;
+        }
+    } else {
+        const int p = t - tB, jj = p / a.nx;
+        i = a.nbx + (p - jj * a.nx);
+        j = a.nby + jj;
+        k = a.nbz + a.nz - 1;
+        top_interior = true;
+    }
     const long long sy = a.nxx, sz = (long long)a.nxx * a.nyy;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nh; q += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(q % a.nxx), j = (int)((q / a.nxx) % a.nyy), k = (int)(q / sz);
-        const int ii = i - a.nbx, jj = j - a.nby, kk = k - a.nbz;
-        const bool hin = ii >= 0 && ii < a.nx && jj >= 0 && jj < a.ny;
-        const bool zin = kk >= 0 && kk < a.nz;
-        int si = ii % a.nx;
-        if (si < 0) si += a.nx;
-        int sj = jj % a.ny;
-        if (sj < 0) sj += a.ny;
-        const long long col = (si + a.nbx) + sy * (sj + a.nby);
-        for (int m = 0; m < a.nf; ++m) {
-            double *f = a.f[m];
-            if (a.staggered[m]) {
-                if (kk == -1 || kk == a.nz - 1) {
-                    f[q] = 0.0;
-                } else if (kk < -1) {
-                    f[q] = a.sign[m] * f[col + sz * (-kk - 2 + a.nbz)];
-                } else if (kk >= a.nz) {
-                    f[q] = a.sign[m] * f[col + sz * (2 * (a.nz - 1) - kk + a.nbz)];
-                } else if (!hin) {
-                    f[q] = f[col + sz * k];
-                }
-            } else {
-                if (hin && zin) continue;
-                if (zin) f[q] = f[col + sz * k];
-                else if (kk < 0) f[q] = a.sign[m] * f[col + sz * (-kk - 1 + a.nbz)];
-                else f[q] = a.sign[m] * f[col + sz * (2 * a.nz - 1 - kk + a.nbz)];
-            }
+    const long long q = i + sy * j + sz * k;
+    const int ii = i - a.nbx, jj = j - a.nby, kk = k - a.nbz;
+    const bool zin = kk >= 0 && kk < a.nz;
+    int si = ii % a.nx;
+    if (si < 0) si += a.nx;
+    int sj = jj % a.ny;
+    if (sj < 0) sj += a.ny;
+    const long long col = (si + a.nbx) + sy * (sj + a.nby);
+    for (int m = 0; m < a.nf; ++m) {
+        double *f = a.f[m];
+        if (a.staggered[m]) {
+            if (kk == -1 || kk == a.nz - 1) f[q] = 0.0;
+            else if (kk < -1) f[q] = a.sign[m] * f[col + sz * (-kk - 2 + a.nbz)];
+            else if (kk >= a.nz) f[q] = a.sign[m] * f[col + sz * (2 * (a.nz - 1) - kk + a.nbz)];
+            else f[q] = f[col + sz * k];
+        } else if (!top_interior) {
+            if (zin) f[q] = f[col + sz * k];
+            else if (kk < 0) f[q] = a.sign[m] * f[col + sz * (-kk - 1 + a.nbz)];
+            else f[q] = a.sign[m] * f[col + sz * (2 * a.nz - 1 - kk + a.nbz)];
         }
     }
 }
@@ -235,11 +275,11 @@ __global__ void __launch_bounds__(256) k_fill_predictands(FillArgs a) {
 // modify_compressible_wind!.jl:52-80 on the interior: u, v, w multiplied
 // (divide = 0) or divided (divide = 1) by the compressible wind factors.
 __global__ void __launch_bounds__(256) k_modify_wind(CorrectArgs a, int divide) {
-    const long long m = (long long)a.nx * a.ny * a.nz;
     const Ix at{a.nxx, (long long)a.nxx * a.nyy};
     const double *J = a.jac, *P = a.p;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < m; q += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(q % a.nx), y = (int)((q / a.nx) % a.ny), z = (int)(q / ((long long)a.nx * a.ny));
+    {
+        const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+        if (x >= a.nx || y >= a.ny) return;
         const long long c = at(x + a.nbx, y + a.nby, z + a.nbz), r = c + 1, f = c + at.sy, t = c + at.sz;
         // explicitly rounded products and sums (no FMA contraction), so the
         // factors and hence u, v, w round exactly as in the reference
@@ -262,34 +302,13 @@ __global__ void __launch_bounds__(256) k_modify_wind(CorrectArgs a, int divide) 
 __device__ __forceinline__ double wind_factor_u(const CorrectArgs &a, long long c, long long o) {
     return a.model == PCF_MODEL_COMPRESSIBLE ? (a.jac[c] * a.p[c] + a.jac[c + o] * a.p[c + o]) / 2 : 1.0;
 }
-__device__ __forceinline__ double wind_factor_w(const CorrectArgs &a, long long c, long long sz) {
-    if (a.model != PCF_MODEL_COMPRESSIBLE) return 1.0;
-    const double jk = a.jac[c], jk1 = a.jac[c + sz];
-    return jk * jk1 * (a.p[c] + a.p[c + sz]) / (jk + jk1);
-}
-
-// compute_volume_force(state, i, j, k, W()) (compute_volume_force.jl:185-206)
-__device__ __forceinline__ double force_w(const CorrectArgs &a, long long c, long long sz) {
-    if (!a.dudt) return 0.0;
-    const double *J = a.jac;
-    const long long u = c + sz;
-    return (J[u] * (a.met13[c] * a.dudt[c] + a.met23[c] * a.dvdt[c]) +
-            J[c] * (a.met13[u] * a.dudt[u] + a.met23[u] * a.dvdt[u])) /
-           (J[c] + J[u]);
-}
-
 // update!(U / V, RHS(), Implicit()) (update!.jl:837-882, :988-1033) over the
-// (nx + 1) x (ny + 1) x nz staggered positions of k_correct_uv, and the
-// backup wold = w (save_backups!.jl:16-24) of the whole haloed array.
-__global__ void __launch_bounds__(256) k_predict_uv(CorrectArgs a) {
-    const long long m = (long long)(a.nx + 1) * (a.ny + 1) * a.nz;
-    const long long nh = (long long)a.nxx * a.nyy * (a.nz + 2 * a.nbz);
+// (nx + 1) x (ny + 1) x nz staggered positions of k_correct_uv.
+__global__ void PCF_POINTWISE_BOUNDS k_predict_uv(CorrectArgs a) {
     const Ix at{a.nxx, (long long)a.nxx * a.nyy};
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nh; q += (long long)gridDim.x * blockDim.x) {
-        a.wold[q] = a.w[q];
-        if (q >= m) continue;
-        const int x = (int)(q % (a.nx + 1)), y = (int)((q / (a.nx + 1)) % (a.ny + 1)),
-                  kk = (int)(q / ((long long)(a.nx + 1) * (a.ny + 1)));
+    {
+        const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, kk = blockIdx.z;
+        if (x > a.nx || y > a.ny) return;
         const int i = a.nbx - 1 + x, j = a.nby - 1 + y, k = a.nbz + kk;
         const long long c = at(i, j, k);
         if (y >= 1) {  // U at i + 1/2 for i in i0-1 .. i1
@@ -317,93 +336,128 @@ __global__ void __launch_bounds__(256) k_predict_uv(CorrectArgs a) {
     }
 }
 
+// compute_compressible_wind_factor (compute_compressible_wind_factor.jl:
+// 102-157) of U (o = 1) or V (o = sy) at the face after c, and of W
+// (o = sz) at c's upper face; 1 outside the Compressible model.
+template <bool COMP>
+__device__ __forceinline__ double jp_uv(const CorrectArgs &a, long long c, long long o) {
+    return COMP ? (a.jac[c] * a.p[c] + a.jac[c + o] * a.p[c + o]) / 2 : 1.0;
+}
+template <bool COMP>
+__device__ __forceinline__ double jp_w(const CorrectArgs &a, long long c, long long sz) {
+    if (!COMP) return 1.0;
+    const double jk = a.jac[c], jk1 = a.jac[c + sz];
+    return jk * jk1 * (a.p[c] + a.p[c + sz]) / (jk + jk1);
+}
+
+// compute_volume_force(state, i, j, k, W()) (compute_volume_force.jl:185-206)
+__device__ __forceinline__ double force_w(const CorrectArgs &a, long long c, long long sz) {
+    if (!a.dudt) return 0.0;
+    const double *J = a.jac;
+    const long long u = c + sz;
+    return (J[u] * (a.met13[c] * a.dudt[c] + a.met23[c] * a.dvdt[c]) +
+            J[c] * (a.met13[u] * a.dudt[u] + a.met23[u] * a.dvdt[u])) /
+           (J[c] + J[u]);
+}
+
+// x / y, or x when y is the non-compressible wind factor 1 (exact either way)
+template <bool COMP>
+__device__ __forceinline__ double over(double x, double y) {
+    return COMP ? x / y : x;
+}
+
 // update!(W, RHS(), Implicit()) (update!.jl:1248-1336) for k in k0 .. k1-1,
 // with the u and v of k_predict_uv and the rho' before its own update.
-__global__ void __launch_bounds__(256) k_predict_w(CorrectArgs a) {
-    const long long m = (long long)a.nx * a.ny * (a.nz - 1);
-    const Ix at{a.nxx, (long long)a.nxx * a.nyy};
+template <bool COMP>
+__global__ void PCF_POINTWISE_BOUNDS k_predict_w(CorrectArgs a) {
+    const long long sy = a.nxx, sz = (long long)a.nxx * a.nyy;
     const double dt2 = a.dt * a.dt;
     const double *J = a.jac;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < m; q += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(q % a.nx), y = (int)((q / a.nx) % a.ny), z = (int)(q / ((long long)a.nx * a.ny));
-        const int i = a.nbx + x, j = a.nby + y, k = a.nbz + z;
-        const long long c = at(i, j, k), u = c + at.sz, l = c - 1, b = c - at.sy;
-        const double rj = J[c] + J[u];
-        double rhoc = a.rho[c];
-        double rhou = a.rho[u];
-        double rhoedgeu = (J[u] * a.rho[c] + J[c] * a.rho[u]) / rj;
-        rhoc += a.rhobar[c];
-        rhou += a.rhobar[u];
-        rhoedgeu += (J[u] * a.rhobar[c] + J[c] * a.rhobar[u]) / rj;
-        const double gradient = grad_w(a, a.pip, at, i, j, k);
-        const double force = force_w(a, c, at.sz);
-        const double n2edgeu = (J[u] * a.n2[c] + J[c] * a.n2[u]) / rj;
-        double factor = 1.0;
-        factor += a.dt * (J[u] * a.betar[c] + J[c] * a.betar[u]) / rj * a.rf;
-        const double bb = -a.g_ndim * (J[u] * a.rhop[c] / rhoc / J[c] + J[c] * a.rhop[u] / rhou / J[u]) / rj;
-        const double uc = 0.5 * (a.u[c] / wind_factor_u(a, c, 1) + a.u[l] / wind_factor_u(a, l, 1));
-        const double uu = 0.5 * (a.u[u] / wind_factor_u(a, u, 1) + a.u[l + at.sz] / wind_factor_u(a, l + at.sz, 1));
-        const double vc = 0.5 * (a.v[c] / wind_factor_u(a, c, at.sy) + a.v[b] / wind_factor_u(a, b, at.sy));
-        const double vu =
-            0.5 * (a.v[u] / wind_factor_u(a, u, at.sy) + a.v[b + at.sz] / wind_factor_u(a, b + at.sz, at.sy));
-        const double jpedgeu = wind_factor_w(a, c, at.sz);
-        double fw;
-        const double den = J[u] * (a.rho[c] + a.rhobar[c]) + J[c] * (a.rho[u] + a.rhobar[u]);
-        if (a.model == PCF_MODEL_COMPRESSIBLE)
-            fw = (J[u] * a.pbar[c] / a.thetabar[c] + J[c] * a.pbar[u] / a.thetabar[u]) / den;
-        else
-            fw = (J[u] * a.rhobar[c] + J[c] * a.rhobar[u]) / den;
-        a.w[c] = 1.0 / (factor + fw * n2edgeu * dt2) *
-                 (a.w[c] - a.dt * gradient * jpedgeu + a.dt * bb * jpedgeu + a.dt * force / rhoedgeu * jpedgeu +
-                  jpedgeu * fw * n2edgeu * dt2 *
-                      (J[u] * (a.met13[c] * uc + a.met23[c] * vc) + J[c] * (a.met13[u] * uu + a.met23[u] * vu)) / rj);
-    }
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    if (x >= a.nx || y >= a.ny) return;
+    const long long c = (a.nbx + x) + sy * (a.nby + y) + sz * (a.nbz + z), u = c + sz, l = c - 1, b = c - sy;
+    const double rj = J[c] + J[u];
+    double rhoc = a.rho[c];
+    double rhou = a.rho[u];
+    double rhoedgeu = (J[u] * a.rho[c] + J[c] * a.rho[u]) / rj;
+    rhoc += a.rhobar[c];
+    rhou += a.rhobar[u];
+    rhoedgeu += (J[u] * a.rhobar[c] + J[c] * a.rhobar[u]) / rj;
+    const double gradient = grad_w_at(a, a.pip, c, sy, sz);
+    const double force = force_w(a, c, sz);
+    const double n2edgeu = (J[u] * a.n2[c] + J[c] * a.n2[u]) / rj;
+    double factor = 1.0;
+    factor += a.dt * (J[u] * a.betar[c] + J[c] * a.betar[u]) / rj * a.rf;
+    const double bb = -a.g_ndim * (J[u] * a.rhop[c] / rhoc / J[c] + J[c] * a.rhop[u] / rhou / J[u]) / rj;
+    const double uc = 0.5 * (over<COMP>(a.u[c], jp_uv<COMP>(a, c, 1)) + over<COMP>(a.u[l], jp_uv<COMP>(a, l, 1)));
+    const double uu = 0.5 * (over<COMP>(a.u[u], jp_uv<COMP>(a, u, 1)) +
+                             over<COMP>(a.u[l + sz], jp_uv<COMP>(a, l + sz, 1)));
+    const double vc = 0.5 * (over<COMP>(a.v[c], jp_uv<COMP>(a, c, sy)) + over<COMP>(a.v[b], jp_uv<COMP>(a, b, sy)));
+    const double vu = 0.5 * (over<COMP>(a.v[u], jp_uv<COMP>(a, u, sy)) +
+                             over<COMP>(a.v[b + sz], jp_uv<COMP>(a, b + sz, sy)));
+    const double jpedgeu = jp_w<COMP>(a, c, sz);
+    double fw;
+    const double den = J[u] * (a.rho[c] + a.rhobar[c]) + J[c] * (a.rho[u] + a.rhobar[u]);
+    if (COMP)
+        fw = (J[u] * a.pbar[c] / a.thetabar[c] + J[c] * a.pbar[u] / a.thetabar[u]) / den;
+    else
+        fw = (J[u] * a.rhobar[c] + J[c] * a.rhobar[u]) / den;
+    a.w[c] = 1.0 / (factor + fw * n2edgeu * dt2) *
+             (a.w[c] - a.dt * gradient * jpedgeu + a.dt * bb * jpedgeu + a.dt * force / rhoedgeu * jpedgeu +
+              jpedgeu * fw * n2edgeu * dt2 *
+                  (J[u] * (a.met13[c] * uc + a.met23[c] * vc) + J[c] * (a.met13[u] * uu + a.met23[u] * vu)) / rj);
 }
 
 // update!(RhoP, RHS(), Implicit()) (update!.jl:632-728) on the interior,
 // after the boundary fill of u, v, w.
-__global__ void __launch_bounds__(256) k_predict_rhop(CorrectArgs a) {
-    const long long m = (long long)a.nx * a.ny * a.nz;
-    const Ix at{a.nxx, (long long)a.nxx * a.nyy};
+template <bool COMP>
+__global__ void PCF_POINTWISE_BOUNDS k_predict_rhop(CorrectArgs a) {
+    const long long sy = a.nxx, sz = (long long)a.nxx * a.nyy;
     const double dt2 = a.dt * a.dt;
     const double *J = a.jac;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < m; q += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(q % a.nx), y = (int)((q / a.nx) % a.ny), z = (int)(q / ((long long)a.nx * a.ny));
-        const int i = a.nbx + x, j = a.nby + y, k = a.nbz + z;
-        const long long c = at(i, j, k), u = c + at.sz, d = c - at.sz, l = c - 1, b = c - at.sy;
-        const double rhoc = a.rho[c] + a.rhobar[c];
-        double rhoedgeu = (J[u] * a.rho[c] + J[c] * a.rho[u]) / (J[c] + J[u]);
-        rhoedgeu += (J[u] * a.rhobar[c] + J[c] * a.rhobar[u]) / (J[c] + J[u]);
-        double rhoedged = (J[d] * a.rho[c] + J[c] * a.rho[d]) / (J[c] + J[d]);
-        rhoedged += (J[d] * a.rhobar[c] + J[c] * a.rhobar[d]) / (J[c] + J[d]);
-        const double wv = 0.5 * (a.wold[c] / wind_factor_w(a, c, at.sz) + a.wold[d] / wind_factor_w(a, d, at.sz));
-        const bool bot = z == 0, top = z == a.nz - 1 && !bot;
-        const double lower_gradient = bot ? 0.0 : grad_w(a, a.pip, at, i, j, k - 1);
-        const double lower_force = bot ? 0.0 : force_w(a, d, at.sz);
-        const double upper_gradient = top ? 0.0 : grad_w(a, a.pip, at, i, j, k);
-        const double upper_force = top ? 0.0 : force_w(a, c, at.sz);
-        const double gradient = 0.5 * (lower_gradient + upper_gradient);
-        const double force = 0.5 * (lower_force / rhoedged + upper_force / rhoedgeu) * rhoc;
-        double factor = 1.0;
-        factor += a.dt * a.betar[c] * a.rf;
-        double bb = -a.g_ndim * a.rhop[c] / (a.rho[c] + a.rhobar[c]);
-        const double fb = a.model == PCF_MODEL_COMPRESSIBLE ? a.pbar[c] / a.thetabar[c] / (a.rho[c] + a.rhobar[c])
-                                                            : a.rhobar[c] / (a.rho[c] + a.rhobar[c]);
-        const double n2c = a.n2[c], jc = J[c];
-        bb = 1.0 / (factor + fb * n2c * dt2) *
-             (-fb * n2c * a.dt * jc * (wv + a.dt * (-gradient + force / rhoc)) + factor * bb +
-              fb * n2c * a.dt * jc * factor * 0.5 *
-                  (a.met13[c] * (a.u[c] / wind_factor_u(a, c, 1) + a.u[l] / wind_factor_u(a, l, 1)) +
-                   a.met23[c] * (a.v[c] / wind_factor_u(a, c, at.sy) + a.v[b] / wind_factor_u(a, b, at.sy))));
-        a.rhop[c] = -bb * (a.rho[c] + a.rhobar[c]) / a.g_ndim;
-    }
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    if (x >= a.nx || y >= a.ny) return;
+    const long long c = (a.nbx + x) + sy * (a.nby + y) + sz * (a.nbz + z), u = c + sz, d = c - sz, l = c - 1,
+                    b = c - sy;
+    const double rhoc = a.rho[c] + a.rhobar[c];
+    double rhoedgeu = (J[u] * a.rho[c] + J[c] * a.rho[u]) / (J[c] + J[u]);
+    rhoedgeu += (J[u] * a.rhobar[c] + J[c] * a.rhobar[u]) / (J[c] + J[u]);
+    double rhoedged = (J[d] * a.rho[c] + J[c] * a.rho[d]) / (J[c] + J[d]);
+    rhoedged += (J[d] * a.rhobar[c] + J[c] * a.rhobar[d]) / (J[c] + J[d]);
+    const double wv = 0.5 * (over<COMP>(a.wold[c], jp_w<COMP>(a, c, sz)) + over<COMP>(a.wold[d], jp_w<COMP>(a, d, sz)));
+    const bool bot = z == 0, top = z == a.nz - 1 && !bot;
+    const double lower_gradient = bot ? 0.0 : grad_w_at(a, a.pip, d, sy, sz);
+    const double lower_force = bot ? 0.0 : force_w(a, d, sz);
+    const double upper_gradient = top ? 0.0 : grad_w_at(a, a.pip, c, sy, sz);
+    const double upper_force = top ? 0.0 : force_w(a, c, sz);
+    const double gradient = 0.5 * (lower_gradient + upper_gradient);
+    const double force = 0.5 * (lower_force / rhoedged + upper_force / rhoedgeu) * rhoc;
+    double factor = 1.0;
+    factor += a.dt * a.betar[c] * a.rf;
+    double bb = -a.g_ndim * a.rhop[c] / (a.rho[c] + a.rhobar[c]);
+    const double fb = COMP ? a.pbar[c] / a.thetabar[c] / (a.rho[c] + a.rhobar[c])
+                           : a.rhobar[c] / (a.rho[c] + a.rhobar[c]);
+    const double n2c = a.n2[c], jc = J[c];
+    bb = 1.0 / (factor + fb * n2c * dt2) *
+         (-fb * n2c * a.dt * jc * (wv + a.dt * (-gradient + force / rhoc)) + factor * bb +
+          fb * n2c * a.dt * jc * factor * 0.5 *
+              (a.met13[c] * (over<COMP>(a.u[c], jp_uv<COMP>(a, c, 1)) + over<COMP>(a.u[l], jp_uv<COMP>(a, l, 1))) +
+               a.met23[c] * (over<COMP>(a.v[c], jp_uv<COMP>(a, c, sy)) + over<COMP>(a.v[b], jp_uv<COMP>(a, b, sy)))));
+    a.rhop[c] = -bb * (a.rho[c] + a.rhobar[c]) / a.g_ndim;
 }
 
 }  // namespace pcf
 
-static unsigned fill_grid(long long n) {
-    long long g2 = (n + 255) / 256;
-    return (unsigned)(g2 < 1 ? 1 : (g2 > 4096 ? 4096 : g2));
+// One thread per point of an X x Y x Z box: 64 x 4 threads per block in the
+// x-y plane (coalesced along x), one z level per block row of the grid.
+struct Box3 {
+    dim3 grid, block;
+};
+static Box3 box3(long long X, long long Y, long long Z) {
+    Box3 b;
+    b.block = dim3(64, 4, 1);
+    b.grid = dim3((unsigned)((X + 63) / 64), (unsigned)((Y + 3) / 4), (unsigned)Z);
+    return b;
 }
 
 // The handle's grid, background and constants in a CorrectArgs; rho, p,
@@ -435,11 +489,15 @@ int pcf_launch_correct(pcf_handle *h, double dt, double rf, int damp_h, double *
                        double *w, double *rhop, double *pip, double *corx, double *cory) {
     pcf::CorrectArgs a = correct_args(h, dt, rf, damp_h);
     a.dpip = dpip; a.u = u; a.v = v; a.w = w; a.rhop = rhop; a.pip = pip; a.corx = corx; a.cory = cory;
-    auto grid = fill_grid;
     h->launches += 3;
-    pcf::k_fill_dpip<<<grid(h->nh), 256, 0, h->stream>>>(a);
-    pcf::k_correct_uv<<<grid((long long)(a.nx + 1) * (a.ny + 1) * a.nz), 256, 0, h->stream>>>(a);
-    pcf::k_correct_w_rhop_pip<<<grid((long long)(a.nx + 2) * (a.ny + 2) * (a.nz + 2)), 256, 0, h->stream>>>(a);
+    const Box3 bf = box3(a.nxx, a.nyy, a.nz + 2 * a.nbz), buv = box3(a.nx + 1, a.ny + 1, a.nz),
+               bw = box3(a.nx + 2, a.ny + 2, a.nz + 2);
+    pcf::k_fill_dpip<<<bf.grid, bf.block, 0, h->stream>>>(a);
+    pcf::k_correct_uv<<<buv.grid, buv.block, 0, h->stream>>>(a);
+    if (a.model == PCF_MODEL_COMPRESSIBLE)
+        pcf::k_correct_w_rhop_pip<true><<<bw.grid, bw.block, 0, h->stream>>>(a);
+    else
+        pcf::k_correct_w_rhop_pip<false><<<bw.grid, bw.block, 0, h->stream>>>(a);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PCF_OK : pcf_set_cuda_error(e);
 }
@@ -468,7 +526,10 @@ int pcf_launch_fill_predictands(pcf_handle *h, double *rho, double *rhop, double
     add(pip, 1.0, 0);
     if (model == PCF_MODEL_COMPRESSIBLE) add(p, 1.0, 0);
     h->launches += 1;
-    pcf::k_fill_predictands<<<fill_grid(h->nh), 256, 0, h->stream>>>(a);
+    const long long plane = (long long)a.nxx * a.nyy, ring = plane - (long long)a.nx * a.ny;
+    const long long cells = 2LL * a.nbz * plane + (long long)a.nz * ring + (long long)a.nx * a.ny;
+    if (cells >= (1LL << 31)) return PCF_ERANGE;
+    pcf::k_fill_predictands<<<(unsigned)((cells + 255) / 256), 256, 0, h->stream>>>(a);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PCF_OK : pcf_set_cuda_error(e);
 }
@@ -479,7 +540,8 @@ int pcf_launch_modify_wind(pcf_handle *h, const double *p, double *u, double *v,
     pcf::CorrectArgs a = correct_args(h, 0.0, 0.0, 0);
     a.p = p; a.u = u; a.v = v; a.w = w;
     h->launches += 1;
-    pcf::k_modify_wind<<<fill_grid((long long)a.nx * a.ny * a.nz), 256, 0, h->stream>>>(a, divide);
+    const Box3 b = box3(a.nx, a.ny, a.nz);
+    pcf::k_modify_wind<<<b.grid, b.block, 0, h->stream>>>(a, divide);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PCF_OK : pcf_set_cuda_error(e);
 }
@@ -496,11 +558,18 @@ int pcf_launch_predictor(pcf_handle *h, double dt, double rf, int damp_h, double
     a.u = u; a.v = v; a.w = w; a.rhop = rhop; a.pip = pip; a.rho = rho; a.p = p; a.betar = betar;
     a.dudt = dudt; a.dvdt = dvdt; a.wold = wold;
     h->launches += 3;
-    pcf::k_predict_uv<<<fill_grid(h->nh), 256, 0, h->stream>>>(a);
-    pcf::k_predict_w<<<fill_grid((long long)a.nx * a.ny * (a.nz - 1)), 256, 0, h->stream>>>(a);
+    // save_backups!(state, :w) (save_backups!.jl:16-24): the whole haloed array
+    cudaError_t e0 = cudaMemcpyAsync(wold, w, sizeof(double) * (size_t)h->nh, cudaMemcpyDeviceToDevice, h->stream);
+    if (e0 != cudaSuccess) return pcf_set_cuda_error(e0);
+    const Box3 buv = box3(a.nx + 1, a.ny + 1, a.nz), bw = box3(a.nx, a.ny, a.nz - 1), br = box3(a.nx, a.ny, a.nz);
+    pcf::k_predict_uv<<<buv.grid, buv.block, 0, h->stream>>>(a);
+    const bool comp = a.model == PCF_MODEL_COMPRESSIBLE;
+    if (comp) pcf::k_predict_w<true><<<bw.grid, bw.block, 0, h->stream>>>(a);
+    else pcf::k_predict_w<false><<<bw.grid, bw.block, 0, h->stream>>>(a);
     int rc = pcf_launch_fill_predictands(h, rho, rhop, u, v, w, pip, p);
     if (rc) return rc;
-    pcf::k_predict_rhop<<<fill_grid((long long)a.nx * a.ny * a.nz), 256, 0, h->stream>>>(a);
+    if (comp) pcf::k_predict_rhop<true><<<br.grid, br.block, 0, h->stream>>>(a);
+    else pcf::k_predict_rhop<false><<<br.grid, br.block, 0, h->stream>>>(a);
     if ((rc = pcf_launch_fill_predictands(h, rho, rhop, u, v, w, pip, p))) return rc;
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PCF_OK : pcf_set_cuda_error(e);

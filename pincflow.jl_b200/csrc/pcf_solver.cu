@@ -65,8 +65,10 @@ struct ProfScope {
     int tag;
     double bytes;
     cudaEvent_t a = nullptr;
-    ProfScope(pcf_handle *h_, int tag_, double bytes_) : h(h_), tag(tag_), bytes(bytes_) {
-        h->launches += 1;
+    // nlaunch: kernel launches the scope covers (counted here unless the
+    // launcher counts them itself, nlaunch = 0)
+    ProfScope(pcf_handle *h_, int tag_, double bytes_, int nlaunch = 1) : h(h_), tag(tag_), bytes(bytes_) {
+        h->launches += nlaunch;
         if (h->prof_on && h->prof) {
             a = prof_event(h);
             if (a) cudaEventRecord(a, h->stream);
@@ -1683,6 +1685,32 @@ int pcf_compute_lhs(pcf_handle *h, const double *u, const double *v, const doubl
     return PCF_OK;
 }
 
+// Algorithmic bytes of the predictor (each field a kernel touches read or
+// written once per point): the U/V kernel reads u, v, pip, rho, rhobar,
+// pbar, met13, met23 (+ betar with damping, jac and p when Compressible,
+// dudt or dvdt with WKB) and writes u, v, and copies w to wold over the
+// haloed grid; the W and RhoP kernels read 14 fields each (+ thetabar and p,
+// + dudt and dvdt) and write one; each of the two boundary fills reads and
+// writes the ghost cells of the model's 5-7 predictands.
+static double predictor_bytes(const pcf_handle *h, int damp, bool wkb) {
+    const bool comp = h->dims.model == PCF_MODEL_COMPRESSIBLE;
+    const double n = (double)h->d.n, nh = (double)h->nh;
+    const int extra = (comp ? 2 : 0) + (wkb ? 2 : 0);
+    const double uv = 8 + (damp ? 1 : 0) + extra + 2, w = 14 + extra + 1, rp = 14 + extra + 1;
+    const int nf = h->dims.model == PCF_MODEL_BOUSSINESQ ? 5 : (comp ? 7 : 6);
+    return 8.0 * (n * (uv + w + rp) + 2.0 * nh + 2.0 * 2.0 * nf * (nh - n));
+}
+
+// Algorithmic bytes of the corrector: the dpip fill (ghost cells read and
+// written), the U/V kernel (dpip, rho, rhobar, pbar, met13, met23, u, v read
+// (+ betar, + jac and p), u, v, corx, cory written) and the W/RhoP/PiP kernel
+// (15 fields read (+ thetabar, p), w, rhop, pip written).
+static double corrector_bytes(const pcf_handle *h, int damp) {
+    const bool comp = h->dims.model == PCF_MODEL_COMPRESSIBLE;
+    const double n = (double)h->d.n, nh = (double)h->nh;
+    return 8.0 * (2.0 * (nh - n) + n * (8 + (damp ? 1 : 0) + (comp ? 2 : 0) + 4) + n * (15 + (comp ? 2 : 0) + 3));
+}
+
 int pcf_correct_device(pcf_handle *h, double dt, double rayleigh_factor, int damp_horizontal_wind_on_rhs,
                        double *d_dpip, double *d_u, double *d_v, double *d_w, double *d_rhop, double *d_pip) {
     if (!h || !d_dpip || !d_u || !d_v || !d_w || !d_rhop || !d_pip) return PCF_EINVAL;
@@ -1692,10 +1720,15 @@ int pcf_correct_device(pcf_handle *h, double dt, double rayleigh_factor, int dam
         int rc = dalloc(h, (void **)&h->corr, 2 * sizeof(double) * (size_t)h->nh);
         if (rc) return rc;
     }
-    int rc = pcf_launch_correct(h, dt, rayleigh_factor, damp_horizontal_wind_on_rhs, d_dpip, d_u, d_v, d_w, d_rhop,
+    int rc;
+    {
+        ProfScope ps(h, PCF_PROF_CORRECT, corrector_bytes(h, damp_horizontal_wind_on_rhs), 0);
+        rc = pcf_launch_correct(h, dt, rayleigh_factor, damp_horizontal_wind_on_rhs, d_dpip, d_u, d_v, d_w, d_rhop,
                                 d_pip, h->corr, h->corr + h->nh);
+    }
     if (rc) return rc;
     PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    prof_flush(h, 0);
     return PCF_OK;
 }
 
@@ -1747,7 +1780,8 @@ static int predictor_ready(pcf_handle *h, const void *u, const void *v, const vo
     if (!h || !u || !v || !w || !rho || !rhop || !pip || !betar) return PCF_EINVAL;
     if ((dudt == nullptr) != (dvdt == nullptr)) return PCF_EINVAL;
     if (h->dims.model == PCF_MODEL_COMPRESSIBLE && !p) return PCF_EINVAL;
-    if (h->d.nz <= h->dims.nbz) return PCF_EINVAL;  // the wall reflections read interior levels only
+    // the wall reflections read interior levels only; W lives on nz - 1 levels
+    if (h->d.nz <= h->dims.nbz || h->d.nz < 2) return PCF_EINVAL;
     if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
     return PCF_OK;
 }
@@ -1793,10 +1827,14 @@ int pcf_implicit_predictor_device(pcf_handle *h, double dt, double rayleigh_fact
     PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
     double *wold = wold_scratch(h, d_wold, &rc);
     if (rc) return rc;
-    if ((rc = pcf_launch_predictor(h, dt, rayleigh_factor, damp_horizontal_wind_on_rhs, d_u, d_v, d_w, d_rho, d_rhop,
-                                   d_pip, d_p, d_betar, d_dudt, d_dvdt, wold)))
-        return rc;
+    {
+        ProfScope ps(h, PCF_PROF_PREDICT, predictor_bytes(h, damp_horizontal_wind_on_rhs, d_dudt != nullptr), 0);
+        if ((rc = pcf_launch_predictor(h, dt, rayleigh_factor, damp_horizontal_wind_on_rhs, d_u, d_v, d_w, d_rho,
+                                       d_rhop, d_pip, d_p, d_betar, d_dudt, d_dvdt, wold)))
+            return rc;
+    }
     PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    prof_flush(h, 0);
     return PCF_OK;
 }
 
@@ -1812,23 +1850,46 @@ int pcf_implicit_step_device(pcf_handle *h, double dt, double rayleigh_factor, c
     double *wold = wold_scratch(h, d_wold, &rc);
     if (rc) return rc;
     const int damp = prm->damp_horizontal_wind_on_rhs;
-    // implicit_integration!.jl:49-63
-    if ((rc = pcf_launch_modify_wind(h, d_p, d_u, d_v, d_w, 0))) return rc;
-    if ((rc = pcf_launch_fill_predictands(h, d_rho, d_rhop, d_u, d_v, d_w, d_pip, d_p))) return rc;
-    if ((rc = pcf_launch_predictor(h, dt, rayleigh_factor, damp, d_u, d_v, d_w, d_rho, d_rhop, d_pip, d_p, d_betar,
-                                   d_dudt, d_dvdt, wold)))
-        return rc;
-    // :65-71: apply_corrector!; like the reference, an unconverged solve
-    // returns with the predicted (uncorrected) fields and errflag set
-    if ((rc = pcf_apply_corrector_device(h, d_u, d_v, d_w, d_rho, d_rhop, d_betar, d_p, d_pip, d_heating, dt,
-                                         rayleigh_factor, prm, d_dpip, res)))
-        return rc;
-    if (res->errflag) return PCF_OK;
-    // :75-77
-    if ((rc = pcf_launch_modify_wind(h, d_p, d_u, d_v, d_w, 1))) return rc;
-    if ((rc = pcf_launch_fill_predictands(h, d_rho, d_rhop, d_u, d_v, d_w, d_pip, d_p))) return rc;
-    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
-    return PCF_OK;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    PCF_CUDA_TRY(cudaEventCreate(&ev[0]));
+    if (cudaEventCreate(&ev[1]) != cudaSuccess) {
+        cudaEventDestroy(ev[0]);
+        return pcf_set_cuda_error(cudaGetLastError());
+    }
+    auto body = [&]() -> int {
+        PCF_CUDA_TRY(cudaEventRecord(ev[0], h->stream));
+        // implicit_integration!.jl:49-63
+        int r;
+        if ((r = pcf_launch_modify_wind(h, d_p, d_u, d_v, d_w, 0))) return r;
+        if ((r = pcf_launch_fill_predictands(h, d_rho, d_rhop, d_u, d_v, d_w, d_pip, d_p))) return r;
+        {
+            ProfScope ps(h, PCF_PROF_PREDICT, predictor_bytes(h, damp, d_dudt != nullptr), 0);
+            if ((r = pcf_launch_predictor(h, dt, rayleigh_factor, damp, d_u, d_v, d_w, d_rho, d_rhop, d_pip, d_p,
+                                          d_betar, d_dudt, d_dvdt, wold)))
+                return r;
+        }
+        // :65-71: apply_corrector!; like the reference, an unconverged solve
+        // returns with the predicted (uncorrected) fields and errflag set
+        if ((r = pcf_apply_corrector_device(h, d_u, d_v, d_w, d_rho, d_rhop, d_betar, d_p, d_pip, d_heating, dt,
+                                            rayleigh_factor, prm, d_dpip, res)))
+            return r;
+        if (!res->errflag) {
+            // :75-77
+            if ((r = pcf_launch_modify_wind(h, d_p, d_u, d_v, d_w, 1))) return r;
+            if ((r = pcf_launch_fill_predictands(h, d_rho, d_rhop, d_u, d_v, d_w, d_pip, d_p))) return r;
+        }
+        PCF_CUDA_TRY(cudaEventRecord(ev[1], h->stream));
+        PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        float ms = 0;
+        PCF_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+        res->ms_total = ms;
+        prof_flush(h, 0);
+        return PCF_OK;
+    };
+    rc = body();
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    return rc;
 }
 
 int pcf_implicit_step(pcf_handle *h, double dt, double rayleigh_factor, const pcf_params *prm, double *u, double *v,

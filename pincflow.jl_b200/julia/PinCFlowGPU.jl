@@ -12,7 +12,12 @@
 # (src/PoissonSolver/apply_corrector!.jl:44-61: compute_lhs!, the solve, the
 # dpip halo fill and correct!) with the same signatures and return convention
 # (errflag, niter); dt == 0 raises as in the reference, a non-converged solve
-# returns (true, niter) and leaves dpip and the fields untouched.
+# returns (true, niter) and leaves dpip and the fields untouched.  With
+# enable!(implicit_step = true) the whole
+#     PinCFlow.Integration.implicit_integration!(state, dtstage, time, ntotalbicg,
+#                                                side, rayleigh_factor, iout,
+#                                                machine_start_time)
+# (src/Integration/implicit_integration!.jl:40-80) is one library call.
 # Single MPI rank only (npx = npy = npz = 1).
 module PinCFlowGPU
 
@@ -179,17 +184,65 @@ function apply_corrector_gpu!(state, dt::AbstractFloat, rayleigh_factor::Abstrac
     return (errflag, niter)
 end
 
+# implicit_integration!.jl:40-80 through the library: modify_compressible_wind!,
+# the predictor update!(U, V, W, RhoP; Implicit()) with set_boundaries!,
+# apply_corrector!, the inverse wind factors and set_boundaries! in one call
+# (pcf_implicit_step).  Tracer boundaries are not the library's: the Julia
+# fills run once afterwards (the step leaves tracers unchanged).
+function implicit_integration_gpu!(state, dtstage::AbstractFloat, time::AbstractFloat, ntotalbicg::Integer,
+                                   side, rayleigh_factor::AbstractFloat, iout::Integer, machine_start_time)
+    h = handle(state)
+    (; rho, rhop, u, v, w, pip, p) = state.variables.predictands
+    (; wold) = state.variables.backups
+    (; dpip) = state.variables.increments
+    (; betar) = state.sponge
+    compressible = state.namelists.atmosphere.model == :Compressible
+    pp = compressible ? p : C_NULL
+    dudt = dvdt = C_NULL
+    if state.namelists.wkb.wkb_mode != :NoWKB
+        (; dudt, dvdt) = state.wkb.tendencies
+    end
+    heating = C_NULL
+    if compressible  # compute_volume_force(P) reads rho and fluxes, which the predictor leaves alone
+        (; i0, i1, j0, j1, k0, k1) = state.domain
+        heating = [PinCFlow.Update.compute_volume_force(state, i, j, k, PinCFlow.P())
+                   for i in i0:i1, j in j0:j1, k in k0:k1]
+    end
+    prm = params(state)
+    res = PcfResult()
+    GC.@preserve u v w rho rhop pip p betar dudt dvdt heating wold dpip begin
+        rc = ccall((:pcf_implicit_step, LIB), Cint,
+                   (Ptr{Cvoid}, Cdouble, Cdouble, Ref{PcfParams}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
+                    Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
+                    Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ref{PcfResult}),
+                   h, dtstage, rayleigh_factor, prm, u, v, w, rho, rhop, pip, pp, betar, dudt, dvdt, heating,
+                   wold, dpip, res)
+    end
+    check(rc, "pcf_implicit_step")
+    if res.errflag != 0
+        iout = PinCFlow.Output.write_output(state, time, iout, machine_start_time)
+        error("BiCGSTAB errored! Output last state into record ", iout, ".")
+    end
+    B = PinCFlow.Boundaries
+    B.set_tracer_zonal_boundaries!(state, B.BoundaryPredictands())
+    B.set_tracer_meridional_boundaries!(state, B.BoundaryPredictands())
+    B.set_tracer_vertical_boundaries!(state, B.BoundaryPredictands())
+    return ntotalbicg + Int(res.niter)
+end
+
 """
-    enable!(; precision = :fp64, multigrid = false, corrector = false, device = 0)
+    enable!(; precision = :fp64, multigrid = false, corrector = false, implicit_step = false, device = 0)
 
 Make `PinCFlow.PoissonSolver.solve_poisson!` run on the GPU.  `precision = :mixed`
 selects the FP32-inner / FP64-refined solve (same FP64 tolerance), and
 `multigrid = true` (with `:mixed`) its multigrid preconditioner.
 `corrector = true` also replaces `apply_corrector!` (compute_lhs!, the solve and
-correct! all on the GPU).
+correct! all on the GPU); `implicit_step = true` replaces the whole
+`implicit_integration!` (the implicit predictor, the corrector and the
+boundary fills of the predictands in one library call per half step).
 """
 function enable!(; precision::Symbol = :fp64, multigrid::Bool = false, corrector::Bool = false,
-                 device::Integer = 0)
+                 implicit_step::Bool = false, device::Integer = 0)
     SETTINGS[] = (precision = precision, multigrid = multigrid, device = device)
     @eval PS function solve_poisson!(state::PinCFlow.State, dt::AbstractFloat,
                                      rayleigh_factor::AbstractFloat, tolref::AbstractFloat)
@@ -199,6 +252,15 @@ function enable!(; precision::Symbol = :fp64, multigrid::Bool = false, corrector
         @eval PS function apply_corrector!(state::PinCFlow.State, dt::AbstractFloat,
                                            rayleigh_factor::AbstractFloat)
             return $(apply_corrector_gpu!)(state, dt, rayleigh_factor)
+        end
+    end
+    if implicit_step
+        @eval PinCFlow.Integration function implicit_integration!(state::PinCFlow.State, dtstage::AbstractFloat,
+                                                                  time::AbstractFloat, ntotalbicg::Integer,
+                                                                  side::RHS, rayleigh_factor::AbstractFloat,
+                                                                  iout::Integer, machine_start_time::DateTime)
+            return $(implicit_integration_gpu!)(state, dtstage, time, ntotalbicg, side, rayleigh_factor, iout,
+                                                machine_start_time)
         end
     end
     return nothing

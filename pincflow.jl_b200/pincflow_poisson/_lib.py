@@ -45,7 +45,7 @@ EXPORTS = [
 ]
 TUNE_KERNELS = ["total32", "total32_diff", "horiz32", "total64", "horiz64"]
 PROF_TAGS = ["apply32", "apply64", "pseudo32", "pseudo64", "thomas32", "thomas64", "update32", "update64",
-             "assemble", "reliable64", "mg", "learned"]
+             "assemble", "reliable64", "mg", "learned", "predict", "correct"]
 
 
 class PcfDims(ctypes.Structure):

@@ -145,3 +145,25 @@ def test_julia_binding_structs_match_the_header(c_name, jl_name):
     ctype = {"int": "Cint", "double": "Cdouble"}
     c = [(n, ctype[t]) for n, t in _c_struct_fields(c_name)]
     assert _julia_struct_fields(jl_name) == c
+
+
+def _header_arity(name):
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    m = re.search(r"\b" + name + r"\s*\(([^;{]*?)\)\s*;", src, flags=re.S)
+    assert m, name
+    params = m.group(1).strip()
+    return 0 if params in ("", "void") else len(params.split(","))
+
+
+def test_julia_ccalls_bind_declared_symbols_with_their_arity():
+    """Every ccall of the Julia binding names a function of the header and
+    lists as many argument types as the header has parameters (Julia is not
+    installed here, so this is the check that the binding would link)."""
+    src = open(os.path.join(REPO, "pincflow.jl_b200", "julia", "PinCFlowGPU.jl")).read()
+    declared = set(declared_functions())
+    calls = re.findall(r"ccall\(\(:(pcf_\w+),\s*LIB\),\s*\w+(?:\{\w+\})?,\s*\((.*?)\),", src, flags=re.S)
+    assert len(calls) >= 9
+    for name, types in calls:
+        assert name in declared, name
+        n = len([t for t in re.split(r",\s*", types.strip()) if t])
+        assert n == _header_arity(name), (name, n, _header_arity(name))
