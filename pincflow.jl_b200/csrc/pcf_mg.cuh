@@ -189,93 +189,4 @@ __global__ void __launch_bounds__(256) k_mg_prolong(const float *__restrict__ e,
     }
 }
 
-// The smoother's column solve on the coarse levels, one warp per column.
-// Both sweeps are first-order linear recurrences (y_k = rhs_k P_k + M_k y_k-1
-// up, x_k = y_k + Q_k x_k+1 down), so each lane composes the affine maps of
-// its own run of levels and a warp scan of the composites gives every run its
-// entry value: the column costs a few dependent steps instead of nz, which
-// is what matters on levels with few columns.  MODE is TH_B (rhs = -deta b)
-// or TH_T (rhs = t, in place allowed).  nz <= 32 * kLevelsPerLane.
-constexpr int kLevelsPerLane = 8;
-
-template <int MODE>
-__global__ void __launch_bounds__(128) k_thomas_warp(ThomasArgs<float> a) {
-    if (krylov_done(a.scal)) return;
-    const int col = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (col >= a.plane) return;  // uniform per warp
-    const float *P = a.fac, *M = a.fac + a.n, *Q = a.fac + 2 * a.n;
-    const long long pl = a.plane;
-    const int per = (a.nz + 31) >> 5;
-    const int kb = lane * per;
-    const float deta = (float)a.deta;
-    float rhs[kLevelsPerLane], mm[kLevelsPerLane], qq[kLevelsPerLane];
-    // forward: affine composite (A, B) of the lane's levels, y_out = A + B y_in
-    float A = 0.0f, B = 1.0f;
-#pragma unroll
-    for (int q = 0; q < kLevelsPerLane; ++q) {
-        const int k = kb + q;
-        if (q < per && k < a.nz) {
-            const long long o = col + pl * k;
-            const float in = a.in[o];
-            const float p = __ldg(P + o);
-            mm[q] = __ldg(M + o);
-            qq[q] = __ldg(Q + o);
-            rhs[q] = (MODE == TH_B ? -deta * in : in) * p;
-            A = fmaf(mm[q], A, rhs[q]);
-            B = mm[q] * B;
-        }
-    }
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const float Ao = __shfl_up_sync(0xffffffffu, A, o), Bo = __shfl_up_sync(0xffffffffu, B, o);
-        if (lane >= o) {
-            A = fmaf(B, Ao, A);
-            B = B * Bo;
-        }
-    }
-    float y = __shfl_up_sync(0xffffffffu, A, 1);
-    if (lane == 0) y = 0.0f;
-    float yv[kLevelsPerLane];
-#pragma unroll
-    for (int q = 0; q < kLevelsPerLane; ++q) {
-        const int k = kb + q;
-        if (q < per && k < a.nz) {
-            y = fmaf(mm[q], y, rhs[q]);
-            yv[q] = y;
-        }
-    }
-    // backward: x_k = y_k + Q_k x_k+1 with x_nz = 0; composite over the lane's
-    // levels from the top down, then a suffix scan across lanes
-    float C = 0.0f, D = 1.0f;  // x_kb = C + D x_(kb+per)
-#pragma unroll
-    for (int q = kLevelsPerLane - 1; q >= 0; --q) {
-        const int k = kb + q;
-        if (q < per && k < a.nz) {
-            const float qk = (k == a.nz - 1) ? 0.0f : qq[q];
-            C = fmaf(qk, C, yv[q]);
-            D = qk * D;
-        }
-    }
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const float Co = __shfl_down_sync(0xffffffffu, C, o), Do = __shfl_down_sync(0xffffffffu, D, o);
-        if (lane + o < 32) {
-            C = fmaf(D, Co, C);
-            D = D * Do;
-        }
-    }
-    float x = __shfl_down_sync(0xffffffffu, C, 1);
-    if (lane == 31) x = 0.0f;
-#pragma unroll
-    for (int q = kLevelsPerLane - 1; q >= 0; --q) {
-        const int k = kb + q;
-        if (q < per && k < a.nz) {
-            const float qk = (k == a.nz - 1) ? 0.0f : qq[q];
-            x = fmaf(qk, x, yv[q]);
-            a.out[col + pl * k] = x;
-        }
-    }
-}
-
 }  // namespace pcf
