@@ -163,7 +163,9 @@ typedef struct pcf_handle pcf_handle;
  * Fills *p with the reference defaults. */
 int pcf_params_default(pcf_params *p);
 
-/* Allocates all device memory of one solver instance (one `State`). */
+/* Allocates all device memory of one solver instance (one `State`).
+ * PCF_EINVAL unless nx, ny >= 1, nz >= 4, nbx, nby >= 1, nbz >= 2;
+ * PCF_ERANGE for 2^31 or more haloed cells. */
 int pcf_create(pcf_handle **h, const pcf_dims *dims);
 int pcf_destroy(pcf_handle *h);
 const char *pcf_strerror(int code);

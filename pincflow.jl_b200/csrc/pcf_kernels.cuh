@@ -831,7 +831,9 @@ __global__ void __launch_bounds__(128) k_build_diff(const double *__restrict__ A
     const long long n = (long long)nx * ny * nz;
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
-    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+    // 32-bit decomposition: any grid whose operator fits in HBM has < 2^31 cells
+    const unsigned cu = (unsigned)c, ux = (unsigned)nx, uy = (unsigned)ny;
+    const int i = (int)(cu % ux), j = (int)((cu / ux) % uy), k = (int)(cu / (ux * uy));
     const long long sy = nxx, sz = (long long)nxx * nyy;
     const long long h = (i + nbx) + sy * (j + nby) + sz * (k + nbz);
     // (di, dj, dk) of each plane in Tensor order
@@ -900,7 +902,8 @@ __global__ void __launch_bounds__(256) k_compute_lhs(LhsArgs a) {
     double s0 = 0.0, s1 = 0.0;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
          q += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(q % a.nx), j = (int)((q / a.nx) % a.ny), k = (int)(q / ((long long)a.nx * a.ny));
+        const unsigned qu = (unsigned)q, ux = (unsigned)a.nx, uy = (unsigned)a.ny;  // n < 2^31 (see k_build_diff)
+        const int i = (int)(qu % ux), j = (int)((qu / ux) % uy), k = (int)(qu / (ux * uy));
         const long long h = (i + a.nbx) + sy * (j + a.nby) + sz * (k + a.nbz);
         const double jc = a.jac[h];
         const double sc = a.c / jc * a.rfch[h];  // Ma^2 kappa / (J fcscal)

@@ -64,7 +64,8 @@ __global__ void __launch_bounds__(256) k_mg_fc(const TF *__restrict__ fc, int nx
     const int NX = nx / CX, NY = ny / CY;
     const long long nc = (long long)NX * NY * nz;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nc; q += (long long)gridDim.x * blockDim.x) {
-        const int I = (int)(q % NX), J = (int)((q / NX) % NY), k = (int)(q / ((long long)NX * NY));
+        const unsigned qu = (unsigned)q, ux = (unsigned)NX, uy = (unsigned)NY;  // n < 2^31
+        const int I = (int)(qu % ux), J = (int)((qu / ux) % uy), k = (int)(qu / (ux * uy));
         double acc = 0.0;
 #pragma unroll
         for (int b = 0; b < CY; ++b)
@@ -88,7 +89,8 @@ __global__ void __launch_bounds__(128) k_mg_coarsen(const TI *__restrict__ coef,
     const long long n = (long long)nx * ny * nz, nc = (long long)NX * NY * nz;
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nc) return;
-    const int I = (int)(q % NX), J = (int)((q / NX) % NY), k = (int)(q / ((long long)NX * NY));
+    const unsigned qu = (unsigned)q, ux = (unsigned)NX, uy = (unsigned)NY;  // n < 2^31
+    const int I = (int)(qu % ux), J = (int)((qu / ux) % uy), k = (int)(qu / (ux * uy));
     double acc[PCF_NCOEF];
 #pragma unroll
     for (int p = 0; p < PCF_NCOEF; ++p) acc[p] = 0.0;
@@ -152,41 +154,94 @@ __global__ void __launch_bounds__(128) k_mg_factors(int plane, int nz, long long
     }
 }
 
-// b_c = sum over the aggregate of (f r) / (cx cy f_c)
+// b_c = sum over the aggregate of (f r) / (cx cy f_c); one thread per
+// coarse point of an (NX, NY, nz) grid of blocks (32 x 8 threads in x-y, one
+// level per grid row).
 template <typename TF, int CX, int CY>
 __global__ void __launch_bounds__(256) k_mg_restrict(const float *__restrict__ r, const TF *__restrict__ fc, int nx,
                                                       int ny, int nz, const float *__restrict__ fcc,
                                                       float *__restrict__ bc, const KrylovScalars *guard) {
     if (krylov_done(guard)) return;
     const int NX = nx / CX, NY = ny / CY;
-    const long long nc = (long long)NX * NY * nz;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nc; q += (long long)gridDim.x * blockDim.x) {
-        const int I = (int)(q % NX), J = (int)((q / NX) % NY), k = (int)(q / ((long long)NX * NY));
-        float acc = 0.0f;
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (I >= NX || J >= NY) return;
+    const long long q = I + (long long)NX * (J + (long long)NY * k);
+    float acc = 0.0f;
 #pragma unroll
-        for (int b = 0; b < CY; ++b)
+    for (int b = 0; b < CY; ++b)
 #pragma unroll
-            for (int a = 0; a < CX; ++a) {
-                const long long c = (CX * I + a) + (long long)nx * ((CY * J + b) + (long long)ny * k);
-                acc += (float)fc[c] * r[c];
-            }
-        bc[q] = acc / ((float)(CX * CY) * fcc[q]);
-    }
+        for (int a = 0; a < CX; ++a) {
+            const long long c = (CX * I + a) + (long long)nx * ((CY * J + b) + (long long)ny * k);
+            acc += (float)fc[c] * r[c];
+        }
+    bc[q] = acc / ((float)(CX * CY) * fcc[q]);
 }
 
-// s += f_c e / f (piecewise-constant prolongation of the coarse correction)
+// s += f_c e / f (piecewise-constant prolongation of the coarse correction);
+// one thread per fine point, 64 x 4 threads in x-y, one level per grid row.
 template <typename TF, int CX, int CY>
 __global__ void __launch_bounds__(256) k_mg_prolong(const float *__restrict__ e, const float *__restrict__ fcc,
                                                      const TF *__restrict__ fc, int nx, int ny, int nz, float *s,
                                                      const KrylovScalars *guard) {
     if (krylov_done(guard)) return;
     const int NX = nx / CX, NY = ny / CY;
-    const long long n = (long long)nx * ny * nz;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
-        const long long q = i / CX + (long long)NX * (j / CY + (long long)NY * k);
-        s[c] += fcc[q] * e[q] / (float)fc[c];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= nx || j >= ny) return;
+    const long long c = i + (long long)nx * (j + (long long)ny * k);
+    const long long q = i / CX + (long long)NX * (j / CY + (long long)NY * k);
+    s[c] += fcc[q] * e[q] / (float)fc[c];
+}
+
+// k_mg_restrict for four consecutive fine x cells per thread (4 / CX coarse
+// points) with 128-bit loads of r and fc (nx % 4 == 0); the sums run in the
+// order of k_mg_restrict.
+template <int CX, int CY>
+__global__ void __launch_bounds__(256) k_mg_restrict4(const float *__restrict__ r, const float *__restrict__ fc,
+                                                       int nx, int ny, int nz, const float *__restrict__ fcc,
+                                                       float *__restrict__ bc, const KrylovScalars *guard) {
+    if (krylov_done(guard)) return;
+    const int NX = nx / CX, NY = ny / CY;
+    const int i4 = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (4 * i4 >= nx || J >= NY) return;
+    constexpr int NC = 4 / CX;  // coarse points of this thread
+    float acc[NC];
+#pragma unroll
+    for (int m = 0; m < NC; ++m) acc[m] = 0.0f;
+#pragma unroll
+    for (int b = 0; b < CY; ++b) {
+        const long long c = 4LL * i4 + (long long)nx * ((CY * J + b) + (long long)ny * k);
+        const float4 rv = *reinterpret_cast<const float4 *>(r + c);
+        const float4 fv = *reinterpret_cast<const float4 *>(fc + c);
+        const float pr[4] = {fv.x * rv.x, fv.y * rv.y, fv.z * rv.z, fv.w * rv.w};
+#pragma unroll
+        for (int a = 0; a < 4; ++a) acc[a / CX] += pr[a];
     }
+    const long long q = (long long)(4 / CX) * i4 + (long long)NX * (J + (long long)NY * k);
+#pragma unroll
+    for (int m = 0; m < NC; ++m) bc[q + m] = acc[m] / ((float)(CX * CY) * fcc[q + m]);
+}
+
+// k_mg_prolong on four consecutive x cells per thread with 128-bit loads
+// and stores of s and fc (nx % 4 == 0, so every row starts 16-byte aligned).
+template <int CX, int CY>
+__global__ void __launch_bounds__(256) k_mg_prolong4(const float *__restrict__ e, const float *__restrict__ fcc,
+                                                      const float *__restrict__ fc, int nx, int ny, int nz, float *s,
+                                                      const KrylovScalars *guard) {
+    if (krylov_done(guard)) return;
+    const int NX = nx / CX, NY = ny / CY;
+    const int i4 = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (4 * i4 >= nx || j >= ny) return;
+    const long long c = 4LL * i4 + (long long)nx * (j + (long long)ny * k);
+    const long long qrow = (long long)NX * (j / CY + (long long)NY * k);
+    const float4 f = *reinterpret_cast<const float4 *>(fc + c);
+    float4 v = *reinterpret_cast<const float4 *>(s + c);
+    const int i = 4 * i4;
+    const long long q0 = qrow + i / CX, q1 = qrow + (i + 1) / CX, q2 = qrow + (i + 2) / CX, q3 = qrow + (i + 3) / CX;
+    v.x += fcc[q0] * e[q0] / f.x;
+    v.y += fcc[q1] * e[q1] / f.y;
+    v.z += fcc[q2] * e[q2] / f.z;
+    v.w += fcc[q3] * e[q3] / f.w;
+    *reinterpret_cast<float4 *>(s + c) = v;
 }
 
 }  // namespace pcf

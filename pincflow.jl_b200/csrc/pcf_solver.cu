@@ -549,13 +549,25 @@ static ThomasArgs<float> mg_targs(const MgLevel &L, const float *fac, const floa
 static int mg_restrict(pcf_handle *h, int l, const float *r, const KrylovScalars *guard) {
     const MgLevel &F = h->mg->lv[l], &Cl = h->mg->lv[l + 1];
     ProfScope ps(h, PCF_PROF_MG, (2.0 + 2.0 / (Cl.cx * Cl.cy)) * 4 * (double)F.d.n);
-    const unsigned g = vec_grid(Cl.d.n);
+    if (F.d.nx % 4 == 0 && ((reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(F.fc)) & 15) == 0) {
+        const int n4 = F.d.nx / 4;
+        const dim3 blk(32, 8, 1), g((unsigned)((n4 + 31) / 32), (unsigned)((Cl.d.ny + 7) / 8), (unsigned)Cl.d.nz);
+        if (Cl.cx == 2 && Cl.cy == 2)
+            k_mg_restrict4<2, 2><<<g, blk, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
+        else if (Cl.cx == 2)
+            k_mg_restrict4<2, 1><<<g, blk, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
+        else
+            k_mg_restrict4<1, 2><<<g, blk, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
+        PCF_CUDA_TRY(cudaGetLastError());
+        return PCF_OK;
+    }
+    const dim3 blk(32, 8, 1), g((unsigned)((Cl.d.nx + 31) / 32), (unsigned)((Cl.d.ny + 7) / 8), (unsigned)Cl.d.nz);
     if (Cl.cx == 2 && Cl.cy == 2)
-        k_mg_restrict<float, 2, 2><<<g, 256, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
+        k_mg_restrict<float, 2, 2><<<g, blk, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
     else if (Cl.cx == 2)
-        k_mg_restrict<float, 2, 1><<<g, 256, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
+        k_mg_restrict<float, 2, 1><<<g, blk, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
     else
-        k_mg_restrict<float, 1, 2><<<g, 256, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
+        k_mg_restrict<float, 1, 2><<<g, blk, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
     PCF_CUDA_TRY(cudaGetLastError());
     return PCF_OK;
 }
@@ -564,13 +576,25 @@ static int mg_restrict(pcf_handle *h, int l, const float *r, const KrylovScalars
 static int mg_prolong(pcf_handle *h, int l, const float *e, float *s, const KrylovScalars *guard) {
     const MgLevel &F = h->mg->lv[l], &Cl = h->mg->lv[l + 1];
     ProfScope ps(h, PCF_PROF_MG, (3.0 + 2.0 / (Cl.cx * Cl.cy)) * 4 * (double)F.d.n);
-    const unsigned g = vec_grid(F.d.n);
+    if (F.d.nx % 4 == 0 && ((reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(F.fc)) & 15) == 0) {
+        const int n4 = F.d.nx / 4;
+        const dim3 blk(32, 8, 1), g((unsigned)((n4 + 31) / 32), (unsigned)((F.d.ny + 7) / 8), (unsigned)F.d.nz);
+        if (Cl.cx == 2 && Cl.cy == 2)
+            k_mg_prolong4<2, 2><<<g, blk, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
+        else if (Cl.cx == 2)
+            k_mg_prolong4<2, 1><<<g, blk, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
+        else
+            k_mg_prolong4<1, 2><<<g, blk, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
+        PCF_CUDA_TRY(cudaGetLastError());
+        return PCF_OK;
+    }
+    const dim3 blk(64, 4, 1), g((unsigned)((F.d.nx + 63) / 64), (unsigned)((F.d.ny + 3) / 4), (unsigned)F.d.nz);
     if (Cl.cx == 2 && Cl.cy == 2)
-        k_mg_prolong<float, 2, 2><<<g, 256, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
+        k_mg_prolong<float, 2, 2><<<g, blk, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
     else if (Cl.cx == 2)
-        k_mg_prolong<float, 2, 1><<<g, 256, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
+        k_mg_prolong<float, 2, 1><<<g, blk, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
     else
-        k_mg_prolong<float, 1, 2><<<g, 256, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
+        k_mg_prolong<float, 1, 2><<<g, blk, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
     PCF_CUDA_TRY(cudaGetLastError());
     return PCF_OK;
 }
@@ -1190,7 +1214,8 @@ __global__ void k_unscale(const double *__restrict__ x, const double *__restrict
                           int nbz, int nxx, int nyy, double *__restrict__ dst, int ox, int oy, int oz, int sx, int sy) {
     const long long n = (long long)nx * ny * nz;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+        const unsigned cu = (unsigned)c, ux = (unsigned)nx, uy = (unsigned)ny;  // n < 2^31 (see k_build_diff)
+        const int i = (int)(cu % ux), j = (int)((cu / ux) % uy), k = (int)(cu / (ux * uy));
         const long long hh = (i + nbx) + (long long)nxx * ((j + nby) + (long long)nyy * (k + nbz));
         const double pb = pbar[hh];
         const double sol = x[c] / sqrt(pb * pb / rhobar[hh]);
@@ -1293,6 +1318,11 @@ int pcf_create(pcf_handle **out, const pcf_dims *dims) {
     if (dims->nx < 1 || dims->ny < 1 || dims->nz < 4 || dims->nbx < 1 || dims->nby < 1 || dims->nbz < 2)
         return PCF_EINVAL;
     if (dims->model < 0 || dims->model > 2) return PCF_EINVAL;
+    // cell indices are decomposed in 32 bits (an FP64 operator of 2^31 cells
+    // would need 430 GB, beyond any single GPU's memory anyway)
+    const long long haloed = (long long)(dims->nx + 2 * dims->nbx) * (dims->ny + 2 * dims->nby) *
+                             (long long)(dims->nz + 2 * dims->nbz);
+    if (haloed >= (1LL << 31)) return PCF_ERANGE;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || dims->device < 0 || dims->device >= ndev) return PCF_ENODEVICE;
     cudaDeviceProp prop;
