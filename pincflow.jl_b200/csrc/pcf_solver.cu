@@ -138,7 +138,11 @@ static int pick_kc(long long xyblocks, int nz) {
     long long chunks = (want + xyblocks - 1) / xyblocks;
     if (chunks < 1) chunks = 1;
     long long kc = (nz + chunks - 1) / chunks;
-    if (kc < 4) kc = 4;
+    // at least 4 levels per block amortise the 5-plane prologue on large
+    // grids; grids of a few x-y tiles (coarse multigrid levels, L2-resident)
+    // are latency-bound, and one level per block shortens each block's chain
+    const long long kmin = xyblocks >= 16 ? 4 : 1;
+    if (kc < kmin) kc = kmin;
     if (kc > nz) kc = nz;
     while (kc < nz && xyblocks * ((nz + kc - 1) / kc) > kMaxPartials) kc = std::min<long long>(2 * kc, nz);
     return (int)kc;
