@@ -67,6 +67,10 @@ __device__ __forceinline__ int wrap(int x, int n) {
     return x < 0 ? x + n : x;
 }
 
+// periodic wrap of x in [-1, n] (an in-range index plus an offset of at most
+// one), without the division of wrap
+__device__ __forceinline__ int wrap1(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
+
 // Block-wide sum of NV values; the result is valid in thread 0.  The order
 // of additions depends only on blockDim, so it is deterministic.
 template <int NV>

@@ -78,19 +78,25 @@ __global__ void __launch_bounds__(256) k_mg_fc(const TF *__restrict__ fc, int nx
     }
 }
 
-// Coarse operator of level l+1 from level l (see the file header).  One
-// thread per coarse cell; TI is the type of the finer level's planes and
-// fcscal (double on the finest level, float below).
-template <typename TI, int CX, int CY>
-__global__ void __launch_bounds__(128) k_mg_coarsen(const TI *__restrict__ coef, const TI *__restrict__ fc, int nx,
-                                                    int ny, int nz, const float *__restrict__ fcc,
-                                                    float *__restrict__ out) {
+// Coarse operator of level l+1 from level l (see the file header).  The
+// aggregation is horizontal, so the fine couplings at vertical offset dz
+// feed only the coarse couplings at dz (re-discretisation moves included):
+// one thread per coarse cell and dz group (blockIdx.y = dz + 2) sums the 5
+// planes of its group, in the plane order of the Tensor struct.  TI is the
+// type of the finer level's planes and fcscal (double on the finest level,
+// float below).
+template <typename TI, int CX, int CY, int DZ>
+__device__ __forceinline__ void coarsen_group(const TI *__restrict__ coef, const TI *__restrict__ fc, int nx, int ny,
+                                              int nz, const float *__restrict__ fcc, float *__restrict__ out,
+                                              long long q, int I, int J, int k) {
     const int NX = nx / CX, NY = ny / CY;
     const long long n = (long long)nx * ny * nz, nc = (long long)NX * NY * nz;
-    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nc) return;
-    const unsigned qu = (unsigned)q, ux = (unsigned)NX, uy = (unsigned)NY;  // n < 2^31
-    const int I = (int)(qu % ux), J = (int)((qu / ux) % uy), k = (int)(qu / (ux * uy));
+    if (k + DZ < 0 || k + DZ >= nz) {  // couplings to a zero z-ghost
+#pragma unroll
+        for (int p = 0; p < PCF_NCOEF; ++p)
+            if (off_z(p) == DZ) out[(long long)p * nc + q] = 0.0f;
+        return;
+    }
     double acc[PCF_NCOEF];
 #pragma unroll
     for (int p = 0; p < PCF_NCOEF; ++p) acc[p] = 0.0;
@@ -103,54 +109,86 @@ __global__ void __launch_bounds__(128) k_mg_coarsen(const TI *__restrict__ coef,
             const double fcv = (double)fc[c];
 #pragma unroll
             for (int p = 0; p < PCF_NCOEF; ++p) {
-                const int dz = off_z(p);
-                if (k + dz < 0 || k + dz >= nz) continue;  // multiplies a zero z-ghost
+                if (off_z(p) != DZ) continue;
                 const int dx = off_x(p), dy = off_y(p);
-                const long long t = wrap(i + dx, nx) + (long long)nx * (wrap(j + dy, ny) + (long long)ny * (k + dz));
+                const long long t = wrap1(i + dx, nx) + (long long)nx * (wrap1(j + dy, ny) + (long long)ny * (k + DZ));
                 const double a0 = fcv * (double)coef[(long long)p * n + c] * (double)fc[t];
-                acc[coef_index(agg_off(a, dx, CX), agg_off(b, dy, CY), dz)] += a0;
+                acc[coef_index(agg_off(a, dx, CX), agg_off(b, dy, CY), DZ)] += a0;
             }
         }
     // re-discretisation scaling of the couplings across aggregate faces
 #pragma unroll
     for (int p = 0; p < PCF_NCOEF; ++p) {
+        if (off_z(p) != DZ) continue;
         const int dx = off_x(p), dy = off_y(p);
         if (dx == 0 && dy == 0) continue;
         const double keep = dx != 0 ? 1.0 / CX : 1.0 / CY;
         const double moved = (1.0 - keep) * acc[p];
         acc[p] -= moved;
-        acc[coef_index(0, 0, off_z(p))] += moved;
+        acc[coef_index(0, 0, DZ)] += moved;
     }
     const double fcI = (double)fcc[q];
 #pragma unroll
     for (int p = 0; p < PCF_NCOEF; ++p) {
-        const int dz = off_z(p);
-        double v = 0.0;
-        if (k + dz >= 0 && k + dz < nz) {
-            const long long t = wrap(I + off_x(p), NX) + (long long)NX * (wrap(J + off_y(p), NY) + (long long)NY * (k + dz));
-            v = acc[p] / ((double)(CX * CY) * fcI * (double)fcc[t]);
-        }
-        out[(long long)p * nc + q] = (float)v;
+        if (off_z(p) != DZ) continue;
+        const long long t = wrap1(I + off_x(p), NX) + (long long)NX * (wrap1(J + off_y(p), NY) + (long long)NY * (k + DZ));
+        out[(long long)p * nc + q] = (float)(acc[p] / ((double)(CX * CY) * fcI * (double)fcc[t]));
     }
 }
 
-// Thomas pivots P, M, Q of a level (as k_factors, from FP32 planes).
+template <typename TI, int CX, int CY>
+__global__ void __launch_bounds__(128) k_mg_coarsen(const TI *__restrict__ coef, const TI *__restrict__ fc, int nx,
+                                                    int ny, int nz, const float *__restrict__ fcc,
+                                                    float *__restrict__ out) {
+    const int NX = nx / CX, NY = ny / CY;
+    const long long nc = (long long)NX * NY * nz;
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nc) return;
+    const unsigned qu = (unsigned)q, ux = (unsigned)NX, uy = (unsigned)NY;  // n < 2^31
+    const int I = (int)(qu % ux), J = (int)((qu / ux) % uy), k = (int)(qu / (ux * uy));
+    switch (blockIdx.y) {
+        case 0: coarsen_group<TI, CX, CY, -2>(coef, fc, nx, ny, nz, fcc, out, q, I, J, k); break;
+        case 1: coarsen_group<TI, CX, CY, -1>(coef, fc, nx, ny, nz, fcc, out, q, I, J, k); break;
+        case 2: coarsen_group<TI, CX, CY, 0>(coef, fc, nx, ny, nz, fcc, out, q, I, J, k); break;
+        case 3: coarsen_group<TI, CX, CY, 1>(coef, fc, nx, ny, nz, fcc, out, q, I, J, k); break;
+        default: coarsen_group<TI, CX, CY, 2>(coef, fc, nx, ny, nz, fcc, out, q, I, J, k); break;
+    }
+}
+
+// Thomas pivots P, M, Q of a level (as k_factors, from FP32 planes; the
+// loads of each block of 8 levels are issued together ahead of the serial
+// recurrence).
 __global__ void __launch_bounds__(128) k_mg_factors(int plane, int nz, long long n, double deta,
                                                     const float *__restrict__ coef, float *__restrict__ fac) {
+    constexpr int CH = 8;
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= plane) return;
     const float *ac = coef + (long long)PCF_AC * n, *ad = coef + (long long)PCF_AD * n,
                 *au = coef + (long long)PCF_AU * n;
     double qprev = 0.0;
-    for (int k = 0; k < nz; ++k) {
-        const long long o = col + (long long)plane * k;
-        const double piv = k == 0 ? 1.0 / (1.0 - deta * ac[o]) : 1.0 / (1.0 - deta * ac[o] - deta * ad[o] * qprev);
-        const double m = k == 0 ? 0.0 : deta * ad[o] * piv;
-        const double qv = deta * au[o] * piv;
-        fac[o] = (float)piv;
-        fac[n + o] = (float)m;
-        fac[2 * n + o] = (float)qv;
-        qprev = qv;
+    for (int k0 = 0; k0 < nz; k0 += CH) {
+        float vc[CH], vd[CH], vu[CH];
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int k = k0 + q;
+            const long long o = col + (long long)plane * (k < nz ? k : 0);
+            vc[q] = ac[o];
+            vd[q] = ad[o];
+            vu[q] = au[o];
+        }
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int k = k0 + q;
+            if (k >= nz) break;
+            const long long o = col + (long long)plane * k;
+            const double piv = k == 0 ? 1.0 / (1.0 - deta * vc[q]) : 1.0 / (1.0 - deta * vc[q] - deta * vd[q] * qprev);
+            const double m = k == 0 ? 0.0 : deta * vd[q] * piv;
+            const double qv = deta * vu[q] * piv;
+            fac[o] = (float)piv;
+            fac[n + o] = (float)m;
+            fac[2 * n + o] = (float)qv;
+            qprev = qv;
+        }
     }
 }
 

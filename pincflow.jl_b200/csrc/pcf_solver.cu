@@ -774,7 +774,8 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
         const MgLevel &F = m.lv[l - 1];
         MgLevel &C = m.lv[l];
         ProfScope ps(h, PCF_PROF_ASSEMBLE, (26.0 * (l == 1 ? 8 : 4) + 32.0 / (C.cx * C.cy)) * (double)F.d.n);
-        const unsigned gf = vec_grid(C.d.n), gc = (unsigned)((C.d.n + 127) / 128);
+        const unsigned gf = vec_grid(C.d.n);
+        const dim3 gc((unsigned)((C.d.n + 127) / 128), 5, 1);  // x: coarse cells, y: the five dz groups
 #define PCF_MG_BUILD(CX, CY)                                                                                          \
     do {                                                                                                              \
         k_mg_fc<float, CX, CY><<<gf, 256, 0, h->stream>>>(F.fc, F.d.nx, F.d.ny, F.d.nz, C.fc);                        \
