@@ -210,10 +210,13 @@ def test_oracle_matches_golden_fixtures(oracle):
                        gold[f"{name}/precond"]) < 1e-12
 
 
-def test_c2_fixture_is_converged():
-    with open(os.path.join(HERE, "golden", "c2_fp64_oracle.json")) as fh:
+@pytest.mark.parametrize("config, lo, hi", [("c2", 300, 700), ("c5", 600, 1200)])
+def test_oracle_iteration_fixtures_are_converged(config, lo, hi):
+    """The oracle's full FP64 solves behind bench.py's CPU baselines
+    (tests/golden/make_oracle_iterations.py) reached 1e-10."""
+    with open(os.path.join(HERE, "golden", f"{config}_fp64_oracle.json")) as fh:
         d = json.load(fh)
-    assert not d["errflag"] and d["true_residual"] <= 1e-10 and 300 < d["niter"] < 700
+    assert not d["errflag"] and d["true_residual"] <= 1e-10 and lo < d["niter"] < hi
 
 
 def test_network_oracle_gradient_matches_finite_differences():
