@@ -138,6 +138,9 @@ typedef struct {
     int mg_min_columns;            /* multigrid: a level with at most this many columns is the coarsest (16) */
     int autotune;                  /* 1: time the stencil tile shapes of every new grid size on first use and keep
                                       the fastest (process-wide table, pcf_autotune_entries); 0: fixed heuristic (0) */
+    int mg_operator_bf16;          /* multigrid: 1: the V-cycle's finest-level residual and smoothing stencils read a
+                                      BF16 copy of the operator (half their bytes; the Krylov operator and the FP64
+                                      true residual are unchanged); 0: the FP32 copy (1) */
 } pcf_params;
 
 typedef struct {
@@ -385,7 +388,8 @@ enum pcf_prof_tag {
     PCF_PROF_LEARNED = 11,  /* learned preconditioner stage: residual, network, combination */
     PCF_PROF_PREDICT = 12,  /* implicit predictor with its predictand boundary fills (FP64) */
     PCF_PROF_CORRECT = 13,  /* corrector: dpip boundary fill and correct! (FP64) */
-    PCF_PROF_NTAGS = 14
+    PCF_PROF_MG_BF16 = 14,  /* V-cycle finest-level residual and smoothing stencils on the BF16 operator copy */
+    PCF_PROF_NTAGS = 15
 };
 long long pcf_launch_count(const pcf_handle *h);
 /* Relative recursive residual after each BiCGSTAB iteration of the last

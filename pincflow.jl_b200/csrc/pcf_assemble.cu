@@ -39,6 +39,7 @@ struct AssembleArgs {
     const double *rfch;  // 1 / fcscal, same grid
     double *coef64;
     float *coef32;
+    __nv_bfloat16 *coef16;  // BF16 copy (when the handle holds one)
 };
 
 // Column offsets of the 5 columns that carry coefficients.
@@ -260,6 +261,7 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
             const long long o = (long long)kPlane[c][z] * n + cell;
             a.coef64[o] = v;
             a.coef32[o] = (float)v;
+            if (a.coef16) a.coef16[o] = __float2bfloat16_rn((float)v);
         }
     }
 }
@@ -328,7 +330,7 @@ int pcf_launch_assemble(pcf_handle *h, double dt, double rf, int damp_h) {
     a.fch = h->fch;
     a.rfch = h->rfch;
     a.rdx = 1.0 / h->dx; a.rdy = 1.0 / h->dy; a.rdz = 1.0 / h->dz;
-    a.coef64 = h->coef64; a.coef32 = h->coef32;
+    a.coef64 = h->coef64; a.coef32 = h->coef32; a.coef16 = h->coef16;
     const long long n = h->d.n;
     const int bs = 128;
     pcf::k_assemble<<<(unsigned)((n + bs - 1) / bs), bs, 0, h->stream>>>(a);

@@ -13,6 +13,7 @@
 // iterations of the mixed-precision solve.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -138,6 +139,7 @@ struct pcf_handle {
     double *stage;       // 6 haloed staging arrays of the host-array wind entry points (on first use)
     double *corr;        // corx, cory of the corrector (2 haloed arrays, on first use)
     double *istage;      // staging of pcf_implicit_step: 12 haloed arrays + 1 interior (on first use)
+    __nv_bfloat16 *coef16;  // BF16 copy of the 25 planes for the V-cycle's finest level (on first use)
     float *rfc32;        // 1 / fcscal on the interior
     double fac_deta;  // d_eta the factors were built with (NaN: none)
     // FP64 Krylov vectors

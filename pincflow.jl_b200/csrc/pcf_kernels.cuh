@@ -52,6 +52,25 @@ __device__ __forceinline__ void load_vec(const T *__restrict__ p, T (&v)[V]) {
     for (int q = 0; q < V; ++q) v[q] = e[q];
 }
 
+// V consecutive BF16 values (2V bytes, 2V-byte aligned) widened to FP32
+template <int V>
+__device__ __forceinline__ void load_bf16(const __nv_bfloat16 *__restrict__ p, float (&v)[V]) {
+    if constexpr (V == 4) {
+        const uint2 x = __ldg(reinterpret_cast<const uint2 *>(p));
+        const __nv_bfloat162 lo = *reinterpret_cast<const __nv_bfloat162 *>(&x.x);
+        const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162 *>(&x.y);
+        const float2 a = __bfloat1622float2(lo), b = __bfloat1622float2(hi);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    } else if constexpr (V == 2) {
+        const unsigned x = __ldg(reinterpret_cast<const unsigned *>(p));
+        const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&x));
+        v[0] = a.x; v[1] = a.y;
+    } else {
+#pragma unroll
+        for (int q = 0; q < V; ++q) v[q] = __bfloat162float(p[q]);
+    }
+}
+
 template <typename T, int V>
 __device__ __forceinline__ void store_vec(T *__restrict__ p, const T (&v)[V]) {
     using VT = typename Vec<T, V>::type;
@@ -290,6 +309,7 @@ enum Epi : int {
 template <typename T>
 struct StencilArgs {
     const T *coef;        // 25 planes
+    const __nv_bfloat16 *coef16 = nullptr;  // the same planes in BF16, read by the C16 kernels
     const T *s;           // input vector
     T *out;
     const T *w1;          // EPI_DOT1/2: second operand; EPI_PSEUDO/RESID: b
@@ -370,8 +390,11 @@ __device__ __forceinline__ void ring_store(T *slot, const T (&rv)[Ring<T, V, TX,
 // space (pi = const) exact, which a rounded A in the plain form does not:
 // its smooth-mode error grows like eps32 / (k h)^2 and stalls the FP32
 // Krylov iteration on large grids.
-template <typename T, int V, int TX, int TY, bool HORIZ, int EPI, bool DIFF = false>
+// C16: the coefficient planes are read from a.coef16 (BF16, half the bytes;
+// FP32 only, for the preconditioner's stencils).
+template <typename T, int V, int TX, int TY, bool HORIZ, int EPI, bool DIFF = false, bool C16 = false>
 __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
+    static_assert(!C16 || sizeof(T) == 4, "BF16 planes feed the FP32 stencil only");
     using R = Ring<T, V, TX, TY>;
     __shared__ __align__(16) T sm[R::NS][R::NR * R::RW];
     if (a.guard_update ? no_update_pending(a.guard) : krylov_done(a.guard)) return;
@@ -407,7 +430,10 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
 #pragma unroll
             for (int p = 0; p < PCF_NCOEF; ++p) {
                 if (HORIZ && (p == PCF_AC || p == PCF_AD || p == PCF_AU)) continue;
-                load_vec<T, V>(a.coef + (long long)p * n + base, c[p]);
+                if constexpr (C16)
+                    load_bf16<V>(a.coef16 + (long long)p * n + base, c[p]);
+                else
+                    load_vec<T, V>(a.coef + (long long)p * n + base, c[p]);
             }
             // the pseudo-step / residual operand is loaded with the coefficients, not
             // after the sum, so that the level costs one HBM round trip, not two

@@ -160,11 +160,23 @@ static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_ov
     const dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)((a.nz + kc - 1) / kc));
     const dim3 block(TX, TY, 1);
     // algorithmic words per cell: coefficient planes + input + output (+ second operand)
-    const int words = (HORIZ ? 22 : 25) + 2 + (EPI == EPI_STORE ? 0 : 1);
+    const int planes = HORIZ ? 22 : 25;
+    const int words = planes + 2 + (EPI == EPI_STORE ? 0 : 1);
     const int tag = tag_override >= 0 ? tag_override
                     : a.guard_update ? PCF_PROF_RELIABLE
                     : HORIZ          ? (sizeof(T) == 4 ? PCF_PROF_PSEUDO32 : PCF_PROF_PSEUDO64)
                                      : (sizeof(T) == 4 ? PCF_PROF_APPLY32 : PCF_PROF_APPLY64);
+    // the preconditioner's stencils may read BF16 planes (a.coef16)
+    constexpr bool c16_ok = sizeof(T) == 4 && !DIFF && (EPI == EPI_PSEUDO || EPI == EPI_RESNR);
+    if constexpr (c16_ok) {
+        if (a.coef16) {
+            ProfScope ps(h, tag_override >= 0 ? tag_override : PCF_PROF_MG_BF16,
+                         ((double)planes * 2 + (double)(words - planes) * sizeof(T)) * (double)a.n);
+            k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF, true><<<grid, block, 0, h->stream>>>(a, kc);
+            PCF_CUDA_TRY(cudaGetLastError());
+            return PCF_OK;
+        }
+    }
     ProfScope ps(h, tag, (double)words * sizeof(T) * (double)a.n);
     k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF><<<grid, block, 0, h->stream>>>(a, kc);
     PCF_CUDA_TRY(cudaGetLastError());
@@ -504,9 +516,15 @@ struct MgState {
     int coarse_iters = 0;
     long long version = -1;  // operator version the coarse operators were built from
     double dtau = 0;
+    bool bf16 = false;       // the finest level's stencils read h->coef16
 };
 
 __global__ void k_to_float(const double *__restrict__ a, float *__restrict__ b, long long n, double scale);
+
+__global__ void k_float_to_bf16(const float *__restrict__ a, __nv_bfloat16 *__restrict__ b, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = __float2bfloat16_rn(a[i]);
+}
 
 // Coarse levels with few columns: k_thomas_split (runs of at most 8 levels,
 // up to 32 threads per column); otherwise the column-per-thread sweep.
@@ -605,9 +623,11 @@ static int mg_prolong(pcf_handle *h, int l, const float *e, float *s, const Kryl
 
 // One pseudo-time step from s on level L: out = s + deta (L_h s - b), then the column solve in place.
 static int mg_pseudo_step(pcf_handle *h, const MgLevel &L, const float *coef, const float *fac, const float *s,
-                          float *out, const float *b, const KrylovScalars *guard, const float *post, int tag) {
+                          float *out, const float *b, const KrylovScalars *guard, const float *post, int tag,
+                          const __nv_bfloat16 *coef16 = nullptr) {
     StencilArgs<float> sa;
     sa.coef = coef;
+    sa.coef16 = coef16;
     sa.s = s;
     sa.out = out;
     sa.w1 = b;
@@ -661,6 +681,7 @@ static int mg_precond(pcf_handle *h, const Work<float> &w, float *bvec, const Kr
                       float *o1, float *o2, const float *post) {
     MgState &m = *h->mg;
     const MgLevel &L = m.lv[0];
+    const __nv_bfloat16 *c16 = m.bf16 ? h->coef16 : nullptr;
     ThomasArgs<float> ta = mg_targs(L, w.fac, bvec, o1, guard);
     ta.r = w.r;
     ta.v = w.v;
@@ -674,7 +695,7 @@ static int mg_precond(pcf_handle *h, const Work<float> &w, float *bvec, const Kr
         float *cur = o1, *oth = o2;
         for (int q = 1; q < m.coarse_iters; ++q) {
             if ((rc = mg_pseudo_step(h, L, w.coef, w.fac, cur, oth, bvec, guard,
-                                     q + 1 == m.coarse_iters ? post : nullptr, -1)))
+                                     q + 1 == m.coarse_iters ? post : nullptr, -1, c16)))
                 return rc;
             std::swap(cur, oth);
         }
@@ -683,6 +704,7 @@ static int mg_precond(pcf_handle *h, const Work<float> &w, float *bvec, const Kr
     }
     StencilArgs<float> sa;
     sa.coef = w.coef;
+    sa.coef16 = c16;
     sa.s = o1;
     sa.out = o2;
     sa.w1 = bvec;
@@ -693,7 +715,7 @@ static int mg_precond(pcf_handle *h, const Work<float> &w, float *bvec, const Kr
     float *e = nullptr;
     if ((rc = mg_cycle(h, 1, guard, &e))) return rc;
     if ((rc = mg_prolong(h, 0, e, o1, guard))) return rc;
-    if ((rc = mg_pseudo_step(h, L, w.coef, w.fac, o1, o2, bvec, guard, post, -1))) return rc;
+    if ((rc = mg_pseudo_step(h, L, w.coef, w.fac, o1, o2, bvec, guard, post, -1, c16))) return rc;
     *result = o2;
     return PCF_OK;
 }
@@ -759,6 +781,21 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
         m.version = -1;
     }
     m.coarse_iters = prm->mg_coarse_iterations;
+    m.bf16 = prm->mg_operator_bf16 != 0;
+    if (m.bf16 && !h->coef16) {
+        // first use: allocate and convert; later assemblies and pcf_set_operator write it themselves
+        const size_t bytes = sizeof(__nv_bfloat16) * (size_t)h->d.n * PCF_NCOEF;
+        const cudaError_t e = cudaMalloc((void **)&h->coef16, bytes);
+        if (e != cudaSuccess) {
+            h->coef16 = nullptr;
+            return pcf_set_cuda_error(e);
+        }
+        h->bytes += (long long)bytes;
+        ProfScope ps(h, PCF_PROF_ASSEMBLE, 6.0 * PCF_NCOEF * (double)h->d.n);
+        k_float_to_bf16<<<vec_grid(h->d.n * PCF_NCOEF), 256, 0, h->stream>>>(h->coef32, h->coef16,
+                                                                              h->d.n * PCF_NCOEF);
+        PCF_CUDA_TRY(cudaGetLastError());
+    }
     for (MgLevel &L : m.lv) L.deta = prm->mg_dtau / (2 * (1 / (L.dx * L.dx) + 1 / (L.dy * L.dy)));
     // the finest level's pivots are the handle's (shared with the reference preconditioner)
     int rc = ensure_factors(h, m.lv[0].deta);
@@ -1007,12 +1044,13 @@ struct RunOut {
 struct GraphKey {
     int tsize, precond, pc_iters, flex, reliable, pi, batch;
     double deta;
-    int mg, mg_levels, mg_coarse_iters;
+    int mg, mg_levels, mg_coarse_iters, mg_bf16;
     const void *net;  // the learned stage's network (null: no stage)
     bool operator==(const GraphKey &o) const {
         return tsize == o.tsize && precond == o.precond && pc_iters == o.pc_iters && flex == o.flex &&
                reliable == o.reliable && pi == o.pi && batch == o.batch && deta == o.deta && mg == o.mg &&
-               mg_levels == o.mg_levels && mg_coarse_iters == o.mg_coarse_iters && net == o.net;
+               mg_levels == o.mg_levels && mg_coarse_iters == o.mg_coarse_iters && mg_bf16 == o.mg_bf16 &&
+               net == o.net;
     }
 };
 struct GraphEntry {
@@ -1125,7 +1163,7 @@ static int run_finish(pcf_handle *h, const Work<T> &w, const LoopCfg &c, bool pr
 static GraphKey graph_key(const pcf_handle *h, int tsize, const LoopCfg &c, bool pi, int check_interval) {
     return GraphKey{tsize, c.precond, c.pc_iters, c.flex, c.reliable, pi, check_interval, c.deta, c.mg,
                     c.mg && h->mg ? (int)h->mg->lv.size() : 0, c.mg && h->mg ? h->mg->coarse_iters : 0,
-                    c.learned_pc ? (const void *)h->net : nullptr};
+                    c.mg && h->mg ? (int)h->mg->bf16 : 0, c.learned_pc ? (const void *)h->net : nullptr};
 }
 
 // A complete BiCGSTAB run: run_start, the iteration batches, run_finish.
@@ -1273,6 +1311,7 @@ int pcf_params_default(pcf_params *p) {
     p->mg_coarse_iterations = 4;
     p->mg_min_columns = 16;
     p->autotune = 0;
+    p->mg_operator_bf16 = 1;
     return PCF_OK;
 }
 
@@ -1288,7 +1327,7 @@ int pcf_destroy(pcf_handle *h) {
     int dev = h->dims.device;
     cudaSetDevice(dev);
     void *ptrs[] = {h->jac, h->met13, h->met23, h->met33, h->pbar, h->rhobar, h->thetabar, h->n2, h->rho, h->betar,
-                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch, h->stage, h->corr, h->istage, h->lr32,
+                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch, h->stage, h->corr, h->istage, h->coef16, h->lr32,
                     h->x64, h->r64, h->r064, h->p64, h->v64, h->s64,
                     h->t64, h->za64, h->zb64, h->b64, h->w64, h->x32, h->r32, h->r032, h->p32, h->v32, h->s32,
                     h->t32, h->za32, h->zb32, h->zc32, h->zd32, h->partials, h->ticket, h->scal64, h->scal32,
@@ -1473,6 +1512,11 @@ int pcf_set_operator(pcf_handle *h, const double *coef) {
     k_coef_to_float<<<vec_grid(m), 256, 0, h->stream>>>(h->coef64, h->coef32, m);
     h->launches += 1;
     PCF_CUDA_TRY(cudaGetLastError());
+    if (h->coef16) {
+        k_float_to_bf16<<<vec_grid(m), 256, 0, h->stream>>>(h->coef32, h->coef16, m);
+        h->launches += 1;
+        PCF_CUDA_TRY(cudaGetLastError());
+    }
     h->operator_set = 1;
     h->op_version += 1;
     h->fac_deta = std::nan("");

@@ -53,6 +53,7 @@ mutable struct PcfParams
     mg_coarse_iterations::Cint
     mg_min_columns::Cint
     autotune::Cint
+    mg_operator_bf16::Cint
 end
 
 mutable struct PcfResult
@@ -116,7 +117,7 @@ end
 function params(state)
     (; tolerance, poisson_iterations, preconditioner, dtau, preconditioner_iterations,
        tolerance_is_relative) = state.namelists.poisson
-    p = PcfParams(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
+    p = PcfParams(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
     ccall((:pcf_params_default, LIB), Cint, (Ref{PcfParams},), p)
     p.tolerance = tolerance
     p.poisson_iterations = poisson_iterations

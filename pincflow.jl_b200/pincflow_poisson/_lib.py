@@ -45,7 +45,7 @@ EXPORTS = [
 ]
 TUNE_KERNELS = ["total32", "total32_diff", "horiz32", "total64", "horiz64"]
 PROF_TAGS = ["apply32", "apply64", "pseudo32", "pseudo64", "thomas32", "thomas64", "update32", "update64",
-             "assemble", "reliable64", "mg", "learned", "predict", "correct"]
+             "assemble", "reliable64", "mg", "learned", "predict", "correct", "mg_bf16"]
 
 
 class PcfDims(ctypes.Structure):
@@ -65,7 +65,7 @@ class PcfParams(ctypes.Structure):
                 ("check_interval", ctypes.c_int), ("restart_interval", ctypes.c_int),
                 ("multigrid", ctypes.c_int), ("mg_dtau", ctypes.c_double),
                 ("mg_coarse_iterations", ctypes.c_int), ("mg_min_columns", ctypes.c_int),
-                ("autotune", ctypes.c_int)]
+                ("autotune", ctypes.c_int), ("mg_operator_bf16", ctypes.c_int)]
 
 
 class PcfTuneEntry(ctypes.Structure):
