@@ -139,8 +139,10 @@ typedef struct {
     int autotune;                  /* 1: time the stencil tile shapes of every new grid size on first use and keep
                                       the fastest (process-wide table, pcf_autotune_entries); 0: fixed heuristic (0) */
     int mg_operator_bf16;          /* multigrid: 1: the V-cycle's finest-level residual and smoothing stencils read a
-                                      BF16 copy of the operator (half their bytes; the Krylov operator and the FP64
-                                      true residual are unchanged); 0: the FP32 copy (1) */
+                                      BF16 copy of the operator (half their bytes; the Krylov operator, the coarse
+                                      levels and the FP64 true residual are unchanged); 0: the FP32 copy.  The learned
+                                      preconditioner stage (learned & 2) always runs the FP32 V-cycle it was trained
+                                      on (1) */
 } pcf_params;
 
 typedef struct {

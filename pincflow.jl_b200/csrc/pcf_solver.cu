@@ -781,7 +781,8 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
         m.version = -1;
     }
     m.coarse_iters = prm->mg_coarse_iterations;
-    m.bf16 = prm->mg_operator_bf16 != 0;
+    // the learned preconditioner stage is trained on, and validated with, the FP32 V-cycle
+    m.bf16 = prm->mg_operator_bf16 != 0 && (prm->learned & 2) == 0;
     if (m.bf16 && !h->coef16) {
         // first use: allocate and convert; later assemblies and pcf_set_operator write it themselves
         const size_t bytes = sizeof(__nv_bfloat16) * (size_t)h->d.n * PCF_NCOEF;

@@ -164,10 +164,12 @@ def preconditioner_pairs(indices, nx=128, ny=128, nz=64, tolerance=1e-8, device=
     """(r2 / RMS(r2), e / RMS(r2)) FP32 pairs for the learned preconditioner
     stage: for a training right-hand side b with plain FP64 solution s*, the
     multigrid V-cycle's output z = M(b) leaves the residual r2 = b - A z and
-    the error e = s* - z, which the stage N(r2) should approximate."""
+    the error e = s* - z, which the stage N(r2) should approximate.  The
+    V-cycle is the FP32 one that the stage runs with (learned & 2 uses the
+    FP32 operator copies)."""
     out = []
     solver = None
-    nl_mg = PoissonNamelist(precision="mixed", multigrid=True, **mg)
+    nl_mg = PoissonNamelist(precision="mixed", multigrid=True, **{"mg_operator_bf16": False, **mg})
     for i in indices:
         cfg = C.c3(int(i), nx=nx, ny=ny, nz=nz)
         if solver is None:

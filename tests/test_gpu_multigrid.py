@@ -79,7 +79,7 @@ def test_vcycle_matches_oracle(name, solvers, oracle, pcf):
     want = _oracle_mg(cfg, coef, **MG).cycle(b)
     assert rel_err(got, want) < 1e-4, rel_err(got, want)
     got16 = s.apply_multigrid(b, pcf.PoissonNamelist(precision="mixed", **MG))
-    assert 0 < rel_err(got16, want) < 2e-2, rel_err(got16, want)
+    assert 0 < rel_err(got16, want) < 1e-1, rel_err(got16, want)
 
 
 @pytest.mark.parametrize("dtau", [2.0, 2.5])
