@@ -172,7 +172,14 @@ static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_ov
         if (a.coef16) {
             ProfScope ps(h, tag_override >= 0 ? tag_override : PCF_PROF_MG_BF16,
                          ((double)planes * 2 + (double)(words - planes) * sizeof(T)) * (double)a.n);
-            k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF, true><<<grid, block, 0, h->stream>>>(a, kc);
+            // half the bytes per level: a quarter of the levels per block keeps
+            // enough loads in flight (measured 137 -> 124 us at 256x256x128,
+            // 721 -> 599 us at 512x512x192; an eighth is slower again)
+            int kc16 = std::max(1, (kc + 3) / 4);
+            if (gx * gy * ((a.nz + kc16 - 1) / kc16) > kMaxPartials) kc16 = kc;  // the grid shape checked above
+            const long long gz16 = (a.nz + kc16 - 1) / kc16;
+            k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF, true>
+                <<<dim3((unsigned)gx, (unsigned)gy, (unsigned)gz16), block, 0, h->stream>>>(a, kc16);
             PCF_CUDA_TRY(cudaGetLastError());
             return PCF_OK;
         }
