@@ -153,7 +153,8 @@ typedef struct {
     double residual;       /* final relative residual as tested (recursive or true) */
     double true_residual;  /* FP64 RMS(b - A x) / RMS(b) */
     double b_norm;         /* RMS of the initial residual */
-    double ms_upload;      /* host -> device copies */
+    double ms_upload;      /* host -> device copies of rho, betar, p (the right-hand side's runs on a second
+                              stream, concurrent with the assembly) */
     double ms_assemble;    /* operator assembly + preconditioner factors */
     double ms_solve;       /* Krylov iterations */
     double ms_download;    /* device -> host copies */

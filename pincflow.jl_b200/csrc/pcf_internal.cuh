@@ -122,6 +122,7 @@ struct pcf_handle {
     double dx, dy, dz;
     int grid_set, background_set, operator_set;
     cudaStream_t stream;
+    cudaStream_t copy_stream;  // pcf_solve: the right-hand side's upload, concurrent with the assembly
     cudaEvent_t ev[8];
 
     // haloed FP64 fields

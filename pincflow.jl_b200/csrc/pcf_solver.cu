@@ -1359,6 +1359,7 @@ int pcf_destroy(pcf_handle *h) {
     for (auto &e : h->ev)
         if (e) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     delete h;
     return PCF_OK;
 }
@@ -1402,6 +1403,7 @@ int pcf_create(pcf_handle **out, const pcf_dims *dims) {
         return code;
     };
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PCF_ECUDA);
+    if (cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PCF_ECUDA);
     for (auto &e : h->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return fail(PCF_ECUDA);
     const size_t nh8 = sizeof(double) * (size_t)h->nh;
@@ -2243,14 +2245,17 @@ static float elapsed(cudaEvent_t a, cudaEvent_t b) {
     return ms;
 }
 
+// rhs_ready: an event the solve waits for after the assembly (the right-hand
+// side's upload on the copy stream), or null.
 static int solve_common(pcf_handle *h, double dt, double rf, double tolref, const pcf_params *prm, pcf_result *res,
-                        const double **x) {
+                        const double **x, cudaEvent_t rhs_ready = nullptr) {
     // solve_poisson!.jl:52-54
     if (dt == 0.0) return PCF_EINVAL;
     int rc;
     PCF_CUDA_TRY(cudaEventRecord(h->ev[1], h->stream));
     if ((rc = assemble_device(h, dt, rf, prm->damp_horizontal_wind_on_rhs))) return rc;
     if (prm->preconditioner && (rc = ensure_factors(h, deta_of(h, prm->dtau)))) return rc;
+    if (rhs_ready) PCF_CUDA_TRY(cudaStreamWaitEvent(h->stream, rhs_ready, 0));
     PCF_CUDA_TRY(cudaEventRecord(h->ev[2], h->stream));
     if ((rc = krylov_solve(h, tolref, prm, x, res))) return rc;
     PCF_CUDA_TRY(cudaEventRecord(h->ev[3], h->stream));
@@ -2267,13 +2272,21 @@ int pcf_solve(pcf_handle *h, const double *rhs, const double *rho, const double 
     PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
     const size_t hb = sizeof(double) * (size_t)h->nh;
     PCF_CUDA_TRY(cudaEventRecord(h->ev[0], h->stream));
+    // the right-hand side is first read by the Krylov loop: it travels on the
+    // copy stream (after all earlier work on the handle's stream) while
+    // rho, betar and p go up and the operator is assembled
+    PCF_CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->ev[0], 0));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->b64, rhs, sizeof(double) * h->d.n, cudaMemcpyHostToDevice, h->copy_stream));
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[7], h->copy_stream));
     PCF_CUDA_TRY(cudaMemcpyAsync(h->rho, rho, hb, cudaMemcpyHostToDevice, h->stream));
     PCF_CUDA_TRY(cudaMemcpyAsync(h->betar, betar, hb, cudaMemcpyHostToDevice, h->stream));
     if (p) PCF_CUDA_TRY(cudaMemcpyAsync(h->p, p, hb, cudaMemcpyHostToDevice, h->stream));
-    PCF_CUDA_TRY(cudaMemcpyAsync(h->b64, rhs, sizeof(double) * h->d.n, cudaMemcpyHostToDevice, h->stream));
     const double *x = nullptr;
-    int rc = solve_common(h, dt, rayleigh_factor, tolref, prm, res, &x);
-    if (rc) return rc;
+    int rc = solve_common(h, dt, rayleigh_factor, tolref, prm, res, &x, h->ev[7]);
+    if (rc) {
+        cudaStreamWaitEvent(h->stream, h->ev[7], 0);  // no later call may meet the copy in flight
+        return rc;
+    }
     if (!res->errflag) {
         k_unscale<<<vec_grid(h->d.n), 256, 0, h->stream>>>(x, h->pbar, h->rhobar, 1.0 / dt, h->d.nx, h->d.ny,
                                                            h->d.nz, h->dims.nbx, h->dims.nby, h->dims.nbz, h->nxx,
