@@ -578,15 +578,15 @@ static ThomasArgs<float> mg_targs(const MgLevel &L, const float *fac, const floa
 static int mg_restrict(pcf_handle *h, int l, const float *r, const KrylovScalars *guard) {
     const MgLevel &F = h->mg->lv[l], &Cl = h->mg->lv[l + 1];
     ProfScope ps(h, PCF_PROF_MG, (2.0 + 2.0 / (Cl.cx * Cl.cy)) * 4 * (double)F.d.n);
-    if (F.d.nx % 4 == 0 && ((reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(F.fc)) & 15) == 0) {
+    // 128-bit path: x aggregated in pairs (cx = 1 only arises for odd nx)
+    if (Cl.cx == 2 && F.d.nx % 4 == 0 &&
+        ((reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(F.fc)) & 15) == 0) {
         const int n4 = F.d.nx / 4;
         const dim3 blk(32, 8, 1), g((unsigned)((n4 + 31) / 32), (unsigned)((Cl.d.ny + 7) / 8), (unsigned)Cl.d.nz);
-        if (Cl.cx == 2 && Cl.cy == 2)
+        if (Cl.cy == 2)
             k_mg_restrict4<2, 2><<<g, blk, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
-        else if (Cl.cx == 2)
-            k_mg_restrict4<2, 1><<<g, blk, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
         else
-            k_mg_restrict4<1, 2><<<g, blk, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
+            k_mg_restrict4<2, 1><<<g, blk, 0, h->stream>>>(r, F.fc, F.d.nx, F.d.ny, F.d.nz, Cl.fc, Cl.b, guard);
         PCF_CUDA_TRY(cudaGetLastError());
         return PCF_OK;
     }
@@ -605,15 +605,15 @@ static int mg_restrict(pcf_handle *h, int l, const float *r, const KrylovScalars
 static int mg_prolong(pcf_handle *h, int l, const float *e, float *s, const KrylovScalars *guard) {
     const MgLevel &F = h->mg->lv[l], &Cl = h->mg->lv[l + 1];
     ProfScope ps(h, PCF_PROF_MG, (3.0 + 2.0 / (Cl.cx * Cl.cy)) * 4 * (double)F.d.n);
-    if (F.d.nx % 4 == 0 && ((reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(F.fc)) & 15) == 0) {
+    // 128-bit path: x aggregated in pairs (cx = 1 only arises for odd nx)
+    if (Cl.cx == 2 && F.d.nx % 4 == 0 &&
+        ((reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(F.fc)) & 15) == 0) {
         const int n4 = F.d.nx / 4;
         const dim3 blk(32, 8, 1), g((unsigned)((n4 + 31) / 32), (unsigned)((F.d.ny + 7) / 8), (unsigned)F.d.nz);
-        if (Cl.cx == 2 && Cl.cy == 2)
+        if (Cl.cy == 2)
             k_mg_prolong4<2, 2><<<g, blk, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
-        else if (Cl.cx == 2)
-            k_mg_prolong4<2, 1><<<g, blk, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
         else
-            k_mg_prolong4<1, 2><<<g, blk, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
+            k_mg_prolong4<2, 1><<<g, blk, 0, h->stream>>>(e, Cl.fc, F.fc, F.d.nx, F.d.ny, F.d.nz, s, guard);
         PCF_CUDA_TRY(cudaGetLastError());
         return PCF_OK;
     }

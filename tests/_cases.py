@@ -39,6 +39,8 @@ def case(name: str):
         cfg["dt"] = 0.5
     elif name == "wide":        # wide tile path (nx >= 128)
         cfg = C.c3(9, nx=160, ny=12, nz=20)
+    elif name == "oddx":        # odd nx, even ny: multigrid aggregates 1 x 2 columns
+        cfg = C.c3(5, nx=25, ny=32, nz=12)
     else:
         raise KeyError(name)
     cfg.setdefault("damp", False)
