@@ -15,9 +15,19 @@
 
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include "../../include/pincflow_poisson.h"
+
+// A named NVTX range for the lifetime of a scope: the phases of the public
+// entry points show up in Nsight timelines (a no-op without an attached tool).
+struct NvtxScope {
+    explicit NvtxScope(const char *name) { nvtxRangePushA(name); }
+    ~NvtxScope() { nvtxRangePop(); }
+    NvtxScope(const NvtxScope &) = delete;
+    NvtxScope &operator=(const NvtxScope &) = delete;
+};
 
 #define PCF_CUDA_TRY(expr)                                    \
     do {                                                      \

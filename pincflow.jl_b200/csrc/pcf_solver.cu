@@ -1850,6 +1850,7 @@ int pcf_apply_corrector_device(pcf_handle *h, double *d_u, double *d_v, double *
     if (!h || !d_u || !d_v || !d_w || !d_rho || !d_rhop || !d_betar || !d_pip || !prm || !d_dpip || !res)
         return PCF_EINVAL;
     PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    NvtxScope r("pcf_apply_corrector_device");
     // apply_corrector!.jl:44-61: compute_lhs!, solve_poisson!, dpip halos, correct!
     double tolref = 0;
     int rc = compute_lhs_device(h, d_u, d_v, d_w, d_heating, h->s64, &tolref);
@@ -1939,6 +1940,7 @@ int pcf_implicit_step_device(pcf_handle *h, double dt, double rayleigh_factor, c
     double *wold = wold_scratch(h, d_wold, &rc);
     if (rc) return rc;
     const int damp = prm->damp_horizontal_wind_on_rhs;
+    NvtxScope r("pcf_implicit_step_device");
     cudaEvent_t ev[2] = {nullptr, nullptr};
     PCF_CUDA_TRY(cudaEventCreate(&ev[0]));
     if (cudaEventCreate(&ev[1]) != cudaSuccess) {
@@ -2253,11 +2255,17 @@ static int solve_common(pcf_handle *h, double dt, double rf, double tolref, cons
     if (dt == 0.0) return PCF_EINVAL;
     int rc;
     PCF_CUDA_TRY(cudaEventRecord(h->ev[1], h->stream));
-    if ((rc = assemble_device(h, dt, rf, prm->damp_horizontal_wind_on_rhs))) return rc;
-    if (prm->preconditioner && (rc = ensure_factors(h, deta_of(h, prm->dtau)))) return rc;
+    {
+        NvtxScope r("pcf assemble");
+        if ((rc = assemble_device(h, dt, rf, prm->damp_horizontal_wind_on_rhs))) return rc;
+        if (prm->preconditioner && (rc = ensure_factors(h, deta_of(h, prm->dtau)))) return rc;
+    }
     if (rhs_ready) PCF_CUDA_TRY(cudaStreamWaitEvent(h->stream, rhs_ready, 0));
     PCF_CUDA_TRY(cudaEventRecord(h->ev[2], h->stream));
-    if ((rc = krylov_solve(h, tolref, prm, x, res))) return rc;
+    {
+        NvtxScope r("pcf krylov");
+        if ((rc = krylov_solve(h, tolref, prm, x, res))) return rc;
+    }
     PCF_CUDA_TRY(cudaEventRecord(h->ev[3], h->stream));
     return PCF_OK;
 }
@@ -2266,6 +2274,7 @@ int pcf_solve(pcf_handle *h, const double *rhs, const double *rho, const double 
               double rayleigh_factor, double tolref, const pcf_params *prm, double *dpip, pcf_result *res) {
     if (!h || !rhs || !rho || !betar || !prm || !dpip || !res) return PCF_EINVAL;
     if (h->dims.model == PCF_MODEL_COMPRESSIBLE && !p) return PCF_EINVAL;
+    NvtxScope r("pcf_solve");
     std::memset(res, 0, sizeof(*res));
     if (dt == 0.0) return PCF_EINVAL;
     if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
@@ -2317,6 +2326,7 @@ int pcf_solve_device(pcf_handle *h, const double *d_rhs, const double *d_rho, co
                      double *d_dpip, pcf_result *res) {
     if (!h || !d_rhs || !d_rho || !d_betar || !prm || !d_dpip || !res) return PCF_EINVAL;
     if (h->dims.model == PCF_MODEL_COMPRESSIBLE && !d_p) return PCF_EINVAL;
+    NvtxScope r("pcf_solve_device");
     std::memset(res, 0, sizeof(*res));
     if (dt == 0.0) return PCF_EINVAL;
     if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
