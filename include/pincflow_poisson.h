@@ -138,11 +138,11 @@ typedef struct {
     int mg_min_columns;            /* multigrid: a level with at most this many columns is the coarsest (16) */
     int autotune;                  /* 1: time the stencil tile shapes of every new grid size on first use and keep
                                       the fastest (process-wide table, pcf_autotune_entries); 0: fixed heuristic (0) */
-    int mg_operator_bf16;          /* multigrid: 1: the V-cycle's finest-level residual and smoothing stencils read a
-                                      BF16 copy of the operator (half their bytes; the Krylov operator, the coarse
-                                      levels and the FP64 true residual are unchanged); 0: the FP32 copy.  The learned
-                                      preconditioner stage (learned & 2) always runs the FP32 V-cycle it was trained
-                                      on (1) */
+    int mg_operator_bf16;          /* multigrid: 1: the V-cycle's residual and smoothing stencils on the finest and
+                                      the first coarse level read BF16 copies of their operators (half their bytes;
+                                      the Krylov operator, the coarser levels and the FP64 true residual are
+                                      unchanged); 0: the FP32 copies.  The learned preconditioner stage (learned & 2)
+                                      always runs the FP32 V-cycle it was trained on (1) */
 } pcf_params;
 
 typedef struct {

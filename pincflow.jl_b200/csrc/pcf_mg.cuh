@@ -88,13 +88,16 @@ __global__ void __launch_bounds__(256) k_mg_fc(const TF *__restrict__ fc, int nx
 template <typename TI, int CX, int CY, int DZ>
 __device__ __forceinline__ void coarsen_group(const TI *__restrict__ coef, const TI *__restrict__ fc, int nx, int ny,
                                               int nz, const float *__restrict__ fcc, float *__restrict__ out,
-                                              long long q, int I, int J, int k) {
+                                              __nv_bfloat16 *__restrict__ out16, long long q, int I, int J, int k) {
     const int NX = nx / CX, NY = ny / CY;
     const long long n = (long long)nx * ny * nz, nc = (long long)NX * NY * nz;
     if (k + DZ < 0 || k + DZ >= nz) {  // couplings to a zero z-ghost
 #pragma unroll
         for (int p = 0; p < PCF_NCOEF; ++p)
-            if (off_z(p) == DZ) out[(long long)p * nc + q] = 0.0f;
+            if (off_z(p) == DZ) {
+                out[(long long)p * nc + q] = 0.0f;
+                if (out16) out16[(long long)p * nc + q] = __float2bfloat16_rn(0.0f);
+            }
         return;
     }
     double acc[PCF_NCOEF];
@@ -132,14 +135,16 @@ __device__ __forceinline__ void coarsen_group(const TI *__restrict__ coef, const
     for (int p = 0; p < PCF_NCOEF; ++p) {
         if (off_z(p) != DZ) continue;
         const long long t = wrap1(I + off_x(p), NX) + (long long)NX * (wrap1(J + off_y(p), NY) + (long long)NY * (k + DZ));
-        out[(long long)p * nc + q] = (float)(acc[p] / ((double)(CX * CY) * fcI * (double)fcc[t]));
+        const float v = (float)(acc[p] / ((double)(CX * CY) * fcI * (double)fcc[t]));
+        out[(long long)p * nc + q] = v;
+        if (out16) out16[(long long)p * nc + q] = __float2bfloat16_rn(v);
     }
 }
 
 template <typename TI, int CX, int CY>
 __global__ void __launch_bounds__(128) k_mg_coarsen(const TI *__restrict__ coef, const TI *__restrict__ fc, int nx,
                                                     int ny, int nz, const float *__restrict__ fcc,
-                                                    float *__restrict__ out) {
+                                                    float *__restrict__ out, __nv_bfloat16 *__restrict__ out16) {
     const int NX = nx / CX, NY = ny / CY;
     const long long nc = (long long)NX * NY * nz;
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -147,11 +152,11 @@ __global__ void __launch_bounds__(128) k_mg_coarsen(const TI *__restrict__ coef,
     const unsigned qu = (unsigned)q, ux = (unsigned)NX, uy = (unsigned)NY;  // n < 2^31
     const int I = (int)(qu % ux), J = (int)((qu / ux) % uy), k = (int)(qu / (ux * uy));
     switch (blockIdx.y) {
-        case 0: coarsen_group<TI, CX, CY, -2>(coef, fc, nx, ny, nz, fcc, out, q, I, J, k); break;
-        case 1: coarsen_group<TI, CX, CY, -1>(coef, fc, nx, ny, nz, fcc, out, q, I, J, k); break;
-        case 2: coarsen_group<TI, CX, CY, 0>(coef, fc, nx, ny, nz, fcc, out, q, I, J, k); break;
-        case 3: coarsen_group<TI, CX, CY, 1>(coef, fc, nx, ny, nz, fcc, out, q, I, J, k); break;
-        default: coarsen_group<TI, CX, CY, 2>(coef, fc, nx, ny, nz, fcc, out, q, I, J, k); break;
+        case 0: coarsen_group<TI, CX, CY, -2>(coef, fc, nx, ny, nz, fcc, out, out16, q, I, J, k); break;
+        case 1: coarsen_group<TI, CX, CY, -1>(coef, fc, nx, ny, nz, fcc, out, out16, q, I, J, k); break;
+        case 2: coarsen_group<TI, CX, CY, 0>(coef, fc, nx, ny, nz, fcc, out, out16, q, I, J, k); break;
+        case 3: coarsen_group<TI, CX, CY, 1>(coef, fc, nx, ny, nz, fcc, out, out16, q, I, J, k); break;
+        default: coarsen_group<TI, CX, CY, 2>(coef, fc, nx, ny, nz, fcc, out, out16, q, I, J, k); break;
     }
 }
 

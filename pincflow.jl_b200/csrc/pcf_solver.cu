@@ -515,6 +515,7 @@ struct MgLevel {
     int cx = 1, cy = 1;  // aggregation from the finer level (levels >= 1)
     double dx = 0, dy = 0, deta = 0;
     float *coef = nullptr, *fac = nullptr, *fc = nullptr, *b = nullptr, *s = nullptr, *t = nullptr;
+    __nv_bfloat16 *coef16 = nullptr;  // level 1: BF16 copy of coef (multigrid BF16 mode)
 };
 struct MgState {
     std::vector<MgLevel> lv;  // lv[0] is the handle's grid (its planes are the handle's)
@@ -651,6 +652,7 @@ static int mg_pseudo_step(pcf_handle *h, const MgLevel &L, const float *coef, co
 static int mg_cycle(pcf_handle *h, int l, const KrylovScalars *guard, float **result) {
     MgState &m = *h->mg;
     const MgLevel &L = m.lv[l];
+    const __nv_bfloat16 *c16 = m.bf16 ? L.coef16 : nullptr;  // level 1 only
     int rc = mg_thomas<TH_B>(h, L, mg_targs(L, L.fac, L.b, L.s, guard), PCF_PROF_MG);
     if (rc) return rc;
     if (l + 1 == (int)m.lv.size()) {
@@ -664,6 +666,7 @@ static int mg_cycle(pcf_handle *h, int l, const KrylovScalars *guard, float **re
     }
     StencilArgs<float> sa;
     sa.coef = L.coef;
+    sa.coef16 = c16;
     sa.s = L.s;
     sa.out = L.t;
     sa.w1 = L.b;
@@ -674,7 +677,7 @@ static int mg_cycle(pcf_handle *h, int l, const KrylovScalars *guard, float **re
     float *e = nullptr;
     if ((rc = mg_cycle(h, l + 1, guard, &e))) return rc;
     if ((rc = mg_prolong(h, l, e, L.s, guard))) return rc;
-    if ((rc = mg_pseudo_step(h, L, L.coef, L.fac, L.s, L.t, L.b, guard, nullptr, PCF_PROF_MG))) return rc;
+    if ((rc = mg_pseudo_step(h, L, L.coef, L.fac, L.s, L.t, L.b, guard, nullptr, PCF_PROF_MG, c16))) return rc;
     *result = L.t;
     return PCF_OK;
 }
@@ -783,6 +786,11 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
                 (rc = alloc(&C.fc, C.d.n)) || (rc = alloc(&C.b, C.d.n)) || (rc = alloc(&C.s, C.d.n)) ||
                 (rc = alloc(&C.t, C.d.n)))
                 return rc;
+            if (l == 1) {  // the first coarse level's BF16 copy, written by its coarsening
+                float *c16 = nullptr;
+                if ((rc = alloc(&c16, (C.d.n * PCF_NCOEF + 1) / 2))) return rc;
+                C.coef16 = reinterpret_cast<__nv_bfloat16 *>(c16);
+            }
         }
         m.min_columns = prm->mg_min_columns;
         m.version = -1;
@@ -826,10 +834,10 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
         k_mg_fc<float, CX, CY><<<gf, 256, 0, h->stream>>>(F.fc, F.d.nx, F.d.ny, F.d.nz, C.fc);                        \
         if (l == 1)                                                                                                   \
             k_mg_coarsen<double, CX, CY><<<gc, 128, 0, h->stream>>>(h->coef64, h->fc64, F.d.nx, F.d.ny, F.d.nz, C.fc, \
-                                                                    C.coef);                                          \
+                                                                    C.coef, C.coef16);                                \
         else                                                                                                          \
             k_mg_coarsen<float, CX, CY><<<gc, 128, 0, h->stream>>>(F.coef, F.fc, F.d.nx, F.d.ny, F.d.nz, C.fc,       \
-                                                                   C.coef);                                           \
+                                                                   C.coef, nullptr);                                  \
     } while (0)
         if (C.cx == 2 && C.cy == 2)
             PCF_MG_BUILD(2, 2);

@@ -53,7 +53,7 @@ class PoissonNamelist:
     mg_coarse_iterations: int = 4     # multigrid: smoothing steps on the coarsest level
     mg_min_columns: int = 16          # multigrid: a level with at most this many columns is the coarsest
     autotune: bool = False            # time the stencil tile shapes of each new grid size on first use
-    mg_operator_bf16: bool = True     # multigrid: finest-level V-cycle stencils read a BF16 copy (not with learned & 2)
+    mg_operator_bf16: bool = True     # multigrid: finest and first coarse level stencils read BF16 copies (not learned & 2)
 
     def to_c(self) -> _lib.PcfParams:
         p = _lib.PcfParams()
