@@ -290,17 +290,30 @@ static int tune_stencil(pcf_handle *h, const Dims &d, const T *coef, const T *sv
     }
     const int saved_prof = h->prof_on;
     h->prof_on = 0;
-    auto time_cfg = [&](int tile, int kc, double *ms) -> int {
-        int rc = launch_tile<T, HORIZ, EPI, DIFF>(h, a, tile, kc, -1);
-        if (rc) return rc;
+    // mean time of reps back-to-back launches
+    auto trial = [&](int tile, int kc, int reps, double *ms) -> int {
+        int rc;
         PCF_CUDA_TRY(cudaEventRecord(e0, h->stream));
-        for (int q = 0; q < 3; ++q)
+        for (int q = 0; q < reps; ++q)
             if ((rc = launch_tile<T, HORIZ, EPI, DIFF>(h, a, tile, kc, -1))) return rc;
         PCF_CUDA_TRY(cudaEventRecord(e1, h->stream));
         PCF_CUDA_TRY(cudaEventSynchronize(e1));
         float f = 0;
         PCF_CUDA_TRY(cudaEventElapsedTime(&f, e0, e1));
-        *ms = f / 3.0;
+        *ms = f / reps;
+        return PCF_OK;
+    };
+    // a warm-up launch, an estimate, then the better of two trials of at
+    // least ~0.3 ms each: small grids' 10-us launches timed 3 at a time were
+    // noisy enough to pick different tiles from run to run
+    auto time_cfg = [&](int tile, int kc, double *ms) -> int {
+        int rc = launch_tile<T, HORIZ, EPI, DIFF>(h, a, tile, kc, -1);
+        if (rc) return rc;
+        double est = 0, t1 = 0, t2 = 0;
+        if ((rc = trial(tile, kc, 3, &est))) return rc;
+        const int reps = std::max(3, std::min(64, (int)std::ceil(0.3 / std::max(est, 1e-3))));
+        if ((rc = trial(tile, kc, reps, &t1)) || (rc = trial(tile, kc, reps, &t2))) return rc;
+        *ms = std::min(t1, t2);
         return PCF_OK;
     };
     PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
