@@ -46,6 +46,14 @@ def apply(coef, s, planes=range(25)):
     return out
 
 
+def bf16(a):
+    """BF16 rounding (to nearest, ties to even) of the FP32 rounding of a, as
+    the GPU's BF16 operator copies store it; returned as float64."""
+    u = np.asarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
 def factors(coef, deta):
     """Thomas pivots P, M, Q (k_factors)."""
     ac, ad, au = coef[AC], coef[AD], coef[AU]
@@ -128,7 +136,10 @@ def coarsen(coef, fc, cx, cy):
 class Multigrid:
     """The hierarchy and V-cycle of the GPU preconditioner (mg_prepare, mg_precond, mg_cycle)."""
 
-    def __init__(self, coef, fcscal, dx, dy, dtau=1.0, coarse_iterations=4, min_columns=16):
+    def __init__(self, coef, fcscal, dx, dy, dtau=1.0, coarse_iterations=4, min_columns=16, bf16_planes=False):
+        """bf16_planes: the residual and pseudo-step stencils of level 0, and
+        of level 1 unless it is the coarsest, read BF16-rounded planes (the
+        GPU's mg_operator_bf16); the Thomas pivots keep the unrounded operator."""
         nz, ny, nx = fcscal.shape
         self.dims = level_dims(nx, ny, nz, min_columns)
         self.ci = coarse_iterations
@@ -141,12 +152,15 @@ class Multigrid:
                 ddx, ddy = ddx * cx, ddy * cy
             deta = dtau / (2 * (1 / ddx ** 2 + 1 / ddy ** 2))
             self.levels.append(dict(coef=c, fc=f, deta=deta, fac=factors(c, deta), cx=cx, cy=cy))
+        for l, L in enumerate(self.levels):
+            rounded = bf16_planes and (l == 0 or (l == 1 and l < len(self.levels) - 1))
+            L["scoef"] = bf16(L["coef"]) if rounded else L["coef"]
 
     def smooth(self, l, b, steps):
         L = self.levels[l]
-        s = pseudo_step(L["coef"], L["fac"], L["deta"], b, None)
+        s = pseudo_step(L["scoef"], L["fac"], L["deta"], b, None)
         for _ in range(steps - 1):
-            s = pseudo_step(L["coef"], L["fac"], L["deta"], b, s)
+            s = pseudo_step(L["scoef"], L["fac"], L["deta"], b, s)
         return s
 
     def cycle(self, b, l=0):
@@ -154,14 +168,14 @@ class Multigrid:
         if l == len(self.levels) - 1:
             return self.smooth(l, b, self.ci)
         s = self.smooth(l, b, 1)
-        r = b - apply(L["coef"], s)
+        r = b - apply(L["scoef"], s)
         C = self.levels[l + 1]
         cx, cy = C["cx"], C["cy"]
         nz, ny, nx = b.shape
         bc = (L["fc"] * r).reshape(nz, ny // cy, cy, nx // cx, cx).sum(axis=(2, 4)) / (cx * cy * C["fc"])
         e = self.cycle(bc, l + 1)
         s = s + np.repeat(np.repeat(C["fc"] * e, cy, axis=1), cx, axis=2) / L["fc"]
-        return pseudo_step(L["coef"], L["fac"], L["deta"], b, s)
+        return pseudo_step(L["scoef"], L["fac"], L["deta"], b, s)
 
 
 def bicgstab(coef, M, b, tol=1e-10, maxit=1000):

@@ -121,6 +121,33 @@ struct ProfState;   // defined in pcf_solver.cu
 struct GraphCache;  // captured iteration batches, defined in pcf_solver.cu
 struct MgState;     // multigrid hierarchy, defined in pcf_solver.cu
 
+// ------------------------------------------------ shared memory, mbarriers --
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Waits for the mbarrier phase of the given parity to complete; gives up
+// after 2 s of %globaltimer and returns false (the caller records the error).
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
+    uint64_t t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(phase)
+            : "memory");
+        if (done) return true;
+        uint64_t t1;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+        if (t1 - t0 > 2000000000ull) return false;  // 2 s
+    }
+}
+
 }  // namespace pcf
 
 // The opaque handle of the C ABI.

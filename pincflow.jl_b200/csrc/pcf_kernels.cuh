@@ -52,15 +52,18 @@ __device__ __forceinline__ void load_vec(const T *__restrict__ p, T (&v)[V]) {
     for (int q = 0; q < V; ++q) v[q] = e[q];
 }
 
+// four BF16 values packed in 8 bytes, widened to FP32
+__device__ __forceinline__ void unpack_bf16x4(uint2 x, float (&v)[4]) {
+    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&x.x));
+    const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&x.y));
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+
 // V consecutive BF16 values (2V bytes, 2V-byte aligned) widened to FP32
 template <int V>
 __device__ __forceinline__ void load_bf16(const __nv_bfloat16 *__restrict__ p, float (&v)[V]) {
     if constexpr (V == 4) {
-        const uint2 x = __ldg(reinterpret_cast<const uint2 *>(p));
-        const __nv_bfloat162 lo = *reinterpret_cast<const __nv_bfloat162 *>(&x.x);
-        const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162 *>(&x.y);
-        const float2 a = __bfloat1622float2(lo), b = __bfloat1622float2(hi);
-        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+        unpack_bf16x4(__ldg(reinterpret_cast<const uint2 *>(p)), v);
     } else if constexpr (V == 2) {
         const unsigned x = __ldg(reinterpret_cast<const unsigned *>(p));
         const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&x));
@@ -79,6 +82,24 @@ __device__ __forceinline__ void store_vec(T *__restrict__ p, const T (&v)[V]) {
 #pragma unroll
     for (int q = 0; q < V; ++q) e[q] = v[q];
     *reinterpret_cast<VT *>(p) = x;
+}
+
+// TMA load of one box of a 4-D tensor map (in global memory) at coordinates
+// (c0, c1, c2, c3) into this CTA's shared memory (a CTA is its own cluster),
+// completing on the mbarrier's transaction count.  c0 * element size must be
+// a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const void *map, int c0, int c1, int c2, int c3,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(dst),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+
+// one arrival on the mbarrier that also expects BYTES of bulk-copy transactions
+__device__ __forceinline__ void mbar_arrive_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
 __device__ __forceinline__ int wrap(int x, int n) {
@@ -310,6 +331,7 @@ template <typename T>
 struct StencilArgs {
     const T *coef;        // 25 planes
     const __nv_bfloat16 *coef16 = nullptr;  // the same planes in BF16, read by the C16 kernels
+    const void *tmap16 = nullptr;           // device array of the three tensor maps of coef16 (make_coef16_maps)
     const T *s;           // input vector
     T *out;
     const T *w1;          // EPI_DOT1/2: second operand; EPI_PSEUDO/RESID: b
@@ -391,13 +413,43 @@ __device__ __forceinline__ void ring_store(T *slot, const T (&rv)[Ring<T, V, TX,
 // its smooth-mode error grows like eps32 / (k h)^2 and stalls the FP32
 // Krylov iteration on large grids.
 // C16: the coefficient planes are read from a.coef16 (BF16, half the bytes;
-// FP32 only, for the preconditioner's stencils).
-template <typename T, int V, int TX, int TY, bool HORIZ, int EPI, bool DIFF = false, bool C16 = false>
+// FP32 only, for the preconditioner's stencils): 1 with a load per plane and
+// level, like the FP32 planes; 2 staged through shared memory by TMA, where
+// one thread loads the block's 128 x 4 tile of every plane for level
+// k + kStencilStages - 1 (one box of a 4-D tensor map over x, y, z and plane,
+// two for the Horizontal operator's 22 planes) while level k is computed,
+// into kStencilStages stages that complete on one mbarrier each, so no thread
+// waits on DRAM for its coefficients.  C16 = 2 needs TX = 32, TY = 4, V = 4,
+// the tensor maps a.tmap16 (make_coef16_maps) and stencil_bulk_smem bytes of
+// dynamic shared memory.  A wait that gives up (2 s) marks the iteration
+// failed (guard status PCF_ECUDA).
+constexpr int kStencilStages = 2;  // 3 measured slower: 2 instead of 3 resident blocks per SM
+template <int TX, int TY, bool HORIZ>
+constexpr int stencil_stage_bytes() {
+    return (HORIZ ? PCF_NCOEF - 3 : PCF_NCOEF) * TY * TX * 4 * 2;
+}
+
+// stage slot of plane p: the Horizontal operator skips AC, AD and AU
+template <bool HORIZ>
+__host__ __device__ constexpr int slot_of_plane(int p) {
+    return HORIZ ? (p < PCF_AD ? p - 1 : p - 3) : p;
+}
+
+template <typename T, int V, int TX, int TY, bool HORIZ, int EPI, bool DIFF = false, int C16 = 0>
 __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
-    static_assert(!C16 || sizeof(T) == 4, "BF16 planes feed the FP32 stencil only");
+    static_assert(C16 == 0 || sizeof(T) == 4, "BF16 planes feed the FP32 stencil only");
+    static_assert(C16 != 2 || (V == 4 && TX == 32 && TY == 4), "the tensor maps' box is 128 x 4");
+    static_assert(PCF_AC == 0 && PCF_AL == 1 && PCF_AD == 5 && PCF_AU == 6 && PCF_ALD == 7, "plane order");
     using R = Ring<T, V, TX, TY>;
     __shared__ __align__(16) T sm[R::NS][R::NR * R::RW];
     if (a.guard_update ? no_update_pending(a.guard) : krylov_done(a.guard)) return;
+    // C16 == 2: kStencilStages coefficient stages, then one mbarrier per stage
+    constexpr int NST = kStencilStages;
+    constexpr int NPL = HORIZ ? PCF_NCOEF - 3 : PCF_NCOEF;
+    constexpr int STAGE = NPL * TY * R::W;  // BF16 values per stage
+    extern __shared__ __align__(128) unsigned char stencil_dyn[];
+    __nv_bfloat16 *stg = reinterpret_cast<__nv_bfloat16 *>(stencil_dyn);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(stencil_dyn + NST * STAGE * sizeof(__nv_bfloat16));
 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int x0 = blockIdx.x * R::W, y0 = blockIdx.y * TY;
@@ -411,6 +463,33 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
     double d0 = 0.0, d1 = 0.0;
     T rv[R::ROWS_PER_THREAD][V];
     T hv;
+    const int lt = tx + TX * ty;
+    // C16 == 2: thread 0 loads level kk's tile of every plane into stage st
+    const char *maps = static_cast<const char *>(a.tmap16);
+    auto issue = [&](int kk, int st) {
+        const uint32_t bar = smem_u32(bars + st), dst = smem_u32(stg + st * STAGE);
+        mbar_arrive_expect(bar, (uint32_t)(STAGE * sizeof(__nv_bfloat16)));  // whole boxes, zero-filled outside
+        if (HORIZ) {
+            tma_load_4d(dst, maps + 128, x0, y0, kk, PCF_AL, bar);
+            tma_load_4d(dst + 4 * TY * R::W * 2, maps + 256, x0, y0, kk, PCF_ALD, bar);
+        } else {
+            tma_load_4d(dst, maps, x0, y0, kk, 0, bar);
+        }
+    };
+    if constexpr (C16 == 2) {
+        if (lt == 0) {
+#pragma unroll
+            for (int q = 0; q < NST; ++q)
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bars + q)));
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            // the maps were written to global memory before the launch
+            for (int q = HORIZ ? 1 : 0; q < (HORIZ ? 3 : 1); ++q)
+                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(maps + 128 * q) : "memory");
+            for (int q = 0; q < NST - 1 && k0 + q < k1; ++q) issue(k0 + q, q);
+        }
+        __syncthreads();
+    }
+    bool failed = false;
     // prologue: planes k0-2 .. k0+2
 #pragma unroll
     for (int dz = -2; dz <= 2; ++dz) {
@@ -419,28 +498,67 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
         ring_store<T, V, TX, TY>(sm[(kk + 12) % R::NS], rv, hv);
     }
     __syncthreads();
+    // C16 == 2: the ring's next plane and the level's b are loaded one level
+    // earlier than in the other variants (registers rv / wn hold them across
+    // the barrier), so that their DRAM latency overlaps a whole level
+    constexpr bool AHEAD = C16 == 2;
+    T rv2[R::ROWS_PER_THREAD][V];
+    T hv2;
+    T wn[V];
+    if constexpr (AHEAD) {
+        ring_fetch<T, V, TX, TY>(a.s, a.nx, a.ny, a.nz, x0, y0, k0 + 3, rv, hv);
+        if (active && k0 < k1) load_vec<T, V>(a.w1 + plane * k0 + (long long)a.nx * y + x, wn);
+    }
 
     const int r = ty + 1;
     for (int k = k0; k < k1; ++k) {
-        // prefetch plane k+3 into registers while level k is computed
-        ring_fetch<T, V, TX, TY>(a.s, a.nx, a.ny, a.nz, x0, y0, k + 3, rv, hv);
+        const int j = k - k0;
+        if constexpr (C16 == 2) {
+            // stage (j + NST - 1) % NST held level k - 1, which every thread finished before the barrier below
+            if (lt == 0 && k + NST - 1 < k1) issue(k + NST - 1, (j + NST - 1) % NST);
+        }
+        // prefetch the ring's next plane into registers while level k is
+        // computed: k+3, stored at the end of this level (AHEAD: k+4, stored
+        // at the end of the next)
+        if constexpr (AHEAD)
+            ring_fetch<T, V, TX, TY>(a.s, a.nx, a.ny, a.nz, x0, y0, k + 4, rv2, hv2);
+        else
+            ring_fetch<T, V, TX, TY>(a.s, a.nx, a.ny, a.nz, x0, y0, k + 3, rv, hv);
         if (active) {
             const long long base = plane * k + (long long)a.nx * y + x;
             T c[PCF_NCOEF][V];
+            if constexpr (C16 == 2) {
+                failed = !mbar_wait(smem_u32(bars + j % NST), (uint32_t)((j / NST) & 1));
+                const __nv_bfloat16 *cs = stg + (j % NST) * STAGE + ty * R::W + tx * V;
 #pragma unroll
-            for (int p = 0; p < PCF_NCOEF; ++p) {
-                if (HORIZ && (p == PCF_AC || p == PCF_AD || p == PCF_AU)) continue;
-                if constexpr (C16)
-                    load_bf16<V>(a.coef16 + (long long)p * n + base, c[p]);
-                else
-                    load_vec<T, V>(a.coef + (long long)p * n + base, c[p]);
+                for (int p = 0; p < PCF_NCOEF; ++p) {
+                    if (HORIZ && (p == PCF_AC || p == PCF_AD || p == PCF_AU)) continue;
+                    const uint2 u = failed ? make_uint2(0u, 0u)
+                                           : *reinterpret_cast<const uint2 *>(cs + slot_of_plane<HORIZ>(p) * TY * R::W);
+                    unpack_bf16x4(u, c[p]);
+                }
+            } else {
+#pragma unroll
+                for (int p = 0; p < PCF_NCOEF; ++p) {
+                    if (HORIZ && (p == PCF_AC || p == PCF_AD || p == PCF_AU)) continue;
+                    if constexpr (C16 == 1)
+                        load_bf16<V>(a.coef16 + (long long)p * n + base, c[p]);
+                    else
+                        load_vec<T, V>(a.coef + (long long)p * n + base, c[p]);
+                }
             }
             // the pseudo-step / residual operand is loaded with the coefficients, not
             // after the sum, so that the level costs one HBM round trip, not two
             // (measured 4.18 -> 4.50 TB/s); the dot-product operand is loaded after
             // the sum, which keeps those variants at 140 registers (5.31 vs 5.06 TB/s)
             T wv[V];
-            if (EPI == EPI_PSEUDO || EPI == EPI_RESID || EPI == EPI_RESNR) load_vec<T, V>(a.w1 + base, wv);
+            if constexpr (AHEAD) {
+#pragma unroll
+                for (int e = 0; e < V; ++e) wv[e] = wn[e];
+                if (k + 1 < k1) load_vec<T, V>(a.w1 + base + plane, wn);
+            } else if (EPI == EPI_PSEUDO || EPI == EPI_RESID || EPI == EPI_RESNR) {
+                load_vec<T, V>(a.w1 + base, wv);
+            }
             const T *sm2 = sm[(k + 10) % R::NS], *sm1 = sm[(k + 11) % R::NS], *s0 = sm[(k + 12) % R::NS],
                     *sp1 = sm[(k + 13) % R::NS], *sp2 = sm[(k + 14) % R::NS];
             T res[V];
@@ -540,7 +658,31 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
             }
         }
         ring_store<T, V, TX, TY>(sm[(k + 15) % R::NS], rv, hv);
-        __syncthreads();
+        if constexpr (AHEAD) {
+#pragma unroll
+            for (int q = 0; q < R::ROWS_PER_THREAD; ++q)
+#pragma unroll
+                for (int e = 0; e < V; ++e) rv[q][e] = rv2[q][e];
+            hv = hv2;
+        }
+        if constexpr (C16 == 2) {
+            if (__syncthreads_or(failed)) {
+                // a stage never completed: record it, let the copies still in
+                // flight land (bounded), and leave
+                if (lt == 0) {
+                    KrylovScalars *g = const_cast<KrylovScalars *>(a.guard);
+                    if (g) {
+                        g->status = PCF_ECUDA;
+                        g->done = 1;
+                    }
+                    for (int q = j; q < j + NST && k0 + q < k1; ++q)
+                        mbar_wait(smem_u32(bars + q % NST), (uint32_t)((q / NST) & 1));
+                }
+                return;
+            }
+        } else {
+            __syncthreads();
+        }
     }
 
     if (EPI == EPI_DOT1 || EPI == EPI_RESID) {

@@ -9,11 +9,14 @@
 // host only polls the status word every `check_interval` iterations; kernels
 // launched after convergence see the done flag and return at once.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <vector>
+
+#include <cuda.h>
 
 #include "pcf_kernels.cuh"
 #include "pcf_mg.cuh"
@@ -148,6 +151,78 @@ static int pick_kc(long long xyblocks, int nz) {
     return (int)kc;
 }
 
+// dynamic shared memory of the staged BF16 stencil: the stages, one mbarrier each
+template <int TX, int TY, bool HORIZ>
+constexpr int stencil_bulk_smem() {
+    return kStencilStages * (stencil_stage_bytes<TX, TY, HORIZ>() + (int)sizeof(uint64_t));
+}
+
+// The three tensor maps of a BF16 operator copy (25 planes of nx x ny x nz
+// values) that the staged stencils load their tiles with, boxes of 128 x 4 x 1
+// values of [0] all 25 planes, [1] the 4 planes AL..AF, [2] the 18 planes
+// ALD..AFUU, written to the device array maps (3 x 128 bytes).  Returns false
+// (and the stencils read the planes directly) when the driver has no
+// tensor-map encoder or the grid breaks the copy's alignment rules (x rows
+// of a multiple of 16 bytes, at least one box wide).
+static bool make_coef16_maps(const __nv_bfloat16 *coef16, const Dims &d, void *maps) {
+    using Encode = decltype(&cuTensorMapEncodeTiled);
+    static Encode encode = [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            fn = nullptr;
+        }
+        return reinterpret_cast<Encode>(fn);
+    }();
+    if (!encode || !coef16 || d.nx % 8 != 0 || d.nx < 128 || (reinterpret_cast<uintptr_t>(coef16) & 15) != 0)
+        return false;
+    CUtensorMap host[3];
+    const cuuint64_t dims[4] = {(cuuint64_t)d.nx, (cuuint64_t)d.ny, (cuuint64_t)d.nz, (cuuint64_t)PCF_NCOEF};
+    const cuuint64_t strides[3] = {2ull * d.nx, 2ull * d.plane, 2ull * (cuuint64_t)d.n};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const cuuint32_t planes[3] = {PCF_NCOEF, PCF_AD - PCF_AL, PCF_NCOEF - PCF_ALD};
+    for (int q = 0; q < 3; ++q) {
+        const cuuint32_t box[4] = {128, 4, 1, planes[q]};
+        if (encode(&host[q], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(coef16), dims, strides,
+                   box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    return cudaMemcpy(maps, host, sizeof(host), cudaMemcpyHostToDevice) == cudaSuccess;
+}
+
+// Raises the staged stencil's dynamic shared-memory limit on the current
+// device (once per device) and returns how many of its blocks the device
+// holds at once (resident blocks per SM x SMs); 0 if the device refuses.
+template <typename T, int V, int TX, int TY, bool HORIZ, int EPI, bool DIFF>
+static int stencil_bulk_ready() {
+    static std::atomic<int> state[64];  // per device: 0 unknown, -1 refused, else the capacity
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return 0;
+    }
+    int st = state[dev].load();
+    if (st == 0) {
+        auto kern = k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF, 2>;
+        int per_sm = 0;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 stencil_bulk_smem<TX, TY, HORIZ>()) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TX * TY, stencil_bulk_smem<TX, TY, HORIZ>()) ==
+                cudaSuccess &&
+            per_sm > 0) {
+            st = per_sm * num_sms();
+        } else {
+            cudaGetLastError();
+            st = -1;
+        }
+        state[dev].store(st);
+    }
+    return st > 0 ? st : 0;
+}
+
 template <typename T, int V, int TX, bool HORIZ, int EPI, bool DIFF>
 static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_override, int kc) {
     constexpr int TY = 128 / TX;
@@ -178,7 +253,31 @@ static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_ov
             int kc16 = std::max(1, (kc + 3) / 4);
             if (gx * gy * ((a.nz + kc16 - 1) / kc16) > kMaxPartials) kc16 = kc;  // the grid shape checked above
             const long long gz16 = (a.nz + kc16 - 1) / kc16;
-            k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF, true>
+            if constexpr (V == 4 && TX == 32) {
+                // the coefficient tiles staged in shared memory by bulk copies
+                const int cap = a.tmap16 ? stencil_bulk_ready<T, V, TX, TY, HORIZ, EPI, DIFF>() : 0;
+                if (cap > 0) {
+                    // z-chunks of pick_kc's length, or half of it when that
+                    // fills the last wave of resident blocks better (measured
+                    // at 512x512x192: 1536 blocks in 444 slots, 3.46 waves,
+                    // 606 us; 3072 blocks, 6.92 waves, 563 us)
+                    auto fill = [&](int kcx) {
+                        const long long blocks = gx * gy * ((a.nz + kcx - 1) / kcx);
+                        return (double)blocks / (double)(((blocks + cap - 1) / cap) * cap);
+                    };
+                    int kcb = kc;
+                    const int half = std::max(1, (kc + 1) / 2);
+                    if (gx * gy * ((a.nz + half - 1) / half) <= kMaxPartials && fill(half) > fill(kc) + 0.02)
+                        kcb = half;
+                    const long long gzb = (a.nz + kcb - 1) / kcb;
+                    k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF, 2>
+                        <<<dim3((unsigned)gx, (unsigned)gy, (unsigned)gzb), block, stencil_bulk_smem<TX, TY, HORIZ>(),
+                           h->stream>>>(a, kcb);
+                    PCF_CUDA_TRY(cudaGetLastError());
+                    return PCF_OK;
+                }
+            }
+            k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF, 1>
                 <<<dim3((unsigned)gx, (unsigned)gy, (unsigned)gz16), block, 0, h->stream>>>(a, kc16);
             PCF_CUDA_TRY(cudaGetLastError());
             return PCF_OK;
@@ -529,6 +628,7 @@ struct MgLevel {
     double dx = 0, dy = 0, deta = 0;
     float *coef = nullptr, *fac = nullptr, *fc = nullptr, *b = nullptr, *s = nullptr, *t = nullptr;
     __nv_bfloat16 *coef16 = nullptr;  // level 1: BF16 copy of coef (multigrid BF16 mode)
+    void *tmap16 = nullptr;           // levels 0 and 1: tensor maps of the BF16 copy (make_coef16_maps), or null
 };
 struct MgState {
     std::vector<MgLevel> lv;  // lv[0] is the handle's grid (its planes are the handle's)
@@ -649,6 +749,7 @@ static int mg_pseudo_step(pcf_handle *h, const MgLevel &L, const float *coef, co
     StencilArgs<float> sa;
     sa.coef = coef;
     sa.coef16 = coef16;
+    sa.tmap16 = coef16 ? L.tmap16 : nullptr;
     sa.s = s;
     sa.out = out;
     sa.w1 = b;
@@ -680,6 +781,7 @@ static int mg_cycle(pcf_handle *h, int l, const KrylovScalars *guard, float **re
     StencilArgs<float> sa;
     sa.coef = L.coef;
     sa.coef16 = c16;
+    sa.tmap16 = c16 ? L.tmap16 : nullptr;
     sa.s = L.s;
     sa.out = L.t;
     sa.w1 = L.b;
@@ -728,6 +830,7 @@ static int mg_precond(pcf_handle *h, const Work<float> &w, float *bvec, const Kr
     StencilArgs<float> sa;
     sa.coef = w.coef;
     sa.coef16 = c16;
+    sa.tmap16 = c16 ? L.tmap16 : nullptr;
     sa.s = o1;
     sa.out = o2;
     sa.w1 = bvec;
@@ -800,9 +903,10 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
                 (rc = alloc(&C.t, C.d.n)))
                 return rc;
             if (l == 1) {  // the first coarse level's BF16 copy, written by its coarsening
-                float *c16 = nullptr;
-                if ((rc = alloc(&c16, (C.d.n * PCF_NCOEF + 1) / 2))) return rc;
+                float *c16 = nullptr, *maps = nullptr;
+                if ((rc = alloc(&c16, (C.d.n * PCF_NCOEF + 1) / 2)) || (rc = alloc(&maps, 3 * 128 / 4))) return rc;
                 C.coef16 = reinterpret_cast<__nv_bfloat16 *>(c16);
+                if (make_coef16_maps(C.coef16, C.d, maps)) C.tmap16 = maps;
             }
         }
         m.min_columns = prm->mg_min_columns;
@@ -824,6 +928,13 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
         k_float_to_bf16<<<vec_grid(h->d.n * PCF_NCOEF), 256, 0, h->stream>>>(h->coef32, h->coef16,
                                                                               h->d.n * PCF_NCOEF);
         PCF_CUDA_TRY(cudaGetLastError());
+    }
+    if (m.bf16 && !m.lv[0].tmap16) {  // the finest level's maps (once per hierarchy)
+        void *maps = nullptr;
+        const cudaError_t e = cudaMalloc(&maps, 3 * 128);
+        if (e != cudaSuccess) return pcf_set_cuda_error(e);
+        m.allocs.push_back(maps);
+        if (make_coef16_maps(h->coef16, h->d, maps)) m.lv[0].tmap16 = maps;
     }
     for (MgLevel &L : m.lv) L.deta = prm->mg_dtau / (2 * (1 / (L.dx * L.dx) + 1 / (L.dy * L.dy)));
     // the finest level's pivots are the handle's (shared with the reference preconditioner)
@@ -1402,6 +1513,10 @@ int pcf_create(pcf_handle **out, const pcf_dims *dims) {
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, dims->device) != cudaSuccess || prop.major < 10) return PCF_ENODEVICE;
     PCF_CUDA_TRY(cudaSetDevice(dims->device));
+    // the staged V-cycle stencils' shared-memory limit, set here rather than
+    // at a first launch that may fall inside a graph capture
+    stencil_bulk_ready<float, 4, 32, 4, false, EPI_RESNR, false>();
+    stencil_bulk_ready<float, 4, 32, 4, true, EPI_PSEUDO, false>();
 
     pcf_handle *h = new pcf_handle;
     std::memset(h, 0, sizeof(*h));

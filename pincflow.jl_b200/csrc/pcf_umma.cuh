@@ -20,6 +20,8 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include "pcf_internal.cuh"
+
 namespace pcf {
 namespace umma {
 
@@ -35,10 +37,6 @@ struct GemmArgs {
     __nv_bfloat16 *outB;   // row-major [M][N] BF16 (nullable)
     int *error;            // set to 1 if an mbarrier wait timed out
 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
 
 // Shared-memory matrix descriptor: K-major, SWIZZLE_NONE.
 __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -62,25 +60,6 @@ __host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
 // byte offset of element (row, k) of a (rows x 64) K-major tile
 __device__ __forceinline__ uint32_t tile_off(int row, int k) {
     return (uint32_t)((((row >> 3) << 3) + (k >> 3)) * 128 + ((row & 7) << 4) + ((k & 7) << 1));
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-    uint64_t t0;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-    for (;;) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(mbar), "r"(phase)
-            : "memory");
-        if (done) return true;
-        uint64_t t1;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-        if (t1 - t0 > 2000000000ull) return false;  // 2 s
-    }
 }
 
 template <int NT>

@@ -41,6 +41,8 @@ def case(name: str):
         cfg = C.c3(9, nx=160, ny=12, nz=20)
     elif name == "oddx":        # odd nx, even ny: multigrid aggregates 1 x 2 columns
         cfg = C.c3(5, nx=25, ny=32, nz=12)
+    elif name == "wide2":       # wide tile with partial x and y tiles (136 = 128 + 8, 10 = 2 x 4 + 2)
+        cfg = C.c3(13, nx=136, ny=10, nz=12)
     else:
         raise KeyError(name)
     cfg.setdefault("damp", False)

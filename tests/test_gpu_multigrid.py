@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 
 MG = dict(multigrid=True, mg_dtau=2.0, mg_coarse_iterations=4, mg_min_columns=16)
 # the parity cases plus one whose hierarchy aggregates 1 x 2 columns
-MG_CASES = CASES + ["oddx"]
+MG_CASES = CASES + ["oddx", "wide2"]
 
 
 @pytest.fixture(scope="module")
@@ -53,7 +53,8 @@ def _oracle_mg(cfg, coef, **kw):
     from oracle.mg_oracle import Multigrid
     f = cfg["fields"]
     return Multigrid(coef, F.fcscal(cfg["dom"], f), f["dx"], f["dy"], dtau=kw.get("mg_dtau", 2.0),
-                     coarse_iterations=kw.get("mg_coarse_iterations", 4), min_columns=kw.get("mg_min_columns", 16))
+                     coarse_iterations=kw.get("mg_coarse_iterations", 4), min_columns=kw.get("mg_min_columns", 16),
+                     bf16_planes=kw.get("bf16_planes", False))
 
 
 @pytest.mark.parametrize("name", MG_CASES)
@@ -80,8 +81,12 @@ def test_vcycle_matches_oracle(name, solvers, oracle, pcf):
     got = s.apply_multigrid(b, pcf.PoissonNamelist(precision="mixed", mg_operator_bf16=False, **MG))
     want = _oracle_mg(cfg, coef, **MG).cycle(b)
     assert rel_err(got, want) < 1e-4, rel_err(got, want)
+    # the BF16 operator copies (shared-memory staged stencils on wide grids)
+    # against the oracle's V-cycle on the same BF16-rounded planes
     got16 = s.apply_multigrid(b, pcf.PoissonNamelist(precision="mixed", **MG))
-    assert 0 < rel_err(got16, want) < 1e-1, rel_err(got16, want)
+    want16 = _oracle_mg(cfg, coef, bf16_planes=True, **MG).cycle(b)
+    assert rel_err(got16, want16) < 1e-4, rel_err(got16, want16)
+    assert rel_err(got16, want) > 10 * rel_err(got16, want16), (rel_err(got16, want), rel_err(got16, want16))
 
 
 @pytest.mark.parametrize("dtau", [2.0, 2.5])

@@ -87,3 +87,34 @@ def test_multigrid_cuts_iterations(mtn):
     assert 3 * it_mg <= it_ref, (it_mg, it_ref)
     r = b - apply(coef, x)
     assert np.sqrt(np.mean(r ** 2)) / np.sqrt(np.mean(b ** 2)) <= 1e-9
+
+
+def test_bf16_rounding_is_round_to_nearest_even():
+    """The oracle's BF16 rounding (of the FP32 rounding) against torch's
+    float32 -> bfloat16 conversion, and on hand-picked ties."""
+    import torch
+    from oracle.mg_oracle import bf16
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(50000) * np.exp(rng.uniform(-40, 40, 50000))
+    want = torch.tensor(x, dtype=torch.float32).to(torch.bfloat16).to(torch.float64).numpy()
+    assert np.array_equal(bf16(x), want)
+    # 1 + 2^-8 is a tie between 1 and 1 + 2^-7: to the even mantissa, 1
+    ties = np.array([1 + 2.0 ** -8, 1 + 3 * 2.0 ** -8, -(1 + 2.0 ** -8)])
+    assert np.array_equal(bf16(ties), [1.0, 1 + 2.0 ** -6, -1.0])
+
+
+def test_vcycle_bf16_planes_differ_only_by_rounding(mtn):
+    """With BF16 stencil planes the V-cycle moves by about the BF16 rounding
+    (2^-9 relative), not more."""
+    from oracle.mg_oracle import Multigrid
+    cfg, coef = mtn
+    f = cfg["fields"]
+    b = np.random.default_rng(3).standard_normal(cfg["dom"].interior_shape)
+    kw = dict(dtau=2.5)
+    e32 = Multigrid(coef, F.fcscal(cfg["dom"], f), f["dx"], f["dy"], **kw).cycle(b)
+    m16 = Multigrid(coef, F.fcscal(cfg["dom"], f), f["dx"], f["dy"], bf16_planes=True, **kw)
+    e16 = m16.cycle(b)
+    assert m16.levels[0]["scoef"] is not m16.levels[0]["coef"]
+    assert m16.levels[-1]["scoef"] is m16.levels[-1]["coef"]
+    rel = np.linalg.norm(e16 - e32) / np.linalg.norm(e32)
+    assert 1e-6 < rel < 5e-2, rel
