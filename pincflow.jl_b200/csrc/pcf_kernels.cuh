@@ -52,6 +52,12 @@ __device__ __forceinline__ void load_vec(const T *__restrict__ p, T (&v)[V]) {
     for (int q = 0; q < V; ++q) v[q] = e[q];
 }
 
+// two BF16 values packed in 4 bytes, widened to FP32
+__device__ __forceinline__ void unpack_bf16x2(unsigned x, float (&v)[2]) {
+    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&x));
+    v[0] = a.x; v[1] = a.y;
+}
+
 // four BF16 values packed in 8 bytes, widened to FP32
 __device__ __forceinline__ void unpack_bf16x4(uint2 x, float (&v)[4]) {
     const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&x.x));
@@ -415,18 +421,19 @@ __device__ __forceinline__ void ring_store(T *slot, const T (&rv)[Ring<T, V, TX,
 // C16: the coefficient planes are read from a.coef16 (BF16, half the bytes;
 // FP32 only, for the preconditioner's stencils): 1 with a load per plane and
 // level, like the FP32 planes; 2 staged through shared memory by TMA, where
-// one thread loads the block's 128 x 4 tile of every plane for level
+// one thread loads the block's 32 V x 4 tile of every plane for level
 // k + kStencilStages - 1 (one box of a 4-D tensor map over x, y, z and plane,
 // two for the Horizontal operator's 22 planes) while level k is computed,
 // into kStencilStages stages that complete on one mbarrier each, so no thread
-// waits on DRAM for its coefficients.  C16 = 2 needs TX = 32, TY = 4, V = 4,
-// the tensor maps a.tmap16 (make_coef16_maps) and stencil_bulk_smem bytes of
-// dynamic shared memory.  A wait that gives up (2 s) marks the iteration
-// failed (guard status PCF_ECUDA).
+// waits on DRAM for its coefficients.  C16 = 2 needs TX = 32, TY = 4, V = 4
+// (128-wide tiles) or 2 (64-wide), the tensor maps a.tmap16
+// (make_coef16_maps: three of box width 128, then three of box width 64)
+// and stencil_bulk_smem bytes of dynamic shared memory.  A wait that gives
+// up (2 s) marks the iteration failed (guard status PCF_ECUDA).
 constexpr int kStencilStages = 2;  // 3 measured slower: 2 instead of 3 resident blocks per SM
-template <int TX, int TY, bool HORIZ>
+template <int V, int TX, int TY, bool HORIZ>
 constexpr int stencil_stage_bytes() {
-    return (HORIZ ? PCF_NCOEF - 3 : PCF_NCOEF) * TY * TX * 4 * 2;
+    return (HORIZ ? PCF_NCOEF - 3 : PCF_NCOEF) * TY * TX * V * 2;
 }
 
 // stage slot of plane p: the Horizontal operator skips AC, AD and AU
@@ -438,7 +445,7 @@ __host__ __device__ constexpr int slot_of_plane(int p) {
 template <typename T, int V, int TX, int TY, bool HORIZ, int EPI, bool DIFF = false, int C16 = 0>
 __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
     static_assert(C16 == 0 || sizeof(T) == 4, "BF16 planes feed the FP32 stencil only");
-    static_assert(C16 != 2 || (V == 4 && TX == 32 && TY == 4), "the tensor maps' box is 128 x 4");
+    static_assert(C16 != 2 || ((V == 4 || V == 2) && TX == 32 && TY == 4), "the tensor maps' boxes are 32 V x 4");
     static_assert(PCF_AC == 0 && PCF_AL == 1 && PCF_AD == 5 && PCF_AU == 6 && PCF_ALD == 7, "plane order");
     using R = Ring<T, V, TX, TY>;
     __shared__ __align__(16) T sm[R::NS][R::NR * R::RW];
@@ -465,7 +472,7 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
     T hv;
     const int lt = tx + TX * ty;
     // C16 == 2: thread 0 loads level kk's tile of every plane into stage st
-    const char *maps = static_cast<const char *>(a.tmap16);
+    const char *maps = C16 == 2 ? static_cast<const char *>(a.tmap16) + (V == 2 ? 3 * 128 : 0) : nullptr;
     auto issue = [&](int kk, int st) {
         const uint32_t bar = smem_u32(bars + st), dst = smem_u32(stg + st * STAGE);
         mbar_arrive_expect(bar, (uint32_t)(STAGE * sizeof(__nv_bfloat16)));  // whole boxes, zero-filled outside
@@ -533,9 +540,11 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
 #pragma unroll
                 for (int p = 0; p < PCF_NCOEF; ++p) {
                     if (HORIZ && (p == PCF_AC || p == PCF_AD || p == PCF_AU)) continue;
-                    const uint2 u = failed ? make_uint2(0u, 0u)
-                                           : *reinterpret_cast<const uint2 *>(cs + slot_of_plane<HORIZ>(p) * TY * R::W);
-                    unpack_bf16x4(u, c[p]);
+                    const __nv_bfloat16 *cp = cs + slot_of_plane<HORIZ>(p) * TY * R::W;
+                    if constexpr (V == 4)
+                        unpack_bf16x4(failed ? make_uint2(0u, 0u) : *reinterpret_cast<const uint2 *>(cp), c[p]);
+                    else if constexpr (V == 2)
+                        unpack_bf16x2(failed ? 0u : *reinterpret_cast<const unsigned *>(cp), c[p]);
                 }
             } else {
 #pragma unroll

@@ -152,18 +152,19 @@ static int pick_kc(long long xyblocks, int nz) {
 }
 
 // dynamic shared memory of the staged BF16 stencil: the stages, one mbarrier each
-template <int TX, int TY, bool HORIZ>
+template <int V, int TX, int TY, bool HORIZ>
 constexpr int stencil_bulk_smem() {
-    return kStencilStages * (stencil_stage_bytes<TX, TY, HORIZ>() + (int)sizeof(uint64_t));
+    return kStencilStages * (stencil_stage_bytes<V, TX, TY, HORIZ>() + (int)sizeof(uint64_t));
 }
 
-// The three tensor maps of a BF16 operator copy (25 planes of nx x ny x nz
-// values) that the staged stencils load their tiles with, boxes of 128 x 4 x 1
-// values of [0] all 25 planes, [1] the 4 planes AL..AF, [2] the 18 planes
-// ALD..AFUU, written to the device array maps (3 x 128 bytes).  Returns false
-// (and the stencils read the planes directly) when the driver has no
-// tensor-map encoder or the grid breaks the copy's alignment rules (x rows
-// of a multiple of 16 bytes, at least one box wide).
+// The tensor maps of a BF16 operator copy (25 planes of nx x ny x nz values)
+// that the staged stencils load their tiles with, written to the device
+// array maps (6 x 128 bytes): boxes of 128 x 4 x 1 values of [0] all 25
+// planes, [1] the 4 planes AL..AF, [2] the 18 planes ALD..AFUU, then [3..5]
+// the same with 64-wide boxes.  Returns false (and the stencils read the
+// planes directly) when the driver has no tensor-map encoder or the grid
+// breaks the copy's alignment rules (x rows of a multiple of 16 bytes, at
+// least one 128-wide box wide).
 static bool make_coef16_maps(const __nv_bfloat16 *coef16, const Dims &d, void *maps) {
     using Encode = decltype(&cuTensorMapEncodeTiled);
     static Encode encode = [] {
@@ -178,13 +179,13 @@ static bool make_coef16_maps(const __nv_bfloat16 *coef16, const Dims &d, void *m
     }();
     if (!encode || !coef16 || d.nx % 8 != 0 || d.nx < 128 || (reinterpret_cast<uintptr_t>(coef16) & 15) != 0)
         return false;
-    CUtensorMap host[3];
+    CUtensorMap host[6];
     const cuuint64_t dims[4] = {(cuuint64_t)d.nx, (cuuint64_t)d.ny, (cuuint64_t)d.nz, (cuuint64_t)PCF_NCOEF};
     const cuuint64_t strides[3] = {2ull * d.nx, 2ull * d.plane, 2ull * (cuuint64_t)d.n};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     const cuuint32_t planes[3] = {PCF_NCOEF, PCF_AD - PCF_AL, PCF_NCOEF - PCF_ALD};
-    for (int q = 0; q < 3; ++q) {
-        const cuuint32_t box[4] = {128, 4, 1, planes[q]};
+    for (int q = 0; q < 6; ++q) {
+        const cuuint32_t box[4] = {q < 3 ? 128u : 64u, 4, 1, planes[q % 3]};
         if (encode(&host[q], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(coef16), dims, strides,
                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
@@ -209,8 +210,8 @@ static int stencil_bulk_ready() {
         auto kern = k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF, 2>;
         int per_sm = 0;
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 stencil_bulk_smem<TX, TY, HORIZ>()) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TX * TY, stencil_bulk_smem<TX, TY, HORIZ>()) ==
+                                 stencil_bulk_smem<V, TX, TY, HORIZ>()) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TX * TY, stencil_bulk_smem<V, TX, TY, HORIZ>()) ==
                 cudaSuccess &&
             per_sm > 0) {
             st = per_sm * num_sms();
@@ -221,6 +222,37 @@ static int stencil_bulk_ready() {
         state[dev].store(st);
     }
     return st > 0 ? st : 0;
+}
+
+// Launches the TMA-staged BF16 stencil with SV x values per thread (tiles of
+// 32 SV x 4 cells) on the handle's stream; false (nothing launched) if the
+// device refuses its shared memory or the grid exceeds the partials buffer.
+template <typename T, int SV, bool HORIZ, int EPI, bool DIFF>
+static bool launch_staged(pcf_handle *h, const StencilArgs<T> &a) {
+    const int cap = stencil_bulk_ready<T, SV, 32, 4, HORIZ, EPI, DIFF>();
+    if (cap <= 0) return false;
+    constexpr int W = 32 * SV;
+    const long long gx = (a.nx + W - 1) / W, gy = (a.ny + 3) / 4, xy = gx * gy;
+    if (gy > 65535) return false;
+    // z-chunks of pick_kc's length, or a half or a quarter of it when that
+    // fills the last wave of resident blocks better (measured at
+    // 512x512x192 with 128-wide tiles: 1536 blocks in 444 slots, 3.46 waves,
+    // 606 us; 3072 blocks, 6.92 waves, 563 us)
+    auto fill = [&](int kcx) {
+        const long long blocks = xy * ((a.nz + kcx - 1) / kcx);
+        return (double)blocks / (double)(((blocks + cap - 1) / cap) * cap);
+    };
+    int kc = std::min(pick_kc(xy, a.nz), a.nz);
+    for (int halvings = 0; halvings < 2; ++halvings) {
+        const int c = std::max(1, (kc + 1) / 2);
+        if (c == kc || xy * ((a.nz + c - 1) / c) > kMaxPartials || !(fill(c) > fill(kc) + 0.02)) break;
+        kc = c;
+    }
+    const long long gz = (a.nz + kc - 1) / kc;
+    if (xy * gz > kMaxPartials) return false;
+    k_stencil<T, SV, 32, 4, HORIZ, EPI, DIFF, 2><<<dim3((unsigned)gx, (unsigned)gy, (unsigned)gz), dim3(32, 4, 1),
+                                                     stencil_bulk_smem<SV, 32, 4, HORIZ>(), h->stream>>>(a, kc);
+    return true;
 }
 
 template <typename T, int V, int TX, bool HORIZ, int EPI, bool DIFF>
@@ -254,25 +286,15 @@ static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_ov
             if (gx * gy * ((a.nz + kc16 - 1) / kc16) > kMaxPartials) kc16 = kc;  // the grid shape checked above
             const long long gz16 = (a.nz + kc16 - 1) / kc16;
             if constexpr (V == 4 && TX == 32) {
-                // the coefficient tiles staged in shared memory by bulk copies
-                const int cap = a.tmap16 ? stencil_bulk_ready<T, V, TX, TY, HORIZ, EPI, DIFF>() : 0;
-                if (cap > 0) {
-                    // z-chunks of pick_kc's length, or half of it when that
-                    // fills the last wave of resident blocks better (measured
-                    // at 512x512x192: 1536 blocks in 444 slots, 3.46 waves,
-                    // 606 us; 3072 blocks, 6.92 waves, 563 us)
-                    auto fill = [&](int kcx) {
-                        const long long blocks = gx * gy * ((a.nz + kcx - 1) / kcx);
-                        return (double)blocks / (double)(((blocks + cap - 1) / cap) * cap);
-                    };
-                    int kcb = kc;
-                    const int half = std::max(1, (kc + 1) / 2);
-                    if (gx * gy * ((a.nz + half - 1) / half) <= kMaxPartials && fill(half) > fill(kc) + 0.02)
-                        kcb = half;
-                    const long long gzb = (a.nz + kcb - 1) / kcb;
-                    k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF, 2>
-                        <<<dim3((unsigned)gx, (unsigned)gy, (unsigned)gzb), block, stencil_bulk_smem<TX, TY, HORIZ>(),
-                           h->stream>>>(a, kcb);
+                // the coefficient tiles staged in shared memory by TMA: 64-wide
+                // tiles (6 blocks per SM) on grids of 10 million cells or more
+                // or rows of 512 or more, 128-wide (3 per SM) otherwise
+                // (measured per launch: 512x512x192 0.512 vs 0.561 ms, and the
+                // 256x256x192 level below it faster too; 256x256x128 0.116 vs
+                // 0.113 ms)
+                const bool narrow = a.n >= 10000000 || a.nx >= 512;
+                if (a.tmap16 && (narrow ? launch_staged<T, 2, HORIZ, EPI, DIFF>(h, a)
+                                        : launch_staged<T, 4, HORIZ, EPI, DIFF>(h, a))) {
                     PCF_CUDA_TRY(cudaGetLastError());
                     return PCF_OK;
                 }
@@ -904,7 +926,7 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
                 return rc;
             if (l == 1) {  // the first coarse level's BF16 copy, written by its coarsening
                 float *c16 = nullptr, *maps = nullptr;
-                if ((rc = alloc(&c16, (C.d.n * PCF_NCOEF + 1) / 2)) || (rc = alloc(&maps, 3 * 128 / 4))) return rc;
+                if ((rc = alloc(&c16, (C.d.n * PCF_NCOEF + 1) / 2)) || (rc = alloc(&maps, 6 * 128 / 4))) return rc;
                 C.coef16 = reinterpret_cast<__nv_bfloat16 *>(c16);
                 if (make_coef16_maps(C.coef16, C.d, maps)) C.tmap16 = maps;
             }
@@ -931,7 +953,7 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
     }
     if (m.bf16 && !m.lv[0].tmap16) {  // the finest level's maps (once per hierarchy)
         void *maps = nullptr;
-        const cudaError_t e = cudaMalloc(&maps, 3 * 128);
+        const cudaError_t e = cudaMalloc(&maps, 6 * 128);
         if (e != cudaSuccess) return pcf_set_cuda_error(e);
         m.allocs.push_back(maps);
         if (make_coef16_maps(h->coef16, h->d, maps)) m.lv[0].tmap16 = maps;
@@ -1517,6 +1539,8 @@ int pcf_create(pcf_handle **out, const pcf_dims *dims) {
     // at a first launch that may fall inside a graph capture
     stencil_bulk_ready<float, 4, 32, 4, false, EPI_RESNR, false>();
     stencil_bulk_ready<float, 4, 32, 4, true, EPI_PSEUDO, false>();
+    stencil_bulk_ready<float, 2, 32, 4, false, EPI_RESNR, false>();
+    stencil_bulk_ready<float, 2, 32, 4, true, EPI_PSEUDO, false>();
 
     pcf_handle *h = new pcf_handle;
     std::memset(h, 0, sizeof(*h));

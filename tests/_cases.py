@@ -43,6 +43,8 @@ def case(name: str):
         cfg = C.c3(5, nx=25, ny=32, nz=12)
     elif name == "wide2":       # wide tile with partial x and y tiles (136 = 128 + 8, 10 = 2 x 4 + 2)
         cfg = C.c3(13, nx=136, ny=10, nz=12)
+    elif name == "wide3":       # 512 wide: the V-cycle's staged stencils take 64-wide tiles; partial y tile
+        cfg = C.c3(15, nx=512, ny=10, nz=8)
     else:
         raise KeyError(name)
     cfg.setdefault("damp", False)

@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 
 MG = dict(multigrid=True, mg_dtau=2.0, mg_coarse_iterations=4, mg_min_columns=16)
 # the parity cases plus one whose hierarchy aggregates 1 x 2 columns
-MG_CASES = CASES + ["oddx", "wide2"]
+MG_CASES = CASES + ["oddx", "wide2", "wide3"]
 
 
 @pytest.fixture(scope="module")
