@@ -842,7 +842,8 @@ def run_ours(args, rank, world, local_rank):
              "apply64": "k_stencil Total apply FP64", "pseudo32": "k_stencil Horizontal apply + pseudo-step FP32",
              "pseudo64": "k_stencil Horizontal apply + pseudo-step FP64",
              "thomas32": "k_thomas column solves FP32", "thomas64": "k_thomas column solves FP64",
-             "mg_bf16": "k_stencil V-cycle finest-level residual / pseudo-step on the BF16 operator copy"}
+             "mg_bf16": "k_stencil V-cycle finest-level residual / pseudo-step on the BF16 operator copy, "
+                        "coefficient tiles staged in shared memory by TMA on grids 128 or more wide"}
 
     def roof(tag):
         v = prof[tag]
