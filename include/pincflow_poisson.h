@@ -141,8 +141,10 @@ typedef struct {
     int mg_operator_bf16;          /* multigrid: 1: the V-cycle's residual and smoothing stencils on the finest and
                                       the first coarse level read BF16 copies of their operators (half their bytes;
                                       the Krylov operator, the coarser levels and the FP64 true residual are
-                                      unchanged); 0: the FP32 copies.  The learned preconditioner stage (learned & 2)
-                                      always runs the FP32 V-cycle it was trained on (1) */
+                                      unchanged); 0: the FP32 copies.  On levels 128 or more cells wide with nx a
+                                      multiple of 8 those stencils load the BF16 tiles into shared memory by TMA
+                                      (same arithmetic, same results).  The learned preconditioner stage
+                                      (learned & 2) always runs the FP32 V-cycle it was trained on (1) */
 } pcf_params;
 
 typedef struct {
