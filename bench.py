@@ -2,21 +2,25 @@
 Poisson solve (PinCFlow.jl PoissonSolver) on B200.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config c2|c5|c1|c4|step] [--method mg|mixed|fp64]
+                  [--config c5|c2|c1|c4|step] [--method mg|mixed|fp64]
 
 A step is one complete solve_poisson! (operator assembly, preconditioned
 BiCGSTAB to FP64 true relative residual 1e-10, unscaling into dpip) of the
-configuration's seeded synthetic workload.  `value` is the device time per
-solve with inputs resident in HBM (CUDA events on the solver's stream, max
-over ranks); `e2e` is the same solve through the public host-array entry
-point with its host<->device copies inside the timed region.  The default
-workload (c2, 256 x 256 x 128) holds a 3.4 GB FP64 + 0.8 GB FP32 operator,
-far larger than the 126 MB L2, so no flush is needed between steps.
+configuration's seeded synthetic workload.  The default workload is the
+512 x 512 x 192 pseudo-incompressible domain (c5), whose 10 GB FP64 + 5 GB
+FP32 operator is far larger than the 126 MB L2, so no flush is needed
+between steps.  `value` is the device time per solve with inputs resident
+in HBM (CUDA events on the solver's stream, max over ranks); `e2e` is the
+host wall clock around the public host-array entry point, its
+host<->device copies inside the timed region.  The same line carries the
+learned arm (`learned`): the network trained on the training configuration
+by the library's own kernels, used as warm start and as preconditioner
+stage of the flexible FP32 BiCGSTAB, timed on the same inputs.
 
 --impl reference times the reference algorithm on the host cores (the CPU
-oracle, a C++ restatement of the Julia code; Julia is not available): each
-step runs the operator assembly plus a bounded number of BiCGSTAB
-iterations on the full workload, scaled to a complete solve by the
+oracle, a C++ restatement of the Julia code; Julia is not available): the
+operator assembly is timed once, and each step runs a bounded number of
+BiCGSTAB iterations on the full workload, scaled to a complete solve by the
 oracle's own iteration count for that workload.
 --config step times the whole implicit half step around the solve
 (implicit_integration!.jl:49-77: predictor, compute_lhs!, solve, correct!)
@@ -55,6 +59,13 @@ WORKLOADS = {
 STEP_METRIC = "time per implicit half step (predictor + compute_lhs! + solve to FP64 true rel. residual 1e-10 + " \
               "correct!), 1 B200"
 
+
+DTYPES = {
+    "mg": "f32+f64 (FP32 Krylov and preconditioner, FP64 true residual, refinement and dots; BF16 coefficient "
+          "copies in the V-cycle's stencils on multigrid levels 0-1)",
+    "mixed": "f32+f64 (FP32 Krylov and preconditioner, FP64 true residual, refinement and dots)",
+    "fp64": "f64",
+}
 
 METHODS = {
     "mg": "flexible FP32 BiCGSTAB inside FP64 iterative refinement (reliable updates on the FP64 true residual), "
@@ -221,20 +232,46 @@ class ClockSampler:
 def oracle_sample(cfg, iters, threads=None):
     """Oracle FP64 assembly + `iters` BiCGSTAB iterations on the full workload.
     Returns (seconds_assembly, seconds_per_iteration, threads)."""
-    from oracle import oracle as O
-    O.build()
-    if threads:
-        O.set_threads(threads)
-    dom, f = cfg["dom"], cfg["fields"]
-    d = O.dims(dom.nx, dom.ny, dom.nz, dom.nbx)
-    t0 = time.perf_counter()
-    coef = O.compute_operator(d, O.MODELS[cfg["model"]], f, cfg["rho"], cfg["betar"], cfg["dt"],
-                              cfg["rayleigh_factor"])
-    t1 = time.perf_counter()
-    _, info = O.bicgstab(d, coef, f["dx"], f["dy"], cfg["rhs"], tolerance=1e-30, tolerance_is_relative=True,
-                         poisson_iterations=iters)
-    t2 = time.perf_counter()
-    return t1 - t0, (t2 - t1) / max(info["niter"], 1), O.get_threads()
+    smp = OracleSampler(cfg, threads)
+    return smp.t_asm, smp.per_iteration(iters), smp.threads
+
+
+# BiCGSTAB iterations per timed CPU sample: about 6 s of the 16 box cores on
+# c2 (0.3 s per iteration) and 8 s on c5 (about 1.9 s per iteration)
+SAMPLE_ITERS = {"c2": 20, "c5": 4, "step": 20}
+
+
+def sample_iters(args):
+    return args.ref_sample_iters or SAMPLE_ITERS.get(args.config, 3)
+
+
+class OracleSampler:
+    """The oracle's FP64 operator assembly of a workload, timed once, and
+    bounded BiCGSTAB samples on that operator.  A sample of k iterations
+    includes the solve's set-up (initial residual and norm, about an eighth
+    of one iteration's work), so its per-iteration time is high by at most
+    1/(8k)."""
+
+    def __init__(self, cfg, threads=None):
+        from oracle import oracle as O
+        O.build()
+        if threads:
+            O.set_threads(threads)
+        self.O, self.cfg = O, cfg
+        dom, f = cfg["dom"], cfg["fields"]
+        self.d = O.dims(dom.nx, dom.ny, dom.nz, dom.nbx)
+        t0 = time.perf_counter()
+        self.coef = O.compute_operator(self.d, O.MODELS[cfg["model"]], f, cfg["rho"], cfg["betar"], cfg["dt"],
+                                       cfg["rayleigh_factor"])
+        self.t_asm = time.perf_counter() - t0
+        self.threads = O.get_threads()
+
+    def per_iteration(self, iters):
+        f = self.cfg["fields"]
+        t0 = time.perf_counter()
+        _, info = self.O.bicgstab(self.d, self.coef, f["dx"], f["dy"], self.cfg["rhs"], tolerance=1e-30,
+                                  tolerance_is_relative=True, poisson_iterations=iters)
+        return (time.perf_counter() - t0) / max(info["niter"], 1)
 
 
 def oracle_iterations(config):
@@ -282,12 +319,12 @@ def run_reference_c4(args, world):
     for step in range(args.warmup + args.steps):
         per = {}
         for nx in sorted(set(sizes)):
-            t_asm, t_it, used = oracle_sample(C.c4(sizes.index(nx), nx), args.ref_sample_iters, os.cpu_count())
+            t_asm, t_it, used = oracle_sample(C.c4(sizes.index(nx), nx), sample_iters(args), os.cpu_count())
             per[nx] = t_asm + t_it * counts[nx]
         if step >= args.warmup:
             times.append(sum(per[nx] for nx in sizes))
     value = len(sizes) / statistics.mean(times)
-    return value, "solves/s", True, used, (f"per step: oracle FP64 assembly + {args.ref_sample_iters} BiCGSTAB "
+    return value, "solves/s", True, used, (f"per step: oracle FP64 assembly + {sample_iters(args)} BiCGSTAB "
                                            "iterations per size class, scaled by the oracle's full-solve count "
                                            "of that class and summed over the 32 members")
 
@@ -316,21 +353,25 @@ def run_reference(args, rank, world):
     niter, src = oracle_iterations(args.config)
     if niter is None:
         niter, src = args.ref_iterations, "--ref-iterations"
-    threads = os.cpu_count()
-    times = []
+    k = sample_iters(args)
+    smp = OracleSampler(cfg, os.cpu_count())  # the assembly, timed once
+    per_it = []
     for step in range(args.warmup + args.steps):
-        t_asm, t_it, used = oracle_sample(cfg, args.ref_sample_iters, threads)
+        t_it = smp.per_iteration(k)
         if step >= args.warmup:
-            times.append(t_asm + t_it * niter)
-    value = statistics.mean(times)
-    sample = (f"per step: oracle FP64 operator assembly + {args.ref_sample_iters} BiCGSTAB iterations of the "
-              f"{args.config} workload on {used} threads, scaled to {niter} iterations ({src})")
+            per_it.append(t_it)
+    t_it = statistics.mean(per_it)
+    value = smp.t_asm + t_it * niter
+    sample = (f"oracle FP64 operator assembly of the {args.config} workload timed once ({smp.t_asm:.2f} s), then "
+              f"{k} BiCGSTAB iterations per step on {smp.threads} threads ({t_it:.3f} s per iteration over "
+              f"{k * args.steps} timed iterations), scaled to {niter} iterations ({src})")
     line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": {"workload": f"{args.config}: {WORKLOADS[args.config]}", "method": "plain FP64 BiCGSTAB "
                        "with the reference preconditioner (CPU restatement of the Julia code)"},
-            "cpu_baseline": {"value": value, "unit": "s", "cores": used, "kind": "port", "sample": sample},
+            "seconds_per_iteration": t_it, "seconds_assembly": smp.t_asm, "iterations_scaled_to": niter,
+            "cpu_baseline": {"value": value, "unit": "s", "cores": smp.threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -424,7 +465,7 @@ def run_step(args, rank, world, local_rank):
     line = {
         "metric": STEP_METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 (predictor, corrector) + " + ("f64" if args.method == "fp64" else "f32+f64"),
+        "vs_baseline": None, "dtype": "f64 (predictor, corrector); solve " + DTYPES[args.method],
         "data": "synthetic",
         "config": {"workload": f"step: {WORKLOADS['step']}", "method": METHODS[args.method],
                    "l2": "fields of 73 MB each, ~20 of them per step: larger than L2, no flush",
@@ -441,7 +482,7 @@ def run_step(args, rank, world, local_rank):
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
-        total, used, sample = reference_step_seconds(cfg, state, args.ref_sample_iters)
+        total, used, sample = reference_step_seconds(cfg, state, sample_iters(args))
         line["cpu_baseline"] = {"value": total, "unit": "s", "cores": used, "kind": "port", "sample": sample}
     print(json.dumps(line), flush=True)
     s.close()
@@ -452,7 +493,7 @@ def run_reference_step(args, world):
     state = step_state(cfg, 777)
     times = []
     for k in range(args.warmup + args.steps):
-        total, used, sample = reference_step_seconds(cfg, state, args.ref_sample_iters)
+        total, used, sample = reference_step_seconds(cfg, state, sample_iters(args))
         if k >= args.warmup:
             times.append(total)
     return statistics.mean(times), "s", False, used, "per step: " + sample
@@ -522,7 +563,7 @@ def run_c1(args, rank, world, local_rank):
         "metric": "time for the 200 pressure solves of 100 steps to FP64 true rel. residual 1e-10, 1 B200",
         "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.method == "fp64" else "f32+f64", "data": "synthetic",
+        "dtype": "f64 (grids of at most 2048 cells take the single-block FP64 solver)", "data": "synthetic",
         "config": {"workload": f"c1: {WORKLOADS['c1']}", "method": METHODS[args.method],
                    "l2": "1600-cell grid: L2-resident by design (latency-bound workload)",
                    "parallelism": f"replicas x{world}"},
@@ -678,7 +719,7 @@ def run_ensemble(args, rank, world, local_rank):
     line = {
         "metric": "ensemble solves/s to FP64 true rel. residual 1e-10 (32 uneven members), 1 B200",
         "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": DTYPES["mg"],
         "data": "synthetic",
         "config": {"workload": f"c4: {WORKLOADS['c4']}", "members": sizes, "cells": cells,
                    "method": METHODS["mg"] + "; all members advanced together, one CUDA graph launch per "
@@ -722,6 +763,78 @@ def run_ensemble(args, rank, world, local_rank):
 
 
 # ----------------------------------------------------------------- GPU arm --
+
+def deviation_vs_oracle(config, dpip):
+    """Max pointwise deviation of the interior pressure `dpip` (nz, ny, nx)
+    from the oracle's converged FP64 pressure of the same workload, at the
+    cells of the committed fingerprint (tests/golden/<config>_fp64_fingerprint.npz,
+    written by tests/golden/make_oracle_iterations.py): both solves leave the
+    constant (null-space) component free, so the mean difference over the
+    sampled cells is removed first; the deviation is relative to the largest
+    |oracle - mean| there.  None without a fingerprint."""
+    p = os.path.join(REPO, "tests", "golden", f"{config}_fp64_fingerprint.npz")
+    if not os.path.exists(p):
+        return None
+    fp = np.load(p)
+    if tuple(fp["shape"]) != tuple(dpip.shape):
+        return None
+    ref = fp["values"]
+    got = dpip.ravel()[fp["indices"]]
+    diff = got - ref
+    dev = float(np.abs(diff - diff.mean()).max() / np.abs(ref - fp["mean"]).max())
+    return {"value": dev, "cells": int(ref.size), "oracle_iterations": int(fp["niter"]),
+            "oracle_true_residual": float(fp["true_residual"])}
+
+
+def learned_arm(args, s, cfg, d_rhs, d_rho, d_betar, d_dpip, local_rank):
+    """The learned part on this workload.  Two networks are trained on the
+    training configuration (configs.c3 problems, 128 x 128 x 64 random
+    Gaussian-hill terrain) by the library's own forward, backward and Adam
+    kernels, on pairs that the plain FP64 solver generates:
+      warm start: x0 = N(b), trained on (b, s) pairs;
+      stage: each preconditioner application z = M(r) + N(r - A M(r)),
+             bias-free, trained on the V-cycle's (residual, error) pairs.
+    Each is then timed on this workload with the multigrid mixed solve to FP64
+    true relative residual 1e-10 (data generation and training are set-up,
+    reported, not timed)."""
+    import pincflow_poisson as pcf
+    from pincflow_poisson import learned as L
+    dom = cfg["dom"]
+    t0 = time.perf_counter()
+    pairs_ws = L.training_pairs(range(args.learned_pairs), device=local_rank)
+    pairs_pc = L.preconditioner_pairs(range(args.learned_pairs), device=local_rank)
+    t1 = time.perf_counter()
+    cols = max(dom.nx * dom.ny, 128 * 128)
+    nets = {"warm_start": L.LearnedNet(device=local_rank, max_columns=cols, seed=0),
+            "stage": L.LearnedNet(device=local_rank, max_columns=cols, seed=1)}
+    nets["stage"].set_bias_free(True)
+    loss = {"warm_start": L.train(nets["warm_start"], pairs_ws, epochs=args.learned_epochs, device=local_rank),
+            "stage": L.train(nets["stage"], pairs_pc, epochs=args.learned_epochs, device=local_rank)}
+    t2 = time.perf_counter()
+    kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000, precision="mixed",
+              residual="true", multigrid=args.method == "mg", mg_dtau=args.mg_dtau)
+    out = {"training": {"configuration": "c3: 128x128x64 Boussinesq, 1-5 Gaussian hills, N ~ U(0.005, 0.02)",
+                        "pairs": len(pairs_ws), "epochs": args.learned_epochs, "generation_s": t1 - t0,
+                        "training_s": t2 - t1, "parameters": L.NPARAM}}
+    for role, bit in (("warm_start", 1), ("stage", 2)):
+        s.attach_network(nets[role])
+        nl = pcf.PoissonNamelist(**kw, learned=bit)
+        infos = []
+        for k in range(1 + min(args.steps, 3)):  # the first solve captures the graphs
+            i = s.solve_poisson_device(d_rhs.data_ptr(), d_rho.data_ptr(), d_betar.data_ptr(), cfg["dt"],
+                                       cfg["rayleigh_factor"], cfg["tolref"], nl, d_dpip.data_ptr())
+            if k:
+                infos.append(i)
+        s.attach_network(None)
+        out[role] = {"s": statistics.mean(i.timings_ms["total"] for i in infos) / 1e3, "iterations": infos[-1].niter,
+                     "true_residual": infos[-1].true_residual, "converged": not infos[-1].errflag,
+                     "loss_first_epoch": float(np.mean(loss[role][:len(pairs_ws)])),
+                     "loss_last_epoch": float(np.mean(loss[role][-len(pairs_ws):]))}
+    for n in nets.values():
+        n.close()
+    return out
+
+
 
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -806,6 +919,10 @@ def run_ours(args, rank, world, local_rank):
     diff = fast_dpip - plain_dpip
     dev_max = float(np.abs(diff - diff.mean()).max() / np.abs(plain_dpip - plain_dpip.mean()).max())
     plain_s = max_over_ranks(statistics.mean(i.timings_ms["total"] for i in plain)) / 1e3
+    dev_oracle = deviation_vs_oracle(args.config, fast_dpip) if rank == 0 and not args.size else None
+
+    # --- the learned arm: warm start + preconditioner stage ---------------
+    learned = None if args.no_learned else learned_arm(args, s, cfg, d_rhs, d_rho, d_betar, d_dpip, local_rank)
 
     # --- end to end through the host-array entry point --------------------
     h_rhs = torch.from_numpy(np.ascontiguousarray(cfg["rhs"])).pin_memory().numpy()
@@ -823,7 +940,7 @@ def run_ours(args, rank, world, local_rank):
             raise RuntimeError(f"e2e solve did not converge: {info}")
         e2e_ms.append(info.timings_ms["total"])
     barrier()
-    e2e_s = max_over_ranks(statistics.mean(e2e_ms)) / 1e3
+    e2e_s = max_over_ranks(statistics.mean(e2e_wall))
     n = dom.nx * dom.ny * dom.nz
     nh = int(np.prod(dom.halo_shape))
     h2d = 8 * (n + 2 * nh)
@@ -866,7 +983,7 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+f64" if f32 else "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": DTYPES[args.method], "data": "synthetic",
         "config": {"workload": f"{args.config}: {WORKLOADS[args.config]}",
                    "method": METHODS[args.method],
                    "convergence": "FP64 true residual RMS(b-Ax)/RMS(b) <= 1e-10",
@@ -877,13 +994,16 @@ def run_ours(args, rank, world, local_rank):
         "iterations": last.niter, "refinements": last.nrefine, "true_residual": last.true_residual,
         "plain_fp64_iterations": plain[-1].niter,
         "max_pointwise_dev_vs_plain_fp64": dev_max,
+        "max_pointwise_dev_vs_oracle": dev_oracle,
         "solves_per_s": world / value,
         "cell_updates_per_s": world * n * (2 * last.niter) / value,
         "gpu_launches": launches,
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "wall_s": statistics.mean(e2e_wall)},
+                "clock": "host wall clock around PoissonSolver.solve_poisson (pcf_solve) on pinned host arrays",
+                "device_events_s": statistics.mean(e2e_ms) / 1e3},
         "roofline": roof(dominant),
         "roofline_krylov_apply": roof(krylov),
+        "learned": learned,
         "kernel_shares": shares, "kernels": per_kernel,
         "kernel_timing": f"CUDA events around every launch of {args.steps} profiled solves run right after the "
                          f"timed region (direct launches; {profiled_ms:.1f} ms per solve)",
@@ -891,13 +1011,16 @@ def run_ours(args, rank, world, local_rank):
     }
     if world == 1 and not args.no_cpu_baseline:
         niter, src = oracle_iterations(args.config)
-        if niter is None:
+        if niter is None or args.size:
             niter, src = plain[-1].niter, "the GPU FP64 solve's iteration count"
-        t_asm, t_it, used = oracle_sample(cfg, args.ref_sample_iters, os.cpu_count())
+        k = sample_iters(args)
+        smp = OracleSampler(cfg, os.cpu_count())
+        t_it = smp.per_iteration(k)
         line["cpu_baseline"] = {
-            "value": t_asm + t_it * niter, "unit": "s", "cores": used, "kind": "port",
-            "sample": f"oracle FP64 assembly + {args.ref_sample_iters} BiCGSTAB iterations of the same workload, "
-                      f"scaled to {niter} iterations ({src})"}
+            "value": smp.t_asm + t_it * niter, "unit": "s", "cores": smp.threads, "kind": "port",
+            "sample": f"oracle FP64 assembly ({smp.t_asm:.2f} s) + {k} BiCGSTAB iterations of the same workload "
+                      f"({t_it:.3f} s each), scaled to {niter} iterations ({src})"}
+        del smp
     print(json.dumps(line), flush=True)
     s.close()
 
@@ -908,14 +1031,18 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--config", default="c5", choices=sorted(WORKLOADS))
     ap.add_argument("--size", default=None, help="c2 only: NXxNYxNZ instead of 256x256x128 (profiling captures)")
     ap.add_argument("--method", default="mg", choices=sorted(METHODS))
     ap.add_argument("--mg-dtau", type=float, default=2.5)
     ap.add_argument("--plain-steps", type=int, default=2)
-    ap.add_argument("--ref-sample-iters", type=int, default=3)
+    ap.add_argument("--ref-sample-iters", type=int, default=None,
+                    help="BiCGSTAB iterations per CPU sample (default: 20 on c2 and step, 4 on c5, 3 on c4)")
     ap.add_argument("--ref-iterations", type=int, default=450)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned arm")
+    ap.add_argument("--learned-pairs", type=int, default=32, help="training pairs of each network")
+    ap.add_argument("--learned-epochs", type=int, default=4)
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

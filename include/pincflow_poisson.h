@@ -3,8 +3,8 @@
  * Poisson solver that replaces PinCFlow.jl's PoissonSolver hot path.
  *
  * The entry points mirror the reference's Julia functions so that a Julia
- * method (package extension or shim) can `ccall` them
- * with the arrays it already owns:
+ * method (the package extension ext/PinCFlowGPUExt.jl of the binding) can
+ * `ccall` them with the arrays it already owns:
  *
  *   pcf_solve              <- solve_poisson!(state, dt, rayleigh_factor, tolref)
  *                             src/PoissonSolver/solve_poisson!.jl:39-75
@@ -388,7 +388,8 @@ enum pcf_prof_tag {
     PCF_PROF_UPDATE32 = 6,  /* BiCGSTAB vector updates, FP32 */
     PCF_PROF_UPDATE64 = 7,
     PCF_PROF_ASSEMBLE = 8,  /* operator assembly + factors */
-    PCF_PROF_RELIABLE = 9,  /* FP64 true-residual applies of reliable updates (mostly skipped launches) */
+    PCF_PROF_RELIABLE = 9,  /* FP64 true-residual applies of reliable updates: every guarded launch's time,
+                               the bytes of the launches that performed an update */
     PCF_PROF_MG = 10,       /* multigrid coarse levels and grid transfers, FP32 */
     PCF_PROF_LEARNED = 11,  /* learned preconditioner stage: residual, network, combination */
     PCF_PROF_PREDICT = 12,  /* implicit predictor with its predictand boundary fills (FP64) */
@@ -452,9 +453,11 @@ int pcf_net_set_bias_free(pcf_net *net, int on);
  * preconditioner (for a bias-free network).  NULL detaches. */
 int pcf_set_network(pcf_handle *h, pcf_net *net);
 
-/* Allocation-free global dot product.  No counterpart in the reference: it
- * is the deterministic sum of pcf_global_dot for callers that cannot let the
- * library allocate device memory -- a host model whose GPU memory belongs to
+/* Allocation-free global dot product.  No counterpart in the reference: a
+ * deterministic, run-to-run reproducible sum that agrees with pcf_global_dot
+ * to rounding (it adds fixed chunks of 32768 elements per block, not
+ * pcf_global_dot's blocking), for callers that cannot let the library
+ * allocate device memory -- a host model whose GPU memory belongs to
  * its own pool allocator (such as Julia's CUDA.jl pool), or a time step being
  * captured into a CUDA graph, where cudaMalloc/cudaFree are not allowed.
  * a, b: device arrays of n doubles; *result: a device double, written
@@ -462,9 +465,10 @@ int pcf_set_network(pcf_handle *h, pcf_net *net);
  * stream).  No handle is needed and nothing is allocated: the scratch is a
  * fixed 64 KB __device__ array that every GPU loading the library holds until
  * the process exits.  n must not exceed 268,435,456 (PCF_ERANGE otherwise).
- * The first call on a device looks up the scratch address; make that call
- * before any stream capture.  All calls share the scratch, so calls that may
- * overlap on the GPU (on different streams) race and must be serialised. */
+ * The first call on a device (and the first after the device's context was
+ * re-created, e.g. by cudaDeviceReset) looks up the scratch address; make that
+ * call before any stream capture.  All calls share the scratch, so calls that
+ * may overlap on the GPU (on different streams) race and must be serialised. */
 int pcf_global_dot_noalloc(const double *a, const double *b, long long n, double *result, void *stream);
 int pcf_profile_enable(pcf_handle *h, int on);  /* also clears the accumulators */
 int pcf_profile_read(const pcf_handle *h, int tag, double *ms, long long *count, double *bytes);

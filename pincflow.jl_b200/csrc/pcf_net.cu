@@ -4,6 +4,7 @@
 // the GPU with the kernels in this file (forward, backward, Adam).  The dense
 // layers run on the tensor cores through pcf_umma.cuh.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -17,15 +18,20 @@ namespace net {
 
 using bf16 = __nv_bfloat16;
 
+// The dynamic shared-memory attribute is a per-device setting of a kernel, so
+// it is recorded per device (up to 64) and kernel instance.
 template <int NT>
 static int launch_gemm(const umma::GemmArgs &g, int ksplit, cudaStream_t st) {
-    static bool attr_set = false;
+    static std::atomic<unsigned long long> attr_set{0};
     constexpr int smem = umma::gemm_smem_bytes<NT>();
-    if (!attr_set) {
+    int dev = 0;
+    PCF_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return PCF_ENODEVICE;
+    if (!(attr_set.load() >> dev & 1ull)) {
         const cudaError_t e =
             cudaFuncSetAttribute(umma::k_gemm_bf16<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return pcf_set_cuda_error(e);
-        attr_set = true;
+        attr_set.fetch_or(1ull << dev);
     }
     const int ksteps = (g.K + 63) / 64;
     if (ksplit > ksteps) ksplit = ksteps;

@@ -11,6 +11,8 @@
 // (the partial sums and the last-block ticket) in a file-scope __device__
 // array of fixed size, which every GPU that loads the library holds until
 // the process exits.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "pcf_internal.cuh"
@@ -76,19 +78,42 @@ __global__ void __launch_bounds__(256) k_dot_noalloc(const double *__restrict__ 
 
 std::mutex g_noalloc_mutex;
 NoallocScratch *g_noalloc_ptr[64] = {};
+CUcontext g_noalloc_ctx[64] = {};
+
+// The driver's cuCtxGetCurrent, resolved once through the runtime (the
+// library does not link libcuda), or null if it cannot be resolved.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return static_cast<CtxGetCurrentFn>(nullptr);
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    return fn;
+}
 
 // Device address of the scratch array for the current device.  In host code
 // the symbol g_noalloc_scratch is only a host-side stand-in, so the address is
-// looked up once per device with cudaGetSymbolAddress.
+// looked up with cudaGetSymbolAddress on the first call on a device, and again
+// whenever the device's current context has changed (after a
+// cudaDeviceReset the module is loaded anew and the old address is stale).
 int noalloc_scratch(NoallocScratch **p) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return PCF_ENODEVICE;
+    CUcontext ctx = nullptr;
+    if (CtxGetCurrentFn f = ctx_get_current()) f(&ctx);
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
+    if (!g_noalloc_ptr[dev] || g_noalloc_ctx[dev] != ctx) {
         void *q = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&q, g_noalloc_scratch);
         if (e != cudaSuccess) return pcf_set_cuda_error(e);
         g_noalloc_ptr[dev] = static_cast<NoallocScratch *>(q);
+        // the context is current only once the runtime has set it up
+        if (CtxGetCurrentFn f = ctx_get_current()) f(&ctx);
+        g_noalloc_ctx[dev] = ctx;
     }
     *p = g_noalloc_ptr[dev];
     return PCF_OK;

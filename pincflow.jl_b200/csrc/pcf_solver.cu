@@ -305,7 +305,9 @@ static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_ov
             return PCF_OK;
         }
     }
-    ProfScope ps(h, tag, (double)words * sizeof(T) * (double)a.n);
+    // a guarded reliable-update launch returns at once unless an update is
+    // pending; its bytes are counted per update performed (reliable_bytes)
+    ProfScope ps(h, tag, a.guard_update ? 0.0 : (double)words * sizeof(T) * (double)a.n);
     k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF><<<grid, block, 0, h->stream>>>(a, kc);
     PCF_CUDA_TRY(cudaGetLastError());
     return PCF_OK;
@@ -1060,6 +1062,13 @@ static int learned_stage(pcf_handle *h, const Work<float> &w, const float *bvec,
     k_learned_combine<<<vec_grid(h->d.n), 256, 0, h->stream>>>(z, cc, w.post, h->d.n, guard);
     PCF_CUDA_TRY(cudaGetLastError());
     return PCF_OK;
+}
+
+// Profiler bytes of the FP64 true-residual applies of `nupdates` reliable
+// updates: 25 coefficient planes + x + b + r words per cell.
+static void reliable_bytes(pcf_handle *h, int nupdates) {
+    if (h->prof_on && h->prof && nupdates > 0)
+        h->prof_acc[PCF_PROF_RELIABLE].bytes += (double)nupdates * 28.0 * sizeof(double) * (double)h->d.n;
 }
 
 // Reliable update (mixed precision): x64 += bnorm64 x32, r64 = b - A64 x64
@@ -2375,6 +2384,7 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
         if (rc) return rc;
         res->niter += ro.iters;
         res->nrefine += ro.nupdates;
+        reliable_bytes(h, ro.nupdates);
         if (ro.nupdates > 0) rel = ro.res;
         if (ro.converged) break;
         if (ro.status == PCF_EBREAKDOWN && restarts < prm->max_refinements && res->niter < maxit) {
@@ -2854,6 +2864,7 @@ int pcf_ensemble_solve_device(pcf_ensemble *e, const double *const *d_rhs, const
             if ((rc = run_finish<float>(h, w, c, false, 0, &xe, &ro))) return rc;
             res[q].niter = ro.iters;
             res[q].nrefine = ro.nupdates;
+            reliable_bytes(h, ro.nupdates);
             res[q].status = ro.status;
             res[q].residual = res[q].true_residual = ro.nupdates > 0 ? ro.res : 1.0;
             res[q].errflag = ro.converged ? 0 : 1;
