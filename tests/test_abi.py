@@ -131,8 +131,13 @@ def _c_struct_fields(name):
     return fields
 
 
+JL_PKG = os.path.join(REPO, "pincflow.jl_b200", "julia", "PinCFlowGPU")
+JL_CORE = os.path.join(JL_PKG, "src", "PinCFlowGPU.jl")
+JL_EXT = os.path.join(JL_PKG, "ext", "PinCFlowGPUExt.jl")
+
+
 def _julia_struct_fields(name):
-    src = open(os.path.join(REPO, "pincflow.jl_b200", "julia", "PinCFlowGPU.jl")).read()
+    src = open(JL_CORE).read()
     body = re.search(r"(?:mutable )?struct " + name + r"\n(.*?)\nend", src, flags=re.S).group(1)
     return [(n, t) for n, t in re.findall(r"(\w+)::(\w+)", body)]
 
@@ -160,7 +165,7 @@ def test_julia_ccalls_bind_declared_symbols_with_their_arity():
     """Every ccall of the Julia binding names a function of the header and
     lists as many argument types as the header has parameters (Julia is not
     installed here, so this is the check that the binding would link)."""
-    src = open(os.path.join(REPO, "pincflow.jl_b200", "julia", "PinCFlowGPU.jl")).read()
+    src = open(JL_CORE).read() + open(JL_EXT).read()
     declared = set(declared_functions())
     calls = re.findall(r"ccall\(\(:(pcf_\w+),\s*LIB\),\s*\w+(?:\{\w+\})?,\s*\((.*?)\),", src, flags=re.S)
     assert len(calls) >= 9
@@ -168,3 +173,27 @@ def test_julia_ccalls_bind_declared_symbols_with_their_arity():
         assert name in declared, name
         n = len([t for t in re.split(r",\s*", types.strip()) if t])
         assert n == _header_arity(name), (name, n, _header_arity(name))
+
+
+def test_julia_package_extension_layout():
+    """PinCFlowGPU is a Julia package whose extension PinCFlowGPUExt loads with
+    PinCFlow (a weak dependency, PinCFlow.jl's own UUID from its Project.toml),
+    the mechanism the reference itself uses for CairoMakie (PinCFlowMakieExt).
+    The extension adds Float64 methods of the three reference functions and
+    falls back to the reference's AbstractFloat methods with `invoke`."""
+    import tomllib
+    with open(os.path.join(JL_PKG, "Project.toml"), "rb") as fh:
+        proj = tomllib.load(fh)
+    assert proj["name"] == "PinCFlowGPU"
+    assert proj["weakdeps"] == {"PinCFlow": "230a4047-f24c-41d9-8d93-b3b8a5ef3847"}
+    assert proj["extensions"] == {"PinCFlowGPUExt": "PinCFlow"}
+    core, ext = open(JL_CORE).read(), open(JL_EXT).read()
+    assert re.search(r"^module PinCFlowGPU$", core, flags=re.M)
+    assert re.search(r"^module PinCFlowGPUExt$", ext, flags=re.M)
+    assert not re.search(r"^using PinCFlow\b", core, flags=re.M)  # the core module loads without PinCFlow
+    for fn, n in (("PS.solve_poisson!", 4), ("PS.apply_corrector!", 3), ("IN.implicit_integration!", 8)):
+        m = re.search(r"^function " + re.escape(fn) + r"\((.*?)\)$", ext, flags=re.M | re.S)
+        assert m, fn
+        assert len(re.findall(r"::", m.group(1))) == n, fn
+        assert "::Float64" in m.group(1)
+        assert re.search(r"invoke\(" + re.escape(fn), ext), fn
