@@ -158,6 +158,14 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def load_bf16_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return float(json.load(fh)["bf16_tflops"])
+    return 1590.0
+
+
 def ncu_traffic(config, kernel="apply32"):
     """Per-launch DRAM bytes of a stencil family from the committed ncu summary, or None."""
     p = os.path.join(REPO, "profiles", f"stencil_{kernel}_{config}.txt")
@@ -830,6 +838,33 @@ def learned_arm(args, s, cfg, d_rhs, d_rho, d_betar, d_dpip, local_rank):
                      "true_residual": infos[-1].true_residual, "converged": not infos[-1].errflag,
                      "loss_first_epoch": float(np.mean(loss[role][:len(pairs_ws)])),
                      "loss_last_epoch": float(np.mean(loss[role][-len(pairs_ws):]))}
+    # the fused network kernel alone on this grid: CUDA events around
+    # back-to-back applications on an FP32 field (the stage's case)
+    import torch
+    shape = (dom.nz, dom.ny, dom.nx)
+    f_in = torch.randn(shape, dtype=torch.float32, device=d_rhs.device)
+    f_out = torch.empty_like(f_in)
+    st = torch.cuda.Stream(d_rhs.device)  # a stream of its own: a null handle would mean the network's stream
+    net = nets["stage"]
+    torch.cuda.synchronize()
+    for _ in range(3):
+        net.apply_device(f_in.data_ptr(), f_out.data_ptr(), shape, stream=st.cuda_stream)
+    reps = 20
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(reps):
+        net.apply_device(f_in.data_ptr(), f_out.data_ptr(), shape, stream=st.cuda_stream)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    cols = dom.nx * dom.ny
+    flop = cols * 2.0 * (2 * 64 * 576 + 64 * 256 + 256 * 256 + 256 * 64)
+    peak_tf = load_bf16_peak()
+    out["network_kernel"] = {"kernel": "k_net_fused (gather, 3x3 convolution, MLP and output convolution in one "
+                                       "cooperative tcgen05 kernel)", "columns": cols, "ms_per_application": ms,
+                             "flop_per_application": flop, "tflops": flop / (ms * 1e-3) / 1e12,
+                             "tensor_peak_tflops": peak_tf, "frac": flop / (ms * 1e-3) / 1e12 / peak_tf}
     for n in nets.values():
         n.close()
     return out
@@ -1041,8 +1076,8 @@ def main():
     ap.add_argument("--ref-iterations", type=int, default=450)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned arm")
-    ap.add_argument("--learned-pairs", type=int, default=32, help="training pairs of each network")
-    ap.add_argument("--learned-epochs", type=int, default=4)
+    ap.add_argument("--learned-pairs", type=int, default=48, help="training pairs of each network")
+    ap.add_argument("--learned-epochs", type=int, default=8)
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

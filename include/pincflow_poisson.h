@@ -413,14 +413,19 @@ int pcf_gemm_bf16(const unsigned short *A, long long a_len, long long a_rs, long
                   int ksplit, float *D);
 
 /* ---- learned warm start / preconditioner (no reference counterpart) ------
- * A per-column network: the column of a field is resampled to 64 levels,
- * then h1 = relu(W1 x + b1), h1 += dwconv3x3(h1), h2 = relu(W2 h1 + b2),
- * h2 += dwconv3x3(h2), y = W3 h2 + b3 (64 -> 256 -> 256 -> 64, depthwise 3x3
- * horizontal convolutions, periodic), resampled back.  BF16 weights and
- * activations, FP32 accumulation on the tensor cores; FP32 master weights
- * trained with Adam on the residual-weighted loss sum (N(b) - x)^2 / sum x^2.
- * Parameter order: W1[256][64], b1[256], K1[256][9], W2[256][256], b2[256],
- * K2[256][9], W3[64][256], b3[64] (tap = (dj+1)*3 + (di+1)). */
+ * A per-column MLP fused with full 3x3 horizontal convolutions.  The column
+ * of a field is resampled to 64 levels (x); with im2col(v)[c] the periodic
+ * 3x3 window of columns around c (tap t = (dj+1)*3 + (di+1)):
+ *   a = relu(C1 im2col(x) + c1), h1 = relu(W1 a + b1), h2 = relu(W2 h1 + b2),
+ *   z = W3 h2 + b3, y = z + C2 im2col(z) + c2 (64 -> 256 -> 256 -> 64),
+ * resampled back.  172,736 parameters; BF16 weights and activations, FP32
+ * accumulation on the tensor cores (tcgen05); FP32 master weights trained
+ * with Adam on the residual-weighted loss sum (N(b) - x)^2 / sum x^2.  An
+ * application (pcf_net_apply_device, pcf_net_forward) is one cooperative
+ * kernel; training keeps the activations and runs the layers as GEMMs.
+ * Parameter order: C1[64][9][64] ([out][tap][in]), c1[64], W1[256][64],
+ * b1[256], W2[256][256], b2[256], W3[64][256], b3[64], C2[64][9][64], c2[64].
+ * A new network outputs zero (W3, C2 and the biases start at zero). */
 typedef struct pcf_net pcf_net;
 int pcf_net_num_params(void);
 int pcf_net_create(pcf_net **net, int device, long long max_columns, unsigned seed);
@@ -439,6 +444,12 @@ int pcf_net_apply_device(pcf_net *net, const void *in, int nx, int ny, int nz, d
  * (nullable host buffer), Adam update when lr > 0 */
 int pcf_net_train_step(pcf_net *net, const float *b, const float *x, int nx, int ny, int nz, double lr,
                        double *loss, float *grad);
+/* Adam over `count` samples given as host arrays b, x (each nz*ny*nx FP32,
+ * normalised; sample q at offset q*nz*ny*nx), uploaded once for the call:
+ * `epochs` passes in an order drawn from `seed`; losses (nullable,
+ * count*epochs doubles) receives every step's loss before its update. */
+int pcf_net_train(pcf_net *net, const float *b, const float *x, int count, int nx, int ny, int nz, int epochs,
+                  double lr, unsigned seed, double *losses);
 /* loss and gradients for host arrays, no update (gradient check) */
 int pcf_net_gradients(pcf_net *net, const double *b, const double *x, int nx, int ny, int nz, double *loss,
                       float *grad);

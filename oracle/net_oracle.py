@@ -1,12 +1,21 @@
-"""CPU oracle of the learned warm-start network (test infrastructure only).
+"""CPU oracle of the learned network (test infrastructure only).
 
 Float64 numpy restatement of the network in pincflow.jl_b200/csrc/pcf_net.cu
 (forward, residual-weighted loss, backward), used to check the GPU kernels'
-outputs and gradients.  With bf16=True it rounds to BF16 exactly where the
-GPU stores BF16 (inputs and activations that feed the tensor-core GEMMs, the
-weight copies and the upstream gradients dY, dZ); with bf16=False it is the
-exact float64 network, whose analytic gradient tests/test_oracle_kat.py
-pins against finite differences.
+outputs and gradients.  With bf=True it rounds to BF16 exactly where the
+GPU stores BF16 (the gathered input, the activations and the convolution
+windows that feed the tensor cores, the weight copies and the upstream
+gradients); with bf=False it is the exact float64 network, whose analytic
+gradient tests/test_oracle_kat.py pins against finite differences.
+
+The network, per column c of the nx x ny grid (x = the column resampled to
+L = 64 levels), with periodic 3 x 3 windows im2col(v)[c] = (v[nbr(c, t)])_t:
+    a  = relu(C1 im2col(x) + c1)        64     C1: 64 x (9 * 64)
+    h1 = relu(W1 a + b1)                256
+    h2 = relu(W2 h1 + b2)               256
+    z  = W3 h2 + b3                     64
+    y  = z + C2 im2col(z) + c2          64     C2: 64 x (9 * 64)
+Tap t = (dj + 1) * 3 + (di + 1) is the neighbour (i + di, j + dj).
 
 The network has no counterpart in the reference; its oracle is written from
 the architecture, not from reference code.
@@ -16,9 +25,11 @@ from __future__ import annotations
 import numpy as np
 
 L, HID, TAPS = 64, 256, 9
-SIZES = [("W1", (HID, L)), ("b1", (HID,)), ("K1", (HID, TAPS)), ("W2", (HID, HID)), ("b2", (HID,)),
-         ("K2", (HID, TAPS)), ("W3", (L, HID)), ("b3", (L,))]
+KC = TAPS * L  # 576: the im2col width
+SIZES = [("C1", (L, KC)), ("c1", (L,)), ("W1", (HID, L)), ("b1", (HID,)), ("W2", (HID, HID)), ("b2", (HID,)),
+         ("W3", (L, HID)), ("b3", (L,)), ("C2", (L, KC)), ("c2", (L,))]
 NPARAM = sum(int(np.prod(s)) for _, s in SIZES)
+BIASES = ("c1", "b1", "b2", "b3", "c2")
 
 
 def unpack(p):
@@ -73,29 +84,39 @@ def _shift(H, ny, nx, tap):
     return np.roll(np.roll(G, -dj, axis=0), -di, axis=1).reshape(ny * nx, -1)
 
 
-def conv(H, K, ny, nx):
-    return H + sum(K[:, t][None, :] * _shift(H, ny, nx, t) for t in range(TAPS))
+def im2col(H, ny, nx):
+    return np.concatenate([_shift(H, ny, nx, t) for t in range(TAPS)], axis=1)
+
+
+def col2im(D, ny, nx):
+    """Adjoint of im2col: sum over taps of the window gradients sent back to
+    the columns they were read from."""
+    F = D.shape[1] // TAPS
+    return sum(_shift(D[:, t * F:(t + 1) * F], ny, nx, TAPS - 1 - t) for t in range(TAPS))
 
 
 def forward(p, b, bf=True):
     P = unpack(p)
     nz, ny, nx = b.shape
     r = bf16 if bf else (lambda x: np.asarray(x, dtype=np.float64))
-    W1, W2, W3 = r(P["W1"]), r(P["W2"]), r(P["W3"])
+    C1, W1, W2, W3, C2 = r(P["C1"]), r(P["W1"]), r(P["W2"]), r(P["W3"]), r(P["C2"])
     x0 = r(gather(b))
-    h1 = r(np.maximum(x0 @ W1.T + P["b1"], 0))
-    h1c = r(conv(h1, P["K1"], ny, nx))
-    h2 = r(np.maximum(h1c @ W2.T + P["b2"], 0))
-    h2c = r(conv(h2, P["K2"], ny, nx))
-    y = h2c @ W3.T + P["b3"]
-    cache = dict(x0=x0, h1=h1, h1c=h1c, h2=h2, h2c=h2c, y=y, W1=W1, W2=W2, W3=W3, shape=(nz, ny, nx))
+    xi = im2col(x0, ny, nx)
+    a = r(np.maximum(xi @ C1.T + P["c1"], 0))
+    h1 = r(np.maximum(a @ W1.T + P["b1"], 0))
+    h2 = r(np.maximum(h1 @ W2.T + P["b2"], 0))
+    z = r(h2 @ W3.T + P["b3"])
+    zi = im2col(z, ny, nx)
+    y = z + zi @ C2.T + P["c2"]
+    cache = dict(x0=x0, xi=xi, a=a, h1=h1, h2=h2, z=z, zi=zi, y=y, C1=C1, W1=W1, W2=W2, W3=W3, C2=C2,
+                 shape=(nz, ny, nx))
     return scatter(y, nz, ny, nx), cache
 
 
 def loss_and_grad(p, b, x, bf=True):
     """Residual-weighted loss sum (y - t)^2 / sum t^2 on the L-level columns and
-    its gradient with respect to the packed parameters."""
-    P = unpack(p)
+    its gradient with respect to the packed parameters (BF16 roundings are
+    passed through unchanged by the gradient)."""
     r = bf16 if bf else (lambda v: np.asarray(v, dtype=np.float64))
     _, c = forward(p, b, bf)
     nz, ny, nx = c["shape"]
@@ -106,23 +127,22 @@ def loss_and_grad(p, b, x, bf=True):
     dy = 2 * d / st2
     dyb = r(dy)
     g = {}
-    g["b3"] = dy.sum(0)
-    g["W3"] = dyb.T @ c["h2c"]
-    dh2c = dyb @ c["W3"]
-
-    def conv_bwd(dhc, h, K):
-        dh = dhc + sum(K[:, TAPS - 1 - t][None, :] * _shift(dhc, ny, nx, t) for t in range(TAPS))
-        dK = np.stack([np.sum(dhc * _shift(h, ny, nx, t), axis=0) for t in range(TAPS)], axis=1)
-        dz = dh * (h > 0)
-        return dz, dK
-
-    dz2, g["K2"] = conv_bwd(dh2c, c["h2"], P["K2"])
-    g["b2"] = dz2.sum(0)
-    dz2b = r(dz2)
-    g["W2"] = dz2b.T @ c["h1c"]
-    dh1c = dz2b @ c["W2"]
-    dz1, g["K1"] = conv_bwd(dh1c, c["h1"], P["K1"])
-    g["b1"] = dz1.sum(0)
-    dz1b = r(dz1)
-    g["W1"] = dz1b.T @ c["x0"]
+    g["c2"] = dy.sum(0)
+    g["C2"] = dyb.T @ c["zi"]
+    dz = dy + col2im(dyb @ c["C2"], ny, nx)
+    dzb = r(dz)
+    g["b3"] = dz.sum(0)
+    g["W3"] = dzb.T @ c["h2"]
+    dg2 = (dzb @ c["W3"]) * (c["h2"] > 0)
+    dg2b = r(dg2)
+    g["b2"] = dg2.sum(0)
+    g["W2"] = dg2b.T @ c["h1"]
+    dg1 = (dg2b @ c["W2"]) * (c["h1"] > 0)
+    dg1b = r(dg1)
+    g["b1"] = dg1.sum(0)
+    g["W1"] = dg1b.T @ c["a"]
+    dga = (dg1b @ c["W1"]) * (c["a"] > 0)
+    dgab = r(dga)
+    g["c1"] = dga.sum(0)
+    g["C1"] = dgab.T @ c["xi"]
     return loss, pack(g)

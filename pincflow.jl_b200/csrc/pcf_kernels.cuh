@@ -145,6 +145,11 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *sh) {
 
 __device__ __forceinline__ bool finite(double x) { return isfinite(x); }
 
+// A recursive residual this many times RMS(b) marks the FP32 iteration of the
+// mixed solve as diverged (PCF_EBREAKDOWN: the solve restarts from its FP64
+// residual, without a learned stage); converging runs stay below 1e2.
+constexpr double kDivergedResidual = 1e3;
+
 // Scalar step run by one thread once all partial sums of a kernel are in.
 template <int NV>
 __device__ void finalize(const ReduceCtx &c, const double (&s)[NV]) {
@@ -210,7 +215,12 @@ __device__ void finalize(const ReduceCtx &c, const double (&s)[NV]) {
                 // residual drop by ru_delta, on reaching tol, or at the cap
                 const double rel = res;
                 if (rel > k->res_max) k->res_max = rel;
-                if (rel <= k->tol || rel <= k->ru_delta * k->res_max || k->iter >= k->maxit) {
+                if (rel > kDivergedResidual) {
+                    // a diverging iteration (e.g. an unsuitable learned stage): stop
+                    // before its correction is folded into the FP64 solution
+                    k->status = PCF_EBREAKDOWN;
+                    k->done = 1;
+                } else if (rel <= k->tol || rel <= k->ru_delta * k->res_max || k->iter >= k->maxit) {
                     k->update = 1;
                     k->alpha_omega = k->alpha / k->omega;
                 } else {

@@ -1,8 +1,35 @@
-// pcf_net.cu -- the learned preconditioner / warm start: a per-column MLP
-// (64 -> 256 -> 256 -> 64) interleaved with depthwise 3x3 horizontal
-// convolutions, BF16 weights and activations, FP32 accumulation, trained on
-// the GPU with the kernels in this file (forward, backward, Adam).  The dense
-// layers run on the tensor cores through pcf_umma.cuh.
+// pcf_net.cu -- the learned preconditioner / warm start (no reference
+// counterpart): a per-column MLP fused with full 3x3 horizontal
+// convolutions, BF16 weights and activations, FP32 accumulation on the
+// tensor cores, trained on the GPU with the kernels in this file (forward,
+// backward, Adam).
+//
+// Per column c of the nx x ny grid, x = the column of a field resampled to
+// L = 64 levels and im2col(v)[c] = (v[nbr(c, t)], t = 0..8) its periodic
+// 3 x 3 window (tap t = (dj+1)*3 + (di+1) is the neighbour (i+di, j+dj)):
+//   a  = relu(C1 im2col(x) + c1)        64      C1: 64 x 576
+//   h1 = relu(W1 a + b1)                256
+//   h2 = relu(W2 h1 + b2)               256
+//   z  = W3 h2 + b3                     64
+//   y  = z + C2 im2col(z) + c2          64      C2: 64 x 576
+// 172,736 parameters.
+//
+// Two implementations of the forward pass:
+//  * the application (pcf_net_apply_device: warm start, preconditioner
+//    stage) is ONE cooperative kernel, k_net_fused: it gathers the input
+//    columns into a haloed BF16 array, then for every tile of 16 x 8 columns
+//    runs the input convolution and the three dense layers back to back on
+//    tcgen05 with the activations in tensor memory and shared memory (TMA
+//    brings each 3 x 3 window and each weight K-block into shared memory),
+//    writes z, and after a grid-wide barrier runs the output convolution and
+//    resamples y back onto the field's levels;
+//  * training (pcf_net_train_step, pcf_net_train) keeps every activation for
+//    the backward pass: the convolutions become GEMMs over im2col matrices on
+//    the general tcgen05 GEMM of pcf_umma.cuh.
+// Both round to BF16 at the same points, so they agree to FP32 summation
+// order.
+#include <cuda.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -17,6 +44,26 @@ namespace pcf {
 namespace net {
 
 using bf16 = __nv_bfloat16;
+
+constexpr int L = 64, HID = 256, TAPS = 9, KC = TAPS * L;  // KC: the im2col width, 576
+constexpr int OFF_C1 = 0;                    // [L][KC]
+constexpr int OFF_c1 = OFF_C1 + L * KC;      // [L]
+constexpr int OFF_W1 = OFF_c1 + L;           // [HID][L]
+constexpr int OFF_B1 = OFF_W1 + HID * L;     // [HID]
+constexpr int OFF_W2 = OFF_B1 + HID;         // [HID][HID]
+constexpr int OFF_B2 = OFF_W2 + HID * HID;   // [HID]
+constexpr int OFF_W3 = OFF_B2 + HID;         // [L][HID]
+constexpr int OFF_B3 = OFF_W3 + L * HID;     // [L]
+constexpr int OFF_C2 = OFF_B3 + L;           // [L][KC]
+constexpr int OFF_c2 = OFF_C2 + L * KC;      // [L]
+constexpr int NPARAM = OFF_c2 + L;           // 172,736
+// the BF16 weight copies, one array: C1 | W1 | W2 | W3 | C2
+constexpr int WB_C1 = 0, WB_W1 = WB_C1 + L * KC, WB_W2 = WB_W1 + HID * L, WB_W3 = WB_W2 + HID * HID,
+              WB_C2 = WB_W3 + L * HID, WB_N = WB_C2 + L * KC;
+constexpr int KSPLIT = 32;                   // split-K of the weight-gradient GEMMs
+constexpr int RED_CHUNK = 64;                // columns per block of the column reductions
+
+// ------------------------------------------------------------ launchers --
 
 // The dynamic shared-memory attribute is a per-device setting of a kernel, so
 // it is recorded per device (up to 64) and kernel instance.
@@ -50,42 +97,48 @@ static int gemm(const umma::GemmArgs &g, int ksplit, cudaStream_t st) {
     return PCF_ERANGE;
 }
 
-// ------------------------------------------------------------------ model --
-//
-// Per column c of the nx x ny grid (input: the column of a field resampled to
-// L = 64 levels, scaled):
-//   h1  = relu(W1 x + b1)                 (256)
-//   h1c = h1 + dwconv3x3(h1; K1)          depthwise, periodic in x and y
-//   h2  = relu(W2 h1c + b2)               (256)
-//   h2c = h2 + dwconv3x3(h2; K2)
-//   y   = W3 h2c + b3                     (64, resampled back to nz levels)
-// Activations are row-major [column][feature]; BF16 where they feed a GEMM.
-constexpr int L = 64, HID = 256, TAPS = 9;
-constexpr int OFF_W1 = 0;                    // [HID][L]
-constexpr int OFF_B1 = OFF_W1 + HID * L;     // [HID]
-constexpr int OFF_K1 = OFF_B1 + HID;         // [HID][9], tap = (dj+1)*3 + (di+1)
-constexpr int OFF_W2 = OFF_K1 + HID * TAPS;  // [HID][HID]
-constexpr int OFF_B2 = OFF_W2 + HID * HID;
-constexpr int OFF_K2 = OFF_B2 + HID;
-constexpr int OFF_W3 = OFF_K2 + HID * TAPS;  // [L][HID]
-constexpr int OFF_B3 = OFF_W3 + L * HID;     // [L]
-constexpr int NPARAM = OFF_B3 + L;           // 103,488
-constexpr int KSPLIT = 32;                   // split-K of the weight-gradient GEMMs
-constexpr int RED_CHUNK = 64;                // columns per block of the column reductions
+static umma::GemmArgs gargs(int M, int N, int K, const bf16 *A, long long a_rs, long long a_ks, const bf16 *B,
+                            long long b_rs, long long b_ks, int *err) {
+    umma::GemmArgs g{};
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.A = A;
+    g.a_rs = a_rs;
+    g.a_ks = a_ks;
+    g.B = B;
+    g.b_rs = b_rs;
+    g.b_ks = b_ks;
+    g.error = err;
+    return g;
+}
+
+// ------------------------------------------------------------------ state --
 
 struct Net {
     int device;
     cudaStream_t stream;
-    long long cap;  // column capacity
+    long long cap;  // column capacity of an application
     float *param, *grad, *m, *v;
-    bf16 *w1b, *w2b, *w3b;
-    bf16 *x0, *h1, *h1c, *h2, *h2c, *dyb, *dz2, *dz1;
-    float *y, *t, *dyf, *dh2c, *dh1c, *part, *red;
-    double *scal;  // [0] loss numerator, [1] sum T^2, [2] loss
+    bf16 *wb;       // BF16 weight copies (WB_* offsets)
+    // the fused application: haloed input columns and z, grid barrier
+    bf16 *xh, *zh;
+    long long hcap;  // haloed columns xh / zh hold
+    unsigned *bar;
+    CUtensorMap wmap[5];  // C1, W1, W2, W3, C2 (K-block boxes)
+    CUtensorMap xmap, zmap;
+    int map_nx, map_ny;
+    // training activations and gradients (allocated on first use, tcap columns)
+    long long tcap;
+    bf16 *x0, *xi, *a, *h1, *h2, *zb, *zi, *dyb, *dzb, *dg2b, *dg1b, *dgab;
+    float *y, *t, *dyf, *dzf, *dh, *dzi, *part;
+    double *red, *scal;   // loss partial sums; [0] numerator, [1] sum t^2, [2] loss
     int *err;
     int step;
     int no_bias;  // biases held at zero: N is then positively homogeneous, N(a x) = a N(x) for a > 0
 };
+
+// ------------------------------------------------------- column transfers --
 
 // level position of output level l when resampling n_in levels to n_out
 __device__ __forceinline__ void interp_pos(int l, int n_in, int n_out, int &k0, int &k1, float &f) {
@@ -115,21 +168,6 @@ __global__ void k_gather(const TIn *__restrict__ field, long long plane, int nz,
     X[c * L + l] = (TOut)(scale * v);
 }
 
-// Y[c][l] (L levels) -> field (nz levels): out = beta * out + scale * interp(Y)
-template <typename TOut>
-__global__ void k_scatter(const float *__restrict__ Y, long long plane, int nz, float scale, float beta,
-                          TOut *__restrict__ out) {
-    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (idx >= plane * nz) return;
-    const int k = (int)(idx / plane);
-    const long long c = idx % plane;
-    int l0, l1;
-    float f;
-    interp_pos(k, L, nz, l0, l1, f);
-    const float v = scale * ((1.f - f) * Y[c * L + l0] + f * Y[c * L + l1]);
-    out[idx] = beta == 0.f ? (TOut)v : (TOut)((float)beta * (float)out[idx] + v);
-}
-
 __device__ __forceinline__ long long nbr(long long c, int nx, int ny, int tap) {
     const int di = tap % 3 - 1, dj = tap / 3 - 1;
     const int i = (int)(c % nx), j = (int)(c / nx);
@@ -137,45 +175,39 @@ __device__ __forceinline__ long long nbr(long long c, int nx, int ny, int tap) {
     return (long long)jj * nx + ii;
 }
 
-// out = in + depthwise 3x3 conv(in), one thread per (column, channel)
-__global__ void k_dwconv(const bf16 *__restrict__ in, const float *__restrict__ Kw, int nx, int ny,
-                         bf16 *__restrict__ out) {
-    const long long c = blockIdx.x;
-    const int f = threadIdx.x;
-    float acc = __bfloat162float(in[c * HID + f]);
-#pragma unroll
-    for (int t = 0; t < TAPS; ++t) acc += Kw[f * TAPS + t] * __bfloat162float(in[nbr(c, nx, ny, t) * HID + f]);
-    out[c * HID + f] = __float2bfloat16(acc);
+// im2col of a [C][L] BF16 array: out[c][t*L + l] = H[nbr(c, t)][l], one thread per 16 bytes
+__global__ void k_im2col(const bf16 *__restrict__ H, long long C, int nx, int ny, bf16 *__restrict__ out) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= C * TAPS * (L / 8)) return;
+    const int q = (int)(idx % (L / 8));
+    const int t = (int)((idx / (L / 8)) % TAPS);
+    const long long c = idx / (TAPS * (L / 8));
+    const uint4 v = *reinterpret_cast<const uint4 *>(H + nbr(c, nx, ny, t) * L + q * 8);
+    *reinterpret_cast<uint4 *>(out + c * KC + t * L + q * 8) = v;
 }
 
-// Backward of h_c = h + dwconv(h) followed by h = relu(z):
-//   dh = dhc + conv^T(dhc), dz = dh * (h > 0)  (BF16, feeds the GEMMs)
-// per block of RED_CHUNK columns: partial sums of dz (bias gradient) and of
-// dhc[c] * h[nbr(c, t)] (kernel gradient), reduced later in block order.
-__global__ void k_dwconv_bwd(const float *__restrict__ dhc, const bf16 *__restrict__ h, const float *__restrict__ Kw,
-                             long long C, int nx, int ny, bf16 *__restrict__ dz, float *__restrict__ part_db,
-                             float *__restrict__ part_dk) {
-    const int f = threadIdx.x;
-    const long long c0 = (long long)blockIdx.x * RED_CHUNK;
-    float db = 0.f, dk[TAPS];
+// The adjoint of im2col plus the residual path of the output convolution:
+// dz[c][l] = dy[c][l] + sum_t D[nbr(c, 8 - t)][t*L + l] (FP32 and BF16)
+__global__ void k_col2im(const float *__restrict__ D, const float *__restrict__ dy, long long C, int nx, int ny,
+                         float *__restrict__ dz, bf16 *__restrict__ dzb) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= C * L) return;
+    const long long c = idx / L;
+    const int l = (int)(idx % L);
+    float acc = dy[idx];
 #pragma unroll
-    for (int t = 0; t < TAPS; ++t) dk[t] = 0.f;
-    for (long long c = c0; c < c0 + RED_CHUNK && c < C; ++c) {
-        float dh = dhc[c * HID + f];
-#pragma unroll
-        for (int t = 0; t < TAPS; ++t) {
-            // conv^T: the tap t of column nbr(c, 8 - t) reaches c
-            dh += Kw[f * TAPS + (TAPS - 1 - t)] * dhc[nbr(c, nx, ny, t) * HID + f];
-            dk[t] += dhc[c * HID + f] * __bfloat162float(h[nbr(c, nx, ny, t) * HID + f]);
-        }
-        const float z = __bfloat162float(h[c * HID + f]) > 0.f ? dh : 0.f;
-        dz[c * HID + f] = __float2bfloat16(z);
-        db += z;
-    }
-    part_db[(long long)blockIdx.x * HID + f] = db;
-#pragma unroll
-    for (int t = 0; t < TAPS; ++t) part_dk[((long long)blockIdx.x * HID + f) * TAPS + t] = dk[t];
+    for (int t = 0; t < TAPS; ++t) acc += D[nbr(c, nx, ny, TAPS - 1 - t) * KC + t * L + l];
+    dz[idx] = acc;
+    dzb[idx] = __float2bfloat16(acc);
 }
+
+// y += z (the output convolution's residual path)
+__global__ void k_add_bf16(float *__restrict__ y, const bf16 *__restrict__ z, long long n) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) y[i] += __bfloat162float(z[i]);
+}
+
+// ------------------------------------------------------------- reductions --
 
 // sum over the first dimension: out[j] = sum_b in[b * n + j] (fixed order)
 __global__ void k_sum_rows(const float *__restrict__ in, int rows, int n, float *__restrict__ out) {
@@ -183,6 +215,17 @@ __global__ void k_sum_rows(const float *__restrict__ in, int rows, int n, float 
     if (j >= n) return;
     float acc = 0.f;
     for (int b = 0; b < rows; ++b) acc += in[(long long)b * n + j];
+    out[j] = acc;
+}
+
+// the same for split-K partials of a transposed gradient: in[b][k][o]
+// (rows x K x O) summed into out[o][k]
+__global__ void k_sum_rows_t(const float *__restrict__ in, int rows, int K, int O, float *__restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;  // j = o * K + k
+    if (j >= K * O) return;
+    const int o = j / K, k = j % K;
+    float acc = 0.f;
+    for (int b = 0; b < rows; ++b) acc += in[((long long)b * K + k) * O + o];
     out[j] = acc;
 }
 
@@ -212,7 +255,9 @@ __global__ void k_loss_part(const float *__restrict__ Y, const float *__restrict
     }
 }
 
-__global__ void k_loss_final(const double *__restrict__ part, int nb, double *__restrict__ scal) {
+// final loss; also stored to log[slot] (log nullable)
+__global__ void k_loss_final(const double *__restrict__ part, int nb, double *__restrict__ scal, double *log,
+                             int slot) {
     double a = 0, b = 0;
     for (int i = 0; i < nb; ++i) {
         a += part[2 * i];
@@ -221,9 +266,10 @@ __global__ void k_loss_final(const double *__restrict__ part, int nb, double *__
     scal[0] = a;
     scal[1] = b;
     scal[2] = b > 0 ? a / b : a;
+    if (log) log[slot] = scal[2];
 }
 
-// dL/dY = 2 (Y - T) / sum T^2 (FP32 and BF16), and its column sums for db3
+// dL/dY = 2 (Y - T) / sum T^2 (FP32 and BF16)
 __global__ void k_dy(const float *__restrict__ Y, const float *__restrict__ T, long long n,
                      const double *__restrict__ scal, float *__restrict__ dyf, bf16 *__restrict__ dyb) {
     const double w = scal[1] > 0 ? 2.0 / scal[1] : 2.0;
@@ -234,7 +280,7 @@ __global__ void k_dy(const float *__restrict__ Y, const float *__restrict__ T, l
     }
 }
 
-// column sums of a [C][L] FP32 array, per block of RED_CHUNK columns
+// column sums of a [C][F] FP32 array, per block of RED_CHUNK columns
 __global__ void k_colsum_part(const float *__restrict__ a, long long C, int F, float *__restrict__ part) {
     const int f = threadIdx.x;
     const long long c0 = (long long)blockIdx.x * RED_CHUNK;
@@ -243,14 +289,42 @@ __global__ void k_colsum_part(const float *__restrict__ a, long long C, int F, f
     part[(long long)blockIdx.x * F + f] = acc;
 }
 
-// Adam (FP32 master weights), then refresh the BF16 copies of W1, W2, W3
-__device__ __forceinline__ bool is_bias(int i) {
-    return (i >= OFF_B1 && i < OFF_B1 + HID) || (i >= OFF_B2 && i < OFF_B2 + HID) || (i >= OFF_B3 && i < OFF_B3 + L);
+// backward through a ReLU: g = dh * (h > 0) as BF16, with the per-block
+// column sums of g (the bias gradient) for RED_CHUNK columns
+__global__ void k_relu_bwd(const float *__restrict__ dh, const bf16 *__restrict__ h, long long C, int F,
+                           bf16 *__restrict__ g, float *__restrict__ part) {
+    const int f = threadIdx.x;
+    const long long c0 = (long long)blockIdx.x * RED_CHUNK;
+    float acc = 0.f;
+    for (long long c = c0; c < c0 + RED_CHUNK && c < C; ++c) {
+        const float v = __bfloat162float(h[c * F + f]) > 0.f ? dh[c * F + f] : 0.f;
+        g[c * F + f] = __float2bfloat16(v);
+        acc += v;
+    }
+    part[(long long)blockIdx.x * F + f] = acc;
 }
 
+// ------------------------------------------------------------------ Adam --
+
+__host__ __device__ constexpr bool is_bias(int i) {
+    return (i >= OFF_c1 && i < OFF_c1 + L) || (i >= OFF_B1 && i < OFF_B1 + HID) ||
+           (i >= OFF_B2 && i < OFF_B2 + HID) || (i >= OFF_B3 && i < OFF_B3 + L) || (i >= OFF_c2 && i < OFF_c2 + L);
+}
+
+// index of parameter i in the BF16 weight copies, -1 for a bias
+__device__ __forceinline__ int wb_index(int i) {
+    if (i < OFF_c1) return WB_C1 + (i - OFF_C1);
+    if (i >= OFF_W1 && i < OFF_B1) return WB_W1 + (i - OFF_W1);
+    if (i >= OFF_W2 && i < OFF_B2) return WB_W2 + (i - OFF_W2);
+    if (i >= OFF_W3 && i < OFF_B3) return WB_W3 + (i - OFF_W3);
+    if (i >= OFF_C2 && i < OFF_c2) return WB_C2 + (i - OFF_C2);
+    return -1;
+}
+
+// Adam (FP32 master weights), then the BF16 copy of the updated weight
 __global__ void k_adam(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
                        float *__restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2,
-                       bf16 *__restrict__ w1b, bf16 *__restrict__ w2b, bf16 *__restrict__ w3b, int no_bias) {
+                       bf16 *__restrict__ wb, int no_bias) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (no_bias && is_bias(i)) return;  // held at zero
@@ -261,116 +335,758 @@ __global__ void k_adam(float *__restrict__ p, const float *__restrict__ g, float
     v[i] = vi;
     const float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
     p[i] = pi;
-    if (i >= OFF_W1 && i < OFF_W1 + HID * L) w1b[i - OFF_W1] = __float2bfloat16(pi);
-    if (i >= OFF_W2 && i < OFF_W2 + HID * HID) w2b[i - OFF_W2] = __float2bfloat16(pi);
-    if (i >= OFF_W3 && i < OFF_W3 + L * HID) w3b[i - OFF_W3] = __float2bfloat16(pi);
+    const int w = wb_index(i);
+    if (w >= 0) wb[w] = __float2bfloat16(pi);
 }
 
-__global__ void k_params_to_bf16(const float *__restrict__ p, bf16 *__restrict__ w1b, bf16 *__restrict__ w2b,
-                                 bf16 *__restrict__ w3b) {
+__global__ void k_params_to_bf16(const float *__restrict__ p, bf16 *__restrict__ wb) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < HID * L) w1b[i] = __float2bfloat16(p[OFF_W1 + i]);
-    if (i < HID * HID) w2b[i] = __float2bfloat16(p[OFF_W2 + i]);
-    if (i < L * HID) w3b[i] = __float2bfloat16(p[OFF_W3 + i]);
+    if (i >= NPARAM) return;
+    const int w = wb_index(i);
+    if (w >= 0) wb[w] = __float2bfloat16(p[i]);
 }
 
-static umma::GemmArgs gargs(int M, int N, int K, const bf16 *A, long long a_rs, long long a_ks, const bf16 *B,
-                            long long b_rs, long long b_ks, int *err) {
-    umma::GemmArgs g{};
-    g.M = M;
-    g.N = N;
-    g.K = K;
-    g.A = A;
-    g.a_rs = a_rs;
-    g.a_ks = a_ks;
-    g.B = B;
-    g.b_rs = b_rs;
-    g.b_ks = b_ks;
-    g.error = err;
-    return g;
+// ================================================= the fused application --
+//
+// One cooperative launch of 192-thread CTAs, one per SM (its shared memory
+// holds one), each owning all 512 TMEM columns:
+//   phase 0  gather: xh[(yh)(nx+2) + xh][l] = BF16(scale_in * column
+//            (xh-1, yh-1) of the input, resampled to L levels), periodic
+//            halo of one column included;
+//   barrier;
+//   phase 1  per tile of 16 x 8 columns (M = 128 rows): 9 K-steps of the
+//            input convolution (A = the TMA box of xh shifted by the tap, B =
+//            the tap's 64 x 64 block of C1), the dense layers W1 (1 step, A =
+//            the activations in shared memory), W2 (4 steps), W3 (4 steps);
+//            z (BF16) goes to zh, periodic images included;
+//   barrier;
+//   phase 2  per tile: 9 K-steps of the output convolution over zh, then
+//            y = z + C2 im2col(z) + c2, resampled to the nz levels of the
+//            output: out = beta * out + scale_out * y.
+// Warp roles: warp 4 (one thread) streams every TMA box of the CTA's K-steps
+// through a three-stage ring, as far ahead as the ring allows (the weights
+// and the windows of xh do not depend on the activations); warp 5 (one
+// thread) issues the tcgen05.mma of each K-step once its stage has landed,
+// frees the stage with tcgen05.commit, and signals each finished layer;
+// warps 0-3 (one TMEM lane = one tile row per thread) run the epilogues --
+// bias, ReLU, BF16 into the shared operand of the next layer, or z / y to
+// global memory -- and signal that the accumulator and operand are ready.
+// Shared-memory operand layout (TMA boxes land in it directly): K-major
+// without swizzle, row r of K-slice q (8 values, 16 bytes) at q * R * 16 +
+// r * 16 for an operand of R rows -- core matrices of 8 rows x 16 bytes are
+// contiguous, 128 B apart along M/N (SBO) and R * 16 B apart along K (LBO).
+// Every wait is bounded (2 s of %globaltimer); a role that gives up stops,
+// the others give up on their next wait, and all leave after the grid
+// barriers (bounded too) with the error flag set.
+
+constexpr int F_TX = 16, F_TY = 8, F_ROWS = F_TX * F_TY;  // tile = 128 rows
+constexpr int F_THREADS = 192;                             // warps 0-3 epilogue, 4 copies, 5 MMAs
+constexpr int F_STAGES = 3;
+constexpr int F_SZA = F_ROWS * L * 2;                      // 16 KB: an A K-block (128 x 64)
+constexpr int F_SZB = HID * L * 2;                         // 32 KB: a B K-block (up to 256 x 64)
+constexpr int F_OFF_A = 0;                                 // F_STAGES A slots
+constexpr int F_OFF_B = F_OFF_A + F_STAGES * F_SZA;        // F_STAGES B slots
+constexpr int F_OFF_ACT = F_OFF_B + F_STAGES * F_SZB;      // a: one A K-block
+constexpr int F_OFF_H = F_OFF_ACT + F_SZA;                 // h1 / h2: 4 A K-blocks; y in phase 2
+constexpr int F_OFF_BAR = F_OFF_H + 4 * F_SZA;
+constexpr int F_NBAR = 2 * F_STAGES + 2;                   // full[], empty[], acc_full, epi_done
+constexpr int F_SMEM = F_OFF_BAR + 8 * F_NBAR + 16;        // 229,456 bytes
+constexpr int F_TMEM_COLS = 512;
+constexpr int F_COL64 = 0, F_COL256 = 256;                 // accumulators: N = 64 and N = 256
+
+// The layers of a tile, in order: phase 1 runs C1, W1, W2, W3; phase 2 C2.
+enum FLayer { F_C1 = 0, F_W1 = 1, F_W2 = 2, F_W3 = 3, F_C2 = 4 };
+__host__ __device__ constexpr int f_steps(int l) { return l == F_W1 ? 1 : (l == F_W2 || l == F_W3) ? HID / 64 : TAPS; }
+__host__ __device__ constexpr int f_n(int l) { return (l == F_W1 || l == F_W2) ? HID : L; }
+__host__ __device__ constexpr bool f_conv(int l) { return l == F_C1 || l == F_C2; }
+
+struct FusedArgs {
+    const void *in;
+    void *out;
+    int nx, ny, nz;
+    float scale_in, scale_out, beta;
+    const float *param;  // FP32 parameters (the biases)
+    bf16 *xh, *zh;
+    unsigned *bar;       // grid barrier counter, zero at launch
+    int *err;
+};
+
+__device__ __forceinline__ void tma3(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+        "%4}], [%5];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
 }
 
-// Forward on the columns already gathered into net->x0 (C columns).
-static int forward(Net *n, long long C, int nx, int ny) {
-    cudaStream_t st = n->stream;
+__device__ __forceinline__ void tma4(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                     uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void arrive_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+// 16 consecutive FP32 accumulator columns of this thread's TMEM lane (row)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&f)[16]) {
+    uint32_t v[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 16; ++q) f[q] = __uint_as_float(v[q]);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    const __nv_bfloat162 p = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&p);
+}
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d)
+                 : "memory");
+}
+
+// barrier among the 128 epilogue threads only (named barrier 1)
+__device__ __forceinline__ void epilogue_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// Grid-wide barrier of a cooperative launch: one arrival per CTA on a
+// counter that starts at zero, wait until it reaches `target`; every thread's
+// generic writes before it become visible to TMA reads after it.  Bounded.
+// Returns false for every thread if the barrier gave up or any thread
+// arrived with ok = false.
+__device__ bool grid_barrier(unsigned *bar, unsigned target, bool ok) {
+    __syncwarp();  // a warp whose lane 0 ran a role alone reconverges first
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    __syncthreads();
+    int fail = ok ? 0 : 1;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+        uint64_t t0, t1;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+        for (;;) {
+            unsigned v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+            if (v >= target) break;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+            if (t1 - t0 > 2000000000ull) {
+                fail = 1;
+                break;
+            }
+            __nanosleep(64);
+        }
+    }
+    const bool passed = __syncthreads_or(fail) == 0;
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    return passed;
+}
+
+// accumulator columns [tcol, tcol + ncols) + bias, ReLU, as BF16 into the
+// shared K-blocks at dst (K-block b at dst + b * F_SZA); thread = row
+__device__ __forceinline__ void epi_to_smem(uint32_t tmem, uint32_t tcol, const float *bias, int ncols, bool relu,
+                                            uint32_t dst) {
+    const int warp = threadIdx.x >> 5, r = threadIdx.x;
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + tcol;
+#pragma unroll 1
+    for (int c0 = 0; c0 < ncols; c0 += 16) {
+        float f[16];
+        tmem_ld16(lane_base + (uint32_t)c0, f);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            f[q] += __ldg(bias + c0 + q);
+            if (relu) f[q] = fmaxf(f[q], 0.f);
+        }
+        const uint32_t blk = dst + (uint32_t)(c0 >> 6) * F_SZA + (uint32_t)r * 16;
+        const int q8 = (c0 & 63) >> 3;
+        st_shared_v4(blk + q8 * (F_ROWS * 16), pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]),
+                     pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
+        st_shared_v4(blk + (q8 + 1) * (F_ROWS * 16), pack_bf16x2(f[8], f[9]), pack_bf16x2(f[10], f[11]),
+                     pack_bf16x2(f[12], f[13]), pack_bf16x2(f[14], f[15]));
+    }
+}
+
+// Producer: the TMA boxes of one layer's K-steps into the ring.
+struct Producer {
+    uint32_t sa, sb, full[F_STAGES], empty[F_STAGES];
+    unsigned g;  // K-steps issued so far
+    __device__ bool layer(int l, const CUtensorMap *amap, const CUtensorMap *bmap, int x0, int y0) {
+        const bool conv = f_conv(l);
+        const uint32_t bytes = (uint32_t)f_n(l) * L * 2 + (conv ? (uint32_t)F_SZA : 0u);
+        for (int i = 0; i < f_steps(l); ++i, ++g) {
+            const int s = (int)(g % F_STAGES);
+            const unsigned use = g / F_STAGES;
+            // the stage's previous use must have been consumed by its MMAs
+            if (use > 0 && !mbar_wait(empty[s], (use - 1u) & 1u)) return false;
+            arrive_expect(full[s], bytes);
+            if (conv) tma4(sa + s * F_SZA, amap, 0, x0 + i % 3, y0 + i / 3, 0, full[s]);
+            tma3(sb + s * F_SZB, bmap, 0, 0, 8 * i, full[s]);
+        }
+        return true;
+    }
+};
+
+// MMA issuer: one layer's K-steps into its accumulator, then the layer's signal.
+struct Issuer {
+    uint32_t sa, sb, full[F_STAGES], empty[F_STAGES], acc_full, epi_done, tmem;
+    unsigned g, nepi;
+    bool first;
+    __device__ bool layer(int l, uint32_t abase) {
+        // the previous layer's epilogue has read its accumulator and written this layer's operand
+        if (!first) {
+            if (!mbar_wait(epi_done, nepi & 1u)) return false;
+            ++nepi;
+        }
+        first = false;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int nn = f_n(l);
+        const bool conv = f_conv(l);
+        const uint32_t idesc = umma::instr_desc(128, nn);
+        const uint32_t lbo_a = F_ROWS * 16, lbo_b = (uint32_t)nn * 16;
+        const uint32_t tcol = nn == HID ? F_COL256 : F_COL64;
+        for (int i = 0; i < f_steps(l); ++i, ++g) {
+            const int s = (int)(g % F_STAGES);
+            if (!mbar_wait(full[s], (g / F_STAGES) & 1u)) return false;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t abuf = conv ? sa + s * F_SZA : abase + (uint32_t)i * F_SZA;
+            const uint32_t bbuf = sb + s * F_SZB;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)  // K = 16 per instruction: two K-slices
+                mma_f16(tmem + tcol, umma::smem_desc(abuf + 2 * j * lbo_a, lbo_a, 128),
+                        umma::smem_desc(bbuf + 2 * j * lbo_b, lbo_b, 128), idesc, (i > 0 || j > 0) ? 1u : 0u);
+            mma_commit(empty[s]);
+        }
+        mma_commit(acc_full);
+        return true;
+    }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(F_THREADS, 1)
+    k_net_fused(const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mz,
+                const __grid_constant__ CUtensorMap mc1, const __grid_constant__ CUtensorMap mw1,
+                const __grid_constant__ CUtensorMap mw2, const __grid_constant__ CUtensorMap mw3,
+                const __grid_constant__ CUtensorMap mc2, const FusedArgs a) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + F_OFF_BAR);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + F_NBAR);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(F_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        for (int q = 0; q < F_NBAR; ++q)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bars + q)),
+                         "r"(q == F_NBAR - 1 ? 128 : 1));  // epi_done: one arrival per epilogue thread
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tslot;
+    uint32_t full[F_STAGES], empty[F_STAGES];
+    for (int q = 0; q < F_STAGES; ++q) {
+        full[q] = smem_u32(bars + q);
+        empty[q] = smem_u32(bars + F_STAGES + q);
+    }
+    const uint32_t acc_full = smem_u32(bars + 2 * F_STAGES), epi_done = smem_u32(bars + 2 * F_STAGES + 1);
+    const uint32_t sa = smem_u32(sm + F_OFF_A), sb = smem_u32(sm + F_OFF_B);
+    const uint32_t s_act = smem_u32(sm + F_OFF_ACT), s_h = smem_u32(sm + F_OFF_H);
+
+    const int nx = a.nx, ny = a.ny, nz = a.nz, nxh = nx + 2, nyh = ny + 2;
+    const long long plane = (long long)nx * ny;
+    const int ntx = (nx + F_TX - 1) / F_TX, nty = (ny + F_TY - 1) / F_TY, ntiles = ntx * nty;
+    bool ok = true;
+
+    // ---- phase 0: the haloed input columns, 8 levels (16 bytes) per thread
+    {
+        const T *in = static_cast<const T *>(a.in);
+        const long long cols = (long long)nxh * nyh, units = cols * (L / 8);
+        for (long long u = (long long)blockIdx.x * blockDim.x + tid; u < units;
+             u += (long long)gridDim.x * blockDim.x) {
+            const long long col = u % cols;
+            const int q = (int)(u / cols);
+            const int xh = (int)(col % nxh), yh = (int)(col / nxh);
+            const int x = xh == 0 ? nx - 1 : (xh > nx ? 0 : xh - 1);
+            const int y = yh == 0 ? ny - 1 : (yh > ny ? 0 : yh - 1);
+            const long long c = (long long)y * nx + x;
+            float v[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                int k0, k1;
+                float f;
+                interp_pos(q * 8 + e, nz, L, k0, k1, f);
+                v[e] = a.scale_in * ((1.f - f) * (float)in[k0 * plane + c] + f * (float)in[k1 * plane + c]);
+            }
+            *reinterpret_cast<uint4 *>(a.xh + col * L + q * 8) =
+                make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                           pack_bf16x2(v[6], v[7]));
+        }
+    }
+    ok = grid_barrier(a.bar, gridDim.x, ok);
+
+    Producer P;
+    Issuer I;
+    P.sa = I.sa = sa;
+    P.sb = I.sb = sb;
+    for (int q = 0; q < F_STAGES; ++q) {
+        P.full[q] = I.full[q] = full[q];
+        P.empty[q] = I.empty[q] = empty[q];
+    }
+    P.g = I.g = 0;
+    I.acc_full = acc_full;
+    I.epi_done = epi_done;
+    I.tmem = tmem;
+    I.nepi = 0;
+    I.first = true;
+    unsigned nacc = 0;  // epilogue: accumulators waited for
+    // epilogue: wait for a layer's accumulator (a warp-uniform outcome: the
+    // TMEM loads that follow are warp-collective)
+    auto wait_acc = [&]() -> bool {
+        const bool r = __all_sync(0xffffffffu, mbar_wait(acc_full, nacc & 1u));
+        ++nacc;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        return r;
+    };
+    // epilogue: accumulator read, operand written (visible to the tensor core)
+    auto epi_signal = [&]() {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        arrive(epi_done);
+    };
+
+    // ---- phase 1: input convolution and the dense layers, z to zh
+    if (ok) {
+        if (warp == 4) {
+            if (lane == 0)
+                for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
+                    const int x0 = (tile % ntx) * F_TX, y0 = (tile / ntx) * F_TY;
+                    // the haloed window of tap t starts at (x0 + t % 3, y0 + t / 3)
+                    ok = P.layer(F_C1, &mx, &mc1, x0, y0) && P.layer(F_W1, nullptr, &mw1, 0, 0) &&
+                         P.layer(F_W2, nullptr, &mw2, 0, 0) && P.layer(F_W3, nullptr, &mw3, 0, 0);
+                }
+        } else if (warp == 5) {
+            if (lane == 0)
+                for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x)
+                    ok = I.layer(F_C1, 0) && I.layer(F_W1, s_act) && I.layer(F_W2, s_h) && I.layer(F_W3, s_h);
+        } else {
+            for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
+                const int x0 = (tile % ntx) * F_TX, y0 = (tile / ntx) * F_TY;
+                if (!(ok = wait_acc())) break;
+                epi_to_smem(tmem, F_COL64, a.param + OFF_c1, L, true, s_act);
+                epi_signal();
+                if (!(ok = wait_acc())) break;
+                epi_to_smem(tmem, F_COL256, a.param + OFF_B1, HID, true, s_h);
+                epi_signal();
+                if (!(ok = wait_acc())) break;
+                epi_to_smem(tmem, F_COL256, a.param + OFF_B2, HID, true, s_h);
+                epi_signal();
+                if (!(ok = wait_acc())) break;
+                // z = acc + b3 as BF16, to the interior row and its periodic images in zh
+                const int x = x0 + (tid % F_TX), y = y0 + (tid / F_TX);
+                uint32_t pk[32];
+                const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + F_COL64;
+#pragma unroll
+                for (int c0 = 0; c0 < L; c0 += 16) {
+                    float f[16];
+                    tmem_ld16(lane_base + (uint32_t)c0, f);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        pk[c0 / 2 + q] = pack_bf16x2(f[2 * q] + __ldg(a.param + OFF_B3 + c0 + 2 * q),
+                                                     f[2 * q + 1] + __ldg(a.param + OFF_B3 + c0 + 2 * q + 1));
+                }
+                epi_signal();
+                if (x < nx && y < ny) {
+                    const int xs[3] = {x + 1, x == nx - 1 ? 0 : -1, x == 0 ? nx + 1 : -1};
+                    const int ys[3] = {y + 1, y == ny - 1 ? 0 : -1, y == 0 ? ny + 1 : -1};
+                    for (int p = 0; p < 3; ++p)
+                        for (int o = 0; o < 3; ++o) {
+                            if (ys[p] < 0 || xs[o] < 0) continue;
+                            uint4 *dst = reinterpret_cast<uint4 *>(a.zh + ((long long)ys[p] * nxh + xs[o]) * L);
+#pragma unroll
+                            for (int q = 0; q < 8; ++q)
+                                dst[q] = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
+                        }
+                }
+            }
+        }
+    }
+    ok = grid_barrier(a.bar, 2u * gridDim.x, ok);
+
+    // ---- phase 2: output convolution, residual, resampling to nz levels
+    if (ok) {
+        if (warp == 4) {
+            if (lane == 0)
+                for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
+                    const int x0 = (tile % ntx) * F_TX, y0 = (tile / ntx) * F_TY;
+                    ok = P.layer(F_C2, &mz, &mc2, x0, y0);
+                }
+        } else if (warp == 5) {
+            if (lane == 0)
+                for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) ok = I.layer(F_C2, 0);
+        } else {
+            float *ysm = reinterpret_cast<float *>(sm + F_OFF_H);  // y of the tile, [L][128]
+            T *out = static_cast<T *>(a.out);
+            for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
+                const int x0 = (tile % ntx) * F_TX, y0 = (tile / ntx) * F_TY;
+                const int x = x0 + (tid % F_TX), y = y0 + (tid / F_TX);
+                const bool inside = x < nx && y < ny;
+                if (!(ok = wait_acc())) break;
+                float acc[L];
+                const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + F_COL64;
+#pragma unroll
+                for (int c0 = 0; c0 < L; c0 += 16) {
+                    float f[16];
+                    tmem_ld16(lane_base + (uint32_t)c0, f);
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) acc[c0 + q] = f[q];
+                }
+                epi_signal();  // the accumulator is free for the next tile's MMAs
+                const uint4 *zr = reinterpret_cast<const uint4 *>(a.zh + ((long long)(y + 1) * nxh + (x + 1)) * L);
+#pragma unroll
+                for (int q = 0; q < L / 8; ++q) {
+                    const uint4 zq = inside ? zr[q] : make_uint4(0, 0, 0, 0);
+                    const __nv_bfloat16 *zb = reinterpret_cast<const __nv_bfloat16 *>(&zq);
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        ysm[(q * 8 + e) * F_ROWS + tid] =
+                            acc[q * 8 + e] + __ldg(a.param + OFF_c2 + q * 8 + e) + __bfloat162float(zb[e]);
+                }
+                epilogue_sync();
+                if (inside) {
+                    const long long c = (long long)y * nx + x;
+                    for (int k = 0; k < nz; ++k) {
+                        int l0, l1;
+                        float f;
+                        interp_pos(k, L, nz, l0, l1, f);
+                        const float v = a.scale_out * ((1.f - f) * ysm[l0 * F_ROWS + tid] + f * ysm[l1 * F_ROWS + tid]);
+                        T *o = out + (long long)k * plane + c;
+                        *o = a.beta == 0.f ? (T)v : (T)((float)a.beta * (float)*o + v);
+                    }
+                }
+                epilogue_sync();  // before the next tile overwrites y
+            }
+        }
+    }
+    __syncwarp();
+    if (__syncthreads_or(!ok) && tid == 0 && a.err) atomicExch(a.err, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(F_TMEM_COLS));
+}
+
+// ---------------------------------------------------------- tensor maps --
+
+using EncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                              const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeFn encoder() {
+    static EncodeFn fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return static_cast<EncodeFn>(nullptr);
+        }
+        return reinterpret_cast<EncodeFn>(f);
+    }();
+    return fn;
+}
+
+// A weight matrix W[N][K] (BF16, row-major) seen as (k % 8, n, k / 8), boxes
+// of 8 x N x 8: one K-block of 64 in the operand layout above.
+static bool weight_map(CUtensorMap *m, const bf16 *w, int N, int K) {
+    EncodeFn enc = encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {8, (cuuint64_t)N, (cuuint64_t)(K / 8)};
+    const cuuint64_t strides[2] = {2ull * K, 16};
+    const cuuint32_t box[3] = {8, (cuuint32_t)N, 8};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16 *>(w), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Haloed columns H[(yh)(nx+2) + xh][L] seen as (l % 8, xh, yh, l / 8), boxes
+// of 8 x 16 x 8 x 8: the 128 rows of a tile (x fastest) of one window.
+static bool column_map(CUtensorMap *m, const bf16 *h, int nx, int ny) {
+    EncodeFn enc = encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[4] = {8, (cuuint64_t)(nx + 2), (cuuint64_t)(ny + 2), L / 8};
+    const cuuint64_t strides[3] = {2ull * L, 2ull * L * (nx + 2), 16};
+    const cuuint32_t box[4] = {8, F_TX, F_TY, L / 8};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(h), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// CTAs of the cooperative launch on the net's device: one per SM (each
+// holds all 512 TMEM columns); 0 if the device refuses the shared memory.
+template <typename T>
+static int fused_grid(Net &n) {
+    static std::atomic<unsigned long long> attr_set{0};
+    if (!(attr_set.load() >> n.device & 1ull)) {
+        PCF_CUDA_TRY(cudaFuncSetAttribute(k_net_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, F_SMEM));
+        attr_set.fetch_or(1ull << n.device);
+    }
+    int per_sm = 0, sms = 0;
+    PCF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_net_fused<T>, F_THREADS, F_SMEM));
+    PCF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, n.device));
+    if (per_sm < 1) return 0;
+    return sms;
+}
+
+template <typename T>
+static int apply_fused(Net &n, const void *in, int nx, int ny, int nz, float si, float so, float beta, void *out,
+                       cudaStream_t st) {
+    if ((long long)(nx + 2) * (ny + 2) > n.hcap) return PCF_ERANGE;
+    if (n.map_nx != nx || n.map_ny != ny) {
+        if (!column_map(&n.xmap, n.xh, nx, ny) || !column_map(&n.zmap, n.zh, nx, ny)) return PCF_ECUDA;
+        n.map_nx = nx;
+        n.map_ny = ny;
+    }
+    const int cap = fused_grid<T>(n);
+    if (cap < 1) return PCF_ECUDA;
+    const int ntiles = ((nx + F_TX - 1) / F_TX) * ((ny + F_TY - 1) / F_TY);
+    const int grid = std::max(1, std::min(cap, ntiles));
+    PCF_CUDA_TRY(cudaMemsetAsync(n.bar, 0, sizeof(unsigned), st));
+    FusedArgs a{};
+    a.in = in;
+    a.out = out;
+    a.nx = nx;
+    a.ny = ny;
+    a.nz = nz;
+    a.scale_in = si;
+    a.scale_out = so;
+    a.beta = beta;
+    a.param = n.param;
+    a.xh = n.xh;
+    a.zh = n.zh;
+    a.bar = n.bar;
+    a.err = n.err;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(F_THREADS);
+    cfg.dynamicSmemBytes = F_SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    PCF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_net_fused<T>, n.xmap, n.zmap, n.wmap[0], n.wmap[1], n.wmap[2], n.wmap[3],
+                                    n.wmap[4], a));
+    return PCF_OK;
+}
+
+// ============================================== training (unfused) path --
+
+static int alloc_training(Net &n, long long C) {
+    if (C <= n.tcap) return PCF_OK;
+    void *ptrs[] = {n.x0, n.xi, n.a, n.h1, n.h2, n.zb, n.zi, n.dyb, n.dzb, n.dg2b, n.dg1b, n.dgab,
+                    n.y, n.t, n.dyf, n.dzf, n.dh, n.dzi, n.part};
+    PCF_CUDA_TRY(cudaStreamSynchronize(n.stream));
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    n.tcap = 0;
+    auto A = [&](void **q, size_t b) -> int {
+        *q = nullptr;
+        const cudaError_t e = cudaMalloc(q, b);
+        return e == cudaSuccess ? PCF_OK : pcf_set_cuda_error(e);
+    };
+    const size_t f4 = sizeof(float), b2 = sizeof(bf16);
+    const long long nchunk = (C + RED_CHUNK - 1) / RED_CHUNK;
+    const size_t part = std::max<size_t>({(size_t)KSPLIT * KC * L, (size_t)KSPLIT * HID * HID,
+                                          (size_t)nchunk * HID});
     int rc;
-    umma::GemmArgs g = gargs((int)C, HID, L, n->x0, L, 1, n->w1b, L, 1, n->err);
-    g.bias = n->param + OFF_B1;
+    if ((rc = A((void **)&n.x0, C * L * b2)) || (rc = A((void **)&n.xi, C * KC * b2)) ||
+        (rc = A((void **)&n.a, C * L * b2)) || (rc = A((void **)&n.h1, C * HID * b2)) ||
+        (rc = A((void **)&n.h2, C * HID * b2)) || (rc = A((void **)&n.zb, C * L * b2)) ||
+        (rc = A((void **)&n.zi, C * KC * b2)) || (rc = A((void **)&n.dyb, C * L * b2)) ||
+        (rc = A((void **)&n.dzb, C * L * b2)) || (rc = A((void **)&n.dg2b, C * HID * b2)) ||
+        (rc = A((void **)&n.dg1b, C * HID * b2)) || (rc = A((void **)&n.dgab, C * L * b2)) ||
+        (rc = A((void **)&n.y, C * L * f4)) || (rc = A((void **)&n.t, C * L * f4)) ||
+        (rc = A((void **)&n.dyf, C * L * f4)) || (rc = A((void **)&n.dzf, C * L * f4)) ||
+        (rc = A((void **)&n.dh, C * HID * f4)) || (rc = A((void **)&n.dzi, C * KC * f4)) ||
+        (rc = A((void **)&n.part, part * f4)))
+        return rc;
+    n.tcap = C;
+    return PCF_OK;
+}
+
+static unsigned blocks(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+// Forward on the columns already gathered into n.x0 (C columns), keeping
+// every activation: a, h1, h2, z (BF16), the im2col matrices, y (FP32).
+static int forward_train(Net &n, long long C, int nx, int ny) {
+    cudaStream_t st = n.stream;
+    int rc;
+    const int M = (int)C;
+    k_im2col<<<blocks(C * TAPS * (L / 8)), 256, 0, st>>>(n.x0, C, nx, ny, n.xi);
+    umma::GemmArgs g = gargs(M, L, KC, n.xi, KC, 1, n.wb + WB_C1, KC, 1, n.err);
+    g.bias = n.param + OFF_c1;
     g.relu = 1;
-    g.outB = n->h1;
+    g.outB = n.a;
     if ((rc = gemm(g, 1, st))) return rc;
-    k_dwconv<<<(unsigned)C, HID, 0, st>>>(n->h1, n->param + OFF_K1, nx, ny, n->h1c);
-    g = gargs((int)C, HID, HID, n->h1c, HID, 1, n->w2b, HID, 1, n->err);
-    g.bias = n->param + OFF_B2;
+    g = gargs(M, HID, L, n.a, L, 1, n.wb + WB_W1, L, 1, n.err);
+    g.bias = n.param + OFF_B1;
     g.relu = 1;
-    g.outB = n->h2;
+    g.outB = n.h1;
     if ((rc = gemm(g, 1, st))) return rc;
-    k_dwconv<<<(unsigned)C, HID, 0, st>>>(n->h2, n->param + OFF_K2, nx, ny, n->h2c);
-    g = gargs((int)C, L, HID, n->h2c, HID, 1, n->w3b, HID, 1, n->err);
-    g.bias = n->param + OFF_B3;
-    g.outF = n->y;
+    g = gargs(M, HID, HID, n.h1, HID, 1, n.wb + WB_W2, HID, 1, n.err);
+    g.bias = n.param + OFF_B2;
+    g.relu = 1;
+    g.outB = n.h2;
     if ((rc = gemm(g, 1, st))) return rc;
+    g = gargs(M, L, HID, n.h2, HID, 1, n.wb + WB_W3, HID, 1, n.err);
+    g.bias = n.param + OFF_B3;
+    g.outB = n.zb;
+    if ((rc = gemm(g, 1, st))) return rc;
+    k_im2col<<<blocks(C * TAPS * (L / 8)), 256, 0, st>>>(n.zb, C, nx, ny, n.zi);
+    g = gargs(M, L, KC, n.zi, KC, 1, n.wb + WB_C2, KC, 1, n.err);
+    g.bias = n.param + OFF_c2;
+    g.outF = n.y;
+    if ((rc = gemm(g, 1, st))) return rc;
+    k_add_bf16<<<blocks(C * L), 256, 0, st>>>(n.y, n.zb, C * L);
     PCF_CUDA_TRY(cudaGetLastError());
     return PCF_OK;
 }
 
-// Loss and gradients (into n->grad) for targets already gathered into n->t.
-static int backward(Net *n, long long C, int nx, int ny) {
-    cudaStream_t st = n->stream;
+// weight gradient D[o][k] = sum_c G[c][o] X[c][k] (G: C x O BF16, X: C x K
+// BF16), split-K over the columns, summed into grad (row-major O x K)
+static int weight_grad(Net &n, const bf16 *G, int O, const bf16 *X, int K, long long C, float *grad) {
+    cudaStream_t st = n.stream;
+    const int used = std::min<int>(KSPLIT, (int)((C + 63) / 64));
     int rc;
-    const long long ny_ = C * L;
-    const int nb = 256;
-    k_loss_part<<<nb, 256, 0, st>>>(n->y, n->t, ny_, reinterpret_cast<double *>(n->red));
-    k_loss_final<<<1, 1, 0, st>>>(reinterpret_cast<double *>(n->red), nb, n->scal);
-    k_dy<<<1024, 256, 0, st>>>(n->y, n->t, ny_, n->scal, n->dyf, n->dyb);
+    if (K <= 256) {
+        umma::GemmArgs g = gargs(O, K, (int)C, G, 1, O, X, 1, K, n.err);
+        g.outF = n.part;
+        if ((rc = gemm(g, KSPLIT, st))) return rc;
+        k_sum_rows<<<blocks((long long)O * K), 256, 0, st>>>(n.part, used, O * K, grad);
+    } else {  // K = 576 (a convolution): D^T[k][o] with M = K, N = O, transposed in the sum
+        umma::GemmArgs g = gargs(K, O, (int)C, X, 1, K, G, 1, O, n.err);
+        g.outF = n.part;
+        if ((rc = gemm(g, KSPLIT, st))) return rc;
+        k_sum_rows_t<<<blocks((long long)O * K), 256, 0, st>>>(n.part, used, K, O, grad);
+    }
+    PCF_CUDA_TRY(cudaGetLastError());
+    return PCF_OK;
+}
+
+// bias gradient: column sums of a C x F FP32 array
+static void bias_grad(Net &n, const float *a, long long C, int F, float *grad) {
     const unsigned nchunk = (unsigned)((C + RED_CHUNK - 1) / RED_CHUNK);
-    float *part_db = n->part, *part_dk = n->part + (long long)nchunk * HID;
-    // b3
-    k_colsum_part<<<nchunk, L, 0, st>>>(n->dyf, C, L, part_db);
-    k_sum_rows<<<1, L, 0, st>>>(part_db, (int)nchunk, L, n->grad + OFF_B3);
-    // W3 = dY^T h2c : [L][HID], K = C
-    umma::GemmArgs g = gargs(L, HID, (int)C, n->dyb, 1, L, n->h2c, 1, HID, n->err);
-    g.outF = n->part;
-    if ((rc = gemm(g, KSPLIT, st))) return rc;
-    k_sum_rows<<<(L * HID + 255) / 256, 256, 0, st>>>(n->part, std::min<int>(KSPLIT, (int)((C + 63) / 64)),
-                                                       L * HID, n->grad + OFF_W3);
-    // dh2c = dY W3 : [C][HID]
-    g = gargs((int)C, HID, L, n->dyb, L, 1, n->w3b, 1, HID, n->err);
-    g.outF = n->dh2c;
+    k_colsum_part<<<nchunk, F, 0, n.stream>>>(a, C, F, n.part);
+    k_sum_rows<<<1, F, 0, n.stream>>>(n.part, (int)nchunk, F, grad);
+}
+
+// Loss and gradients (into n.grad) for targets already gathered into n.t.
+static int backward(Net &n, long long C, int nx, int ny, double *log, int slot) {
+    cudaStream_t st = n.stream;
+    int rc;
+    const int M = (int)C;
+    const unsigned nchunk = (unsigned)((C + RED_CHUNK - 1) / RED_CHUNK);
+    k_loss_part<<<256, 256, 0, st>>>(n.y, n.t, C * L, n.red);
+    k_loss_final<<<1, 1, 0, st>>>(n.red, 256, n.scal, log, slot);
+    k_dy<<<1024, 256, 0, st>>>(n.y, n.t, C * L, n.scal, n.dyf, n.dyb);
+    // output convolution: c2, C2, then dz = dy + col2im(dy C2)
+    bias_grad(n, n.dyf, C, L, n.grad + OFF_c2);
+    if ((rc = weight_grad(n, n.dyb, L, n.zi, KC, C, n.grad + OFF_C2))) return rc;
+    for (int nb = 0; nb < 3; ++nb) {  // dzi = dy C2 in three column blocks of 192
+        umma::GemmArgs g = gargs(M, 192, L, n.dyb, L, 1, n.wb + WB_C2 + nb * 192, 1, KC, n.err);
+        g.outF = n.dzi + nb * 192;
+        g.ldo = KC;
+        if ((rc = gemm(g, 1, st))) return rc;
+    }
+    k_col2im<<<blocks(C * L), 256, 0, st>>>(n.dzi, n.dyf, C, nx, ny, n.dzf, n.dzb);
+    // W3, b3; dh2 = dz W3
+    bias_grad(n, n.dzf, C, L, n.grad + OFF_B3);
+    if ((rc = weight_grad(n, n.dzb, L, n.h2, HID, C, n.grad + OFF_W3))) return rc;
+    umma::GemmArgs g = gargs(M, HID, L, n.dzb, L, 1, n.wb + WB_W3, 1, HID, n.err);
+    g.outF = n.dh;
     if ((rc = gemm(g, 1, st))) return rc;
-    // conv2 / relu2 backward -> dz2, b2, K2
-    k_dwconv_bwd<<<nchunk, HID, 0, st>>>(n->dh2c, n->h2, n->param + OFF_K2, C, nx, ny, n->dz2, part_db, part_dk);
-    k_sum_rows<<<1, HID, 0, st>>>(part_db, (int)nchunk, HID, n->grad + OFF_B2);
-    k_sum_rows<<<(HID * TAPS + 255) / 256, 256, 0, st>>>(part_dk, (int)nchunk, HID * TAPS, n->grad + OFF_K2);
-    // W2 = dz2^T h1c : [HID][HID]
-    g = gargs(HID, HID, (int)C, n->dz2, 1, HID, n->h1c, 1, HID, n->err);
-    g.outF = n->part;
-    if ((rc = gemm(g, KSPLIT, st))) return rc;
-    k_sum_rows<<<(HID * HID + 255) / 256, 256, 0, st>>>(n->part, std::min<int>(KSPLIT, (int)((C + 63) / 64)),
-                                                         HID * HID, n->grad + OFF_W2);
-    // dh1c = dz2 W2
-    g = gargs((int)C, HID, HID, n->dz2, HID, 1, n->w2b, 1, HID, n->err);
-    g.outF = n->dh1c;
+    k_relu_bwd<<<nchunk, HID, 0, st>>>(n.dh, n.h2, C, HID, n.dg2b, n.part);
+    k_sum_rows<<<1, HID, 0, st>>>(n.part, (int)nchunk, HID, n.grad + OFF_B2);
+    // W2; dh1 = dg2 W2
+    if ((rc = weight_grad(n, n.dg2b, HID, n.h1, HID, C, n.grad + OFF_W2))) return rc;
+    g = gargs(M, HID, HID, n.dg2b, HID, 1, n.wb + WB_W2, 1, HID, n.err);
+    g.outF = n.dh;
     if ((rc = gemm(g, 1, st))) return rc;
-    // conv1 / relu1 backward -> dz1, b1, K1
-    k_dwconv_bwd<<<nchunk, HID, 0, st>>>(n->dh1c, n->h1, n->param + OFF_K1, C, nx, ny, n->dz1, part_db, part_dk);
-    k_sum_rows<<<1, HID, 0, st>>>(part_db, (int)nchunk, HID, n->grad + OFF_B1);
-    k_sum_rows<<<(HID * TAPS + 255) / 256, 256, 0, st>>>(part_dk, (int)nchunk, HID * TAPS, n->grad + OFF_K1);
-    // W1 = dz1^T x0 : [HID][L]
-    g = gargs(HID, L, (int)C, n->dz1, 1, HID, n->x0, 1, L, n->err);
-    g.outF = n->part;
-    if ((rc = gemm(g, KSPLIT, st))) return rc;
-    k_sum_rows<<<(HID * L + 255) / 256, 256, 0, st>>>(n->part, std::min<int>(KSPLIT, (int)((C + 63) / 64)), HID * L,
-                                                       n->grad + OFF_W1);
+    k_relu_bwd<<<nchunk, HID, 0, st>>>(n.dh, n.h1, C, HID, n.dg1b, n.part);
+    k_sum_rows<<<1, HID, 0, st>>>(n.part, (int)nchunk, HID, n.grad + OFF_B1);
+    // W1; da = dg1 W1
+    if ((rc = weight_grad(n, n.dg1b, HID, n.a, L, C, n.grad + OFF_W1))) return rc;
+    g = gargs(M, L, HID, n.dg1b, HID, 1, n.wb + WB_W1, 1, L, n.err);
+    g.outF = n.dh;
+    if ((rc = gemm(g, 1, st))) return rc;
+    k_relu_bwd<<<nchunk, L, 0, st>>>(n.dh, n.a, C, L, n.dgab, n.part);
+    k_sum_rows<<<1, L, 0, st>>>(n.part, (int)nchunk, L, n.grad + OFF_c1);
+    // input convolution: C1
+    if ((rc = weight_grad(n, n.dgab, L, n.xi, KC, C, n.grad + OFF_C1))) return rc;
     PCF_CUDA_TRY(cudaGetLastError());
     return PCF_OK;
 }
 
-static int check_err(Net *n) {
+static int check_err(Net &n) {
     int e = 0;
-    PCF_CUDA_TRY(cudaMemcpyAsync(&e, n->err, sizeof(int), cudaMemcpyDeviceToHost, n->stream));
-    PCF_CUDA_TRY(cudaStreamSynchronize(n->stream));
+    PCF_CUDA_TRY(cudaMemcpyAsync(&e, n.err, sizeof(int), cudaMemcpyDeviceToHost, n.stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(n.stream));
     return e ? PCF_ECUDA : PCF_OK;
+}
+
+// gather b (the input) and x (the target) of one sample, forward, backward,
+// and (lr > 0) an Adam step; the loss goes to log[slot] (nullable)
+static int train_one(Net &n, const float *b, const float *x, int nx, int ny, int nz, double lr, double *log,
+                     int slot) {
+    const long long C = (long long)nx * ny;
+    int rc;
+    if ((rc = alloc_training(n, C))) return rc;
+    cudaStream_t st = n.stream;
+    k_gather<float, bf16><<<blocks(C * L), 256, 0, st>>>(b, C, nz, 1.0f, n.x0);
+    k_gather<float, float><<<blocks(C * L), 256, 0, st>>>(x, C, nz, 1.0f, n.t);
+    PCF_CUDA_TRY(cudaGetLastError());
+    if ((rc = forward_train(n, C, nx, ny))) return rc;
+    if ((rc = backward(n, C, nx, ny, log, slot))) return rc;
+    if (lr > 0) {
+        n.step += 1;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.f - std::pow(b1, (float)n.step), c2 = 1.f - std::pow(b2, (float)n.step);
+        k_adam<<<blocks(NPARAM), 256, 0, st>>>(n.param, n.grad, n.m, n.v, NPARAM, (float)lr, b1, b2, 1e-8f, c1, c2,
+                                               n.wb, n.no_bias);
+        PCF_CUDA_TRY(cudaGetLastError());
+    }
+    return PCF_OK;
 }
 
 }  // namespace net
@@ -457,10 +1173,10 @@ int pcf_gemm_bf16(const unsigned short *A, long long a_len, long long a_rs, long
 
 namespace {
 
-// deterministic parameter initialisation: He-uniform weights, zero biases,
-// zero convolution kernels (so the network starts as a plain MLP)
+// Deterministic initialisation: He-uniform C1, W1, W2; zero W3, C2 and
+// biases, so that the untrained network outputs zero (loss 1 against any
+// target) and training starts from "no correction".
 void init_params(std::vector<float> &p, unsigned seed) {
-    using namespace pcf::net;
     uint64_t s = 0x9E3779B97F4A7C15ull ^ (uint64_t)seed;
     auto uni = [&]() {
         s ^= s << 13;
@@ -473,55 +1189,40 @@ void init_params(std::vector<float> &p, unsigned seed) {
         const double a = std::sqrt(6.0 / fan_in);
         for (int i = 0; i < n; ++i) p[off + i] = (float)((2 * uni() - 1) * a);
     };
+    fill(OFF_C1, L * KC, KC);
     fill(OFF_W1, HID * L, L);
     fill(OFF_W2, HID * HID, HID);
-    fill(OFF_W3, L * HID, HID);
-    for (int i = 0; i < L * HID; ++i) p[OFF_W3 + i] *= 0.1f;  // small initial output
 }
 
-int net_alloc(pcf::net::Net &n, long long cap) {
-    using namespace pcf::net;
-    auto A = [&](void **q, size_t b) -> int {
-        const cudaError_t e = cudaMalloc(q, b);
-        return e == cudaSuccess ? PCF_OK : pcf_set_cuda_error(e);
-    };
-    const size_t f4 = sizeof(float), b2 = sizeof(bf16);
-    const long long nchunk = (cap + RED_CHUNK - 1) / RED_CHUNK;
-    const size_t part = std::max<size_t>((size_t)KSPLIT * HID * HID, (size_t)nchunk * HID * (TAPS + 1));
-    int rc;
-    if ((rc = A((void **)&n.param, NPARAM * f4)) || (rc = A((void **)&n.grad, NPARAM * f4)) ||
-        (rc = A((void **)&n.m, NPARAM * f4)) || (rc = A((void **)&n.v, NPARAM * f4)) ||
-        (rc = A((void **)&n.w1b, HID * L * b2)) || (rc = A((void **)&n.w2b, HID * HID * b2)) ||
-        (rc = A((void **)&n.w3b, L * HID * b2)) || (rc = A((void **)&n.x0, cap * L * b2)) ||
-        (rc = A((void **)&n.h1, cap * HID * b2)) || (rc = A((void **)&n.h1c, cap * HID * b2)) ||
-        (rc = A((void **)&n.h2, cap * HID * b2)) || (rc = A((void **)&n.h2c, cap * HID * b2)) ||
-        (rc = A((void **)&n.dyb, cap * L * b2)) || (rc = A((void **)&n.dz2, cap * HID * b2)) ||
-        (rc = A((void **)&n.dz1, cap * HID * b2)) || (rc = A((void **)&n.y, cap * L * f4)) ||
-        (rc = A((void **)&n.t, cap * L * f4)) || (rc = A((void **)&n.dyf, cap * L * f4)) ||
-        (rc = A((void **)&n.dh2c, cap * HID * f4)) || (rc = A((void **)&n.dh1c, cap * HID * f4)) ||
-        (rc = A((void **)&n.part, part * f4)) || (rc = A((void **)&n.red, 1024 * sizeof(double))) ||
-        (rc = A((void **)&n.scal, 4 * sizeof(double))) || (rc = A((void **)&n.err, sizeof(int))))
-        return rc;
-    return PCF_OK;
-}
-
-int net_upload_params(pcf::net::Net &n, const float *host) {
-    using namespace pcf::net;
+int net_upload_params(Net &n, const float *host) {
     PCF_CUDA_TRY(cudaMemcpyAsync(n.param, host, NPARAM * sizeof(float), cudaMemcpyHostToDevice, n.stream));
-    k_params_to_bf16<<<(HID * HID + 255) / 256, 256, 0, n.stream>>>(n.param, n.w1b, n.w2b, n.w3b);
+    k_params_to_bf16<<<(NPARAM + 255) / 256, 256, 0, n.stream>>>(n.param, n.wb);
     PCF_CUDA_TRY(cudaGetLastError());
     PCF_CUDA_TRY(cudaStreamSynchronize(n.stream));
     return PCF_OK;
 }
 
-template <typename T>
-int net_gather(pcf::net::Net &n, const T *field, long long plane, int nz, float scale, float *dstF, bf16 *dstB) {
-    using namespace pcf::net;
-    const long long total = plane * L;
-    const unsigned grid = (unsigned)((total + 255) / 256);
-    if (dstB) k_gather<T, bf16><<<grid, 256, 0, n.stream>>>(field, plane, nz, scale, dstB);
-    if (dstF) k_gather<T, float><<<grid, 256, 0, n.stream>>>(field, plane, nz, scale, dstF);
-    PCF_CUDA_TRY(cudaGetLastError());
+int net_alloc(Net &n, long long cap) {
+    auto A = [&](void **q, size_t b) -> int {
+        const cudaError_t e = cudaMalloc(q, b);
+        return e == cudaSuccess ? PCF_OK : pcf_set_cuda_error(e);
+    };
+    const size_t f4 = sizeof(float);
+    // a grid of at most cap columns has at most 3 cap + 6 haloed columns (ny = 1)
+    n.hcap = 3 * cap + 6;
+    int rc;
+    if ((rc = A((void **)&n.param, NPARAM * f4)) || (rc = A((void **)&n.grad, NPARAM * f4)) ||
+        (rc = A((void **)&n.m, NPARAM * f4)) || (rc = A((void **)&n.v, NPARAM * f4)) ||
+        (rc = A((void **)&n.wb, WB_N * sizeof(bf16))) || (rc = A((void **)&n.xh, n.hcap * L * sizeof(bf16))) ||
+        (rc = A((void **)&n.zh, n.hcap * L * sizeof(bf16))) || (rc = A((void **)&n.bar, sizeof(unsigned))) ||
+        (rc = A((void **)&n.red, 512 * sizeof(double))) || (rc = A((void **)&n.scal, 4 * sizeof(double))) ||
+        (rc = A((void **)&n.err, sizeof(int))))
+        return rc;
+    if (!weight_map(&n.wmap[0], n.wb + WB_C1, L, KC) || !weight_map(&n.wmap[1], n.wb + WB_W1, HID, L) ||
+        !weight_map(&n.wmap[2], n.wb + WB_W2, HID, HID) || !weight_map(&n.wmap[3], n.wb + WB_W3, L, HID) ||
+        !weight_map(&n.wmap[4], n.wb + WB_C2, L, KC))
+        return PCF_ECUDA;
+    n.map_nx = n.map_ny = -1;
     return PCF_OK;
 }
 
@@ -529,7 +1230,7 @@ int net_gather(pcf::net::Net &n, const T *field, long long plane, int nz, float 
 
 extern "C" {
 
-int pcf_net_num_params(void) { return pcf::net::NPARAM; }
+int pcf_net_num_params(void) { return NPARAM; }
 
 int pcf_net_create(pcf_net **out, int device, long long max_columns, unsigned seed) {
     if (!out || max_columns < 1) return PCF_EINVAL;
@@ -548,9 +1249,9 @@ int pcf_net_create(pcf_net **out, int device, long long max_columns, unsigned se
     init_params(p, seed);
     if (!rc) rc = net_upload_params(w->n, p.data());
     if (!rc) {
-        cudaMemsetAsync(w->n.m, 0, pcf::net::NPARAM * sizeof(float), w->n.stream);
-        cudaMemsetAsync(w->n.v, 0, pcf::net::NPARAM * sizeof(float), w->n.stream);
-        cudaMemsetAsync(w->n.grad, 0, pcf::net::NPARAM * sizeof(float), w->n.stream);
+        cudaMemsetAsync(w->n.m, 0, NPARAM * sizeof(float), w->n.stream);
+        cudaMemsetAsync(w->n.v, 0, NPARAM * sizeof(float), w->n.stream);
+        cudaMemsetAsync(w->n.grad, 0, NPARAM * sizeof(float), w->n.stream);
         cudaMemsetAsync(w->n.err, 0, sizeof(int), w->n.stream);
         if (cudaStreamSynchronize(w->n.stream) != cudaSuccess) rc = PCF_ECUDA;
     }
@@ -564,10 +1265,12 @@ int pcf_net_create(pcf_net **out, int device, long long max_columns, unsigned se
 
 int pcf_net_destroy(pcf_net *w) {
     if (!w) return PCF_OK;
-    pcf::net::Net &n = w->n;
+    Net &n = w->n;
     cudaSetDevice(n.device);
-    void *ptrs[] = {n.param, n.grad, n.m, n.v, n.w1b, n.w2b, n.w3b, n.x0, n.h1, n.h1c, n.h2, n.h2c,
-                    n.dyb, n.dz2, n.dz1, n.y, n.t, n.dyf, n.dh2c, n.dh1c, n.part, n.red, n.scal, n.err};
+    if (n.stream) cudaStreamSynchronize(n.stream);
+    void *ptrs[] = {n.param, n.grad, n.m,   n.v,   n.wb,  n.xh,   n.zh,   n.bar,  n.red, n.scal, n.err,
+                    n.x0,    n.xi,   n.a,   n.h1,  n.h2,  n.zb,   n.zi,   n.dyb,  n.dzb, n.dg2b, n.dg1b,
+                    n.dgab,  n.y,    n.t,   n.dyf, n.dzf, n.dh,   n.dzi,  n.part};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (n.stream) cudaStreamDestroy(n.stream);
@@ -578,7 +1281,8 @@ int pcf_net_destroy(pcf_net *w) {
 int pcf_net_get_params(pcf_net *w, float *host) {
     if (!w || !host) return PCF_EINVAL;
     PCF_CUDA_TRY(cudaSetDevice(w->n.device));
-    PCF_CUDA_TRY(cudaMemcpy(host, w->n.param, pcf::net::NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+    PCF_CUDA_TRY(cudaStreamSynchronize(w->n.stream));
+    PCF_CUDA_TRY(cudaMemcpy(host, w->n.param, NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
     return PCF_OK;
 }
 
@@ -586,48 +1290,32 @@ int pcf_net_set_params(pcf_net *w, const float *host) {
     if (!w || !host) return PCF_EINVAL;
     PCF_CUDA_TRY(cudaSetDevice(w->n.device));
     w->n.step = 0;
-    cudaMemsetAsync(w->n.m, 0, pcf::net::NPARAM * sizeof(float), w->n.stream);
-    cudaMemsetAsync(w->n.v, 0, pcf::net::NPARAM * sizeof(float), w->n.stream);
+    cudaMemsetAsync(w->n.m, 0, NPARAM * sizeof(float), w->n.stream);
+    cudaMemsetAsync(w->n.v, 0, NPARAM * sizeof(float), w->n.stream);
     return net_upload_params(w->n, host);
 }
 
-// Network output for a device field: out = beta * out + scale_out * N(scale_in * in).
-// in / out: nz x ny x nx (x fastest), device memory; double or float by `fp64`.
+// Network output for a device field: out = beta * out + scale_out * N(scale_in * in),
+// by the fused kernel.  in / out: nz x ny x nx (x fastest), device memory;
+// double or float by `fp64`.
 int pcf_net_apply_device(pcf_net *w, const void *in, int nx, int ny, int nz, double scale_in, double scale_out,
                          double beta, void *out, int fp64, void *stream) {
     if (!w || !in || !out || nx < 1 || ny < 1 || nz < 1) return PCF_EINVAL;
-    pcf::net::Net &n = w->n;
-    const long long plane = (long long)nx * ny;
-    if (plane > n.cap) return PCF_ERANGE;
-    cudaStream_t caller = static_cast<cudaStream_t>(stream);
-    cudaStream_t keep = n.stream;
-    if (caller) n.stream = caller;  // run on the caller's stream
-    int rc = fp64 ? net_gather<double>(n, (const double *)in, plane, nz, (float)scale_in, nullptr, n.x0)
-                  : net_gather<float>(n, (const float *)in, plane, nz, (float)scale_in, nullptr, n.x0);
-    if (!rc) rc = pcf::net::forward(&n, plane, nx, ny);
-    if (!rc) {
-        const unsigned grid = (unsigned)((plane * nz + 255) / 256);
-        if (fp64)
-            pcf::net::k_scatter<double><<<grid, 256, 0, n.stream>>>(n.y, plane, nz, (float)scale_out, (float)beta,
-                                                                   (double *)out);
-        else
-            pcf::net::k_scatter<float><<<grid, 256, 0, n.stream>>>(n.y, plane, nz, (float)scale_out, (float)beta,
-                                                                  (float *)out);
-        if (cudaGetLastError() != cudaSuccess) rc = PCF_ECUDA;
-    }
-    n.stream = keep;
-    return rc;
+    Net &n = w->n;
+    if ((long long)nx * ny > n.cap) return PCF_ERANGE;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : n.stream;
+    return fp64 ? apply_fused<double>(n, in, nx, ny, nz, (float)scale_in, (float)scale_out, (float)beta, out, st)
+                : apply_fused<float>(n, in, nx, ny, nz, (float)scale_in, (float)scale_out, (float)beta, out, st);
 }
 
 int pcf_net_set_bias_free(pcf_net *w, int on) {
     if (!w) return PCF_EINVAL;
-    using namespace pcf::net;
     Net &n = w->n;
     PCF_CUDA_TRY(cudaSetDevice(n.device));
     n.no_bias = on ? 1 : 0;
     if (on) {
-        const int offs[3] = {OFF_B1, OFF_B2, OFF_B3}, lens[3] = {HID, HID, L};
-        for (int q = 0; q < 3; ++q)
+        const int offs[5] = {OFF_c1, OFF_B1, OFF_B2, OFF_B3, OFF_c2}, lens[5] = {L, HID, HID, L, L};
+        for (int q = 0; q < 5; ++q)
             for (float *a : {n.param, n.m, n.v})
                 PCF_CUDA_TRY(cudaMemsetAsync(a + offs[q], 0, sizeof(float) * lens[q], n.stream));
         PCF_CUDA_TRY(cudaStreamSynchronize(n.stream));
@@ -637,7 +1325,7 @@ int pcf_net_set_bias_free(pcf_net *w, int on) {
 
 // Host-array forward (tests): out = N(in), both nz x ny x nx doubles.
 int pcf_net_forward(pcf_net *w, const double *in, int nx, int ny, int nz, double *out) {
-    if (!w || !in || !out) return PCF_EINVAL;
+    if (!w || !in || !out || nx < 1 || ny < 1 || nz < 1) return PCF_EINVAL;
     PCF_CUDA_TRY(cudaSetDevice(w->n.device));
     const size_t bytes = sizeof(double) * (size_t)nx * ny * nz;
     double *d = nullptr;
@@ -646,7 +1334,7 @@ int pcf_net_forward(pcf_net *w, const double *in, int nx, int ny, int nz, double
     if (cudaMemcpy(d, in, bytes, cudaMemcpyHostToDevice) != cudaSuccess) rc = PCF_ECUDA;
     if (!rc) rc = pcf_net_apply_device(w, d, nx, ny, nz, 1.0, 1.0, 0.0, d + (size_t)nx * ny * nz, 1, nullptr);
     if (!rc && cudaStreamSynchronize(w->n.stream) != cudaSuccess) rc = PCF_ECUDA;
-    if (!rc) rc = pcf::net::check_err(&w->n);
+    if (!rc) rc = check_err(w->n);
     if (!rc && cudaMemcpy(out, d + (size_t)nx * ny * nz, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) rc = PCF_ECUDA;
     cudaFree(d);
     return rc;
@@ -658,32 +1346,64 @@ int pcf_net_forward(pcf_net *w, const double *in, int nx, int ny, int nz, double
 // loss before the step; grad (nullable, host, NPARAM floats) the gradients.
 int pcf_net_train_step(pcf_net *w, const float *b, const float *x, int nx, int ny, int nz, double lr,
                        double *loss, float *grad) {
-    using namespace pcf::net;
     if (!w || !b || !x || nx < 1 || ny < 1 || nz < 1) return PCF_EINVAL;
     Net &n = w->n;
-    const long long plane = (long long)nx * ny;
-    if (plane > n.cap) return PCF_ERANGE;
     PCF_CUDA_TRY(cudaSetDevice(n.device));
-    int rc = net_gather<float>(n, b, plane, nz, 1.0f, nullptr, n.x0);
-    if (!rc) rc = net_gather<float>(n, x, plane, nz, 1.0f, n.t, nullptr);
-    if (!rc) rc = forward(&n, plane, nx, ny);
-    if (!rc) rc = backward(&n, plane, nx, ny);
+    int rc = train_one(n, b, x, nx, ny, nz, lr, nullptr, 0);
     if (rc) return rc;
-    if (lr > 0) {
-        n.step += 1;
-        const float b1 = 0.9f, b2 = 0.999f;
-        const float c1 = 1.f - std::pow(b1, (float)n.step), c2 = 1.f - std::pow(b2, (float)n.step);
-        k_adam<<<(NPARAM + 255) / 256, 256, 0, n.stream>>>(n.param, n.grad, n.m, n.v, NPARAM, (float)lr, b1, b2,
-                                                           1e-8f, c1, c2, n.w1b, n.w2b, n.w3b, n.no_bias);
-        PCF_CUDA_TRY(cudaGetLastError());
-    }
     double s[3];
     PCF_CUDA_TRY(cudaMemcpyAsync(s, n.scal, sizeof(s), cudaMemcpyDeviceToHost, n.stream));
     if (grad) PCF_CUDA_TRY(cudaMemcpyAsync(grad, n.grad, NPARAM * sizeof(float), cudaMemcpyDeviceToHost, n.stream));
     PCF_CUDA_TRY(cudaStreamSynchronize(n.stream));
-    if ((rc = check_err(&n))) return rc;
+    if ((rc = check_err(n))) return rc;
     if (loss) *loss = s[2];
     return PCF_OK;
+}
+
+// Adam over a data set of `count` samples given as host arrays (each nz x ny
+// x nx FP32, normalised), uploaded once to device memory held for the call:
+// `epochs` passes, each in an order drawn from `seed`; losses (nullable,
+// count * epochs doubles) receives the loss of every step.
+int pcf_net_train(pcf_net *w, const float *b, const float *x, int count, int nx, int ny, int nz, int epochs,
+                  double lr, unsigned seed, double *losses) {
+    if (!w || !b || !x || count < 1 || nx < 1 || ny < 1 || nz < 1 || epochs < 1 || !(lr > 0)) return PCF_EINVAL;
+    Net &n = w->n;
+    PCF_CUDA_TRY(cudaSetDevice(n.device));
+    const size_t per = (size_t)nx * ny * nz, bytes = per * sizeof(float) * (size_t)count;
+    float *db = nullptr, *dx = nullptr;
+    double *dl = nullptr;
+    const long long steps = (long long)count * epochs;
+    int rc = PCF_OK;
+    if (cudaMalloc(&db, bytes) != cudaSuccess || cudaMalloc(&dx, bytes) != cudaSuccess ||
+        cudaMalloc(&dl, steps * sizeof(double)) != cudaSuccess)
+        rc = PCF_ENOMEM;
+    if (!rc && (cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, n.stream) != cudaSuccess ||
+                cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, n.stream) != cudaSuccess))
+        rc = PCF_ECUDA;
+    std::vector<int> order(count);
+    uint64_t s = 0x2545F4914F6CDD1Dull ^ ((uint64_t)seed << 1);
+    long long k = 0;
+    for (int ep = 0; !rc && ep < epochs; ++ep) {
+        for (int i = 0; i < count; ++i) order[i] = i;
+        for (int i = count - 1; i > 0; --i) {  // Fisher-Yates with a xorshift generator
+            s ^= s << 13;
+            s ^= s >> 7;
+            s ^= s << 17;
+            std::swap(order[i], order[(int)(s % (uint64_t)(i + 1))]);
+        }
+        for (int i = 0; !rc && i < count; ++i, ++k)
+            rc = train_one(n, db + per * order[i], dx + per * order[i], nx, ny, nz, lr, dl, (int)k);
+    }
+    if (!rc && losses &&
+        cudaMemcpyAsync(losses, dl, steps * sizeof(double), cudaMemcpyDeviceToHost, n.stream) != cudaSuccess)
+        rc = PCF_ECUDA;
+    if (!rc && cudaStreamSynchronize(n.stream) != cudaSuccess) rc = PCF_ECUDA;
+    if (!rc) rc = check_err(n);
+    cudaStreamSynchronize(n.stream);
+    cudaFree(db);
+    cudaFree(dx);
+    cudaFree(dl);
+    return rc;
 }
 
 // Host-array variant for the gradient check: loss and gradients, no update.
@@ -704,16 +1424,16 @@ int pcf_net_gradients(pcf_net *w, const double *b, const double *x, int nx, int 
     return rc;
 }
 
-// Weights file: "PCFNET01", int32 NPARAM, int32 Adam step, then NPARAM FP32 values.
+// Weights file: "PCFNET02", int32 NPARAM, int32 Adam step, then NPARAM FP32 values.
 int pcf_net_save(pcf_net *w, const char *path) {
     if (!w || !path) return PCF_EINVAL;
-    std::vector<float> p(pcf::net::NPARAM);
+    std::vector<float> p(NPARAM);
     int rc = pcf_net_get_params(w, p.data());
     if (rc) return rc;
     FILE *f = std::fopen(path, "wb");
     if (!f) return PCF_EINVAL;
-    const int hdr[2] = {pcf::net::NPARAM, w->n.step};
-    const bool ok = std::fwrite("PCFNET01", 1, 8, f) == 8 && std::fwrite(hdr, sizeof(int), 2, f) == 2 &&
+    const int hdr[2] = {NPARAM, w->n.step};
+    const bool ok = std::fwrite("PCFNET02", 1, 8, f) == 8 && std::fwrite(hdr, sizeof(int), 2, f) == 2 &&
                     std::fwrite(p.data(), sizeof(float), p.size(), f) == p.size();
     std::fclose(f);
     return ok ? PCF_OK : PCF_EINVAL;
@@ -725,9 +1445,9 @@ int pcf_net_load(pcf_net *w, const char *path) {
     if (!f) return PCF_EINVAL;
     char magic[8];
     int hdr[2];
-    std::vector<float> p(pcf::net::NPARAM);
-    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PCFNET01", 8) == 0 &&
-              std::fread(hdr, sizeof(int), 2, f) == 2 && hdr[0] == pcf::net::NPARAM &&
+    std::vector<float> p(NPARAM);
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PCFNET02", 8) == 0 &&
+              std::fread(hdr, sizeof(int), 2, f) == 2 && hdr[0] == NPARAM &&
               std::fread(p.data(), sizeof(float), p.size(), f) == p.size();
     std::fclose(f);
     if (!ok) return PCF_EINVAL;

@@ -2388,10 +2388,18 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
         if (ro.nupdates > 0) rel = ro.res;
         if (ro.converged) break;
         if (ro.status == PCF_EBREAKDOWN && restarts < prm->max_refinements && res->niter < maxit) {
-            // fold what the broken-down iteration accumulated, then restart from the true residual
-            k_axpy_f2d<<<vec_grid(h->d.n), 256, 0, h->stream>>>(w.x, h->x64, h->fc64, h->d.n, b_norm);
-            h->launches += 1;
-            PCF_CUDA_TRY(cudaGetLastError());
+            if (cm.learned_pc) {
+                // the plain preconditioner is the fallback: a breakdown or divergence
+                // with the learned stage drops the stage for the rest of the solve and
+                // discards the FP32 correction since the last reliable update
+                cm.learned_pc = 0;
+            } else {
+                // fold what the broken-down iteration accumulated
+                k_axpy_f2d<<<vec_grid(h->d.n), 256, 0, h->stream>>>(w.x, h->x64, h->fc64, h->d.n, b_norm);
+                h->launches += 1;
+                PCF_CUDA_TRY(cudaGetLastError());
+            }
+            // restart from the true residual
             if ((rc = true_residual(h, h->b64, h->x64, &rnorm))) return rc;
             rel = rnorm / b_norm;
             restarts += 1;

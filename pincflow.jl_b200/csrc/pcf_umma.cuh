@@ -33,8 +33,9 @@ struct GemmArgs {
     long long b_rs, b_ks;
     const float *bias;     // per column n (nullable; not with split-K)
     int relu;              // apply max(0, .) after the bias
-    float *outF;           // row-major [M][N] FP32 (split-K: [gridDim.z][M][N] partials)
-    __nv_bfloat16 *outB;   // row-major [M][N] BF16 (nullable)
+    float *outF;           // row-major [M][ldo] FP32 (split-K: [gridDim.z][M][N] partials)
+    __nv_bfloat16 *outB;   // row-major [M][ldo] BF16 (nullable)
+    long long ldo;         // output row length (0: N); lets a launch write a column block of a wider matrix
     int *error;            // set to 1 if an mbarrier wait timed out
 };
 
@@ -166,6 +167,7 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(GemmArgs g) {
     // epilogue: warp w reads TMEM lanes (rows) 32w .. 32w+31, 16 columns at a time
     const int row = m0 + warp * 32 + lane;
     const bool partial = gridDim.z > 1;
+    const long long ldo = g.ldo > 0 ? g.ldo : g.N;
 #pragma unroll 1
     for (int c0 = 0; c0 < NT; c0 += 16) {
         uint32_t v[16];
@@ -189,8 +191,8 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(GemmArgs g) {
                 } else {
                     if (g.bias) d += g.bias[col];
                     if (g.relu) d = fmaxf(d, 0.0f);
-                    if (g.outF) g.outF[(long long)row * g.N + col] = d;
-                    if (g.outB) g.outB[(long long)row * g.N + col] = __float2bfloat16(d);
+                    if (g.outF) g.outF[(long long)row * ldo + col] = d;
+                    if (g.outB) g.outB[(long long)row * ldo + col] = __float2bfloat16(d);
                 }
             }
         } else if (ok && row < g.M && partial) {

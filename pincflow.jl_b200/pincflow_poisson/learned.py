@@ -1,15 +1,22 @@
-"""Learned warm start for the Poisson solve (no reference counterpart).
+"""Learned warm start and preconditioner stage for the Poisson solve (no
+reference counterpart).
 
-The network (pcf_net in include/pincflow_poisson.h) maps the right-hand side
-b of the scaled Poisson system A s = b to an estimate of s, column by column
-(64 -> 256 -> 256 -> 64 with depthwise 3x3 horizontal convolutions between
-the layers).  It is trained on the GPU by the library's own forward,
-backward and Adam kernels, on (right-hand side, solution) pairs that the
-plain FP64 solver itself produces on the training configuration (random
-Gaussian-hill terrain, 128 x 128 x 64; pincflow_poisson.configs.c3).
-Attached to a solver (PoissonSolver.attach_network) it provides the initial
-guess of the mixed-precision solve when PoissonNamelist.learned is set; the
-FP64 true residual still decides convergence.
+The network (pcf_net in include/pincflow_poisson.h) works column by column:
+a full 3x3 horizontal convolution of the input columns (resampled to 64
+levels), a per-column MLP 64 -> 256 -> 256 -> 64, and a residual 3x3
+convolution of its output; 172,736 parameters, BF16 weights, FP32
+accumulation on the tensor cores.  It is trained on the GPU by the
+library's own forward, backward and Adam kernels (pcf_net_train), on pairs
+that the plain FP64 solver itself produces on the training configuration
+(random Gaussian-hill terrain, 128 x 128 x 64; pincflow_poisson.configs.c3):
+  * warm start: (right-hand side b, solution s) pairs; attached to a solver
+    (PoissonSolver.attach_network) it provides the initial guess of the
+    mixed-precision solve when PoissonNamelist.learned has bit 1;
+  * preconditioner stage: bias-free, on the multigrid V-cycle's (residual,
+    error) pairs; with bit 2 each preconditioner application of the flexible
+    FP32 BiCGSTAB becomes z = M(r) + N(r - A M(r)).
+The FP64 true residual still decides convergence.  No PyTorch: data sets go
+to the device through the library.
 """
 from __future__ import annotations
 
@@ -22,7 +29,7 @@ from . import _lib
 from . import configs as C
 from .solver import PoissonNamelist, PoissonSolver
 
-NPARAM = 103_488
+NPARAM = 172_736
 
 
 def _bind(lib):
@@ -41,11 +48,15 @@ def _bind(lib):
     lib.pcf_net_train_step.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                        dp, fp]
     lib.pcf_net_gradients.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, fp]
+    lib.pcf_net_train.argtypes = [vp, fp, fp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_double, ctypes.c_uint, dp]
+    lib.pcf_net_apply_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_double, vp, ctypes.c_int, vp]
     lib.pcf_set_network.argtypes = [vp, vp]
     lib.pcf_net_set_bias_free.argtypes = [vp, ctypes.c_int]
     for name in ("pcf_net_create", "pcf_net_destroy", "pcf_net_get_params", "pcf_net_set_params", "pcf_net_save",
                  "pcf_net_load", "pcf_net_forward", "pcf_net_train_step", "pcf_net_gradients", "pcf_set_network",
-                 "pcf_net_set_bias_free"):
+                 "pcf_net_set_bias_free", "pcf_net_train", "pcf_net_apply_device"):
         getattr(lib, name).restype = ctypes.c_int
     lib._net_bound = True
     return lib
@@ -110,6 +121,17 @@ class LearnedNet:
         out = np.zeros_like(f)
         _lib.check(self.lib.pcf_net_forward(self._h, _lib.dptr(f), nx, ny, nz, _lib.dptr(out)), "pcf_net_forward")
         return out
+
+    def apply_device(self, d_in: int, d_out: int, shape, fp64: bool = False, scale_in: float = 1.0,
+                     scale_out: float = 1.0, beta: float = 0.0, stream: int | None = None):
+        """out = beta * out + scale_out * N(scale_in * in) on device fields (raw
+        pointers, nz x ny x nx, FP64 or FP32), asynchronously on `stream` (a
+        cudaStream_t as an integer; None: the network's own stream)."""
+        nz, ny, nx = shape
+        _lib.check(self.lib.pcf_net_apply_device(self._h, ctypes.c_void_p(d_in), nx, ny, nz, scale_in, scale_out,
+                                                 beta, ctypes.c_void_p(d_out), int(bool(fp64)),
+                                                 ctypes.c_void_p(stream) if stream else None),
+                   "pcf_net_apply_device")
 
     def gradients(self, b: np.ndarray, x: np.ndarray):
         """(loss, gradient vector) for one sample, host arrays (nz, ny, nx)."""
@@ -191,23 +213,23 @@ def preconditioner_pairs(indices, nx=128, ny=128, nz=64, tolerance=1e-8, device=
     return out
 
 
-def train(net: LearnedNet, pairs, epochs: int = 4, lr: float = 1e-3, device: int = 0, log=None):
-    """Adam over the pairs (one sample per step), on device.  Returns the
-    per-step losses."""
-    import torch
-    dev = torch.device("cuda", device)
-    data = [(torch.from_numpy(b).to(dev), torch.from_numpy(x).to(dev)) for b, x in pairs]
-    torch.cuda.synchronize()
-    losses = []
+def train(net: LearnedNet, pairs, epochs: int = 4, lr: float = 1e-3, device: int = 0, log=None, seed: int = 0):
+    """Adam over the pairs (one sample per step, `epochs` shuffled passes) on
+    the device, through pcf_net_train.  Returns the per-step losses."""
+    del device  # the network's own device
+    b = np.ascontiguousarray(np.stack([p[0] for p in pairs]), dtype=np.float32)
+    x = np.ascontiguousarray(np.stack([p[1] for p in pairs]), dtype=np.float32)
+    count, nz, ny, nx = b.shape
+    losses = np.zeros(count * epochs)
     t0 = time.time()
-    for ep in range(epochs):
-        order = np.random.default_rng(ep).permutation(len(data))
-        for k in order:
-            b, x = data[k]
-            losses.append(net.train_step(b.data_ptr(), x.data_ptr(), tuple(b.shape), lr))
-        if log:
-            log(f"epoch {ep}: mean loss {np.mean(losses[-len(data):]):.4f} ({time.time() - t0:.1f} s)")
-    return losses
+    fp = ctypes.POINTER(ctypes.c_float)
+    _lib.check(net.lib.pcf_net_train(net.handle, b.ctypes.data_as(fp), x.ctypes.data_as(fp), count, nx, ny, nz,
+                                     epochs, lr, seed, _lib.dptr(losses)), "pcf_net_train")
+    if log:
+        for ep in range(epochs):
+            log(f"epoch {ep}: mean loss {np.mean(losses[ep * count:(ep + 1) * count]):.4f}")
+        log(f"{count * epochs} steps in {time.time() - t0:.1f} s")
+    return losses.tolist()
 
 
 def evaluate(net: LearnedNet, indices, nx=128, ny=128, nz=64, device=0, **namelist):
