@@ -364,7 +364,7 @@ __global__ void k_params_to_bf16(const float *__restrict__ p, bf16 *__restrict__
 //            y = z + C2 im2col(z) + c2, resampled to the nz levels of the
 //            output: out = beta * out + scale_out * y.
 // Warp roles: warp 4 (one thread) streams every TMA box of the CTA's K-steps
-// through a three-stage ring, as far ahead as the ring allows (the weights
+// through a four-stage ring, as far ahead as the ring allows (the weights
 // and the windows of xh do not depend on the activations); warp 5 (one
 // thread) issues the tcgen05.mma of each K-step once its stage has landed,
 // frees the stage with tcgen05.commit, and signals each finished layer;
@@ -372,25 +372,33 @@ __global__ void k_params_to_bf16(const float *__restrict__ p, bf16 *__restrict__
 // bias, ReLU, BF16 into the shared operand of the next layer, or z / y to
 // global memory -- and signal that the accumulator and operand are ready.
 // Shared-memory operand layout (TMA boxes land in it directly): K-major
-// without swizzle, row r of K-slice q (8 values, 16 bytes) at q * R * 16 +
-// r * 16 for an operand of R rows -- core matrices of 8 rows x 16 bytes are
-// contiguous, 128 B apart along M/N (SBO) and R * 16 B apart along K (LBO).
+// with the 128-byte swizzle, one 64-value K-block per operand block: row r
+// is the 128 bytes at r * 128, its 16-byte chunk c at ((c ^ (r % 8)) * 16),
+// 8-row groups 1024 B apart (SBO); blocks are 1024-byte aligned.  A TMA box
+// row is then 128 bytes, and a K-step of 16 values advances the descriptor's
+// start address by 32 bytes.
 // Every wait is bounded (2 s of %globaltimer); a role that gives up stops,
 // the others give up on their next wait, and all leave after the grid
 // barriers (bounded too) with the error flag set.
 
 constexpr int F_TX = 16, F_TY = 8, F_ROWS = F_TX * F_TY;  // tile = 128 rows
 constexpr int F_THREADS = 192;                             // warps 0-3 epilogue, 4 copies, 5 MMAs
-constexpr int F_STAGES = 3;
+constexpr int F_STAGES = 4;
 constexpr int F_SZA = F_ROWS * L * 2;                      // 16 KB: an A K-block (128 x 64)
-constexpr int F_SZB = HID * L * 2;                         // 32 KB: a B K-block (up to 256 x 64)
-constexpr int F_OFF_A = 0;                                 // F_STAGES A slots
-constexpr int F_OFF_B = F_OFF_A + F_STAGES * F_SZA;        // F_STAGES B slots
-constexpr int F_OFF_ACT = F_OFF_B + F_STAGES * F_SZB;      // a: one A K-block
+constexpr int F_SZS = HID * L * 2;                         // 32 KB stage: a B K-block (256 x 64), or
+                                                           // A (16 KB) + B (64 x 64, 8 KB) of a window
+constexpr int F_OFF_S = 0;                                 // F_STAGES stages
+constexpr int F_OFF_ACT = F_OFF_S + F_STAGES * F_SZS;      // a: one A K-block
 constexpr int F_OFF_H = F_OFF_ACT + F_SZA;                 // h1 / h2: 4 A K-blocks; y in phase 2
-constexpr int F_OFF_BAR = F_OFF_H + 4 * F_SZA;
+constexpr int F_NBIAS = L + HID + HID + L + L;             // c1 | b1 | b2 | b3 | c2
+constexpr int F_OFF_BIAS = F_OFF_H + 4 * F_SZA;
+constexpr int F_OFF_GTAB = F_OFF_BIAS + 4 * F_NBIAS;       // resampling nz -> L: L entries
+constexpr int F_OFF_STAB = F_OFF_GTAB + 8 * L;             // resampling L -> nz: F_STAB entries
+constexpr int F_STAB = 1536;                               // levels beyond it are computed on the fly
+constexpr int F_OFF_BAR = F_OFF_STAB + 8 * F_STAB;
 constexpr int F_NBAR = 2 * F_STAGES + 2;                   // full[], empty[], acc_full, epi_done
-constexpr int F_SMEM = F_OFF_BAR + 8 * F_NBAR + 16;        // 229,456 bytes
+constexpr int F_SMEM = F_OFF_BAR + 8 * F_NBAR + 16;        // 228,704 bytes
+constexpr int F_SMEM_ALLOC = F_SMEM + 1024;                // the layout starts at the next 1024-byte boundary
 constexpr int F_TMEM_COLS = 512;
 constexpr int F_COL64 = 0, F_COL256 = 256;                 // accumulators: N = 64 and N = 256
 
@@ -411,20 +419,26 @@ struct FusedArgs {
     int *err;
 };
 
+// Shared-memory matrix descriptor, K-major, 128-byte swizzle (layout type 2,
+// bits [61,64)); SBO = 1024 B between 8-row groups; LBO unused for this
+// layout (set to 16 B).
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+    return umma::smem_desc(saddr, 16, 1024) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void tma2(uint32_t dst, const CUtensorMap *map, int c0, int c1, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(bar)
+        : "memory");
+}
+
 __device__ __forceinline__ void tma3(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, uint32_t bar) {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
         "%4}], [%5];" ::"r"(dst),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
-        : "memory");
-}
-
-__device__ __forceinline__ void tma4(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
-                                     uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-        "%5}], [%6];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
         : "memory");
 }
 
@@ -449,18 +463,33 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
                  : "memory");
 }
 
-// 16 consecutive FP32 accumulator columns of this thread's TMEM lane (row)
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&f)[16]) {
-    uint32_t v[16];
+// 32 consecutive FP32 accumulator columns of this thread's TMEM lane (row)
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&f)[32]) {
+    uint32_t v[32];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int q = 0; q < 16; ++q) f[q] = __uint_as_float(v[q]);
+    for (int q = 0; q < 32; ++q) f[q] = __uint_as_float(v[q]);
+}
+
+// the two source levels and the weight of the second, for resampling level l
+struct Interp {
+    unsigned short k0, k1;
+    float f;
+};
+__device__ __forceinline__ Interp make_interp(int l, int n_in, int n_out) {
+    int k0, k1;
+    float f;
+    interp_pos(l, n_in, n_out, k0, k1, f);
+    return Interp{(unsigned short)k0, (unsigned short)k1, f};
 }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
@@ -471,6 +500,26 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
 __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
     asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d)
                  : "memory");
+}
+
+// out[0..3] = (beta ? beta * out : 0) + v, four consecutive values
+__device__ __forceinline__ void store4(float *o, float v0, float v1, float v2, float v3, float beta) {
+    float4 r = make_float4(v0, v1, v2, v3);
+    if (beta != 0.f) {
+        const float4 p = *reinterpret_cast<const float4 *>(o);
+        r = make_float4(beta * p.x + v0, beta * p.y + v1, beta * p.z + v2, beta * p.w + v3);
+    }
+    *reinterpret_cast<float4 *>(o) = r;
+}
+__device__ __forceinline__ void store4(double *o, float v0, float v1, float v2, float v3, float beta) {
+    double2 r0 = make_double2(v0, v1), r1 = make_double2(v2, v3);
+    if (beta != 0.f) {
+        const double2 p0 = reinterpret_cast<const double2 *>(o)[0], p1 = reinterpret_cast<const double2 *>(o)[1];
+        r0 = make_double2((double)((float)beta * (float)p0.x + v0), (double)((float)beta * (float)p0.y + v1));
+        r1 = make_double2((double)((float)beta * (float)p1.x + v2), (double)((float)beta * (float)p1.y + v3));
+    }
+    reinterpret_cast<double2 *>(o)[0] = r0;
+    reinterpret_cast<double2 *>(o)[1] = r1;
 }
 
 // barrier among the 128 epilogue threads only (named barrier 1)
@@ -515,26 +564,28 @@ __device__ __forceinline__ void epi_to_smem(uint32_t tmem, uint32_t tcol, const 
     const int warp = threadIdx.x >> 5, r = threadIdx.x;
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + tcol;
 #pragma unroll 1
-    for (int c0 = 0; c0 < ncols; c0 += 16) {
-        float f[16];
-        tmem_ld16(lane_base + (uint32_t)c0, f);
+    for (int c0 = 0; c0 < ncols; c0 += 32) {
+        float f[32];
+        tmem_ld32(lane_base + (uint32_t)c0, f);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            f[q] += __ldg(bias + c0 + q);
+        for (int q = 0; q < 32; ++q) {
+            f[q] += bias[c0 + q];
             if (relu) f[q] = fmaxf(f[q], 0.f);
         }
-        const uint32_t blk = dst + (uint32_t)(c0 >> 6) * F_SZA + (uint32_t)r * 16;
+        const uint32_t row = dst + (uint32_t)(c0 >> 6) * F_SZA + (uint32_t)r * 128;
         const int q8 = (c0 & 63) >> 3;
-        st_shared_v4(blk + q8 * (F_ROWS * 16), pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]),
-                     pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
-        st_shared_v4(blk + (q8 + 1) * (F_ROWS * 16), pack_bf16x2(f[8], f[9]), pack_bf16x2(f[10], f[11]),
-                     pack_bf16x2(f[12], f[13]), pack_bf16x2(f[14], f[15]));
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+            st_shared_v4(row + (uint32_t)(((q8 + h) ^ (r & 7)) * 16), pack_bf16x2(f[8 * h], f[8 * h + 1]),
+                         pack_bf16x2(f[8 * h + 2], f[8 * h + 3]), pack_bf16x2(f[8 * h + 4], f[8 * h + 5]),
+                         pack_bf16x2(f[8 * h + 6], f[8 * h + 7]));
     }
 }
 
-// Producer: the TMA boxes of one layer's K-steps into the ring.
+// Producer: the TMA boxes of one layer's K-steps into the ring.  A window
+// step's stage holds A at its start and B 16 KB in; a dense step's holds B.
 struct Producer {
-    uint32_t sa, sb, full[F_STAGES], empty[F_STAGES];
+    uint32_t ss, full[F_STAGES], empty[F_STAGES];
     unsigned g;  // K-steps issued so far
     __device__ bool layer(int l, const CUtensorMap *amap, const CUtensorMap *bmap, int x0, int y0) {
         const bool conv = f_conv(l);
@@ -545,8 +596,9 @@ struct Producer {
             // the stage's previous use must have been consumed by its MMAs
             if (use > 0 && !mbar_wait(empty[s], (use - 1u) & 1u)) return false;
             arrive_expect(full[s], bytes);
-            if (conv) tma4(sa + s * F_SZA, amap, 0, x0 + i % 3, y0 + i / 3, 0, full[s]);
-            tma3(sb + s * F_SZB, bmap, 0, 0, 8 * i, full[s]);
+            const uint32_t st = ss + s * F_SZS;
+            if (conv) tma3(st, amap, 0, x0 + i % 3, y0 + i / 3, full[s]);
+            tma2(st + (conv ? F_SZA : 0), bmap, 64 * i, 0, full[s]);
         }
         return true;
     }
@@ -554,7 +606,7 @@ struct Producer {
 
 // MMA issuer: one layer's K-steps into its accumulator, then the layer's signal.
 struct Issuer {
-    uint32_t sa, sb, full[F_STAGES], empty[F_STAGES], acc_full, epi_done, tmem;
+    uint32_t ss, full[F_STAGES], empty[F_STAGES], acc_full, epi_done, tmem;
     unsigned g, nepi;
     bool first;
     __device__ bool layer(int l, uint32_t abase) {
@@ -568,18 +620,18 @@ struct Issuer {
         const int nn = f_n(l);
         const bool conv = f_conv(l);
         const uint32_t idesc = umma::instr_desc(128, nn);
-        const uint32_t lbo_a = F_ROWS * 16, lbo_b = (uint32_t)nn * 16;
         const uint32_t tcol = nn == HID ? F_COL256 : F_COL64;
         for (int i = 0; i < f_steps(l); ++i, ++g) {
             const int s = (int)(g % F_STAGES);
             if (!mbar_wait(full[s], (g / F_STAGES) & 1u)) return false;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t abuf = conv ? sa + s * F_SZA : abase + (uint32_t)i * F_SZA;
-            const uint32_t bbuf = sb + s * F_SZB;
+            const uint32_t st = ss + s * F_SZS;
+            const uint32_t abuf = conv ? st : abase + (uint32_t)i * F_SZA;
+            const uint32_t bbuf = conv ? st + F_SZA : st;
 #pragma unroll
-            for (int j = 0; j < 4; ++j)  // K = 16 per instruction: two K-slices
-                mma_f16(tmem + tcol, umma::smem_desc(abuf + 2 * j * lbo_a, lbo_a, 128),
-                        umma::smem_desc(bbuf + 2 * j * lbo_b, lbo_b, 128), idesc, (i > 0 || j > 0) ? 1u : 0u);
+            for (int j = 0; j < 4; ++j)  // K = 16 per instruction: 32 bytes along the swizzled rows
+                mma_f16(tmem + tcol, desc_sw128(abuf + 32 * j), desc_sw128(bbuf + 32 * j), idesc,
+                        (i > 0 || j > 0) ? 1u : 0u);
             mma_commit(empty[s]);
         }
         mma_commit(acc_full);
@@ -593,7 +645,9 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                 const __grid_constant__ CUtensorMap mc1, const __grid_constant__ CUtensorMap mw1,
                 const __grid_constant__ CUtensorMap mw2, const __grid_constant__ CUtensorMap mw3,
                 const __grid_constant__ CUtensorMap mc2, const FusedArgs a) {
-    extern __shared__ __align__(1024) uint8_t sm[];
+    extern __shared__ __align__(1024) uint8_t sm_raw[];
+    // the swizzled operand blocks must start on 1024-byte boundaries
+    uint8_t *sm = sm_raw + ((1024u - (smem_u32(sm_raw) & 1023u)) & 1023u);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     uint64_t *bars = reinterpret_cast<uint64_t *>(sm + F_OFF_BAR);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + F_NBAR);
@@ -618,45 +672,75 @@ __global__ void __launch_bounds__(F_THREADS, 1)
         empty[q] = smem_u32(bars + F_STAGES + q);
     }
     const uint32_t acc_full = smem_u32(bars + 2 * F_STAGES), epi_done = smem_u32(bars + 2 * F_STAGES + 1);
-    const uint32_t sa = smem_u32(sm + F_OFF_A), sb = smem_u32(sm + F_OFF_B);
+    const uint32_t ss = smem_u32(sm + F_OFF_S);
     const uint32_t s_act = smem_u32(sm + F_OFF_ACT), s_h = smem_u32(sm + F_OFF_H);
 
     const int nx = a.nx, ny = a.ny, nz = a.nz, nxh = nx + 2, nyh = ny + 2;
     const long long plane = (long long)nx * ny;
     const int ntx = (nx + F_TX - 1) / F_TX, nty = (ny + F_TY - 1) / F_TY, ntiles = ntx * nty;
     bool ok = true;
+    // the biases and the level-resampling tables in shared memory
+    float *bias = reinterpret_cast<float *>(sm + F_OFF_BIAS);
+    Interp *gtab = reinterpret_cast<Interp *>(sm + F_OFF_GTAB), *stab = reinterpret_cast<Interp *>(sm + F_OFF_STAB);
+    for (int i = tid; i < F_NBIAS; i += blockDim.x)
+        bias[i] = i < L ? a.param[OFF_c1 + i]
+                : i < L + HID ? a.param[OFF_B1 + i - L]
+                : i < L + 2 * HID ? a.param[OFF_B2 + i - L - HID]
+                : i < 2 * L + 2 * HID ? a.param[OFF_B3 + i - L - 2 * HID] : a.param[OFF_c2 + i - 2 * L - 2 * HID];
+    for (int i = tid; i < L; i += blockDim.x) gtab[i] = make_interp(i, nz, L);
+    for (int i = tid; i < min(nz, F_STAB); i += blockDim.x) stab[i] = make_interp(i, L, nz);
+    __syncthreads();
+    const float *b_c1 = bias, *b_b1 = bias + L, *b_b2 = bias + L + HID, *b_b3 = bias + L + 2 * HID,
+                *b_c2 = bias + 2 * L + 2 * HID;
 
     // ---- phase 0: the haloed input columns, 8 levels (16 bytes) per thread
+    // (four units per thread and pass, every load issued before the first is
+    // used: one CTA per SM needs many loads in flight; 32-bit indices, the
+    // haloed column count is below 2^28)
     {
         const T *in = static_cast<const T *>(a.in);
-        const long long cols = (long long)nxh * nyh, units = cols * (L / 8);
-        for (long long u = (long long)blockIdx.x * blockDim.x + tid; u < units;
-             u += (long long)gridDim.x * blockDim.x) {
-            const long long col = u % cols;
-            const int q = (int)(u / cols);
-            const int xh = (int)(col % nxh), yh = (int)(col / nxh);
-            const int x = xh == 0 ? nx - 1 : (xh > nx ? 0 : xh - 1);
-            const int y = yh == 0 ? ny - 1 : (yh > ny ? 0 : yh - 1);
-            const long long c = (long long)y * nx + x;
-            float v[8];
+        const unsigned cols = (unsigned)nxh * (unsigned)nyh, units = cols * (L / 8);
+        const unsigned stride = gridDim.x * blockDim.x;
+        for (unsigned u0 = blockIdx.x * blockDim.x + tid; u0 < units; u0 += 4 * stride) {
+            float x0[4][8], x1[4][8];
+            unsigned dst[4];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                int k0, k1;
-                float f;
-                interp_pos(q * 8 + e, nz, L, k0, k1, f);
-                v[e] = a.scale_in * ((1.f - f) * (float)in[k0 * plane + c] + f * (float)in[k1 * plane + c]);
+            for (int r = 0; r < 4; ++r) {
+                const unsigned u = min(u0 + r * stride, units - 1);
+                const unsigned col = u % cols, q = u / cols;
+                const unsigned xh = col % (unsigned)nxh, yh = col / (unsigned)nxh;
+                const int x = xh == 0 ? nx - 1 : ((int)xh > nx ? 0 : (int)xh - 1);
+                const int y = yh == 0 ? ny - 1 : ((int)yh > ny ? 0 : (int)yh - 1);
+                const long long c = (long long)y * nx + x;
+                dst[r] = col * L + q * 8;
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const Interp w = gtab[q * 8 + e];
+                    x0[r][e] = (float)in[w.k0 * plane + c];
+                    x1[r][e] = (float)in[w.k1 * plane + c];
+                }
             }
-            *reinterpret_cast<uint4 *>(a.xh + col * L + q * 8) =
-                make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
-                           pack_bf16x2(v[6], v[7]));
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if (u0 + r * stride >= units) continue;
+                const unsigned q = (dst[r] % L) / 8;
+                float v[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const float f = gtab[q * 8 + e].f;
+                    v[e] = a.scale_in * ((1.f - f) * x0[r][e] + f * x1[r][e]);
+                }
+                *reinterpret_cast<uint4 *>(a.xh + dst[r]) =
+                    make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                               pack_bf16x2(v[6], v[7]));
+            }
         }
     }
     ok = grid_barrier(a.bar, gridDim.x, ok);
 
     Producer P;
     Issuer I;
-    P.sa = I.sa = sa;
-    P.sb = I.sb = sb;
+    P.ss = I.ss = ss;
     for (int q = 0; q < F_STAGES; ++q) {
         P.full[q] = I.full[q] = full[q];
         P.empty[q] = I.empty[q] = empty[q];
@@ -701,13 +785,13 @@ __global__ void __launch_bounds__(F_THREADS, 1)
             for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
                 const int x0 = (tile % ntx) * F_TX, y0 = (tile / ntx) * F_TY;
                 if (!(ok = wait_acc())) break;
-                epi_to_smem(tmem, F_COL64, a.param + OFF_c1, L, true, s_act);
+                epi_to_smem(tmem, F_COL64, b_c1, L, true, s_act);
                 epi_signal();
                 if (!(ok = wait_acc())) break;
-                epi_to_smem(tmem, F_COL256, a.param + OFF_B1, HID, true, s_h);
+                epi_to_smem(tmem, F_COL256, b_b1, HID, true, s_h);
                 epi_signal();
                 if (!(ok = wait_acc())) break;
-                epi_to_smem(tmem, F_COL256, a.param + OFF_B2, HID, true, s_h);
+                epi_to_smem(tmem, F_COL256, b_b2, HID, true, s_h);
                 epi_signal();
                 if (!(ok = wait_acc())) break;
                 // z = acc + b3 as BF16, to the interior row and its periodic images in zh
@@ -715,13 +799,12 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                 uint32_t pk[32];
                 const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + F_COL64;
 #pragma unroll
-                for (int c0 = 0; c0 < L; c0 += 16) {
-                    float f[16];
-                    tmem_ld16(lane_base + (uint32_t)c0, f);
+                for (int c0 = 0; c0 < L; c0 += 32) {
+                    float f[32];
+                    tmem_ld32(lane_base + (uint32_t)c0, f);
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        pk[c0 / 2 + q] = pack_bf16x2(f[2 * q] + __ldg(a.param + OFF_B3 + c0 + 2 * q),
-                                                     f[2 * q + 1] + __ldg(a.param + OFF_B3 + c0 + 2 * q + 1));
+                    for (int q = 0; q < 16; ++q)
+                        pk[c0 / 2 + q] = pack_bf16x2(f[2 * q] + b_b3[c0 + 2 * q], f[2 * q + 1] + b_b3[c0 + 2 * q + 1]);
                 }
                 epi_signal();
                 if (x < nx && y < ny) {
@@ -755,6 +838,8 @@ __global__ void __launch_bounds__(F_THREADS, 1)
         } else {
             float *ysm = reinterpret_cast<float *>(sm + F_OFF_H);  // y of the tile, [L][128]
             T *out = static_cast<T *>(a.out);
+            // vector stores need rows of a multiple of 4 values and an aligned field
+            const bool vec4 = nx % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & (4 * sizeof(T) - 1)) == 0;
             for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
                 const int x0 = (tile % ntx) * F_TX, y0 = (tile / ntx) * F_TY;
                 const int x = x0 + (tid % F_TX), y = y0 + (tid / F_TX);
@@ -763,11 +848,11 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                 float acc[L];
                 const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + F_COL64;
 #pragma unroll
-                for (int c0 = 0; c0 < L; c0 += 16) {
-                    float f[16];
-                    tmem_ld16(lane_base + (uint32_t)c0, f);
+                for (int c0 = 0; c0 < L; c0 += 32) {
+                    float f[32];
+                    tmem_ld32(lane_base + (uint32_t)c0, f);
 #pragma unroll
-                    for (int q = 0; q < 16; ++q) acc[c0 + q] = f[q];
+                    for (int q = 0; q < 32; ++q) acc[c0 + q] = f[q];
                 }
                 epi_signal();  // the accumulator is free for the next tile's MMAs
                 const uint4 *zr = reinterpret_cast<const uint4 *>(a.zh + ((long long)(y + 1) * nxh + (x + 1)) * L);
@@ -778,16 +863,31 @@ __global__ void __launch_bounds__(F_THREADS, 1)
 #pragma unroll
                     for (int e = 0; e < 8; ++e)
                         ysm[(q * 8 + e) * F_ROWS + tid] =
-                            acc[q * 8 + e] + __ldg(a.param + OFF_c2 + q * 8 + e) + __bfloat162float(zb[e]);
+                            acc[q * 8 + e] + b_c2[q * 8 + e] + __bfloat162float(zb[e]);
                 }
                 epilogue_sync();
-                if (inside) {
+                if (vec4 && x0 + F_TX <= nx) {
+                    // four consecutive x per thread and level (16-byte rows of y in
+                    // shared memory, vector stores): thread = (level phase, tile row, x group)
+                    const int lo = tid >> 5, yr = (tid >> 2) & 7, xg = tid & 3;
+                    if (y0 + yr < ny) {
+                        const long long c = (long long)(y0 + yr) * nx + x0 + 4 * xg;
+                        const int row = yr * F_TX + 4 * xg;
+                        for (int k = lo; k < nz; k += 4) {
+                            const Interp w = k < F_STAB ? stab[k] : make_interp(k, L, nz);
+                            const float4 p0 = *reinterpret_cast<const float4 *>(ysm + w.k0 * F_ROWS + row);
+                            const float4 p1 = *reinterpret_cast<const float4 *>(ysm + w.k1 * F_ROWS + row);
+                            const float g0 = a.scale_out * (1.f - w.f), g1 = a.scale_out * w.f;
+                            store4(out + (long long)k * plane + c, g0 * p0.x + g1 * p1.x, g0 * p0.y + g1 * p1.y,
+                                   g0 * p0.z + g1 * p1.z, g0 * p0.w + g1 * p1.w, a.beta);
+                        }
+                    }
+                } else if (inside) {
                     const long long c = (long long)y * nx + x;
                     for (int k = 0; k < nz; ++k) {
-                        int l0, l1;
-                        float f;
-                        interp_pos(k, L, nz, l0, l1, f);
-                        const float v = a.scale_out * ((1.f - f) * ysm[l0 * F_ROWS + tid] + f * ysm[l1 * F_ROWS + tid]);
+                        const Interp w = k < F_STAB ? stab[k] : make_interp(k, L, nz);
+                        const float v =
+                            a.scale_out * ((1.f - w.f) * ysm[w.k0 * F_ROWS + tid] + w.f * ysm[w.k1 * F_ROWS + tid]);
                         T *o = out + (long long)k * plane + c;
                         *o = a.beta == 0.f ? (T)v : (T)((float)a.beta * (float)*o + v);
                     }
@@ -823,31 +923,31 @@ static EncodeFn encoder() {
     return fn;
 }
 
-// A weight matrix W[N][K] (BF16, row-major) seen as (k % 8, n, k / 8), boxes
-// of 8 x N x 8: one K-block of 64 in the operand layout above.
+// A weight matrix W[N][K] (BF16, row-major), boxes of 64 x N: one K-block of
+// 64 values of every row, 128-byte swizzled.
 static bool weight_map(CUtensorMap *m, const bf16 *w, int N, int K) {
     EncodeFn enc = encoder();
     if (!enc) return false;
-    const cuuint64_t dims[3] = {8, (cuuint64_t)N, (cuuint64_t)(K / 8)};
-    const cuuint64_t strides[2] = {2ull * K, 16};
-    const cuuint32_t box[3] = {8, (cuuint32_t)N, 8};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16 *>(w), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)N};
+    const cuuint64_t strides[1] = {2ull * K};
+    const cuuint32_t box[2] = {64, (cuuint32_t)N};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(w), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Haloed columns H[(yh)(nx+2) + xh][L] seen as (l % 8, xh, yh, l / 8), boxes
-// of 8 x 16 x 8 x 8: the 128 rows of a tile (x fastest) of one window.
+// Haloed columns H[(yh)(nx+2) + xh][L] seen as (l, xh, yh), boxes of 64 x 16
+// x 8: the 128 rows of a tile (x fastest) of one window, 128-byte swizzled.
 static bool column_map(CUtensorMap *m, const bf16 *h, int nx, int ny) {
     EncodeFn enc = encoder();
     if (!enc) return false;
-    const cuuint64_t dims[4] = {8, (cuuint64_t)(nx + 2), (cuuint64_t)(ny + 2), L / 8};
-    const cuuint64_t strides[3] = {2ull * L, 2ull * L * (nx + 2), 16};
-    const cuuint32_t box[4] = {8, F_TX, F_TY, L / 8};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(h), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+    const cuuint64_t dims[3] = {L, (cuuint64_t)(nx + 2), (cuuint64_t)(ny + 2)};
+    const cuuint64_t strides[2] = {2ull * L, 2ull * L * (nx + 2)};
+    const cuuint32_t box[3] = {L, F_TX, F_TY};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16 *>(h), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -857,11 +957,11 @@ template <typename T>
 static int fused_grid(Net &n) {
     static std::atomic<unsigned long long> attr_set{0};
     if (!(attr_set.load() >> n.device & 1ull)) {
-        PCF_CUDA_TRY(cudaFuncSetAttribute(k_net_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, F_SMEM));
+        PCF_CUDA_TRY(cudaFuncSetAttribute(k_net_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, F_SMEM_ALLOC));
         attr_set.fetch_or(1ull << n.device);
     }
     int per_sm = 0, sms = 0;
-    PCF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_net_fused<T>, F_THREADS, F_SMEM));
+    PCF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_net_fused<T>, F_THREADS, F_SMEM_ALLOC));
     PCF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, n.device));
     if (per_sm < 1) return 0;
     return sms;
@@ -870,7 +970,7 @@ static int fused_grid(Net &n) {
 template <typename T>
 static int apply_fused(Net &n, const void *in, int nx, int ny, int nz, float si, float so, float beta, void *out,
                        cudaStream_t st) {
-    if ((long long)(nx + 2) * (ny + 2) > n.hcap) return PCF_ERANGE;
+    if ((long long)(nx + 2) * (ny + 2) > n.hcap || (long long)(nx + 2) * (ny + 2) >= (1ll << 28)) return PCF_ERANGE;
     if (n.map_nx != nx || n.map_ny != ny) {
         if (!column_map(&n.xmap, n.xh, nx, ny) || !column_map(&n.zmap, n.zh, nx, ny)) return PCF_ECUDA;
         n.map_nx = nx;
@@ -898,7 +998,7 @@ static int apply_fused(Net &n, const void *in, int nx, int ny, int nz, float si,
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)grid);
     cfg.blockDim = dim3(F_THREADS);
-    cfg.dynamicSmemBytes = F_SMEM;
+    cfg.dynamicSmemBytes = F_SMEM_ALLOC;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -1302,7 +1402,7 @@ int pcf_net_apply_device(pcf_net *w, const void *in, int nx, int ny, int nz, dou
                          double beta, void *out, int fp64, void *stream) {
     if (!w || !in || !out || nx < 1 || ny < 1 || nz < 1) return PCF_EINVAL;
     Net &n = w->n;
-    if ((long long)nx * ny > n.cap) return PCF_ERANGE;
+    if ((long long)nx * ny > n.cap || nz > 65535) return PCF_ERANGE;
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : n.stream;
     return fp64 ? apply_fused<double>(n, in, nx, ny, nz, (float)scale_in, (float)scale_out, (float)beta, out, st)
                 : apply_fused<float>(n, in, nx, ny, nz, (float)scale_in, (float)scale_out, (float)beta, out, st);
