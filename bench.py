@@ -809,22 +809,31 @@ def learned_arm(args, s, cfg, d_rhs, d_rho, d_betar, d_dpip, local_rank):
     from pincflow_poisson import learned as L
     dom = cfg["dom"]
     t0 = time.perf_counter()
-    pairs_ws = L.training_pairs(range(args.learned_pairs), device=local_rank)
-    pairs_pc = L.preconditioner_pairs(range(args.learned_pairs), device=local_rank)
+    pairs = {"warm_start": L.training_pairs(range(args.learned_pairs), device=local_rank),
+             "stage": L.preconditioner_pairs(range(args.learned_pairs), device=local_rank)}
+    if args.config == "c5":
+        # the same stage trained on 128 x 128 x 192 patches of the workload's own family
+        pairs["stage_c5_patches"] = L.preconditioner_pairs(range(args.learned_pairs), nx=128, ny=128, nz=192,
+                                                           device=local_rank, family="c5")
     t1 = time.perf_counter()
     cols = max(dom.nx * dom.ny, 128 * 128)
-    nets = {"warm_start": L.LearnedNet(device=local_rank, max_columns=cols, seed=0),
-            "stage": L.LearnedNet(device=local_rank, max_columns=cols, seed=1)}
-    nets["stage"].set_bias_free(True)
-    loss = {"warm_start": L.train(nets["warm_start"], pairs_ws, epochs=args.learned_epochs, device=local_rank),
-            "stage": L.train(nets["stage"], pairs_pc, epochs=args.learned_epochs, device=local_rank)}
+    nets, loss = {}, {}
+    for q, role in enumerate(pairs):
+        nets[role] = L.LearnedNet(device=local_rank, max_columns=cols, seed=q)
+        if role != "warm_start":
+            nets[role].set_bias_free(True)
+        loss[role] = L.train(nets[role], pairs[role], epochs=args.learned_epochs, lr=args.learned_lr,
+                             device=local_rank)
     t2 = time.perf_counter()
     kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000, precision="mixed",
               residual="true", multigrid=args.method == "mg", mg_dtau=args.mg_dtau)
-    out = {"training": {"configuration": "c3: 128x128x64 Boussinesq, 1-5 Gaussian hills, N ~ U(0.005, 0.02)",
-                        "pairs": len(pairs_ws), "epochs": args.learned_epochs, "generation_s": t1 - t0,
-                        "training_s": t2 - t1, "parameters": L.NPARAM}}
-    for role, bit in (("warm_start", 1), ("stage", 2)):
+    out = {"training": {"configuration": "c3: 128x128x64 Boussinesq, 1-5 Gaussian hills, N ~ U(0.005, 0.02); "
+                                         "stage_c5_patches: 128x128x192 patches of the c5 family at its resolution",
+                        "pairs": {r: len(p) for r, p in pairs.items()}, "epochs": args.learned_epochs,
+                        "lr": args.learned_lr,
+                        "generation_s": t1 - t0, "training_s": t2 - t1, "parameters": L.NPARAM}}
+    for role in nets:
+        bit = 1 if role == "warm_start" else 2
         s.attach_network(nets[role])
         nl = pcf.PoissonNamelist(**kw, learned=bit)
         infos = []
@@ -836,8 +845,8 @@ def learned_arm(args, s, cfg, d_rhs, d_rho, d_betar, d_dpip, local_rank):
         s.attach_network(None)
         out[role] = {"s": statistics.mean(i.timings_ms["total"] for i in infos) / 1e3, "iterations": infos[-1].niter,
                      "true_residual": infos[-1].true_residual, "converged": not infos[-1].errflag,
-                     "loss_first_epoch": float(np.mean(loss[role][:len(pairs_ws)])),
-                     "loss_last_epoch": float(np.mean(loss[role][-len(pairs_ws):]))}
+                     "loss_first_epoch": float(np.mean(loss[role][:len(pairs[role])])),
+                     "loss_last_epoch": float(np.mean(loss[role][-len(pairs[role]):]))}
     # the fused network kernel alone on this grid: CUDA events around
     # back-to-back applications on an FP32 field (the stage's case)
     import torch
@@ -1077,7 +1086,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned arm")
     ap.add_argument("--learned-pairs", type=int, default=48, help="training pairs of each network")
-    ap.add_argument("--learned-epochs", type=int, default=8)
+    ap.add_argument("--learned-epochs", type=int, default=16)
+    ap.add_argument("--learned-lr", type=float, default=2e-3)
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

@@ -143,8 +143,8 @@ typedef struct {
                                       the Krylov operator, the coarser levels and the FP64 true residual are
                                       unchanged); 0: the FP32 copies.  On levels 128 or more cells wide with nx a
                                       multiple of 8 those stencils load the BF16 tiles into shared memory by TMA
-                                      (same arithmetic, same results).  The learned preconditioner stage
-                                      (learned & 2) always runs the FP32 V-cycle it was trained on (1) */
+                                      (same arithmetic, same results); the learned preconditioner stage
+                                      (learned & 2) runs the same V-cycle, which its training pairs come from (1) */
 } pcf_params;
 
 typedef struct {
@@ -481,6 +481,15 @@ int pcf_set_network(pcf_handle *h, pcf_net *net);
  * call before any stream capture.  All calls share the scratch, so calls that
  * may overlap on the GPU (on different streams) race and must be serialised. */
 int pcf_global_dot_noalloc(const double *a, const double *b, long long n, double *result, void *stream);
+/* Test hook of the failure path (no reference counterpart): in the stencils
+ * that stage their BF16 coefficient tiles by TMA, the copy of z-level `level`
+ * is not issued, and every wait for a copy gives up after wait_limit_s
+ * seconds (at most 10).  The wait for the missing copy then runs out, the
+ * kernel records PCF_ECUDA in the solve's status and leaves, and the solve
+ * returns errflag = 1 with status PCF_ECUDA.  level < 0 turns the hook off
+ * (waits bounded by 2 s again).  Drops the handle's captured iteration
+ * batches. */
+int pcf_test_stall_staged_copy(pcf_handle *h, int level, double wait_limit_s);
 int pcf_profile_enable(pcf_handle *h, int on);  /* also clears the accumulators */
 int pcf_profile_read(const pcf_handle *h, int tag, double *ms, long long *count, double *bytes);
 

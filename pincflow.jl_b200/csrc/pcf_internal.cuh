@@ -128,8 +128,10 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 }
 
 // Waits for the mbarrier phase of the given parity to complete; gives up
-// after 2 s of %globaltimer and returns false (the caller records the error).
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
+// after limit_ns of %globaltimer (2 s by default) and returns false (the
+// caller records the error).
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase,
+                                          unsigned long long limit_ns = 2000000000ull) {
     uint64_t t0;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
     for (;;) {
@@ -144,7 +146,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
         if (done) return true;
         uint64_t t1;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-        if (t1 - t0 > 2000000000ull) return false;  // 2 s
+        if (t1 - t0 > limit_ns) return false;
     }
 }
 
@@ -205,4 +207,9 @@ struct pcf_handle {
     pcf::MgState *mg;            // multigrid hierarchy (allocated on first use)
     float *lr32;                 // learned preconditioner stage: residual and correction (2 n, on first use)
     long long op_version;        // incremented whenever the operator changes
+    // test hook (pcf_test_stall_staged_copy): 1 + the z-level whose staged
+    // coefficient copy is not issued (0: off), and the staged stencils' wait
+    // limit (0: the default 2 s)
+    int test_stall;
+    unsigned long long test_wait_ns;
 };

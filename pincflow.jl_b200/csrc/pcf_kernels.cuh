@@ -357,6 +357,11 @@ struct StencilArgs {
     ReduceCtx red{};
     const KrylovScalars *guard = nullptr;  // skip when guard->done (may be null)
     int guard_update = 0;                  // 1: run only while guard->update is pending
+    // staged stencils (C16 = 2): the bound of each wait for a copy, and a test
+    // hook -- the z-level whose copy is never issued, so that its wait runs out
+    // (-1: none)
+    unsigned long long wait_ns = 2000000000ull;
+    int stall_level = -1;
 };
 
 // Shared-memory ring of z-planes of the input: NS slots of (TY+2) x (TX*V+2)
@@ -484,6 +489,7 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
     // C16 == 2: thread 0 loads level kk's tile of every plane into stage st
     const char *maps = C16 == 2 ? static_cast<const char *>(a.tmap16) + (V == 2 ? 3 * 128 : 0) : nullptr;
     auto issue = [&](int kk, int st) {
+        if (kk == a.stall_level) return;  // test hook: no copy in flight, the wait for it runs out
         const uint32_t bar = smem_u32(bars + st), dst = smem_u32(stg + st * STAGE);
         mbar_arrive_expect(bar, (uint32_t)(STAGE * sizeof(__nv_bfloat16)));  // whole boxes, zero-filled outside
         if (HORIZ) {
@@ -545,7 +551,7 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
             const long long base = plane * k + (long long)a.nx * y + x;
             T c[PCF_NCOEF][V];
             if constexpr (C16 == 2) {
-                failed = !mbar_wait(smem_u32(bars + j % NST), (uint32_t)((j / NST) & 1));
+                failed = !mbar_wait(smem_u32(bars + j % NST), (uint32_t)((j / NST) & 1), a.wait_ns);
                 const __nv_bfloat16 *cs = stg + (j % NST) * STAGE + ty * R::W + tx * V;
 #pragma unroll
                 for (int p = 0; p < PCF_NCOEF; ++p) {
@@ -695,7 +701,7 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
                         g->done = 1;
                     }
                     for (int q = j; q < j + NST && k0 + q < k1; ++q)
-                        mbar_wait(smem_u32(bars + q % NST), (uint32_t)((q / NST) & 1));
+                        mbar_wait(smem_u32(bars + q % NST), (uint32_t)((q / NST) & 1), a.wait_ns);
                 }
                 return;
             }

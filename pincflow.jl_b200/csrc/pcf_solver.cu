@@ -228,7 +228,10 @@ static int stencil_bulk_ready() {
 // 32 SV x 4 cells) on the handle's stream; false (nothing launched) if the
 // device refuses its shared memory or the grid exceeds the partials buffer.
 template <typename T, int SV, bool HORIZ, int EPI, bool DIFF>
-static bool launch_staged(pcf_handle *h, const StencilArgs<T> &a) {
+static bool launch_staged(pcf_handle *h, const StencilArgs<T> &a0) {
+    StencilArgs<T> a = a0;
+    if (h->test_stall) a.stall_level = h->test_stall - 1;
+    if (h->test_wait_ns) a.wait_ns = h->test_wait_ns;
     const int cap = stencil_bulk_ready<T, SV, 32, 4, HORIZ, EPI, DIFF>();
     if (cap <= 0) return false;
     constexpr int W = 32 * SV;
@@ -938,7 +941,7 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
     }
     m.coarse_iters = prm->mg_coarse_iterations;
     // the learned preconditioner stage is trained on, and validated with, the FP32 V-cycle
-    m.bf16 = prm->mg_operator_bf16 != 0 && (prm->learned & 2) == 0;
+    m.bf16 = prm->mg_operator_bf16 != 0;
     if (m.bf16 && !h->coef16) {
         // first use: allocate and convert; later assemblies and pcf_set_operator write it themselves
         const size_t bytes = sizeof(__nv_bfloat16) * (size_t)h->d.n * PCF_NCOEF;
@@ -1311,6 +1314,11 @@ static int run_finish(pcf_handle *h, const Work<T> &w, const LoopCfg &c, bool pr
     // the latest status (a batch issued after convergence leaves it unchanged)
     PCF_CUDA_TRY(cudaMemcpy(h->h_scal, w.scal, sizeof(KrylovScalars), cudaMemcpyDeviceToHost));
     const KrylovScalars s = *h->h_scal;
+    if (s.status == PCF_ECUDA) {
+        // a stencil block that gave up on its copies left before the reduction,
+        // so the reduction ticket was not returned to zero
+        PCF_CUDA_TRY(cudaMemsetAsync(h->ticket, 0, sizeof(unsigned int) * 4, h->stream));
+    }
     h->prof_iter = -1;
     prof_flush(h, s.iter);
     h->hist_len = std::min(hist_off + s.iter, kHistCap);
@@ -2565,6 +2573,17 @@ long long pcf_launch_count(const pcf_handle *h) { return h ? h->launches : 0; }
 int pcf_set_network(pcf_handle *h, pcf_net *net) {
     if (!h) return PCF_EINVAL;
     h->net = net;
+    return PCF_OK;
+}
+
+int pcf_test_stall_staged_copy(pcf_handle *h, int level, double wait_limit_s) {
+    if (!h || !(wait_limit_s >= 0.0) || wait_limit_s > 10.0) return PCF_EINVAL;
+    PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->test_stall = level >= 0 ? level + 1 : 0;
+    h->test_wait_ns = level >= 0 ? (unsigned long long)(wait_limit_s * 1e9) : 0ull;
+    if (level >= 0 && h->test_wait_ns == 0) h->test_wait_ns = 1;
+    clear_graphs(h);  // captured batches hold the previous setting
     return PCF_OK;
 }
 

@@ -42,6 +42,7 @@ EXPORTS = [
     "pcf_correct", "pcf_correct_device", "pcf_apply_corrector_device",
     "pcf_set_predictand_boundaries_device", "pcf_modify_compressible_wind_device",
     "pcf_implicit_predictor_device", "pcf_implicit_step_device", "pcf_implicit_step",
+    "pcf_test_stall_staged_copy",
 ]
 TUNE_KERNELS = ["total32", "total32_diff", "horiz32", "total64", "horiz64"]
 PROF_TAGS = ["apply32", "apply64", "pseudo32", "pseudo64", "thomas32", "thomas64", "update32", "update64",
@@ -149,6 +150,7 @@ def load(path: str | None = None):
     lib.pcf_implicit_predictor_device.argtypes = [vp, f64, f64, ctypes.c_int] + [vp] * 11
     lib.pcf_implicit_step_device.argtypes = [vp, f64, f64, P(PcfParams)] + [vp] * 13 + [P(PcfResult)]
     lib.pcf_implicit_step.argtypes = [vp, f64, f64, P(PcfParams)] + [dp] * 13 + [P(PcfResult)]
+    lib.pcf_test_stall_staged_copy.argtypes = [vp, ctypes.c_int, f64]
     for name in EXPORTS:
         getattr(lib, name).restype = getattr(lib, name).restype or ctypes.c_int
     lib.pcf_strerror.restype = ctypes.c_char_p

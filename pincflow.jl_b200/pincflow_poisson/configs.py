@@ -116,12 +116,15 @@ def c4(index: int, nx: int):
     return c3(10_000 + index, nx=nx, ny=nx, nz=nx // 2) | {"name": "c4"}
 
 
-def c5(seed: int = 5, nx: int = 512, ny: int = 512, nz: int = 192):
+def c5(seed: int = 5, nx: int = 512, ny: int = 512, nz: int = 192, lx: float = 400e3, ly: float = 400e3,
+       ridges: int = 20):
+    """The large domain; smaller lx, ly and ridge counts give patches of the
+    same family at the same resolution (training data of the learned part)."""
     dom = F.Domain(nx, ny, nz)
-    lx, ly, lz = 400e3, 400e3, 40e3
+    lz = 40e3
     rng = np.random.default_rng(seed)
     xs, ys = F.cell_centres(dom, lx, ly)
-    hb = gaussian_hills(xs, ys, lx, ly, rng, 20, 2000.0, 5e3, 20e3, ridge=True)
+    hb = gaussian_hills(xs, ys, lx, ly, rng, ridges, 2000.0, 5e3, 20e3, ridge=True)
     if hb.max() > 2000.0:
         hb *= 2000.0 / hb.max()
     g = F.grid(dom, lx, ly, lz, hb)
@@ -134,6 +137,15 @@ def c5(seed: int = 5, nx: int = 512, ny: int = 512, nz: int = 192):
     env = np.exp(-((X / 40e3) ** 2 + (Y / 40e3) ** 2 + ((zc - lz / 2) / (lz / 6)) ** 2))
     rhs = 1e-3 * env * np.cos(k * X + k * zc) + 1e-2 * rng.standard_normal(dom.interior_shape)
     return _finish(dom, "PseudoIncompressible", g, atm, rhs, 1.0, 1.0, None, seed, "c5")
+
+
+def c5_patch(index: int, n: int = 128):
+    """An n x n x 192 patch of the c5 family at c5's resolution (781 m x
+    781 m cells, lz = 40 km), with ridges in proportion to its area and its own
+    seed: the learned part's training problems for the c5 workload."""
+    frac = n / 512
+    return c5(seed=20_000 + index, nx=n, ny=n, nz=192, lx=400e3 * frac, ly=400e3 * frac,
+              ridges=max(1, round(20 * frac * frac))) | {"name": "c5_patch"}
 
 
 CONFIGS = {"c1": c1, "c2": c2, "c3": c3, "c5": c5}

@@ -159,13 +159,21 @@ def attach(solver: PoissonSolver, net: LearnedNet | None):
     solver._net = net
 
 
-def training_pairs(indices, nx=128, ny=128, nz=64, tolerance=1e-8, device=0):
+def _problem(family, i, nx, ny, nz):
+    """Training problem i: configs.c3 (the training configuration) or, with
+    family "c5", a patch of the c5 family at c5's resolution (nx = ny)."""
+    if family == "c5":
+        return C.c5_patch(int(i), n=nx)
+    return C.c3(int(i), nx=nx, ny=ny, nz=nz)
+
+
+def training_pairs(indices, nx=128, ny=128, nz=64, tolerance=1e-8, device=0, family="c3"):
     """(b / RMS(b), s / RMS(b)) FP32 pairs from plain FP64 solves of the training
-    configuration (configs.c3 with seeds `indices`)."""
+    configuration (configs.c3 with seeds `indices`, or c5 patches)."""
     out = []
     solver = None
     for i in indices:
-        cfg = C.c3(int(i), nx=nx, ny=ny, nz=nz)
+        cfg = _problem(family, i, nx, ny, nz)
         if solver is None:
             solver = PoissonSolver(cfg["dom"], cfg["model"], device=device)
         solver.set_grid(cfg["fields"])
@@ -182,18 +190,18 @@ def training_pairs(indices, nx=128, ny=128, nz=64, tolerance=1e-8, device=0):
     return out
 
 
-def preconditioner_pairs(indices, nx=128, ny=128, nz=64, tolerance=1e-8, device=0, **mg):
+def preconditioner_pairs(indices, nx=128, ny=128, nz=64, tolerance=1e-8, device=0, family="c3", **mg):
     """(r2 / RMS(r2), e / RMS(r2)) FP32 pairs for the learned preconditioner
     stage: for a training right-hand side b with plain FP64 solution s*, the
     multigrid V-cycle's output z = M(b) leaves the residual r2 = b - A z and
     the error e = s* - z, which the stage N(r2) should approximate.  The
-    V-cycle is the FP32 one that the stage runs with (learned & 2 uses the
-    FP32 operator copies)."""
+    V-cycle is the solver's default one (BF16 operator copies on the two
+    finest levels), as in the stage's solves; mg overrides its settings."""
     out = []
     solver = None
-    nl_mg = PoissonNamelist(precision="mixed", multigrid=True, **{"mg_operator_bf16": False, **mg})
+    nl_mg = PoissonNamelist(precision="mixed", multigrid=True, **mg)
     for i in indices:
-        cfg = C.c3(int(i), nx=nx, ny=ny, nz=nz)
+        cfg = _problem(family, i, nx, ny, nz)
         if solver is None:
             solver = PoissonSolver(cfg["dom"], cfg["model"], device=device)
         solver.set_grid(cfg["fields"])

@@ -53,7 +53,7 @@ class PoissonNamelist:
     mg_coarse_iterations: int = 4     # multigrid: smoothing steps on the coarsest level
     mg_min_columns: int = 16          # multigrid: a level with at most this many columns is the coarsest
     autotune: bool = False            # time the stencil tile shapes of each new grid size on first use
-    mg_operator_bf16: bool = True     # multigrid: finest and first coarse level stencils read BF16 copies (not learned & 2)
+    mg_operator_bf16: bool = True     # multigrid: finest and first coarse level stencils read BF16 copies
 
     def to_c(self) -> _lib.PcfParams:
         p = _lib.PcfParams()
@@ -144,6 +144,13 @@ class PoissonSolver:
         with PoissonNamelist(learned=True); None detaches."""
         from .learned import attach
         attach(self, net)
+
+    def test_stall_staged_copy(self, level: int, wait_limit_s: float = 1e-3):
+        """Test hook of the failure path: the TMA-staged stencils skip the copy
+        of z-level `level` and bound every copy wait by wait_limit_s, so that
+        the next solve gives up with status PCF_ECUDA; level < 0 turns it off."""
+        _lib.check(self.lib.pcf_test_stall_staged_copy(self._h, int(level), float(wait_limit_s)),
+                   "pcf_test_stall_staged_copy")
 
     def residual_history(self) -> np.ndarray:
         """Relative recursive residual after each iteration of the last solve."""

@@ -293,3 +293,43 @@ def test_tiny_grid_solves_in_one_block(solvers, oracle, pcf):
         assert rel_err(_drop_null(cfg, got), _drop_null(cfg, ref)) < 1e-6
         hist = s.residual_history()
         assert len(hist) == info.niter and hist[-1] <= 1e-10
+
+
+@pytest.mark.parametrize("level", [0, 5, 31])
+def test_staged_stencil_wait_gives_up_and_next_solve_succeeds(pcf, level):
+    """The failure path of the TMA-staged V-cycle stencils: with the test hook
+    the copy of one z-level is never issued (nothing is in flight for it) and
+    every copy wait is bounded by 1 ms, so the wait runs out; the kernel drains
+    its other copy, records PCF_ECUDA and leaves.  The solve reports errflag and
+    status PCF_ECUDA without a device fault, dpip stays untouched, and with the
+    hook off the next solve on the same handle converges to the same pressure
+    as a fresh handle (the reduction state was reset)."""
+    from pincflow_poisson import configs as C
+    cfg = C.c2(nx=128, ny=64, nz=32)  # 128 wide: the finest level's stencils stage their tiles
+    dom = cfg["dom"]
+    kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=2000, residual="true",
+              precision="mixed", multigrid=True)
+    args = (cfg["rhs"], cfg["rho"], cfg["betar"], cfg["dt"], cfg["rayleigh_factor"], cfg["tolref"],
+            pcf.PoissonNamelist(**kw))
+
+    def handle():
+        s = pcf.PoissonSolver(dom, cfg["model"])
+        s.set_grid(cfg["fields"])
+        s.set_background(cfg["fields"])
+        return s
+
+    with handle() as ref:
+        good = np.zeros(dom.halo_shape)
+        ok = ref.solve_poisson(*args, good)
+        assert not ok.errflag
+    with handle() as s:
+        s.test_stall_staged_copy(level, 1e-3)
+        dpip = np.full(dom.halo_shape, 3.0)
+        info = s.solve_poisson(*args, dpip)
+        assert info.errflag and info.status == pcf._lib.PCF_ECUDA, info
+        assert (dpip == 3.0).all()
+        s.test_stall_staged_copy(-1)
+        again = s.solve_poisson(*args, dpip)
+        assert not again.errflag and again.true_residual <= 1e-10, again
+        assert again.niter == ok.niter
+        assert np.abs(dpip - good).max() <= 1e-12 * np.abs(good).max()
