@@ -332,4 +332,5 @@ def test_staged_stencil_wait_gives_up_and_next_solve_succeeds(pcf, level):
         again = s.solve_poisson(*args, dpip)
         assert not again.errflag and again.true_residual <= 1e-10, again
         assert again.niter == ok.niter
-        assert np.abs(dpip - good).max() <= 1e-12 * np.abs(good).max()
+        inner, ref_inner = dom.interior(dpip), dom.interior(good)
+        assert np.abs(inner - ref_inner).max() <= 1e-12 * np.abs(ref_inner).max()
