@@ -490,6 +490,13 @@ int pcf_global_dot_noalloc(const double *a, const double *b, long long n, double
  * (waits bounded by 2 s again).  Drops the handle's captured iteration
  * batches. */
 int pcf_test_stall_staged_copy(pcf_handle *h, int level, double wait_limit_s);
+/* Bounds checking (no reference counterpart): in the library built with
+ * -DPCF_BOUNDS_CHECK (libpincflow_poisson_checked.so) the kernels check their
+ * global indices against the arrays' extents, skip an access out of range and
+ * record the first one.  Sets *enabled (1 in that build, 0 otherwise) and the
+ * first recorded event since the last call -- the check site (0: none) and the
+ * index -- then clears the records; synchronises the current device. */
+int pcf_bounds_check_status(int *enabled, long long *site, long long *index);
 int pcf_profile_enable(pcf_handle *h, int on);  /* also clears the accumulators */
 int pcf_profile_read(const pcf_handle *h, int tag, double *ms, long long *count, double *bytes);
 

@@ -1,9 +1,12 @@
 """Builds libpincflow_poisson.so (the C-ABI solver library) for sm_100a.
 
-Usage: python pincflow.jl_b200/build.py [--force] [--verbose]
+Usage: python pincflow.jl_b200/build.py [--force] [--verbose] [--checked]
 
 The library is written in-tree to pincflow.jl_b200/lib/ so that it travels
-with the repository snapshot.  Each .cu file is compiled separately (in
+with the repository snapshot.  --checked builds the bounds-checked variant
+libpincflow_poisson_checked.so (-DPCF_BOUNDS_CHECK: every instrumented
+global index is checked against its array's extent; pcf_bounds_check_status
+reports the first failure).  Each .cu file is compiled separately (in
 parallel) and linked with nvcc; a file is rebuilt when it or any header is
 newer than its object.
 """
@@ -22,6 +25,8 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 OBJDIR = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libpincflow_poisson.so")
+OBJDIR_CHECKED = os.path.join(HERE, "_build_checked")
+LIB_CHECKED = os.path.join(LIBDIR, "libpincflow_poisson_checked.so")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -40,9 +45,9 @@ def _stale(src: str, obj: str) -> bool:
     return any(os.path.getmtime(p) > t for p in [src] + _headers())
 
 
-def _compile(src: str, verbose: bool) -> str:
-    obj = os.path.join(OBJDIR, os.path.basename(src).replace(".cu", ".o"))
-    cmd = [NVCC] + ARCH + FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", src, "-o", obj]
+def _compile(src: str, verbose: bool, objdir: str = OBJDIR, extra=()) -> str:
+    obj = os.path.join(objdir, os.path.basename(src).replace(".cu", ".o"))
+    cmd = [NVCC] + ARCH + FLAGS + list(extra) + (["-Xptxas", "-v"] if verbose else []) + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
@@ -51,25 +56,29 @@ def _compile(src: str, verbose: bool) -> str:
     return obj
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    os.makedirs(OBJDIR, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, checked: bool = False) -> str:
+    objdir, lib = (OBJDIR_CHECKED, LIB_CHECKED) if checked else (OBJDIR, LIB)
+    extra = ["-DPCF_BOUNDS_CHECK"] if checked else []
+    os.makedirs(objdir, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
-    todo = [s for s in srcs if force or _stale(s, os.path.join(OBJDIR, os.path.basename(s).replace(".cu", ".o")))]
+    obj_of = lambda s: os.path.join(objdir, os.path.basename(s).replace(".cu", ".o"))  # noqa: E731
+    todo = [s for s in srcs if force or _stale(s, obj_of(s))]
     with cf.ThreadPoolExecutor(max_workers=min(8, max(1, len(todo)))) as ex:
-        list(ex.map(lambda s: _compile(s, verbose), todo))
-    objs = [os.path.join(OBJDIR, os.path.basename(s).replace(".cu", ".o")) for s in srcs]
-    if force or todo or not os.path.exists(LIB):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        list(ex.map(lambda s: _compile(s, verbose, objdir, extra), todo))
+    objs = [obj_of(s) for s in srcs]
+    if force or todo or not os.path.exists(lib):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--checked", action="store_true")
     args = ap.parse_args()
-    print(build(args.force, args.verbose))
+    print(build(args.force, args.verbose, args.checked))

@@ -78,6 +78,9 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
     const int i = ii + a.nbx, j = jj + a.nby, k = kk + a.nbz;
     const long long sx = 1, sy = a.nxx, sz = (long long)a.nxx * a.nyy;
     const long long h = i * sx + j * sy + k * sz;
+    // the reads below reach one cell in x and y and two in z around h
+    const long long nh = sz * (a.nz + 2 * a.nbz);
+    if (!PCF_IN(h - 2 * sz - sy - 1, nh, 401) || !PCF_IN(h + 2 * sz + sy + 1, nh, 402)) return;
 
     auto J = [&](int di, int dj, int dk) { return __ldg(a.jac + h + di * sx + dj * sy + dk * sz); };
     auto PB = [&](int di, int dj, int dk) { return __ldg(a.pbar + h + di * sx + dj * sy + dk * sz); };
@@ -259,6 +262,7 @@ __global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
         for (int z = 0; z < 5; ++z) {
             const double v = A[c][z] * rfcc * RFC(di, dj, z - 2);
             const long long o = (long long)kPlane[c][z] * n + cell;
+            if (!PCF_IN(o, (long long)PCF_NCOEF * n, 403)) continue;
             a.coef64[o] = v;
             a.coef32[o] = (float)v;
             if (a.coef16) a.coef16[o] = __float2bfloat16_rn((float)v);
@@ -298,6 +302,7 @@ __global__ void k_factors(int plane, int nz, long long n, double deta, const dou
             const int k = k0 + q;
             if (k >= nz) break;
             const long long o = col + (long long)plane * k;
+            if (!PCF_IN(o, n, 404)) break;
             const double piv = k == 0 ? 1.0 / (1.0 - deta * vc[q])
                                       : 1.0 / (1.0 - deta * vc[q] - deta * vd[q] * qprev);
             const double m = k == 0 ? 0.0 : deta * vd[q] * piv;
@@ -347,3 +352,5 @@ int pcf_launch_factors(pcf_handle *h, double deta) {
     h->fac_deta = deta;
     return PCF_OK;
 }
+
+unsigned long long pcf_bounds_take_assemble() { return pcf_bounds_take_local(); }

@@ -114,6 +114,9 @@ __global__ void PCF_POINTWISE_BOUNDS k_correct_uv(CorrectArgs a) {
         if (x > a.nx || y > a.ny) return;
         const int i = a.nbx - 1 + x, j = a.nby - 1 + y, k = a.nbz + kk;
         const long long c = at(i, j, k);
+        // the gradients reach one cell around (i, j, k) and the faces beyond it
+        const long long nh = at.sz * (a.nz + 2 * a.nbz);
+        if (!PCF_IN(c - at.sz - at.sy - 1, nh, 501) || !PCF_IN(c + at.sz + 2 * at.sy + 2, nh, 502)) return;
         if (y >= 1) {  // U at i + 1/2 for i in i0-1 .. i1
             double factor = 1.0;
             if (a.damp_h) factor += a.dt * 0.5 * (a.betar[c] + a.betar[c + 1]) * a.rf;
@@ -147,6 +150,7 @@ __global__ void PCF_POINTWISE_BOUNDS k_correct_w_rhop_pip(CorrectArgs a) {
     if (x >= bx || y >= by) return;
     const int i = a.nbx - 1 + x, j = a.nby - 1 + y, k = a.nbz - 1 + z;
     const long long c = i + sy * j + sz * k;
+    if (!PCF_IN(c, sz * (a.nz + 2 * a.nbz), 503)) return;
     a.pip[c] += a.dpip[c];
     const bool interior = x >= 1 && x <= a.nx && y >= 1 && y <= a.ny && z >= 1 && z <= a.nz;
     if (!interior) return;
@@ -574,3 +578,5 @@ int pcf_launch_predictor(pcf_handle *h, double dt, double rf, int damp_h, double
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PCF_OK : pcf_set_cuda_error(e);
 }
+
+unsigned long long pcf_bounds_take_correct() { return pcf_bounds_take_local(); }

@@ -37,6 +37,38 @@ struct NvtxScope {
 
 int pcf_set_cuda_error(cudaError_t e);
 
+// ------------------------------------------------------- bounds checking --
+// Built with -DPCF_BOUNDS_CHECK (build.py --checked: the library
+// libpincflow_poisson_checked.so), every instrumented global access first
+// checks its index against the array's extent.  An index out of range skips
+// the access (a load reads 0) and records the first such event of this
+// translation unit as (site << 40) | (index & (2^40 - 1)); the host reads and
+// clears the records with pcf_bounds_check_status.  No trap, no device
+// assert: the kernel runs on and the host sees a status.  Without the flag
+// PCF_IN is the constant true and the code is unchanged.
+#ifdef PCF_BOUNDS_CHECK
+static __device__ unsigned long long pcf_bounds_first;  // one record per translation unit
+__device__ __forceinline__ bool pcf_in_range(long long i, long long n, int site) {
+    if (i >= 0 && i < n) return true;
+    atomicCAS(&pcf_bounds_first, 0ull, ((unsigned long long)site << 40) | ((unsigned long long)i & 0xFFFFFFFFFFull));
+    return false;
+}
+#define PCF_IN(i, n, site) pcf_in_range((long long)(i), (long long)(n), (site))
+// this translation unit's record, cleared (host; the device is synchronised)
+static inline unsigned long long pcf_bounds_take_local() {
+    unsigned long long v = 0, z = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess) return ~0ull;
+    cudaMemcpyFromSymbol(&v, pcf_bounds_first, sizeof(v));
+    cudaMemcpyToSymbol(pcf_bounds_first, &z, sizeof(z));
+    return v;
+}
+#define PCF_BOUNDS_CHECKED 1
+#else
+#define PCF_IN(i, n, site) true
+static inline unsigned long long pcf_bounds_take_local() { return 0ull; }
+#define PCF_BOUNDS_CHECKED 0
+#endif
+
 namespace pcf {
 
 constexpr int kNumCoef = PCF_NCOEF;

@@ -388,10 +388,11 @@ __device__ __forceinline__ void ring_fetch(const T *__restrict__ s, int nx, int 
 #pragma unroll
     for (int q = 0; q < R::ROWS_PER_THREAD; ++q) {
         const int rr = ty + q * TY;
-        if (rr < R::NR && inz) {
-            const int y = wrap(y0 - 1 + rr, ny);
-            const int x = wrap(x0 + tx * V, nx);
-            load_vec<T, V>(s + zoff + (long long)nx * y + x, rv[q]);
+        const int y = wrap(y0 - 1 + rr, ny);
+        const int x = wrap(x0 + tx * V, nx);
+        const long long o = zoff + (long long)nx * y + x;
+        if (rr < R::NR && inz && PCF_IN(o, (long long)nx * ny * nz - (V - 1), 101)) {
+            load_vec<T, V>(s + o, rv[q]);
         } else {
 #pragma unroll
             for (int e = 0; e < V; ++e) rv[q][e] = T(0);
@@ -403,7 +404,8 @@ __device__ __forceinline__ void ring_fetch(const T *__restrict__ s, int nx, int 
         const int rr = lt >> 1;
         const int y = wrap(y0 - 1 + rr, ny);
         const int x = (lt & 1) ? wrap(x0 + R::W, nx) : wrap(x0 - 1, nx);
-        hv = __ldg(s + zoff + (long long)nx * y + x);
+        const long long o = zoff + (long long)nx * y + x;
+        if (PCF_IN(o, (long long)nx * ny * nz, 102)) hv = __ldg(s + o);
     }
 }
 
@@ -547,8 +549,10 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
             ring_fetch<T, V, TX, TY>(a.s, a.nx, a.ny, a.nz, x0, y0, k + 4, rv2, hv2);
         else
             ring_fetch<T, V, TX, TY>(a.s, a.nx, a.ny, a.nz, x0, y0, k + 3, rv, hv);
-        if (active) {
-            const long long base = plane * k + (long long)a.nx * y + x;
+        const long long base = plane * k + (long long)a.nx * y + x;
+        // every global index of this level is base (+ p n, + plane for the next level's b)
+        if (active && PCF_IN(base, n - (V - 1), 103) &&
+            (!AHEAD || k + 1 >= k1 || PCF_IN(base + plane, n - (V - 1), 104))) {
             T c[PCF_NCOEF][V];
             if constexpr (C16 == 2) {
                 failed = !mbar_wait(smem_u32(bars + j % NST), (uint32_t)((j / NST) & 1), a.wait_ns);
@@ -770,7 +774,7 @@ __global__ void __launch_bounds__(128) k_thomas(ThomasArgs<T> a) {
         T u0[D], u1[D], u2[D], pp[D], mm[D];
 #pragma unroll
         for (int q = 0; q < D; ++q) {
-            if (q < cnt) {
+            if (q < cnt && PCF_IN(col + pl * (k0 + q), a.n, 201)) {
                 const long long o = col + pl * (k0 + q);
                 pp[q] = __ldg(P + o);
                 mm[q] = __ldg(M + o);
@@ -790,7 +794,7 @@ __global__ void __launch_bounds__(128) k_thomas(ThomasArgs<T> a) {
         }
 #pragma unroll
         for (int q = 0; q < D; ++q) {
-            if (q < cnt) {
+            if (q < cnt && PCF_IN(col + pl * (k0 + q), a.n, 202)) {
                 const long long o = col + pl * (k0 + q);
                 T rhs;
                 if (MODE == TH_B) {
@@ -812,7 +816,7 @@ __global__ void __launch_bounds__(128) k_thomas(ThomasArgs<T> a) {
         }
     }
     T xs = y;
-    if (a.post) {
+    if (a.post && PCF_IN(col + pl * (a.nz - 1), a.n, 205)) {
         const long long o = col + pl * (a.nz - 1);
         a.out[o] = xs * __ldg(a.post + o);
     }
@@ -821,7 +825,7 @@ __global__ void __launch_bounds__(128) k_thomas(ThomasArgs<T> a) {
         T yy[D], qq[D], ps[D];
 #pragma unroll
         for (int q = 0; q < D; ++q) {
-            if (q < cnt) {
+            if (q < cnt && PCF_IN(col + pl * (k1 - q), a.n, 203)) {
                 const long long o = col + pl * (k1 - q);
                 yy[q] = a.out[o];
                 qq[q] = __ldg(Q + o);
@@ -830,7 +834,7 @@ __global__ void __launch_bounds__(128) k_thomas(ThomasArgs<T> a) {
         }
 #pragma unroll
         for (int q = 0; q < D; ++q) {
-            if (q < cnt) {
+            if (q < cnt && PCF_IN(col + pl * (k1 - q), a.n, 204)) {
                 const long long o = col + pl * (k1 - q);
                 xs = yy[q] + qq[q] * xs;
                 a.out[o] = a.post ? xs * ps[q] : xs;
@@ -872,7 +876,7 @@ __global__ void __launch_bounds__(32 * LPC) k_thomas_split(ThomasArgs<float> a) 
 #pragma unroll
     for (int q = 0; q < CH; ++q) {
         const int k = kb + q;
-        const bool on = q < nv;
+        const bool on = q < nv && PCF_IN(col + pl * k, a.n, 211);
         const long long o = col + pl * (on ? k : 0);
         yv[q] = on ? a.in[o] : 0.f;
         pp[q] = on ? __ldg(P + o) : 0.f;
@@ -913,7 +917,7 @@ __global__ void __launch_bounds__(32 * LPC) k_thomas_split(ThomasArgs<float> a) 
 #pragma unroll
     for (int q = CH - 1; q >= 0; --q) {
         x = qq[q] * x + yv[q];
-        if (q < nv) a.out[col + pl * (kb + q)] = x;
+        if (q < nv && PCF_IN(col + pl * (kb + q), a.n, 212)) a.out[col + pl * (kb + q)] = x;
     }
 }
 

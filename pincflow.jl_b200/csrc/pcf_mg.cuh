@@ -215,9 +215,9 @@ __global__ void __launch_bounds__(256) k_mg_restrict(const float *__restrict__ r
 #pragma unroll
         for (int a = 0; a < CX; ++a) {
             const long long c = (CX * I + a) + (long long)nx * ((CY * J + b) + (long long)ny * k);
-            acc += (float)fc[c] * r[c];
+            if (PCF_IN(c, (long long)nx * ny * nz, 301)) acc += (float)fc[c] * r[c];
         }
-    bc[q] = acc / ((float)(CX * CY) * fcc[q]);
+    if (PCF_IN(q, (long long)NX * NY * nz, 302)) bc[q] = acc / ((float)(CX * CY) * fcc[q]);
 }
 
 // s += f_c e / f (piecewise-constant prolongation of the coarse correction);
@@ -232,7 +232,8 @@ __global__ void __launch_bounds__(256) k_mg_prolong(const float *__restrict__ e,
     if (i >= nx || j >= ny) return;
     const long long c = i + (long long)nx * (j + (long long)ny * k);
     const long long q = i / CX + (long long)NX * (j / CY + (long long)NY * k);
-    s[c] += fcc[q] * e[q] / (float)fc[c];
+    if (PCF_IN(c, (long long)nx * ny * nz, 303) && PCF_IN(q, (long long)NX * NY * nz, 304))
+        s[c] += fcc[q] * e[q] / (float)fc[c];
 }
 
 // k_mg_restrict for four consecutive fine x cells per thread (4 / CX coarse
@@ -253,6 +254,7 @@ __global__ void __launch_bounds__(256) k_mg_restrict4(const float *__restrict__ 
 #pragma unroll
     for (int b = 0; b < CY; ++b) {
         const long long c = 4LL * i4 + (long long)nx * ((CY * J + b) + (long long)ny * k);
+        if (!PCF_IN(c, (long long)nx * ny * nz - 3, 305)) continue;
         const float4 rv = *reinterpret_cast<const float4 *>(r + c);
         const float4 fv = *reinterpret_cast<const float4 *>(fc + c);
         const float pr[4] = {fv.x * rv.x, fv.y * rv.y, fv.z * rv.z, fv.w * rv.w};
@@ -261,7 +263,8 @@ __global__ void __launch_bounds__(256) k_mg_restrict4(const float *__restrict__ 
     }
     const long long q = (long long)(4 / CX) * i4 + (long long)NX * (J + (long long)NY * k);
 #pragma unroll
-    for (int m = 0; m < NC; ++m) bc[q + m] = acc[m] / ((float)(CX * CY) * fcc[q + m]);
+    for (int m = 0; m < NC; ++m)
+        if (PCF_IN(q + m, (long long)NX * NY * nz, 306)) bc[q + m] = acc[m] / ((float)(CX * CY) * fcc[q + m]);
 }
 
 // k_mg_prolong on four consecutive x cells per thread with 128-bit loads
@@ -276,6 +279,8 @@ __global__ void __launch_bounds__(256) k_mg_prolong4(const float *__restrict__ e
     if (4 * i4 >= nx || j >= ny) return;
     const long long c = 4LL * i4 + (long long)nx * (j + (long long)ny * k);
     const long long qrow = (long long)NX * (j / CY + (long long)NY * k);
+    if (!PCF_IN(c, (long long)nx * ny * nz - 3, 307) || !PCF_IN(qrow + (4 * i4 + 3) / CX, (long long)NX * NY * nz, 308))
+        return;
     const float4 f = *reinterpret_cast<const float4 *>(fc + c);
     float4 v = *reinterpret_cast<const float4 *>(s + c);
     const int i = 4 * i4;

@@ -1555,3 +1555,5 @@ int pcf_net_load(pcf_net *w, const char *path) {
 }
 
 }  // extern "C"
+
+unsigned long long pcf_bounds_take_net() { return pcf_bounds_take_local(); }

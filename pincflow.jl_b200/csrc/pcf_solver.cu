@@ -2576,6 +2576,30 @@ int pcf_set_network(pcf_handle *h, pcf_net *net) {
     return PCF_OK;
 }
 
+extern "C++" {  // the other translation units' records (pcf_assemble.cu, pcf_correct.cu, pcf_net.cu)
+unsigned long long pcf_bounds_take_assemble();
+unsigned long long pcf_bounds_take_correct();
+unsigned long long pcf_bounds_take_net();
+}
+
+int pcf_bounds_check_status(int *enabled, long long *site, long long *index) {
+    if (!enabled || !site || !index) return PCF_EINVAL;
+    *enabled = PCF_BOUNDS_CHECKED;
+    *site = 0;
+    *index = 0;
+    const unsigned long long recs[4] = {pcf_bounds_take_local(), pcf_bounds_take_assemble(),
+                                        pcf_bounds_take_correct(), pcf_bounds_take_net()};
+    for (unsigned long long r : recs) {
+        if (r == ~0ull) return PCF_ECUDA;
+        if (r && !*site) {
+            *site = (long long)(r >> 40);
+            const long long i = (long long)(r & 0xFFFFFFFFFFull);
+            *index = i >= (1ll << 39) ? i - (1ll << 40) : i;  // 40-bit two's complement
+        }
+    }
+    return PCF_OK;
+}
+
 int pcf_test_stall_staged_copy(pcf_handle *h, int level, double wait_limit_s) {
     if (!h || !(wait_limit_s >= 0.0) || wait_limit_s > 10.0) return PCF_EINVAL;
     PCF_CUDA_TRY(cudaSetDevice(h->dims.device));

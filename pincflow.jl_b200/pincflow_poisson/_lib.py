@@ -12,7 +12,9 @@ import os
 import numpy as np
 
 PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_ROOT, "lib", "libpincflow_poisson.so")
+# PCF_LIB_VARIANT=checked selects the bounds-checked build (build.py --checked)
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libpincflow_poisson_checked.so"
+                        if os.environ.get("PCF_LIB_VARIANT") == "checked" else "libpincflow_poisson.so")
 
 # enum values of include/pincflow_poisson.h
 PCF_OK = 0
@@ -42,7 +44,7 @@ EXPORTS = [
     "pcf_correct", "pcf_correct_device", "pcf_apply_corrector_device",
     "pcf_set_predictand_boundaries_device", "pcf_modify_compressible_wind_device",
     "pcf_implicit_predictor_device", "pcf_implicit_step_device", "pcf_implicit_step",
-    "pcf_test_stall_staged_copy",
+    "pcf_test_stall_staged_copy", "pcf_bounds_check_status",
 ]
 TUNE_KERNELS = ["total32", "total32_diff", "horiz32", "total64", "horiz64"]
 PROF_TAGS = ["apply32", "apply64", "pseudo32", "pseudo64", "thomas32", "thomas64", "update32", "update64",
@@ -151,6 +153,7 @@ def load(path: str | None = None):
     lib.pcf_implicit_step_device.argtypes = [vp, f64, f64, P(PcfParams)] + [vp] * 13 + [P(PcfResult)]
     lib.pcf_implicit_step.argtypes = [vp, f64, f64, P(PcfParams)] + [dp] * 13 + [P(PcfResult)]
     lib.pcf_test_stall_staged_copy.argtypes = [vp, ctypes.c_int, f64]
+    lib.pcf_bounds_check_status.argtypes = [P(ctypes.c_int), P(ctypes.c_longlong), P(ctypes.c_longlong)]
     for name in EXPORTS:
         getattr(lib, name).restype = getattr(lib, name).restype or ctypes.c_int
     lib.pcf_strerror.restype = ctypes.c_char_p
@@ -179,3 +182,14 @@ def dptr(a):
     if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]):
         raise TypeError("expected a C-contiguous float64 numpy array")
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def bounds_check_status():
+    """(enabled, site, index) of pcf_bounds_check_status: whether the loaded
+    library is the bounds-checked build, and its first out-of-range access
+    since the last call (site 0: none)."""
+    lib = load()
+    en, site, idx = ctypes.c_int(), ctypes.c_longlong(), ctypes.c_longlong()
+    check(lib.pcf_bounds_check_status(ctypes.byref(en), ctypes.byref(site), ctypes.byref(idx)),
+          "pcf_bounds_check_status")
+    return bool(en.value), int(site.value), int(idx.value)

@@ -26,3 +26,17 @@ def pcf():
     import pincflow_poisson
     pincflow_poisson.load()
     return pincflow_poisson
+
+
+@pytest.fixture(autouse=True)
+def _bounds_checked_build(request):
+    """With PCF_LIB_VARIANT=checked (tests/test_gpu_bounds.py runs the GPU
+    parity suites that way) every GPU test also requires that the
+    bounds-checked library recorded no out-of-range access."""
+    yield
+    if os.environ.get("PCF_LIB_VARIANT") != "checked" or request.node.get_closest_marker("gpu") is None:
+        return
+    from pincflow_poisson import _lib
+    enabled, site, index = _lib.bounds_check_status()
+    assert enabled, "the bounds-checked library is not the one loaded"
+    assert site == 0, f"out-of-range access: check site {site}, index {index}"

@@ -32,6 +32,18 @@ def test_library_exports_every_declared_symbol(pcf):
     assert set(names) <= exported, set(names) - exported
 
 
+def test_bounds_checked_library_exports_the_same_symbols():
+    """The -DPCF_BOUNDS_CHECK build (build.py --checked) is a drop-in
+    replacement of the library: same declared entry points."""
+    path = os.path.join(REPO, "pincflow.jl_b200", "lib", "libpincflow_poisson_checked.so")
+    if not os.path.exists(path):
+        pytest.skip("checked library not built")
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (pcf_\w+)", out))
+    names = declared_functions()
+    assert set(names) <= exported, set(names) - exported
+
+
 def _c_layout():
     code = r"""
 #include <stdio.h>
