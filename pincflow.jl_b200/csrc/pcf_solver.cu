@@ -2661,11 +2661,29 @@ struct pcf_ensemble {
     long long graph_launches = 0;
     long long launches = 0;
     bool key_valid = false;
-    int key_ci = 0, key_precond = 0, key_pc_iters = 0, key_mg = 0, key_mg_ci = 0, key_mg_min = 0;
+    int key_ci = 0, key_precond = 0, key_pc_iters = 0, key_mg = 0, key_mg_ci = 0, key_mg_min = 0, key_maxit = 0;
     double key_dtau = 0, key_mg_dtau = 0;
     KrylovScalars *h_status = nullptr;  // pinned, 2 slots x members
     double *h_norm = nullptr;           // pinned, members
+    // the whole solve as one graph launch: a conditional WHILE node around
+    // the batch, whose last kernel decides on the device whether to go on
+    cudaGraphExec_t loop_exec = nullptr;
+    KrylovScalars **d_scal = nullptr;   // device array: every member's FP32 scalars
+    int *d_batches = nullptr;           // batches run by the loop (reset before each launch)
 };
+
+// Last kernel of the ensemble's loop body: counts the batch and keeps the
+// loop going while any member is still iterating and fewer than max_batches
+// batches have run.
+__global__ void k_ensemble_continue(KrylovScalars *const *scal, int n, int *batches, int max_batches,
+                                    cudaGraphConditionalHandle cond) {
+    if (threadIdx.x != 0) return;
+    const int b = *batches + 1;
+    *batches = b;
+    bool any = false;
+    for (int q = 0; q < n; ++q) any = any || !scal[q]->done;
+    cudaGraphSetConditional(cond, (any && b < max_batches) ? 1u : 0u);
+}
 
 static LoopCfg ensemble_loop_cfg(pcf_handle *h, const pcf_params *prm) {
     LoopCfg c;
@@ -2679,14 +2697,12 @@ static LoopCfg ensemble_loop_cfg(pcf_handle *h, const pcf_params *prm) {
     return c;
 }
 
-static int ensemble_capture(pcf_ensemble *e, const pcf_params *prm, int ci) {
-    if (e->exec) {
-        cudaGraphExecDestroy(e->exec);
-        e->exec = nullptr;
-    }
+// Records one batch (ci iterations of every member, members as parallel
+// branches forked from and joined to the origin stream) into the graph being
+// captured on the origin stream; adds the member kernels to *nl.
+static int ensemble_record_batch(pcf_ensemble *e, const pcf_params *prm, int ci, long long *nl) {
     std::vector<long long> l0(e->m.size());
     for (size_t q = 0; q < e->m.size(); ++q) l0[q] = e->m[q]->launches;
-    PCF_CUDA_TRY(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal));
     int rc = PCF_OK;
     cudaError_t ce = cudaEventRecord(e->fork, e->origin);
     for (size_t q = 0; q < e->m.size() && rc == PCF_OK && ce == cudaSuccess; ++q) {
@@ -2700,17 +2716,92 @@ static int ensemble_capture(pcf_ensemble *e, const pcf_params *prm, int ci) {
         ce = cudaEventRecord(e->join[q], h->stream);
         if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->origin, e->join[q], 0);
     }
-    cudaGraph_t graph = nullptr;
-    const cudaError_t ee = cudaStreamEndCapture(e->origin, &graph);
-    long long nl = 0;
     for (size_t q = 0; q < e->m.size(); ++q) {
-        nl += e->m[q]->launches - l0[q];
+        *nl += e->m[q]->launches - l0[q];
         e->m[q]->launches = l0[q];  // captured, not launched
     }
+    if (rc) return rc;
+    return ce == cudaSuccess ? PCF_OK : pcf_set_cuda_error(ce);
+}
+
+// The whole iteration as one executable graph: a conditional WHILE node
+// whose body is one batch followed by k_ensemble_continue.  Returns PCF_OK
+// with e->loop_exec null if the driver has no conditional nodes (the solve
+// then launches the batch graph per batch).
+static int ensemble_capture_loop(pcf_ensemble *e, const pcf_params *prm, int ci, int max_batches) {
+    if (e->loop_exec) {
+        cudaGraphExecDestroy(e->loop_exec);
+        e->loop_exec = nullptr;
+    }
+    const int n = (int)e->m.size();
+    if (!e->d_scal) {
+        PCF_CUDA_TRY(cudaMalloc(&e->d_scal, sizeof(KrylovScalars *) * n));
+        PCF_CUDA_TRY(cudaMalloc(&e->d_batches, sizeof(int)));
+        std::vector<KrylovScalars *> ptrs(n);
+        for (int q = 0; q < n; ++q) ptrs[q] = e->m[q]->scal32;
+        PCF_CUDA_TRY(cudaMemcpy(e->d_scal, ptrs.data(), sizeof(KrylovScalars *) * n, cudaMemcpyHostToDevice));
+    }
+    cudaGraph_t g = nullptr;
+    PCF_CUDA_TRY(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle cond;
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t node;
+    if (cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphDestroy(g);
+        return PCF_OK;
+    }
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if (cudaGraphAddNode(&node, g, nullptr, 0, &cp) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphDestroy(g);
+        return PCF_OK;
+    }
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    cudaError_t ce = cudaStreamBeginCaptureToGraph(e->origin, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return pcf_set_cuda_error(ce);
+    }
+    long long nl = 0;
+    int rc = ensemble_record_batch(e, prm, ci, &nl);
+    if (!rc) {
+        k_ensemble_continue<<<1, 32, 0, e->origin>>>(e->d_scal, n, e->d_batches, max_batches, cond);
+        ce = cudaGetLastError();
+    }
+    cudaGraph_t out = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(e->origin, &out);
     if (rc || ce != cudaSuccess || ee != cudaSuccess) {
-        if (graph) cudaGraphDestroy(graph);
+        cudaGraphDestroy(g);
         if (rc) return rc;
         return pcf_set_cuda_error(ce != cudaSuccess ? ce : ee);
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&e->loop_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        e->loop_exec = nullptr;
+        return pcf_set_cuda_error(ei);
+    }
+    return PCF_OK;
+}
+
+static int ensemble_capture(pcf_ensemble *e, const pcf_params *prm, int ci) {
+    if (e->exec) {
+        cudaGraphExecDestroy(e->exec);
+        e->exec = nullptr;
+    }
+    PCF_CUDA_TRY(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal));
+    long long nl = 0;
+    const int rc = ensemble_record_batch(e, prm, ci, &nl);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(e->origin, &graph);
+    if (rc || ee != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (rc) return rc;
+        return pcf_set_cuda_error(ee);
     }
     const cudaError_t ei = cudaGraphInstantiate(&e->exec, graph, 0);
     cudaGraphDestroy(graph);
@@ -2725,13 +2816,17 @@ static int ensemble_capture(pcf_ensemble *e, const pcf_params *prm, int ci) {
     e->key_mg_ci = prm->mg_coarse_iterations;
     e->key_mg_min = prm->mg_min_columns;
     e->key_mg_dtau = prm->mg_dtau;
-    return PCF_OK;
+    e->key_maxit = prm->poisson_iterations;
+    return ensemble_capture_loop(e, prm, ci, (prm->poisson_iterations + ci - 1) / ci);
 }
 
 int pcf_ensemble_destroy(pcf_ensemble *e) {
     if (!e) return PCF_OK;
     cudaSetDevice(e->device);
     if (e->exec) cudaGraphExecDestroy(e->exec);
+    if (e->loop_exec) cudaGraphExecDestroy(e->loop_exec);
+    if (e->d_scal) cudaFree(e->d_scal);
+    if (e->d_batches) cudaFree(e->d_batches);
     cudaEvent_t evs[] = {e->fork, e->t0, e->t1, e->t2, e->done, e->slot_ev[0], e->slot_ev[1]};
     for (cudaEvent_t x : evs)
         if (x) cudaEventDestroy(x);
@@ -2832,7 +2927,7 @@ int pcf_ensemble_solve_device(pcf_ensemble *e, const double *const *d_rhs, const
     if (!e->exec || !e->key_valid || e->key_ci != ci || e->key_precond != prm->preconditioner ||
         e->key_pc_iters != prm->preconditioner_iterations || e->key_dtau != prm->dtau || e->key_mg != prm->multigrid ||
         e->key_mg_ci != prm->mg_coarse_iterations || e->key_mg_min != prm->mg_min_columns ||
-        e->key_mg_dtau != prm->mg_dtau) {
+        e->key_mg_dtau != prm->mg_dtau || e->key_maxit != prm->poisson_iterations) {
         if ((rc = ensemble_capture(e, prm, ci))) return rc;
     }
     std::vector<double> bnorm(n), tol(n);
@@ -2872,9 +2967,20 @@ int pcf_ensemble_solve_device(pcf_ensemble *e, const double *const *d_rhs, const
         PCF_CUDA_TRY(cudaStreamWaitEvent(e->origin, e->join[q], 0));
     }
     PCF_CUDA_TRY(cudaEventRecord(e->t1, e->origin));
-    // batches: one graph launch for all members, status of batch b read while b + 1 runs
+    // the whole iteration as one graph launch (the loop decides on the device
+    // when every member has finished); without conditional nodes, one graph
+    // launch per batch with the status of batch b read while b + 1 runs
     int launched = 0, inflight = 0, slot = 0;
     bool all_done = nactive == 0;
+    if (!all_done && e->loop_exec) {
+        PCF_CUDA_TRY(cudaMemsetAsync(e->d_batches, 0, sizeof(int), e->origin));
+        PCF_CUDA_TRY(cudaGraphLaunch(e->loop_exec, e->origin));
+        int batches = 0;
+        PCF_CUDA_TRY(cudaMemcpyAsync(&batches, e->d_batches, sizeof(int), cudaMemcpyDeviceToHost, e->origin));
+        PCF_CUDA_TRY(cudaStreamSynchronize(e->origin));
+        e->launches += e->graph_launches * batches + batches;  // + the loop's control kernel
+        all_done = true;
+    }
     while (!all_done) {
         if (launched < maxit) {
             PCF_CUDA_TRY(cudaGraphLaunch(e->exec, e->origin));
