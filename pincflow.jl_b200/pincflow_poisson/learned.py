@@ -305,8 +305,22 @@ def main(argv=None):
     ap.add_argument("--out", default=None, help="weights file to write")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--stage", action="store_true", help="train the preconditioner stage (bias-free)")
+    ap.add_argument("--apply", type=int, default=0, metavar="N",
+                    help="no training: apply a network with seeded random weights N times to a seeded random "
+                         "field of --size (host arrays through pcf_net_forward; for profiling the fused kernel)")
     a = ap.parse_args(argv)
     nx, ny, nz = (int(v) for v in a.size.lower().split("x"))
+    if a.apply:
+        rng = np.random.default_rng(0)
+        with LearnedNet(device=a.device, max_columns=nx * ny, seed=0) as net:
+            p = net.get_params()
+            p[:] = rng.uniform(-1, 1, p.size) * 0.05
+            net.set_params(p)
+            field = rng.standard_normal((nz, ny, nx))
+            for _ in range(a.apply):
+                out = net.forward(field)
+        print(json.dumps({"applied": a.apply, "size": [nx, ny, nz], "mean_abs_out": float(np.abs(out).mean())}))
+        return None
     t0 = time.time()
     make = preconditioner_pairs if a.stage else training_pairs
     pairs = make(range(a.pairs), nx=nx, ny=ny, nz=nz, device=a.device)
