@@ -145,6 +145,10 @@ typedef struct {
                                       multiple of 8 those stencils load the BF16 tiles into shared memory by TMA
                                       (same arithmetic, same results); the learned preconditioner stage
                                       (learned & 2) runs the same V-cycle, which its training pairs come from (1) */
+    int mg_fused_coarse;           /* multigrid: 1: the levels of at most 1024 columns (nz <= 256) run as one
+                                      cooperative launch per cycle (column solves by warp scans, grid barriers
+                                      between the steps); 0: one kernel per step as on the finer levels (0:
+                                      measured no faster at 256 x 256 x 128 and slower for the ensemble) */
 } pcf_params;
 
 typedef struct {

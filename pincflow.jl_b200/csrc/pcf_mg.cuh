@@ -292,4 +292,260 @@ __global__ void __launch_bounds__(256) k_mg_prolong4(const float *__restrict__ e
     *reinterpret_cast<float4 *>(s + c) = v;
 }
 
+// ===================================== the coarse V-cycle in one launch --
+//
+// The coarse levels of the V-cycle (from the first level with at most
+// kCoarseColumns columns down to the coarsest) are latency-bound: each of
+// their ~40 kernels per cycle moves a few MB.  k_mg_coarse runs that whole
+// part of the cycle -- the same steps as the per-kernel path (column solve
+// from zero, residual, restriction, ..., coarsest smoothing, prolongation,
+// pseudo-time step, column solve) -- as phases of one cooperative launch
+// separated by grid barriers.  Phases are cell-parallel (stencils and grid
+// transfers, the stencil's terms summed in k_stencil's order) or
+// column-parallel (the Thomas sweeps: one warp per column, each lane a run of
+// at most 8 levels, the runs' affine maps chained by warp-shuffle scans).
+constexpr int kCoarseColumns = 1024;   // levels of at most 32 x 32 columns
+constexpr int kCoarseMaxLevels = 12;
+constexpr int kCoarseThreads = 256;
+
+struct CoarseLevel {
+    int nx, ny, nz, cx, cy;  // cx, cy: the aggregation from the next finer level
+    long long plane, n;
+    float deta;
+    const float *coef, *fac, *fc;
+    float *s, *t, *b;
+};
+
+struct CoarseArgs {
+    CoarseLevel lv[kCoarseMaxLevels];
+    int nlev;          // lv[0] is the first level of the coarse part
+    int coarse_iters;  // smoothing steps on the coarsest level
+    const KrylovScalars *guard;
+    unsigned *bar;     // grid barrier counter, zero at launch
+};
+
+// Grid-wide barrier number `gen` (0, 1, ...) of the launch; bounded (2 s):
+// a barrier that gives up marks the solve failed (PCF_ECUDA) and returns false.
+__device__ __forceinline__ bool coarse_barrier(const CoarseArgs &a, unsigned gen) {
+    __syncthreads();
+    __shared__ int fail;
+    if (threadIdx.x == 0) {
+        fail = 0;
+        __threadfence();
+        atomicAdd(a.bar, 1u);
+        const unsigned target = (gen + 1u) * gridDim.x;
+        uint64_t t0, t1;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+        for (;;) {
+            unsigned v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a.bar) : "memory");
+            if (v >= target) break;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+            if (t1 - t0 > 2000000000ull) {
+                fail = 1;
+                KrylovScalars *g = const_cast<KrylovScalars *>(a.guard);
+                if (g) {
+                    g->status = PCF_ECUDA;
+                    g->done = 1;
+                }
+                break;
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return !fail;
+}
+
+// Column solves of level L, one warp per column: mode TH_B solves from -deta b
+// into out, TH_T solves t in place.  Forward y_k = rhs_k P_k + M_k y_(k-1),
+// back x_k = y_k + Q_k x_(k+1) (x_(nz-1) = y_(nz-1)), as k_thomas.
+template <int MODE>
+__device__ void coarse_thomas(const CoarseLevel &L, const float *in, float *out) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int R = (L.nz + 31) / 32;  // levels per lane, at most 8 (nz <= 256)
+    const float *P = L.fac, *M = L.fac + L.n, *Q = L.fac + 2 * L.n;
+    for (long long col = warp; col < L.plane; col += nwarps) {
+        float yv[8], pp[8], mm[8], qq[8];
+        const int k0 = lane * R;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int k = k0 + q;
+            const bool on = q < R && k < L.nz;
+            const long long o = col + L.plane * (on ? k : 0);
+            const float v = on ? in[o] : 0.f;
+            yv[q] = MODE == TH_B ? -L.deta * v : v;
+            pp[q] = on ? P[o] : 0.f;
+            mm[q] = on ? M[o] : 1.f;
+            qq[q] = (on && k != L.nz - 1) ? Q[o] : (on ? 0.f : 1.f);
+        }
+        // forward: this lane's run as y_out = A + B y_in, then an inclusive scan over lanes
+        float A = 0.f, B = 1.f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            yv[q] *= pp[q];
+            A = mm[q] * A + yv[q];
+            B = mm[q] * B;
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const float a2 = __shfl_up_sync(0xffffffffu, A, off), b2 = __shfl_up_sync(0xffffffffu, B, off);
+            if (lane >= off) {
+                A = A + B * a2;
+                B = B * b2;
+            }
+        }
+        float y = __shfl_up_sync(0xffffffffu, A, 1);
+        if (lane == 0) y = 0.f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            y = mm[q] * y + yv[q];
+            yv[q] = (q < R && k0 + q < L.nz) ? y : 0.f;  // levels past the run: identity maps below
+        }
+        // back: this lane's run as x_start = C + D x_in, then a reverse inclusive scan
+        float C = 0.f, D = 1.f;
+#pragma unroll
+        for (int q = 7; q >= 0; --q) {
+            C = yv[q] + qq[q] * C;
+            D = qq[q] * D;
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const float c2 = __shfl_down_sync(0xffffffffu, C, off), d2 = __shfl_down_sync(0xffffffffu, D, off);
+            if (lane + off < 32) {
+                C = C + D * c2;
+                D = D * d2;
+            }
+        }
+        float x = __shfl_down_sync(0xffffffffu, C, 1);
+        if (lane == 31) x = 0.f;
+#pragma unroll
+        for (int q = 7; q >= 0; --q) {
+            const int k = k0 + q;
+            x = yv[q] + qq[q] * x;
+            if (q < R && k < L.nz) out[col + L.plane * k] = x;
+        }
+    }
+}
+
+// Stencil of level L on s (periodic in x and y, zero beyond the walls), cell
+// parallel.  HORIZ: out = s + deta (L_h s - b); otherwise out = b - A s.  The
+// terms are summed in the order of k_stencil.
+template <bool HORIZ>
+__device__ void coarse_stencil(const CoarseLevel &L, const float *s, const float *b, float *out) {
+    const int nx = L.nx, ny = L.ny, nz = L.nz;
+    const long long n = L.n, plane = L.plane;
+    // 32-bit index arithmetic: pcf_create admits fewer than 2^31 cells
+    for (unsigned c = blockIdx.x * blockDim.x + threadIdx.x; c < (unsigned)n; c += gridDim.x * blockDim.x) {
+        const unsigned cx = c % (unsigned)nx, rest = c / (unsigned)nx;
+        const int i = (int)cx, j = (int)(rest % (unsigned)ny), k = (int)(rest / (unsigned)ny);
+        const int il = i == 0 ? nx - 1 : i - 1, ir = i == nx - 1 ? 0 : i + 1;
+        const int jb = j == 0 ? ny - 1 : j - 1, jf = j == ny - 1 ? 0 : j + 1;
+        auto S = [&](int ii, int jj, int kk) -> float {
+            return (kk < 0 || kk >= nz) ? 0.f : s[ii + (long long)nx * (jj + (long long)ny * kk)];
+        };
+        const float *A = L.coef + c;
+        auto K = [&](int p) { return A[(long long)p * n]; };
+        float acc;
+        if (HORIZ) {
+            acc = K(PCF_AL) * S(il, j, k);
+        } else {
+            acc = K(PCF_AC) * S(i, j, k);
+            acc = fmaf(K(PCF_AD), S(i, j, k - 1), acc);
+            acc = fmaf(K(PCF_AU), S(i, j, k + 1), acc);
+            acc = fmaf(K(PCF_AL), S(il, j, k), acc);
+        }
+        acc = fmaf(K(PCF_AR), S(ir, j, k), acc);
+        acc = fmaf(K(PCF_AB), S(i, jb, k), acc);
+        acc = fmaf(K(PCF_AF), S(i, jf, k), acc);
+        acc = fmaf(K(PCF_ALD), S(il, j, k - 1), acc);
+        acc = fmaf(K(PCF_ALU), S(il, j, k + 1), acc);
+        acc = fmaf(K(PCF_ARD), S(ir, j, k - 1), acc);
+        acc = fmaf(K(PCF_ARU), S(ir, j, k + 1), acc);
+        acc = fmaf(K(PCF_ABD), S(i, jb, k - 1), acc);
+        acc = fmaf(K(PCF_ABU), S(i, jb, k + 1), acc);
+        acc = fmaf(K(PCF_AFD), S(i, jf, k - 1), acc);
+        acc = fmaf(K(PCF_AFU), S(i, jf, k + 1), acc);
+        acc = fmaf(K(PCF_ADD), S(i, j, k - 2), acc);
+        acc = fmaf(K(PCF_AUU), S(i, j, k + 2), acc);
+        acc = fmaf(K(PCF_ALDD), S(il, j, k - 2), acc);
+        acc = fmaf(K(PCF_ALUU), S(il, j, k + 2), acc);
+        acc = fmaf(K(PCF_ARDD), S(ir, j, k - 2), acc);
+        acc = fmaf(K(PCF_ARUU), S(ir, j, k + 2), acc);
+        acc = fmaf(K(PCF_ABDD), S(i, jb, k - 2), acc);
+        acc = fmaf(K(PCF_ABUU), S(i, jb, k + 2), acc);
+        acc = fmaf(K(PCF_AFDD), S(i, jf, k - 2), acc);
+        acc = fmaf(K(PCF_AFUU), S(i, jf, k + 2), acc);
+        out[c] = HORIZ ? S(i, j, k) + L.deta * (acc - b[c]) : b[c] - acc;
+    }
+}
+
+// b of level C from the residual r of the finer level F (k_mg_restrict's sums)
+__device__ void coarse_restrict(const CoarseLevel &F, const CoarseLevel &C, const float *r) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < C.n;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int I = (int)(q % C.nx), J = (int)((q / C.nx) % C.ny), k = (int)(q / C.plane);
+        float acc = 0.f;
+        for (int bb = 0; bb < C.cy; ++bb)
+            for (int aa = 0; aa < C.cx; ++aa) {
+                const long long c = (C.cx * I + aa) + (long long)F.nx * ((C.cy * J + bb) + (long long)F.ny * k);
+                acc += F.fc[c] * r[c];
+            }
+        C.b[q] = acc / ((float)(C.cx * C.cy) * C.fc[q]);
+    }
+}
+
+// s of level F += f_c e / f (k_mg_prolong)
+__device__ void coarse_prolong(const CoarseLevel &F, const CoarseLevel &C, const float *e) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < F.n; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % F.nx), j = (int)((c / F.nx) % F.ny), k = (int)(c / F.plane);
+        const long long q = i / C.cx + (long long)C.nx * (j / C.cy + (long long)C.ny * k);
+        F.s[c] += C.fc[q] * e[q] / F.fc[c];
+    }
+}
+
+__global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(const __grid_constant__ CoarseArgs a) {
+    if (krylov_done(a.guard)) return;
+    unsigned gen = 0;
+    const int top = a.nlev - 1;
+    // descent: column solve from zero, residual, restriction
+    for (int l = 0; l < top; ++l) {
+        const CoarseLevel &L = a.lv[l];
+        coarse_thomas<TH_B>(L, L.b, L.s);
+        if (!coarse_barrier(a, gen++)) return;
+        coarse_stencil<false>(L, L.s, L.b, L.t);
+        if (!coarse_barrier(a, gen++)) return;
+        coarse_restrict(L, a.lv[l + 1], L.t);
+        if (!coarse_barrier(a, gen++)) return;
+    }
+    // the coarsest level: a column solve from zero, then pseudo-time steps
+    const CoarseLevel &Z = a.lv[top];
+    coarse_thomas<TH_B>(Z, Z.b, Z.s);
+    if (!coarse_barrier(a, gen++)) return;
+    float *cur = Z.s, *oth = Z.t;
+    for (int q = 1; q < a.coarse_iters; ++q) {
+        coarse_stencil<true>(Z, cur, Z.b, oth);
+        if (!coarse_barrier(a, gen++)) return;
+        coarse_thomas<TH_T>(Z, oth, oth);
+        if (!coarse_barrier(a, gen++)) return;
+        float *w = cur;
+        cur = oth;
+        oth = w;
+    }
+    // ascent: prolongation, pseudo-time step, column solve
+    const float *e = cur;
+    for (int l = top - 1; l >= 0; --l) {
+        const CoarseLevel &L = a.lv[l];
+        coarse_prolong(L, a.lv[l + 1], e);
+        if (!coarse_barrier(a, gen++)) return;
+        coarse_stencil<true>(L, L.s, L.b, L.t);
+        if (!coarse_barrier(a, gen++)) return;
+        coarse_thomas<TH_T>(L, L.t, L.t);
+        if (l > 0 && !coarse_barrier(a, gen++)) return;
+        e = L.t;
+    }
+}
+
 }  // namespace pcf

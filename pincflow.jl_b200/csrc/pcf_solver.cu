@@ -665,6 +665,9 @@ struct MgState {
     long long version = -1;  // operator version the coarse operators were built from
     double dtau = 0;
     bool bf16 = false;       // the finest level's stencils read h->coef16
+    int fused_from = -1;     // first level of the one-launch coarse cycle (k_mg_coarse), -1: none
+    unsigned *coarse_bar = nullptr;  // its grid barrier counter
+    int coarse_grid = 0;     // its CTAs (co-resident)
 };
 
 __global__ void k_to_float(const double *__restrict__ a, float *__restrict__ b, long long n, double scale);
@@ -789,9 +792,59 @@ static int mg_pseudo_step(pcf_handle *h, const MgLevel &L, const float *coef, co
     return tag == PCF_PROF_MG ? mg_thomas<TH_T>(h, L, ta, tag) : launch_thomas<float, TH_T>(h, ta);
 }
 
+// The coarse part of the cycle from level l = m.fused_from down, as one
+// cooperative launch of k_mg_coarse; *result as mg_cycle.
+static int mg_coarse_launch(pcf_handle *h, int l, const KrylovScalars *guard, float **result) {
+    MgState &m = *h->mg;
+    CoarseArgs a{};
+    a.nlev = (int)m.lv.size() - l;
+    double bytes = 0;
+    for (int q = 0; q < a.nlev; ++q) {
+        const MgLevel &L = m.lv[l + q];
+        CoarseLevel &c = a.lv[q];
+        c.nx = L.d.nx;
+        c.ny = L.d.ny;
+        c.nz = L.d.nz;
+        c.cx = L.cx;
+        c.cy = L.cy;
+        c.plane = L.d.plane;
+        c.n = L.d.n;
+        c.deta = (float)L.deta;
+        c.coef = L.coef;
+        c.fac = L.fac;
+        c.fc = L.fc;
+        c.s = L.s;
+        c.t = L.t;
+        c.b = L.b;
+        bytes += (2.0 * 25 + 6 * 5 + 10) * 4 * (double)L.d.n;  // two stencils, two column solves, transfers
+    }
+    a.coarse_iters = m.coarse_iters;
+    a.guard = guard;
+    a.bar = m.coarse_bar;
+    ProfScope ps(h, PCF_PROF_MG, bytes);
+    PCF_CUDA_TRY(cudaMemsetAsync(m.coarse_bar, 0, sizeof(unsigned), h->stream));
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)m.coarse_grid);
+    cfg.blockDim = dim3(kCoarseThreads);
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    PCF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_mg_coarse, a));
+    h->launches += 1;  // the memset is not a kernel
+    if (a.nlev == 1)
+        *result = (m.coarse_iters - 1) % 2 == 0 ? m.lv[l].s : m.lv[l].t;
+    else
+        *result = m.lv[l].t;
+    return PCF_OK;
+}
+
 // Cycle on a coarse level l >= 1 with right-hand side lv[l].b; *result is lv[l].s or lv[l].t.
 static int mg_cycle(pcf_handle *h, int l, const KrylovScalars *guard, float **result) {
     MgState &m = *h->mg;
+    if (l == m.fused_from) return mg_coarse_launch(h, l, guard, result);
     const MgLevel &L = m.lv[l];
     const __nv_bfloat16 *c16 = m.bf16 ? L.coef16 : nullptr;  // level 1 only
     int rc = mg_thomas<TH_B>(h, L, mg_targs(L, L.fac, L.b, L.s, guard), PCF_PROF_MG);
@@ -940,8 +993,29 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
         m.version = -1;
     }
     m.coarse_iters = prm->mg_coarse_iterations;
-    // the learned preconditioner stage is trained on, and validated with, the FP32 V-cycle
     m.bf16 = prm->mg_operator_bf16 != 0;
+    // the coarse part of the cycle in one launch: from the first level of at most
+    // kCoarseColumns columns (from level 2 on when level 1 reads a BF16 copy),
+    // if its columns fit the warp sweeps (nz <= 256)
+    m.fused_from = -1;
+    if (prm->mg_fused_coarse && h->d.nz <= 256) {
+        for (int l = m.bf16 ? 2 : 1; l < (int)m.lv.size(); ++l)
+            if (m.lv[l].d.plane <= kCoarseColumns) {
+                if ((int)m.lv.size() - l <= kCoarseMaxLevels) m.fused_from = l;
+                break;
+            }
+    }
+    if (m.fused_from >= 0 && !m.coarse_bar) {
+        void *p = nullptr;
+        const cudaError_t e = cudaMalloc(&p, sizeof(unsigned));
+        if (e != cudaSuccess) return pcf_set_cuda_error(e);
+        m.allocs.push_back(p);
+        m.coarse_bar = static_cast<unsigned *>(p);
+        int per_sm = 0;
+        PCF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_coarse, kCoarseThreads, 0));
+        if (per_sm < 1) return PCF_ECUDA;
+        m.coarse_grid = num_sms();  // one CTA per SM: the cheapest grid barrier
+    }
     if (m.bf16 && !h->coef16) {
         // first use: allocate and convert; later assemblies and pcf_set_operator write it themselves
         const size_t bytes = sizeof(__nv_bfloat16) * (size_t)h->d.n * PCF_NCOEF;
@@ -1342,7 +1416,8 @@ static int run_finish(pcf_handle *h, const Work<T> &w, const LoopCfg &c, bool pr
 static GraphKey graph_key(const pcf_handle *h, int tsize, const LoopCfg &c, bool pi, int check_interval) {
     return GraphKey{tsize, c.precond, c.pc_iters, c.flex, c.reliable, pi, check_interval, c.deta, c.mg,
                     c.mg && h->mg ? (int)h->mg->lv.size() : 0, c.mg && h->mg ? h->mg->coarse_iters : 0,
-                    c.mg && h->mg ? (int)h->mg->bf16 : 0, c.learned_pc ? (const void *)h->net : nullptr};
+                    c.mg && h->mg ? (int)h->mg->bf16 | (h->mg->fused_from + 1) << 1 : 0,
+                    c.learned_pc ? (const void *)h->net : nullptr};
 }
 
 // A complete BiCGSTAB run: run_start, the iteration batches, run_finish.
@@ -1491,6 +1566,7 @@ int pcf_params_default(pcf_params *p) {
     p->mg_min_columns = 16;
     p->autotune = 0;
     p->mg_operator_bf16 = 1;
+    p->mg_fused_coarse = 0;
     return PCF_OK;
 }
 

@@ -68,7 +68,8 @@ class PcfParams(ctypes.Structure):
                 ("check_interval", ctypes.c_int), ("restart_interval", ctypes.c_int),
                 ("multigrid", ctypes.c_int), ("mg_dtau", ctypes.c_double),
                 ("mg_coarse_iterations", ctypes.c_int), ("mg_min_columns", ctypes.c_int),
-                ("autotune", ctypes.c_int), ("mg_operator_bf16", ctypes.c_int)]
+                ("autotune", ctypes.c_int), ("mg_operator_bf16", ctypes.c_int),
+                ("mg_fused_coarse", ctypes.c_int)]
 
 
 class PcfTuneEntry(ctypes.Structure):

@@ -54,6 +54,7 @@ class PoissonNamelist:
     mg_min_columns: int = 16          # multigrid: a level with at most this many columns is the coarsest
     autotune: bool = False            # time the stencil tile shapes of each new grid size on first use
     mg_operator_bf16: bool = True     # multigrid: finest and first coarse level stencils read BF16 copies
+    mg_fused_coarse: bool = False     # multigrid: levels of <= 1024 columns in one cooperative launch per cycle
 
     def to_c(self) -> _lib.PcfParams:
         p = _lib.PcfParams()
@@ -78,6 +79,7 @@ class PoissonNamelist:
         p.mg_min_columns = int(self.mg_min_columns)
         p.autotune = int(bool(self.autotune))
         p.mg_operator_bf16 = int(bool(self.mg_operator_bf16))
+        p.mg_fused_coarse = int(bool(self.mg_fused_coarse))
         return p
 
 

@@ -89,6 +89,30 @@ def test_vcycle_matches_oracle(name, solvers, oracle, pcf):
     assert rel_err(got16, want) > 10 * rel_err(got16, want16), (rel_err(got16, want), rel_err(got16, want16))
 
 
+@pytest.mark.parametrize("name", MG_CASES)
+def test_fused_coarse_cycle_matches_oracle(name, solvers, oracle, pcf):
+    """mg_fused_coarse: the levels of at most 1024 columns as one
+    cooperative launch per cycle give the same V-cycle (FP32 and BF16 copies)
+    and, on the parity cases, the same solve as one kernel per step."""
+    cfg, s = solvers(name)
+    d, coef = oracle_operator(oracle, cfg)
+    s.set_operator(coef)
+    b = np.random.default_rng(17).standard_normal(cfg["dom"].interior_shape)
+    for bf16 in (False, True):
+        got = s.apply_multigrid(b, pcf.PoissonNamelist(precision="mixed", mg_operator_bf16=bf16,
+                                                       mg_fused_coarse=True, **MG))
+        want = _oracle_mg(cfg, coef, bf16_planes=bf16, **MG).cycle(b)
+        assert rel_err(got, want) < 1e-4, (bf16, rel_err(got, want))
+    if name not in CASES:
+        return  # wide3 takes 500-900 iterations either way: counts there are rounding noise
+    rhs = consistent_rhs(oracle, cfg)
+    kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=4000, precision="mixed", **MG)
+    _, fused = s.apply_bicgstab(rhs, 1.0, pcf.PoissonNamelist(mg_fused_coarse=True, **kw))
+    _, steps = s.apply_bicgstab(rhs, 1.0, pcf.PoissonNamelist(**kw))
+    assert not fused.errflag and fused.true_residual <= 1e-10, fused
+    assert iterations_agree(fused.niter, steps.niter), (fused.niter, steps.niter)
+
+
 @pytest.mark.parametrize("dtau", [2.0, 2.5])
 @pytest.mark.parametrize("name", CASES)
 def test_multigrid_solve_reaches_fp64_residual(name, dtau, solvers, oracle, pcf):
