@@ -21,9 +21,11 @@
 // (:855-860).  compute_buoyancy_factor(W) (src/Update/compute_buoyancy_factor.jl:
 // 135-172) is evaluated inline.
 //
-// One thread per cell, FP64 throughout; the FP32 copy is rounded from the
-// FP64 result.  Assembly runs once per solve, so this kernel favours clarity
-// over bandwidth (about 34 words per cell, L2-resident neighbour reads).
+// One thread per cell, FP64 throughout; the FP32 and BF16 copies and the
+// difference form are rounded from the FP64 result.  The inputs of a tile of
+// columns are staged level by level in shared memory (below).
+#include <atomic>
+
 #include "pcf_internal.cuh"
 
 namespace pcf {
@@ -40,19 +42,13 @@ struct AssembleArgs {
     double *coef64;
     float *coef32;
     __nv_bfloat16 *coef16;  // BF16 copy (when the handle holds one)
+    float *diff32;          // difference-form FP32 operator (k_build_diff's planes)
+    double *fc64;           // fcscal on the interior
+    float *rfc32;           // 1 / fcscal on the interior
 };
 
 // Column offsets of the 5 columns that carry coefficients.
 enum Col { CC = 0, CR = 1, CL = 2, CF = 3, CB = 4 };
-
-// Plane index of (column, vertical offset -2..2) in Tensor order.
-__device__ __constant__ int kPlane[5][5] = {
-    {PCF_ADD, PCF_AD, PCF_AC, PCF_AU, PCF_AUU},
-    {PCF_ARDD, PCF_ARD, PCF_AR, PCF_ARU, PCF_ARUU},
-    {PCF_ALDD, PCF_ALD, PCF_AL, PCF_ALU, PCF_ALUU},
-    {PCF_AFDD, PCF_AFD, PCF_AF, PCF_AFU, PCF_AFUU},
-    {PCF_ABDD, PCF_ABD, PCF_AB, PCF_ABU, PCF_ABUU},
-};
 
 // Vertical case of a level, first match of the reference's chain
 // (ko + k == k0, k0 + 1, z_size + nbz - 1, z_size + nbz).
@@ -66,207 +62,339 @@ __device__ __forceinline__ int level_case(int kg, int nbz, int z_size) {
     return K_IN;
 }
 
-__global__ void __launch_bounds__(128) k_assemble(AssembleArgs a) {
-    const long long n = (long long)a.nx * a.ny * a.nz;
-    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= n) return;
-    // 32-bit decomposition: pcf_create admits fewer than 2^31 cells
-    const unsigned ucell = (unsigned)cell, ux = (unsigned)a.nx, uy = (unsigned)a.ny;
-    const int ii = (int)(ucell % ux);
-    const int jj = (int)((ucell / ux) % uy);
-    const int kk = (int)(ucell / (ux * uy));
-    const int i = ii + a.nbx, j = jj + a.nby, k = kk + a.nbz;
-    const long long sx = 1, sy = a.nxx, sz = (long long)a.nxx * a.nyy;
-    const long long h = i * sx + j * sy + k * sz;
-    // the reads below reach one cell in x and y and two in z around h
-    const long long nh = sz * (a.nz + 2 * a.nbz);
-    if (!PCF_IN(h - 2 * sz - sy - 1, nh, 401) || !PCF_IN(h + 2 * sz + sy + 1, nh, 402)) return;
+// ---- staging -------------------------------------------------------------
+// A block assembles a tile of AX x AY columns over AKC levels, marching up in
+// z.  Every input it reads lies within one column in x and y and two levels
+// in z of the cell, so each level of each input field is copied once per block
+// into a shared-memory ring (cp.async, 8 bytes per element) and every cell
+// reads its neighbourhood from there.  The copy of level k + 2 (k + 3 for the
+// 5-level fields) is in flight while level k is computed.
+constexpr int AX = 32, AY = 4, AKC = 16;
+constexpr int AHX = AX + 2, AHY = AY + 2, AT = AHX * AHY;  // the tile with its 1-column halo
+// fields with a halo and a 3-level window (k-1..k+1): J, pbar, rhobar, rho', betar, met13, met23
+constexpr int NH3 = 7, F_J = 0, F_PB = 1, F_RB = 2, F_RO = 3, F_BR = 4, F_M13 = 5, F_M23 = 6;
+// fields with a halo and a 5-level window (k-2..k+2): 1 / fcscal, fcscal
+constexpr int NH5 = 2, F_RFC = 0, F_FCH = 1;
+// centre-column fields with a 3-level window: met33, N^2, thetabar
+constexpr int NC3 = 3, F_M33 = 0, F_N2 = 1, F_TH = 2;
+constexpr int S3 = 4, S5 = 6;  // ring slots: the window plus the level in flight
+constexpr int ASM_H3 = 0, ASM_H5 = ASM_H3 + NH3 * S3 * AT, ASM_C3 = ASM_H5 + NH5 * S5 * AT,
+              ASM_DOUBLES = ASM_C3 + NC3 * S3 * AX * AY;
+constexpr int ASM_SMEM = ASM_DOUBLES * (int)sizeof(double);
 
-    auto J = [&](int di, int dj, int dk) { return __ldg(a.jac + h + di * sx + dj * sy + dk * sz); };
-    auto PB = [&](int di, int dj, int dk) { return __ldg(a.pbar + h + di * sx + dj * sy + dk * sz); };
-    auto RB = [&](int di, int dj, int dk) { return __ldg(a.rhobar + h + di * sx + dj * sy + dk * sz); };
-    auto RO = [&](int di, int dj, int dk) { return __ldg(a.rho + h + di * sx + dj * sy + dk * sz); };
-    auto BR = [&](int di, int dj, int dk) { return __ldg(a.betar + h + di * sx + dj * sy + dk * sz); };
-    auto M13 = [&](int di, int dj, int dk) { return __ldg(a.met13 + h + di * sx + dj * sy + dk * sz); };
-    auto M23 = [&](int di, int dj, int dk) { return __ldg(a.met23 + h + di * sx + dj * sy + dk * sz); };
-    auto M33 = [&](int di, int dj, int dk) { return __ldg(a.met33 + h + di * sx + dj * sy + dk * sz); };
-    auto N2 = [&](int dk) { return __ldg(a.n2 + h + dk * sz); };
-    auto RFC = [&](int di, int dj, int dk) { return __ldg(a.rfch + h + di * sx + dj * sy + dk * sz); };
-    // Jacobian-weighted value at the w-level between dk and dk + up (up = +-1):
-    // (J(dk+up) X(dk) + J(dk) X(dk+up)) / (J(dk) + J(dk+up)); rj = 1 / (J(dk) + J(dk+up)).
-    // Divisions are the kernel's main cost in FP64, so every repeated
-    // denominator is inverted once.
-    auto zint = [&](double xk, double xn, double jk, double jn, double rj) { return (jn * xk + jk * xn) * rj; };
+// (di, dj, dk) of plane p in Tensor order (pincflow_poisson.h: AC, AL, AR, AB,
+// AF, AD, AU, ...), and the column index (Col) of (di, dj).
+__host__ __device__ constexpr int plane_di(int p) {
+    return (p == PCF_AL || p == PCF_ALD || p == PCF_ALU || p == PCF_ALDD || p == PCF_ALUU)   ? -1
+           : (p == PCF_AR || p == PCF_ARD || p == PCF_ARU || p == PCF_ARDD || p == PCF_ARUU) ? 1
+                                                                                               : 0;
+}
+__host__ __device__ constexpr int plane_dj(int p) {
+    return (p == PCF_AB || p == PCF_ABD || p == PCF_ABU || p == PCF_ABDD || p == PCF_ABUU)   ? -1
+           : (p == PCF_AF || p == PCF_AFD || p == PCF_AFU || p == PCF_AFDD || p == PCF_AFUU) ? 1
+                                                                                               : 0;
+}
+__host__ __device__ constexpr int plane_dk(int p) {
+    return (p == PCF_ADD || p == PCF_ALDD || p == PCF_ARDD || p == PCF_ABDD || p == PCF_AFDD)   ? -2
+           : (p == PCF_AUU || p == PCF_ALUU || p == PCF_ARUU || p == PCF_ABUU || p == PCF_AFUU) ? 2
+           : (p == PCF_AD || p == PCF_ALD || p == PCF_ARD || p == PCF_ABD || p == PCF_AFD)      ? -1
+           : (p == PCF_AU || p == PCF_ALU || p == PCF_ARU || p == PCF_ABU || p == PCF_AFU)      ? 1
+                                                                                                 : 0;
+}
+__host__ __device__ constexpr int plane_col(int p) {
+    return plane_di(p) == 1 ? CR : plane_di(p) == -1 ? CL : plane_dj(p) == 1 ? CF : plane_dj(p) == -1 ? CB : CC;
+}
+
+// the 25 planes are 25 distinct (column, dk) pairs
+__host__ __device__ constexpr bool planes_distinct() {
+    for (int p = 0; p < PCF_NCOEF; ++p)
+        for (int q = p + 1; q < PCF_NCOEF; ++q)
+            if (plane_col(p) == plane_col(q) && plane_dk(p) == plane_dk(q)) return false;
+    return plane_col(PCF_AC) == CC && plane_col(PCF_AL) == CL && plane_col(PCF_AR) == CR &&
+           plane_col(PCF_AB) == CB && plane_col(PCF_AF) == CF;
+}
+static_assert(planes_distinct(), "plane offsets");
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Copies level kk (interior index, -2..nz+1) of a haloed field into one ring
+// slot: the tile plus its 1-column halo, or the tile alone (centre fields).
+template <bool HALO>
+__device__ __forceinline__ void stage_level(double *dst, const double *src, const AssembleArgs &a, int i0, int j0,
+                                            int kk, int tid) {
+    const long long sy = a.nxx, sz = (long long)a.nxx * a.nyy;
+    const long long nh = sz * (a.nz + 2 * a.nbz);
+    constexpr int W = HALO ? AHX : AX, CNT = HALO ? AT : AX * AY, O = HALO ? 1 : 0;
+    for (int t = tid; t < CNT; t += AX * AY) {
+        const int ty = t / W, tx = t - ty * W;
+        const int i = i0 - O + tx, j = j0 - O + ty;  // interior indices, -1..nx and -1..ny
+        if (i > a.nx || j > a.ny) continue;            // beyond the halo of a partial tile
+        const long long g = (i + a.nbx) + sy * (j + a.nby) + sz * (kk + a.nbz);
+        if (!PCF_IN(g, nh, 401)) continue;
+        cp_async8(dst + t, src + g);
+    }
+}
+
+// One thread per cell, FP64 throughout, the arithmetic of compute_operator!.jl
+// in the face-flux form described at the top of this file.  Besides the FP64,
+// FP32 and (when the handle holds one) BF16 planes it writes the
+// difference-form FP32 operator for pi = s / fcscal (the planes A_nb fcscal_nb
+// and their sum in plane AC, summed in plane order in FP64), fcscal and
+// 1 / fcscal on the interior.
+__global__ void __launch_bounds__(AX * AY, 2) k_assemble(AssembleArgs a) {
+    extern __shared__ double asm_sm[];
+    const int tid = threadIdx.x + AX * threadIdx.y;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i0 = blockIdx.x * AX, j0 = blockIdx.y * AY, k0 = blockIdx.z * AKC;
+    const int k1 = min(k0 + AKC, a.nz);
+    const int ii = i0 + tx, jj = j0 + ty;
+    const bool live = ii < a.nx && jj < a.ny;
+    const long long n = (long long)a.nx * a.ny * a.nz;
+    const long long sy = a.nxx, sz = (long long)a.nxx * a.nyy;
+
+    const double *h3src[NH3] = {a.jac, a.pbar, a.rhobar, a.rho, a.betar, a.met13, a.met23};
+    const double *h5src[NH5] = {a.rfch, a.fch};
+    const double *c3src[NC3] = {a.met33, a.n2, a.thetabar};
+    const bool have_th = a.model == PCF_MODEL_COMPRESSIBLE && a.thetabar;
+    auto slot3 = [](int kk) { return (kk + 4) & 3; };  // kk >= -2
+    auto slot5 = [](int kk) { return (kk + 6) % 6; };  // kk >= -2
+    auto stage3 = [&](int kk) {
+#pragma unroll
+        for (int f = 0; f < NH3; ++f)
+            stage_level<true>(asm_sm + ASM_H3 + (f * S3 + slot3(kk)) * AT, h3src[f], a, i0, j0, kk, tid);
+#pragma unroll
+        for (int f = 0; f < NC3; ++f)
+            if (f != F_TH || have_th)
+                stage_level<false>(asm_sm + ASM_C3 + (f * S3 + slot3(kk)) * AX * AY, c3src[f], a, i0, j0, kk, tid);
+    };
+    auto stage5 = [&](int kk) {
+#pragma unroll
+        for (int f = 0; f < NH5; ++f)
+            stage_level<true>(asm_sm + ASM_H5 + (f * S5 + slot5(kk)) * AT, h5src[f], a, i0, j0, kk, tid);
+    };
+    // the windows of the first level
+    for (int kk = k0 - 1; kk <= k0 + 1; ++kk) stage3(kk);
+    for (int kk = k0 - 2; kk <= k0 + 2; ++kk) stage5(kk);
+    cp_async_wait_all();
+    __syncthreads();
 
     const double dt2 = a.dt * a.dt;
-    const double jc = J(0, 0, 0), ju = J(0, 0, 1), jd = J(0, 0, -1);
-    const double rju = 1.0 / (jc + ju), rjd = 1.0 / (jc + jd);
-    const double jacinv = 1.0 / jc;
-    const double pc = PB(0, 0, 0);
-    const double jpc = jc * pc;
-
-    // buoyancy factor at k+1/2 (up = +1) and k-1/2 (up = -1)
-    auto fw = [&](int lo) {  // W() factor between levels lo and lo + 1
-        const double jl = J(0, 0, lo), jh = J(0, 0, lo + 1);
-        const double rl = RB(0, 0, lo), rh = RB(0, 0, lo + 1);
-        const double den = jh * (RO(0, 0, lo) + rl) + jl * (RO(0, 0, lo + 1) + rh);
-        if (a.model == PCF_MODEL_COMPRESSIBLE)
-            return (jh * PB(0, 0, lo) / __ldg(a.thetabar + h + lo * sz) +
-                    jl * PB(0, 0, lo + 1) / __ldg(a.thetabar + h + (lo + 1) * sz)) / den;
-        return (jh * rl + jl * rh) / den;
-    };
-    const double fwu = fw(0), fwd = fw(-1);
-
-    // vertical face quantities
-    const double pudiv = jc * ju * (pc + PB(0, 0, 1)) * rju;
-    const double pddiv = jc * jd * (pc + PB(0, 0, -1)) * rjd;
-    const double n2u = zint(N2(0), N2(1), jc, ju, rju), n2d = zint(N2(0), N2(-1), jc, jd, rjd);
-    const double facu = 1.0 + a.dt * zint(BR(0, 0, 0), BR(0, 0, 1), jc, ju, rju) * a.rf;
-    const double facd = 1.0 + a.dt * zint(BR(0, 0, 0), BR(0, 0, -1), jc, jd, rjd) * a.rf;
-    const double impu = 1.0 / (facu + fwu * n2u * dt2);
-    const double impd = 1.0 / (facd + fwd * n2d * dt2);
-    // buoyancy-coupling factors shared by every horizontal face
-    const double cu = jacinv * a.rdz * pudiv * impu * fwu * n2u * dt2 * 0.5;
-    const double cd = jacinv * a.rdz * pddiv * impd * fwd * n2d * dt2 * 0.5;
-
-    const int kg = a.ko + k;
-    const bool bot = kg == a.nbz, top = kg == a.z_size + a.nbz - 1;
-    const int case_k = level_case(kg, a.nbz, a.z_size);
-
-    double A[5][5];
-#pragma unroll
-    for (int c = 0; c < 5; ++c)
-#pragma unroll
-        for (int z = 0; z < 5; ++z) A[c][z] = 0.0;
-
-    // Adds flux * (one-sided or centred d/dz at level L = k + dl) * met / dz to
-    // the two columns c0, c1 adjacent to a horizontal face.
-    auto add_vz = [&](int c0, int c1, int dl, double w) {
-        const int cs = level_case(kg + dl, a.nbz, a.z_size);
-        const int z0 = dl + 2;  // index of level L in the -2..2 window
-        if (cs == K_BOT) {
-            A[c0][z0] += -0.75 * w; A[c0][z0 + 1] += w; A[c0][z0 + 2] += -0.25 * w;
-            A[c1][z0] += -0.75 * w; A[c1][z0 + 1] += w; A[c1][z0 + 2] += -0.25 * w;
-        } else if (cs == K_TOP) {
-            A[c0][z0] += 0.75 * w; A[c0][z0 - 1] += -w; A[c0][z0 - 2] += 0.25 * w;
-            A[c1][z0] += 0.75 * w; A[c1][z0 - 1] += -w; A[c1][z0 - 2] += 0.25 * w;
-        } else {
-            A[c0][z0 + 1] += 0.25 * w; A[c0][z0 - 1] += -0.25 * w;
-            A[c1][z0 + 1] += 0.25 * w; A[c1][z0 - 1] += -0.25 * w;
+    for (int kk = k0; kk < k1; ++kk) {
+        if (kk + 1 < k1) {  // the next level's new rows
+            stage3(kk + 2);
+            stage5(kk + 3);
         }
-    };
+        if (live) {
+            const int k = kk + a.nbz;  // haloed level
+            // ring bases of levels kk-1..kk+1 and kk-2..kk+2
+            const int b3[3] = {slot3(kk - 1), slot3(kk), slot3(kk + 1)};
+            const int b5[5] = {slot5(kk - 2), slot5(kk - 1), slot5(kk), slot5(kk + 1), slot5(kk + 2)};
+            const int cxy = (ty + 1) * AHX + tx + 1;
+            auto H3 = [&](int f, int di, int dj, int dk) {
+                return asm_sm[ASM_H3 + (f * S3 + b3[dk + 1]) * AT + cxy + di + dj * AHX];
+            };
+            auto H5 = [&](int f, int di, int dj, int dk) {
+                return asm_sm[ASM_H5 + (f * S5 + b5[dk + 2]) * AT + cxy + di + dj * AHX];
+            };
+            auto C3 = [&](int f, int dk) { return asm_sm[ASM_C3 + (f * S3 + b3[dk + 1]) * AX * AY + tid]; };
+            auto J = [&](int di, int dj, int dk) { return H3(F_J, di, dj, dk); };
+            auto PB = [&](int di, int dj, int dk) { return H3(F_PB, di, dj, dk); };
+            auto RB = [&](int di, int dj, int dk) { return H3(F_RB, di, dj, dk); };
+            auto RO = [&](int di, int dj, int dk) { return H3(F_RO, di, dj, dk); };
+            auto BR = [&](int di, int dj, int dk) { return H3(F_BR, di, dj, dk); };
+            auto M13 = [&](int di, int dj, int dk) { return H3(F_M13, di, dj, dk); };
+            auto M23 = [&](int di, int dj, int dk) { return H3(F_M23, di, dj, dk); };
+            auto M33 = [&](int dk) { return C3(F_M33, dk); };
+            auto N2 = [&](int dk) { return C3(F_N2, dk); };
+            auto TH = [&](int dk) { return C3(F_TH, dk); };
+            // Jacobian-weighted value at the w-level between dk and dk + up (up = +-1):
+            // (J(dk+up) X(dk) + J(dk) X(dk+up)) / (J(dk) + J(dk+up)); rj = 1 / (J(dk) + J(dk+up)).
+            // Divisions are the kernel's main cost in FP64, so every repeated
+            // denominator is inverted once.
+            auto zint = [&](double xk, double xn, double jk, double jn, double rj) { return (jn * xk + jk * xn) * rj; };
 
-    // ---- the 12 horizontal faces -------------------------------------------
-    // dir: 0 = r (i+1/2), 1 = l (i-1/2), 2 = f (j+1/2), 3 = b (j-1/2)
+            const double jc = J(0, 0, 0), ju = J(0, 0, 1), jd = J(0, 0, -1);
+            const double rju = 1.0 / (jc + ju), rjd = 1.0 / (jc + jd);
+            const double jacinv = 1.0 / jc;
+            const double pc = PB(0, 0, 0);
+            const double jpc = jc * pc;
+
+            // buoyancy factor at k+1/2 (up = +1) and k-1/2 (up = -1)
+            auto fw = [&](int lo) {  // W() factor between levels lo and lo + 1
+                const double jl = J(0, 0, lo), jh = J(0, 0, lo + 1);
+                const double rl = RB(0, 0, lo), rh = RB(0, 0, lo + 1);
+                const double den = jh * (RO(0, 0, lo) + rl) + jl * (RO(0, 0, lo + 1) + rh);
+                if (a.model == PCF_MODEL_COMPRESSIBLE)
+                    return (jh * PB(0, 0, lo) / TH(lo) + jl * PB(0, 0, lo + 1) / TH(lo + 1)) / den;
+                return (jh * rl + jl * rh) / den;
+            };
+            const double fwu = fw(0), fwd = fw(-1);
+
+            // vertical face quantities
+            const double pudiv = jc * ju * (pc + PB(0, 0, 1)) * rju;
+            const double pddiv = jc * jd * (pc + PB(0, 0, -1)) * rjd;
+            const double n2u = zint(N2(0), N2(1), jc, ju, rju), n2d = zint(N2(0), N2(-1), jc, jd, rjd);
+            const double facu = 1.0 + a.dt * zint(BR(0, 0, 0), BR(0, 0, 1), jc, ju, rju) * a.rf;
+            const double facd = 1.0 + a.dt * zint(BR(0, 0, 0), BR(0, 0, -1), jc, jd, rjd) * a.rf;
+            const double impu = 1.0 / (facu + fwu * n2u * dt2);
+            const double impd = 1.0 / (facd + fwd * n2d * dt2);
+            // buoyancy-coupling factors shared by every horizontal face
+            const double cu = jacinv * a.rdz * pudiv * impu * fwu * n2u * dt2 * 0.5;
+            const double cd = jacinv * a.rdz * pddiv * impd * fwd * n2d * dt2 * 0.5;
+
+            const int kg = a.ko + k;
+            const bool bot = kg == a.nbz, top = kg == a.z_size + a.nbz - 1;
+
+            double A[5][5];
 #pragma unroll
-    for (int dir = 0; dir < 4; ++dir) {
-        const int di = dir == 0 ? 1 : (dir == 1 ? -1 : 0);
-        const int dj = dir == 2 ? 1 : (dir == 3 ? -1 : 0);
-        const int cn = dir == 0 ? CR : (dir == 1 ? CL : (dir == 2 ? CF : CB));
-        const double sgn = (dir == 0 || dir == 2) ? 1.0 : -1.0;  // outward normal
-        const double rdh = dir < 2 ? a.rdx : a.rdy;
-        const double *met = dir < 2 ? a.met13 : a.met23;
-        auto MH = [&](int dk) { return __ldg(met + h + dk * sz); };
-        auto MHn = [&](int dk) { return __ldg(met + h + di * sx + dj * sy + dk * sz); };
+            for (int c = 0; c < 5; ++c)
 #pragma unroll
-        for (int dl = -1; dl <= 1; ++dl) {
-            // skip the faces whose g vanishes: level k+1 at the top, k-1 at the bottom
-            if ((dl == 1 && top) || (dl == -1 && bot)) continue;
-            const double pgra = 0.5 * (PB(0, 0, dl) + PB(di, dj, dl));
-            const double rho_e = 0.5 * (RO(0, 0, dl) + RO(di, dj, dl) + RB(0, 0, dl) + RB(di, dj, dl));
-            const double fac = a.damp_h ? 1.0 + a.dt * 0.5 * (BR(0, 0, dl) + BR(di, dj, dl)) * a.rf : 1.0;
-            const double imp_over_rho = 1.0 / (fac * rho_e);
-            double g;
-            if (dl == 0) {
-                // gedge{r,l,f,b} (:426-639): horizontal gradient plus the two vertical couplings
-                const double pdiv = 0.5 * (jpc + J(di, dj, 0) * PB(di, dj, 0));
-                g = sgn * jacinv * rdh * pdiv;
-                if (!top) g += cu * MH(0) * ju * rju;
-                if (!bot) g -= cd * MH(0) * jd * rjd;
-                g *= imp_over_rho;
-            } else if (dl == 1) {
-                // guedge{r,l,f,b} (:656-722)
-                g = cu * MH(1) * jc * rju * imp_over_rho;
-            } else {
-                // gdedge{r,l,f,b} (:725-791)
-                g = -cd * MH(-1) * jc * rjd * imp_over_rho;
+                for (int z = 0; z < 5; ++z) A[c][z] = 0.0;
+
+            // Adds flux * (one-sided or centred d/dz at level L = k + dl) * met / dz to
+            // the two columns c0, c1 adjacent to a horizontal face.
+            auto add_vz = [&](int c0, int c1, int dl, double w) {
+                const int cs = level_case(kg + dl, a.nbz, a.z_size);
+                const int z0 = dl + 2;  // index of level L in the -2..2 window
+                if (cs == K_BOT) {
+                    A[c0][z0] += -0.75 * w; A[c0][z0 + 1] += w; A[c0][z0 + 2] += -0.25 * w;
+                    A[c1][z0] += -0.75 * w; A[c1][z0 + 1] += w; A[c1][z0 + 2] += -0.25 * w;
+                } else if (cs == K_TOP) {
+                    A[c0][z0] += 0.75 * w; A[c0][z0 - 1] += -w; A[c0][z0 - 2] += 0.25 * w;
+                    A[c1][z0] += 0.75 * w; A[c1][z0 - 1] += -w; A[c1][z0 - 2] += 0.25 * w;
+                } else {
+                    A[c0][z0 + 1] += 0.25 * w; A[c0][z0 - 1] += -0.25 * w;
+                    A[c1][z0 + 1] += 0.25 * w; A[c1][z0 - 1] += -0.25 * w;
+                }
+            };
+
+            // ---- the 12 horizontal faces ---------------------------------------
+            // dir: 0 = r (i+1/2), 1 = l (i-1/2), 2 = f (j+1/2), 3 = b (j-1/2)
+#pragma unroll
+            for (int dir = 0; dir < 4; ++dir) {
+                const int di = dir == 0 ? 1 : (dir == 1 ? -1 : 0);
+                const int dj = dir == 2 ? 1 : (dir == 3 ? -1 : 0);
+                const int cn = dir == 0 ? CR : (dir == 1 ? CL : (dir == 2 ? CF : CB));
+                const double sgn = (dir == 0 || dir == 2) ? 1.0 : -1.0;  // outward normal
+                const double rdh = dir < 2 ? a.rdx : a.rdy;
+                const int fm = dir < 2 ? F_M13 : F_M23;
+                auto MH = [&](int dk) { return H3(fm, 0, 0, dk); };
+                auto MHn = [&](int dk) { return H3(fm, di, dj, dk); };
+#pragma unroll
+                for (int dl = -1; dl <= 1; ++dl) {
+                    // skip the faces whose g vanishes: level k+1 at the top, k-1 at the bottom
+                    if ((dl == 1 && top) || (dl == -1 && bot)) continue;
+                    const double pgra = 0.5 * (PB(0, 0, dl) + PB(di, dj, dl));
+                    const double rho_e = 0.5 * (RO(0, 0, dl) + RO(di, dj, dl) + RB(0, 0, dl) + RB(di, dj, dl));
+                    const double fac = a.damp_h ? 1.0 + a.dt * 0.5 * (BR(0, 0, dl) + BR(di, dj, dl)) * a.rf : 1.0;
+                    const double imp_over_rho = 1.0 / (fac * rho_e);
+                    double g;
+                    if (dl == 0) {
+                        // gedge{r,l,f,b} (:426-639): horizontal gradient plus the two vertical couplings
+                        const double pdiv = 0.5 * (jpc + J(di, dj, 0) * PB(di, dj, 0));
+                        g = sgn * jacinv * rdh * pdiv;
+                        if (!top) g += cu * MH(0) * ju * rju;
+                        if (!bot) g -= cd * MH(0) * jd * rjd;
+                        g *= imp_over_rho;
+                    } else if (dl == 1) {
+                        // guedge{r,l,f,b} (:656-722)
+                        g = cu * MH(1) * jc * rju * imp_over_rho;
+                    } else {
+                        // gdedge{r,l,f,b} (:725-791)
+                        g = -cd * MH(-1) * jc * rjd * imp_over_rho;
+                    }
+                    const double flux = g * pgra;
+                    const double metf = 0.5 * (MH(dl) + MHn(dl));
+                    // horizontal difference (s_hi - s_lo)/dh, hi = neighbour for r/f, cell for l/b
+                    const double wh = flux * rdh;
+                    A[cn][dl + 2] += sgn * wh;
+                    A[CC][dl + 2] -= sgn * wh;
+                    add_vz(CC, cn, dl, flux * metf * a.rdz);
+                }
             }
-            const double flux = g * pgra;
-            const double metf = 0.5 * (MH(dl) + MHn(dl));
-            // horizontal difference (s_hi - s_lo)/dh, hi = neighbour for r/f, cell for l/b
-            const double wh = flux * rdh;
-            A[cn][dl + 2] += sgn * wh;
-            A[CC][dl + 2] -= sgn * wh;
-            add_vz(CC, cn, dl, flux * metf * a.rdz);
-        }
-    }
 
-    // ---- the 2 vertical faces ------------------------------------------------
-    if (!top) {  // G(k + 1/2) (:642-646)
-        const double rho_u =
-            zint(RO(0, 0, 0), RO(0, 0, 1), jc, ju, rju) + zint(RB(0, 0, 0), RB(0, 0, 1), jc, ju, rju);
-        const double g = jacinv * a.rdz * pudiv * impu / rho_u;
-        const double flux = g * zint(pc, PB(0, 0, 1), jc, ju, rju);
-        const double w33 = flux * zint(M33(0, 0, 0), M33(0, 0, 1), jc, ju, rju) * a.rdz;
-        A[CC][3] += w33;
-        A[CC][2] -= w33;
-        const double w13 = flux * zint(M13(0, 0, 0), M13(0, 0, 1), jc, ju, rju) * 0.5 * a.rdx;
-        const double w23 = flux * zint(M23(0, 0, 0), M23(0, 0, 1), jc, ju, rju) * 0.5 * a.rdy;
+            // ---- the 2 vertical faces ------------------------------------------
+            if (!top) {  // G(k + 1/2) (:642-646)
+                const double rho_u =
+                    zint(RO(0, 0, 0), RO(0, 0, 1), jc, ju, rju) + zint(RB(0, 0, 0), RB(0, 0, 1), jc, ju, rju);
+                const double g = jacinv * a.rdz * pudiv * impu / rho_u;
+                const double flux = g * zint(pc, PB(0, 0, 1), jc, ju, rju);
+                const double w33 = flux * zint(M33(0), M33(1), jc, ju, rju) * a.rdz;
+                A[CC][3] += w33;
+                A[CC][2] -= w33;
+                const double w13 = flux * zint(M13(0, 0, 0), M13(0, 0, 1), jc, ju, rju) * 0.5 * a.rdx;
+                const double w23 = flux * zint(M23(0, 0, 0), M23(0, 0, 1), jc, ju, rju) * 0.5 * a.rdy;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int di = q == 0 ? 1 : (q == 1 ? -1 : 0), dj = q == 2 ? 1 : (q == 3 ? -1 : 0);
-            const int cn = q == 0 ? CR : (q == 1 ? CL : (q == 2 ? CF : CB));
-            const double w = (q < 2 ? w13 : w23) * ((q == 0 || q == 2) ? 1.0 : -1.0);
-            const double j0 = J(di, dj, 0), j1 = J(di, dj, 1);
-            const double r01 = w / (j0 + j1);
-            A[cn][2] += j1 * r01;
-            A[cn][3] += j0 * r01;
-        }
-    }
-    if (!bot) {  // G(k - 1/2) (:649-653)
-        const double rho_d =
-            zint(RO(0, 0, 0), RO(0, 0, -1), jc, jd, rjd) + zint(RB(0, 0, 0), RB(0, 0, -1), jc, jd, rjd);
-        const double g = -jacinv * a.rdz * pddiv * impd / rho_d;
-        const double flux = g * zint(pc, PB(0, 0, -1), jc, jd, rjd);
-        const double w33 = flux * zint(M33(0, 0, 0), M33(0, 0, -1), jc, jd, rjd) * a.rdz;
-        A[CC][2] += w33;
-        A[CC][1] -= w33;
-        const double w13 = flux * zint(M13(0, 0, 0), M13(0, 0, -1), jc, jd, rjd) * 0.5 * a.rdx;
-        const double w23 = flux * zint(M23(0, 0, 0), M23(0, 0, -1), jc, jd, rjd) * 0.5 * a.rdy;
+                for (int q = 0; q < 4; ++q) {
+                    const int di = q == 0 ? 1 : (q == 1 ? -1 : 0), dj = q == 2 ? 1 : (q == 3 ? -1 : 0);
+                    const int cn = q == 0 ? CR : (q == 1 ? CL : (q == 2 ? CF : CB));
+                    const double w = (q < 2 ? w13 : w23) * ((q == 0 || q == 2) ? 1.0 : -1.0);
+                    const double j0v = J(di, dj, 0), j1v = J(di, dj, 1);
+                    const double r01 = w / (j0v + j1v);
+                    A[cn][2] += j1v * r01;
+                    A[cn][3] += j0v * r01;
+                }
+            }
+            if (!bot) {  // G(k - 1/2) (:649-653)
+                const double rho_d =
+                    zint(RO(0, 0, 0), RO(0, 0, -1), jc, jd, rjd) + zint(RB(0, 0, 0), RB(0, 0, -1), jc, jd, rjd);
+                const double g = -jacinv * a.rdz * pddiv * impd / rho_d;
+                const double flux = g * zint(pc, PB(0, 0, -1), jc, jd, rjd);
+                const double w33 = flux * zint(M33(0), M33(-1), jc, jd, rjd) * a.rdz;
+                A[CC][2] += w33;
+                A[CC][1] -= w33;
+                const double w13 = flux * zint(M13(0, 0, 0), M13(0, 0, -1), jc, jd, rjd) * 0.5 * a.rdx;
+                const double w23 = flux * zint(M23(0, 0, 0), M23(0, 0, -1), jc, jd, rjd) * 0.5 * a.rdy;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int di = q == 0 ? 1 : (q == 1 ? -1 : 0), dj = q == 2 ? 1 : (q == 3 ? -1 : 0);
-            const int cn = q == 0 ? CR : (q == 1 ? CL : (q == 2 ? CF : CB));
-            const double w = (q < 2 ? w13 : w23) * ((q == 0 || q == 2) ? 1.0 : -1.0);
-            const double j0 = J(di, dj, 0), j1 = J(di, dj, -1);
-            const double r01 = w / (j0 + j1);
-            A[cn][2] += j1 * r01;
-            A[cn][1] += j0 * r01;
-        }
-    }
+                for (int q = 0; q < 4; ++q) {
+                    const int di = q == 0 ? 1 : (q == 1 ? -1 : 0), dj = q == 2 ? 1 : (q == 3 ? -1 : 0);
+                    const int cn = q == 0 ? CR : (q == 1 ? CL : (q == 2 ? CF : CB));
+                    const double w = (q < 2 ? w13 : w23) * ((q == 0 || q == 2) ? 1.0 : -1.0);
+                    const double j0v = J(di, dj, 0), j1v = J(di, dj, -1);
+                    const double r01 = w / (j0v + j1v);
+                    A[cn][2] += j1v * r01;
+                    A[cn][1] += j0v * r01;
+                }
+            }
 
-    if (a.model == PCF_MODEL_COMPRESSIBLE) {
-        const double dpdpi = 1.0 / (a.gamma - 1.0) * pow(a.rsp / a.pref, 1.0 - a.gamma) *
-                             pow(__ldg(a.p + h), 2.0 - a.gamma);
-        A[CC][2] -= (dpdpi / a.dt) / (a.dt * a.rsp / a.kappa);
-    }
-    (void)case_k;
+            const long long cell = ii + (long long)a.nx * (jj + (long long)a.ny * kk);
+            if (a.model == PCF_MODEL_COMPRESSIBLE) {
+                const long long hp = (ii + a.nbx) + sy * (jj + a.nby) + sz * k;
+                const double dpdpi = 1.0 / (a.gamma - 1.0) * pow(a.rsp / a.pref, 1.0 - a.gamma) *
+                                     pow(__ldg(a.p + hp), 2.0 - a.gamma);
+                A[CC][2] -= (dpdpi / a.dt) / (a.dt * a.rsp / a.kappa);
+            }
 
-    // ---- scaling by 1 / (fcscal fcscal_neighbour) and store ----------------
-    const double rfcc = RFC(0, 0, 0);
+            // ---- scaling by 1 / (fcscal fcscal_neighbour), stores, and the
+            // difference form B_p = A_p fcscal_nb with the defect sum in plane AC
+            const double rfcc = H5(F_RFC, 0, 0, 0);
+            double defect = 0.0;
 #pragma unroll
-    for (int c = 0; c < 5; ++c) {
-        const int di = c == CR ? 1 : (c == CL ? -1 : 0);
-        const int dj = c == CF ? 1 : (c == CB ? -1 : 0);
-#pragma unroll
-        for (int z = 0; z < 5; ++z) {
-            const double v = A[c][z] * rfcc * RFC(di, dj, z - 2);
-            const long long o = (long long)kPlane[c][z] * n + cell;
-            if (!PCF_IN(o, (long long)PCF_NCOEF * n, 403)) continue;
-            a.coef64[o] = v;
-            a.coef32[o] = (float)v;
-            if (a.coef16) a.coef16[o] = __float2bfloat16_rn((float)v);
+            for (int p = 0; p < PCF_NCOEF; ++p) {
+                const int c = plane_col(p), z = plane_dk(p) + 2;
+                const double v = A[c][z] * rfcc * H5(F_RFC, plane_di(p), plane_dj(p), plane_dk(p));
+                const long long o = (long long)p * n + cell;
+                if (!PCF_IN(o, (long long)PCF_NCOEF * n, 403)) continue;
+                a.coef64[o] = v;
+                a.coef32[o] = (float)v;
+                if (a.coef16) a.coef16[o] = __float2bfloat16_rn((float)v);
+                const double b = v * H5(F_FCH, plane_di(p), plane_dj(p), plane_dk(p));
+                defect += b;
+                if (p != PCF_AC) a.diff32[o] = (float)b;
+            }
+            if (PCF_IN(cell, n, 404)) {
+                a.diff32[(long long)PCF_AC * n + cell] = (float)defect;
+                const double f = H5(F_FCH, 0, 0, 0);
+                a.fc64[cell] = f;
+                a.rfc32[cell] = (float)(1.0 / f);
+            }
         }
+        cp_async_wait_all();
+        __syncthreads();
     }
 }
 
@@ -336,9 +464,19 @@ int pcf_launch_assemble(pcf_handle *h, double dt, double rf, int damp_h) {
     a.rfch = h->rfch;
     a.rdx = 1.0 / h->dx; a.rdy = 1.0 / h->dy; a.rdz = 1.0 / h->dz;
     a.coef64 = h->coef64; a.coef32 = h->coef32; a.coef16 = h->coef16;
-    const long long n = h->d.n;
-    const int bs = 128;
-    pcf::k_assemble<<<(unsigned)((n + bs - 1) / bs), bs, 0, h->stream>>>(a);
+    a.diff32 = h->coefB32; a.fc64 = h->fc64; a.rfc32 = h->rfc32;
+    // the dynamic shared-memory attribute is a per-device setting of the kernel
+    static std::atomic<unsigned long long> attr_set{0};
+    int dev = 0;
+    PCF_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return PCF_ENODEVICE;
+    if (!(attr_set.load() >> dev & 1ull)) {
+        PCF_CUDA_TRY(cudaFuncSetAttribute(pcf::k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, pcf::ASM_SMEM));
+        attr_set.fetch_or(1ull << dev);
+    }
+    const dim3 grid((unsigned)((h->d.nx + pcf::AX - 1) / pcf::AX), (unsigned)((h->d.ny + pcf::AY - 1) / pcf::AY),
+                    (unsigned)((h->d.nz + pcf::AKC - 1) / pcf::AKC));
+    pcf::k_assemble<<<grid, dim3(pcf::AX, pcf::AY), pcf::ASM_SMEM, h->stream>>>(a);
     PCF_CUDA_TRY(cudaGetLastError());
     h->fac_deta = __builtin_nan("");
     return PCF_OK;

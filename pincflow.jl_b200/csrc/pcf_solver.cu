@@ -1737,15 +1737,17 @@ int pcf_set_background(pcf_handle *h, const double *pbar, const double *rhobar, 
 
 static int assemble_device(pcf_handle *h, double dt, double rf, int damp_h) {
     if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
-    // about 9 haloed fields read, 25 FP64 + 25 FP32 planes written per cell
+    // 11 haloed fields read; 25 FP64, 25 FP32, 25 difference-form FP32 (and
+    // 25 BF16) planes, fcscal and 1 / fcscal written per cell
     {
-        ProfScope ps(h, PCF_PROF_ASSEMBLE, (9.0 * 8 + 25.0 * 12) * (double)h->d.n);
+        ProfScope ps(h, PCF_PROF_ASSEMBLE,
+                     (11.0 * 8 + 25.0 * 16 + (h->coef16 ? 25.0 * 2 : 0.0) + 12.0) * (double)h->d.n);
         int rc = pcf_launch_assemble(h, dt, rf, damp_h);
         if (rc) return rc;
     }
     h->operator_set = 1;
     h->op_version += 1;
-    return build_diff(h, 1);
+    return PCF_OK;
 }
 
 int pcf_compute_operator(pcf_handle *h, const double *rho, const double *betar, const double *p, double dt,
@@ -2543,15 +2545,17 @@ int pcf_solve(pcf_handle *h, const double *rhs, const double *rho, const double 
     PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
     const size_t hb = sizeof(double) * (size_t)h->nh;
     PCF_CUDA_TRY(cudaEventRecord(h->ev[0], h->stream));
-    // the right-hand side is first read by the Krylov loop: it travels on the
-    // copy stream (after all earlier work on the handle's stream) while
-    // rho, betar and p go up and the operator is assembled
-    PCF_CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->ev[0], 0));
-    PCF_CUDA_TRY(cudaMemcpyAsync(h->b64, rhs, sizeof(double) * h->d.n, cudaMemcpyHostToDevice, h->copy_stream));
-    PCF_CUDA_TRY(cudaEventRecord(h->ev[7], h->copy_stream));
     PCF_CUDA_TRY(cudaMemcpyAsync(h->rho, rho, hb, cudaMemcpyHostToDevice, h->stream));
     PCF_CUDA_TRY(cudaMemcpyAsync(h->betar, betar, hb, cudaMemcpyHostToDevice, h->stream));
     if (p) PCF_CUDA_TRY(cudaMemcpyAsync(h->p, p, hb, cudaMemcpyHostToDevice, h->stream));
+    // the right-hand side is first read by the Krylov loop: it goes up on the
+    // copy stream once the assembly's inputs are up (host-to-device copies
+    // share one link, so starting it earlier would only delay them) while the
+    // operator and the multigrid hierarchy are built
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[5], h->stream));
+    PCF_CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->ev[5], 0));
+    PCF_CUDA_TRY(cudaMemcpyAsync(h->b64, rhs, sizeof(double) * h->d.n, cudaMemcpyHostToDevice, h->copy_stream));
+    PCF_CUDA_TRY(cudaEventRecord(h->ev[7], h->copy_stream));
     const double *x = nullptr;
     int rc = solve_common(h, dt, rayleigh_factor, tolref, prm, res, &x, h->ev[7]);
     if (rc) {

@@ -58,6 +58,23 @@ def test_assembly_matches_oracle(name, solvers, oracle):
 
 
 @pytest.mark.parametrize("name", CASES)
+def test_assembly_writes_every_operator_form(name, solvers):
+    """The assembly writes the FP64, FP32 and difference-form FP32 operators
+    (and fcscal) in one pass; uploading its FP64 planes with set_operator
+    rebuilds the FP32 copy and the difference form from them.  Every form
+    must come out the same either way: the applies agree bitwise."""
+    cfg, s = solvers(name)
+    coef = s.compute_operator(cfg["rho"], cfg["betar"], cfg["dt"], cfg["rayleigh_factor"], cfg["damp"], cfg["p"])
+    x = np.random.default_rng(8).standard_normal(cfg["dom"].interior_shape)
+    forms = [("fp64", False), ("fp32", False), ("fp32", True), ("mixed", False)]
+    fused = [s.apply_operator(x, horizontal=h, precision=p) for p, h in forms]
+    s.set_operator(coef)
+    rebuilt = [s.apply_operator(x, horizontal=h, precision=p) for p, h in forms]
+    for (p, h), a, b in zip(forms, fused, rebuilt):
+        assert np.array_equal(a, b), (name, p, h, np.abs(a - b).max())
+
+
+@pytest.mark.parametrize("name", CASES)
 @pytest.mark.parametrize("horizontal", [False, True])
 def test_apply_operator_matches_oracle(name, horizontal, solvers, oracle):
     cfg, s = solvers(name)
