@@ -75,12 +75,11 @@ constexpr int AHX = AX + 2, AHY = AY + 2, AT = AHX * AHY;  // the tile with its 
 constexpr int NH3 = 7, F_J = 0, F_PB = 1, F_RB = 2, F_RO = 3, F_BR = 4, F_M13 = 5, F_M23 = 6;
 // fields with a halo and a 5-level window (k-2..k+2): 1 / fcscal, fcscal
 constexpr int NH5 = 2, F_RFC = 0, F_FCH = 1;
-// centre-column fields with a 3-level window: met33, N^2, thetabar
+// centre-column fields with a 3-level window, held in registers: met33, N^2, thetabar
 constexpr int NC3 = 3, F_M33 = 0, F_N2 = 1, F_TH = 2;
 constexpr int S3 = 4, S5 = 6;  // ring slots: the window plus the level in flight
-constexpr int ASM_H3 = 0, ASM_H5 = ASM_H3 + NH3 * S3 * AT, ASM_C3 = ASM_H5 + NH5 * S5 * AT,
-              ASM_DOUBLES = ASM_C3 + NC3 * S3 * AX * AY;
-constexpr int ASM_SMEM = ASM_DOUBLES * (int)sizeof(double);
+constexpr int ASM_H3 = 0, ASM_H5 = ASM_H3 + NH3 * S3 * AT, ASM_DOUBLES = ASM_H5 + NH5 * S5 * AT;
+constexpr int ASM_SMEM = ASM_DOUBLES * (int)sizeof(double);  // 65,280 bytes: three blocks per SM
 
 // (di, dj, dk) of plane p in Tensor order (pincflow_poisson.h: AC, AL, AR, AB,
 // AF, AD, AU, ...), and the column index (Col) of (di, dj).
@@ -122,16 +121,14 @@ __device__ __forceinline__ void cp_async8(double *dst, const double *src) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Copies level kk (interior index, -2..nz+1) of a haloed field into one ring
-// slot: the tile plus its 1-column halo, or the tile alone (centre fields).
-template <bool HALO>
+// slot: the tile plus its 1-column halo.
 __device__ __forceinline__ void stage_level(double *dst, const double *src, const AssembleArgs &a, int i0, int j0,
                                             int kk, int tid) {
     const long long sy = a.nxx, sz = (long long)a.nxx * a.nyy;
     const long long nh = sz * (a.nz + 2 * a.nbz);
-    constexpr int W = HALO ? AHX : AX, CNT = HALO ? AT : AX * AY, O = HALO ? 1 : 0;
-    for (int t = tid; t < CNT; t += AX * AY) {
-        const int ty = t / W, tx = t - ty * W;
-        const int i = i0 - O + tx, j = j0 - O + ty;  // interior indices, -1..nx and -1..ny
+    for (int t = tid; t < AT; t += AX * AY) {
+        const int ty = t / AHX, tx = t - ty * AHX;
+        const int i = i0 - 1 + tx, j = j0 - 1 + ty;  // interior indices, -1..nx and -1..ny
         if (i > a.nx || j > a.ny) continue;            // beyond the halo of a partial tile
         const long long g = (i + a.nbx) + sy * (j + a.nby) + sz * (kk + a.nbz);
         if (!PCF_IN(g, nh, 401)) continue;
@@ -145,7 +142,7 @@ __device__ __forceinline__ void stage_level(double *dst, const double *src, cons
 // difference-form FP32 operator for pi = s / fcscal (the planes A_nb fcscal_nb
 // and their sum in plane AC, summed in plane order in FP64), fcscal and
 // 1 / fcscal on the interior.
-__global__ void __launch_bounds__(AX * AY, 2) k_assemble(AssembleArgs a) {
+__global__ void __launch_bounds__(AX * AY, 3) k_assemble(AssembleArgs a) {
     extern __shared__ double asm_sm[];
     const int tid = threadIdx.x + AX * threadIdx.y;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -165,20 +162,29 @@ __global__ void __launch_bounds__(AX * AY, 2) k_assemble(AssembleArgs a) {
     auto stage3 = [&](int kk) {
 #pragma unroll
         for (int f = 0; f < NH3; ++f)
-            stage_level<true>(asm_sm + ASM_H3 + (f * S3 + slot3(kk)) * AT, h3src[f], a, i0, j0, kk, tid);
-#pragma unroll
-        for (int f = 0; f < NC3; ++f)
-            if (f != F_TH || have_th)
-                stage_level<false>(asm_sm + ASM_C3 + (f * S3 + slot3(kk)) * AX * AY, c3src[f], a, i0, j0, kk, tid);
+            stage_level(asm_sm + ASM_H3 + (f * S3 + slot3(kk)) * AT, h3src[f], a, i0, j0, kk, tid);
     };
     auto stage5 = [&](int kk) {
 #pragma unroll
         for (int f = 0; f < NH5; ++f)
-            stage_level<true>(asm_sm + ASM_H5 + (f * S5 + slot5(kk)) * AT, h5src[f], a, i0, j0, kk, tid);
+            stage_level(asm_sm + ASM_H5 + (f * S5 + slot5(kk)) * AT, h5src[f], a, i0, j0, kk, tid);
+    };
+    // centre-column fields at level kk, straight from global memory (coalesced)
+    const long long col = (ii + a.nbx) + sy * (jj + a.nby);
+    const long long nh = sz * (a.nz + 2 * a.nbz);
+    auto centre = [&](double (&dst)[NC3], int kk) {
+        const long long g = col + sz * (kk + a.nbz);
+        if (!live || !PCF_IN(g, nh, 405)) return;
+#pragma unroll
+        for (int f = 0; f < NC3; ++f) dst[f] = (f != F_TH || have_th) ? __ldg(c3src[f] + g) : 0.0;
     };
     // the windows of the first level
     for (int kk = k0 - 1; kk <= k0 + 1; ++kk) stage3(kk);
     for (int kk = k0 - 2; kk <= k0 + 2; ++kk) stage5(kk);
+    double cw[3][NC3] = {}, cnext[NC3] = {};  // centre fields at levels kk-1, kk, kk+1; kk+2
+    centre(cw[0], k0 - 1);
+    centre(cw[1], k0);
+    centre(cw[2], k0 + 1);
     cp_async_wait_all();
     __syncthreads();
 
@@ -187,6 +193,7 @@ __global__ void __launch_bounds__(AX * AY, 2) k_assemble(AssembleArgs a) {
         if (kk + 1 < k1) {  // the next level's new rows
             stage3(kk + 2);
             stage5(kk + 3);
+            centre(cnext, kk + 2);
         }
         if (live) {
             const int k = kk + a.nbz;  // haloed level
@@ -200,7 +207,7 @@ __global__ void __launch_bounds__(AX * AY, 2) k_assemble(AssembleArgs a) {
             auto H5 = [&](int f, int di, int dj, int dk) {
                 return asm_sm[ASM_H5 + (f * S5 + b5[dk + 2]) * AT + cxy + di + dj * AHX];
             };
-            auto C3 = [&](int f, int dk) { return asm_sm[ASM_C3 + (f * S3 + b3[dk + 1]) * AX * AY + tid]; };
+            auto C3 = [&](int f, int dk) { return cw[dk + 1][f]; };
             auto J = [&](int di, int dj, int dk) { return H3(F_J, di, dj, dk); };
             auto PB = [&](int di, int dj, int dk) { return H3(F_PB, di, dj, dk); };
             auto RB = [&](int di, int dj, int dk) { return H3(F_RB, di, dj, dk); };
@@ -392,6 +399,12 @@ __global__ void __launch_bounds__(AX * AY, 2) k_assemble(AssembleArgs a) {
                 a.fc64[cell] = f;
                 a.rfc32[cell] = (float)(1.0 / f);
             }
+        }
+#pragma unroll
+        for (int f = 0; f < NC3; ++f) {
+            cw[0][f] = cw[1][f];
+            cw[1][f] = cw[2][f];
+            cw[2][f] = cnext[f];
         }
         cp_async_wait_all();
         __syncthreads();
