@@ -3,7 +3,8 @@ residual 1e-10 on a full benchmark workload and records
   * tests/golden/<config>_fp64_oracle.json: the iteration count, the final
     residual and the run time (bench.py scales its bounded CPU samples by
     these counts);
-  * tests/golden/<config>_fp64_fingerprint.npz (c2, c5): a fingerprint of
+  * tests/golden/<config>_fp64_fingerprint.npz (c2, c5; c4_<nx>_... for the
+    first member of each c4 size class): a fingerprint of
     the oracle's converged pressure dpip = solution / fcscal / dt
     (solve_poisson!.jl:65-72): its values at FINGERPRINT_POINTS seeded
     interior cells, its mean and the RMS of each z-level with the mean
@@ -84,7 +85,8 @@ def main():
         out = {"workload": "c4 ensemble (seed 4): first member of each size class", "classes": {}}
         for nx in sorted(set(sizes)):
             q = sizes.index(nx)
-            out["classes"][str(nx)] = dict(full_solve(C.c4(q, nx), f"c4 member {q}, {nx}x{nx}x{nx // 2}"),
+            fpq = os.path.join(HERE, f"c4_{nx}_fp64_fingerprint.npz")
+            out["classes"][str(nx)] = dict(full_solve(C.c4(q, nx), f"c4 member {q}, {nx}x{nx}x{nx // 2}", fpq),
                                            member=q)
             print(nx, out["classes"][str(nx)], flush=True)
     else:

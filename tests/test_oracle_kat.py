@@ -219,6 +219,52 @@ def test_oracle_iteration_fixtures_are_converged(config, lo, hi):
     assert not d["errflag"] and d["true_residual"] <= 1e-10 and lo < d["niter"] < hi
 
 
+FINGERPRINTS = ["c2", "c5", "c4_64", "c4_96", "c4_128", "c4_192"]
+
+
+@pytest.mark.parametrize("name", FINGERPRINTS)
+def test_fingerprints_agree_with_their_records(name):
+    """Every committed fingerprint of an oracle solve (the parity target of
+    tests/test_gpu_baseline.py) belongs to the recorded full solve: same
+    iteration count and true residual, distinct in-range sample indices."""
+    fp = np.load(os.path.join(HERE, "golden", f"{name}_fp64_fingerprint.npz"))
+    config = name.split("_")[0]
+    with open(os.path.join(HERE, "golden", f"{config}_fp64_oracle.json")) as fh:
+        rec = json.load(fh)
+    if config == "c4":
+        rec = rec["classes"][name.split("_")[1]]
+    assert int(fp["niter"]) == rec["niter"] and float(fp["true_residual"]) == rec["true_residual"] <= 1e-10
+    n = int(np.prod(fp["shape"]))
+    idx = fp["indices"]
+    assert len(np.unique(idx)) == len(idx) == min(65536, n) and idx.min() >= 0 and idx.max() < n
+    assert fp["level_rms"].shape == (int(fp["shape"][0]),) and np.all(fp["level_rms"] > 0)
+
+
+def test_oracle_reproduces_the_smallest_c4_fingerprint(oracle):
+    """The oracle's FP64 solve of the 64 x 64 x 32 c4 member (about 1 s)
+    reproduces its committed fingerprint bitwise: the oracle behind the
+    full-size parity targets has not drifted."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    from make_oracle_iterations import fingerprint_indices
+    fp = np.load(os.path.join(HERE, "golden", "c4_64_fp64_fingerprint.npz"))
+    sizes = C.c4_sizes()
+    q = sizes.index(64)
+    cfg = C.c4(q, 64)
+    dom, f = cfg["dom"], cfg["fields"]
+    d = oracle.dims(dom.nx, dom.ny, dom.nz, dom.nbx)
+    coef = oracle.compute_operator(d, oracle.MODELS[cfg["model"]], f, cfg["rho"], cfg["betar"], cfg["dt"],
+                                   cfg["rayleigh_factor"])
+    sol, info = oracle.bicgstab(d, coef, f["dx"], f["dy"], cfg["rhs"], tolerance=1e-10, tolerance_is_relative=True,
+                                poisson_iterations=5000)
+    assert info["niter"] == int(fp["niter"])
+    pb, rb = dom.interior(f["pbar"]), dom.interior(f["rhobar"])
+    dpip = sol / np.sqrt(pb * pb / rb) / cfg["dt"]
+    idx = fingerprint_indices(dpip.size)
+    assert np.array_equal(idx, fp["indices"])
+    assert np.array_equal(dpip.ravel()[idx], fp["values"])
+
+
 def test_network_oracle_gradient_matches_finite_differences():
     """Pins the network oracle: its analytic gradient (exact float64 network)
     against central differences along random directions."""
