@@ -33,6 +33,7 @@ namespace pcf {
 struct AssembleArgs {
     int nx, ny, nz, nxx, nyy, nbx, nby, nbz;
     int z_size, ko, model, damp_h;
+    int kc0;  // first z-chunk (of AKC levels) of the launch
     double dx, dy, dz, dt, rf;
     double rdx, rdy, rdz;  // 1 / dx, 1 / dy, 1 / dz
     double gamma, kappa, rsp, pref;
@@ -146,7 +147,7 @@ __global__ void __launch_bounds__(AX * AY, 3) k_assemble(AssembleArgs a) {
     extern __shared__ double asm_sm[];
     const int tid = threadIdx.x + AX * threadIdx.y;
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const int i0 = blockIdx.x * AX, j0 = blockIdx.y * AY, k0 = blockIdx.z * AKC;
+    const int i0 = blockIdx.x * AX, j0 = blockIdx.y * AY, k0 = (blockIdx.z + a.kc0) * AKC;
     const int k1 = min(k0 + AKC, a.nz);
     const int ii = i0 + tx, jj = j0 + ty;
     const bool live = ii < a.nx && jj < a.ny;
@@ -461,7 +462,10 @@ __global__ void k_factors(int plane, int nz, long long n, double deta, const dou
 
 }  // namespace pcf
 
-int pcf_launch_assemble(pcf_handle *h, double dt, double rf, int damp_h) {
+int pcf_assemble_chunk_levels() { return pcf::AKC; }
+
+// Assembles the z-chunks [c0, c1) of AKC levels each (c1 < 0: to the top).
+int pcf_launch_assemble(pcf_handle *h, double dt, double rf, int damp_h, int c0, int c1) {
     pcf::AssembleArgs a;
     a.nx = h->d.nx; a.ny = h->d.ny; a.nz = h->d.nz;
     a.nxx = h->nxx; a.nyy = h->nyy;
@@ -487,8 +491,12 @@ int pcf_launch_assemble(pcf_handle *h, double dt, double rf, int damp_h) {
         PCF_CUDA_TRY(cudaFuncSetAttribute(pcf::k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, pcf::ASM_SMEM));
         attr_set.fetch_or(1ull << dev);
     }
+    const int nchunks = (h->d.nz + pcf::AKC - 1) / pcf::AKC;
+    if (c1 < 0 || c1 > nchunks) c1 = nchunks;
+    if (c0 < 0 || c0 >= c1) return PCF_OK;
+    a.kc0 = c0;
     const dim3 grid((unsigned)((h->d.nx + pcf::AX - 1) / pcf::AX), (unsigned)((h->d.ny + pcf::AY - 1) / pcf::AY),
-                    (unsigned)((h->d.nz + pcf::AKC - 1) / pcf::AKC));
+                    (unsigned)(c1 - c0));
     pcf::k_assemble<<<grid, dim3(pcf::AX, pcf::AY), pcf::ASM_SMEM, h->stream>>>(a);
     PCF_CUDA_TRY(cudaGetLastError());
     h->fac_deta = __builtin_nan("");

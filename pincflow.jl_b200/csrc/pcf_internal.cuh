@@ -193,7 +193,8 @@ struct pcf_handle {
     double dx, dy, dz;
     int grid_set, background_set, operator_set;
     cudaStream_t stream;
-    cudaStream_t copy_stream;  // pcf_solve: the right-hand side's upload, concurrent with the assembly
+    cudaStream_t copy_stream;  // pcf_solve: the uploads, concurrent with the assembly
+    cudaEvent_t slab_ev[4];    // pcf_solve: a z-slab of the assembly's inputs is up
     cudaEvent_t ev[8];
 
     // haloed FP64 fields

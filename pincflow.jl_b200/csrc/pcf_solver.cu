@@ -31,7 +31,8 @@ int pcf_set_cuda_error(cudaError_t e) {
     return e == cudaErrorMemoryAllocation ? PCF_ENOMEM : PCF_ECUDA;
 }
 
-int pcf_launch_assemble(pcf_handle *h, double dt, double rf, int damp_h);
+int pcf_launch_assemble(pcf_handle *h, double dt, double rf, int damp_h, int c0 = 0, int c1 = -1);
+int pcf_assemble_chunk_levels();
 int pcf_launch_factors(pcf_handle *h, double deta);
 int pcf_launch_correct(pcf_handle *h, double dt, double rf, int damp_h, double *dpip, double *u, double *v,
                        double *w, double *rhop, double *pip, double *corx, double *cory);
@@ -1605,6 +1606,8 @@ int pcf_destroy(pcf_handle *h) {
     }
     for (auto &e : h->ev)
         if (e) cudaEventDestroy(e);
+    for (auto &e : h->slab_ev)
+        if (e) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     delete h;
@@ -1659,6 +1662,8 @@ int pcf_create(pcf_handle **out, const pcf_dims *dims) {
     if (cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PCF_ECUDA);
     for (auto &e : h->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return fail(PCF_ECUDA);
+    for (auto &e : h->slab_ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail(PCF_ECUDA);
     const size_t nh8 = sizeof(double) * (size_t)h->nh;
     const size_t n8 = sizeof(double) * (size_t)h->d.n, n4 = sizeof(float) * (size_t)h->d.n;
     double **fields[] = {&h->jac, &h->met13, &h->met23, &h->met33, &h->pbar, &h->rhobar, &h->thetabar, &h->n2,
@@ -1735,19 +1740,29 @@ int pcf_set_background(pcf_handle *h, const double *pbar, const double *rhobar, 
     return PCF_OK;
 }
 
-static int assemble_device(pcf_handle *h, double dt, double rf, int damp_h) {
-    if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
+// Assembles z-chunks [c0, c1) (c1 < 0: to the top); the operator is set
+// once the last chunk is queued.
+static int assemble_chunks(pcf_handle *h, double dt, double rf, int damp_h, int c0, int c1) {
+    const int nchunks = (h->d.nz + pcf_assemble_chunk_levels() - 1) / pcf_assemble_chunk_levels();
+    if (c1 < 0 || c1 > nchunks) c1 = nchunks;
     // 11 haloed fields read; 25 FP64, 25 FP32, 25 difference-form FP32 (and
     // 25 BF16) planes, fcscal and 1 / fcscal written per cell
     {
-        ProfScope ps(h, PCF_PROF_ASSEMBLE,
-                     (11.0 * 8 + 25.0 * 16 + (h->coef16 ? 25.0 * 2 : 0.0) + 12.0) * (double)h->d.n);
-        int rc = pcf_launch_assemble(h, dt, rf, damp_h);
+        const double cells = (double)h->d.n * (c1 - c0) / nchunks;
+        ProfScope ps(h, PCF_PROF_ASSEMBLE, (11.0 * 8 + 25.0 * 16 + (h->coef16 ? 25.0 * 2 : 0.0) + 12.0) * cells);
+        int rc = pcf_launch_assemble(h, dt, rf, damp_h, c0, c1);
         if (rc) return rc;
     }
-    h->operator_set = 1;
-    h->op_version += 1;
+    if (c1 == nchunks) {
+        h->operator_set = 1;
+        h->op_version += 1;
+    }
     return PCF_OK;
+}
+
+static int assemble_device(pcf_handle *h, double dt, double rf, int damp_h) {
+    if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
+    return assemble_chunks(h, dt, rf, damp_h, 0, -1);
 }
 
 int pcf_compute_operator(pcf_handle *h, const double *rho, const double *betar, const double *p, double dt,
@@ -2512,16 +2527,17 @@ static float elapsed(cudaEvent_t a, cudaEvent_t b) {
 }
 
 // rhs_ready: an event the solve waits for after the assembly (the right-hand
-// side's upload on the copy stream), or null.
+// side's upload on the copy stream), or null.  assembled: the caller queued
+// the assembly (and recorded ev[1] where it starts).
 static int solve_common(pcf_handle *h, double dt, double rf, double tolref, const pcf_params *prm, pcf_result *res,
-                        const double **x, cudaEvent_t rhs_ready = nullptr) {
+                        const double **x, cudaEvent_t rhs_ready = nullptr, bool assembled = false) {
     // solve_poisson!.jl:52-54
     if (dt == 0.0) return PCF_EINVAL;
     int rc;
-    PCF_CUDA_TRY(cudaEventRecord(h->ev[1], h->stream));
+    if (!assembled) PCF_CUDA_TRY(cudaEventRecord(h->ev[1], h->stream));
     {
         NvtxScope r("pcf assemble");
-        if ((rc = assemble_device(h, dt, rf, prm->damp_horizontal_wind_on_rhs))) return rc;
+        if (!assembled && (rc = assemble_device(h, dt, rf, prm->damp_horizontal_wind_on_rhs))) return rc;
         if (prm->preconditioner && (rc = ensure_factors(h, deta_of(h, prm->dtau)))) return rc;
     }
     if (rhs_ready) PCF_CUDA_TRY(cudaStreamWaitEvent(h->stream, rhs_ready, 0));
@@ -2543,21 +2559,41 @@ int pcf_solve(pcf_handle *h, const double *rhs, const double *rho, const double 
     if (dt == 0.0) return PCF_EINVAL;
     if (!h->grid_set || !h->background_set) return PCF_ENOTREADY;
     PCF_CUDA_TRY(cudaSetDevice(h->dims.device));
-    const size_t hb = sizeof(double) * (size_t)h->nh;
     PCF_CUDA_TRY(cudaEventRecord(h->ev[0], h->stream));
-    PCF_CUDA_TRY(cudaMemcpyAsync(h->rho, rho, hb, cudaMemcpyHostToDevice, h->stream));
-    PCF_CUDA_TRY(cudaMemcpyAsync(h->betar, betar, hb, cudaMemcpyHostToDevice, h->stream));
-    if (p) PCF_CUDA_TRY(cudaMemcpyAsync(h->p, p, hb, cudaMemcpyHostToDevice, h->stream));
-    // the right-hand side is first read by the Krylov loop: it goes up on the
-    // copy stream once the assembly's inputs are up (host-to-device copies
-    // share one link, so starting it earlier would only delay them) while the
-    // operator and the multigrid hierarchy are built
-    PCF_CUDA_TRY(cudaEventRecord(h->ev[5], h->stream));
-    PCF_CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->ev[5], 0));
+    // The assembly's inputs go up in z-slabs on the copy stream (after all
+    // earlier work on the handle's stream), and each slab's part of the
+    // assembly starts on the handle's stream as soon as the planes it reads
+    // are up, so the assembly runs under the remaining uploads.  The
+    // right-hand side follows (host-to-device copies share one link, so
+    // starting it earlier would only delay them); the Krylov loop, its first
+    // reader, waits for it.
+    PCF_CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->ev[0], 0));
+    const int akc = pcf_assemble_chunk_levels();
+    const int nchunks = (h->d.nz + akc - 1) / akc;
+    const int slabs = std::min(nchunks, (int)(sizeof(h->slab_ev) / sizeof(h->slab_ev[0])));
+    const long long plane = (long long)h->nxx * h->nyy, nzz = h->nh / plane;
+    long long up = 0;  // haloed z-planes uploaded
+    int rc = PCF_OK;
+    for (int sl = 0; sl < slabs; ++sl) {
+        const int c0 = (int)((long long)nchunks * sl / slabs), c1 = (int)((long long)nchunks * (sl + 1) / slabs);
+        // chunk c reads the interior levels up to AKC c1 + 1, haloed plane AKC c1 + 1 + nbz
+        const long long end = sl + 1 == slabs ? nzz : std::min(nzz, (long long)akc * c1 + 2 + h->dims.nbz);
+        if (end > up) {
+            const size_t off = (size_t)(up * plane), cnt = sizeof(double) * (size_t)((end - up) * plane);
+            PCF_CUDA_TRY(cudaMemcpyAsync(h->rho + off, rho + off, cnt, cudaMemcpyHostToDevice, h->copy_stream));
+            PCF_CUDA_TRY(cudaMemcpyAsync(h->betar + off, betar + off, cnt, cudaMemcpyHostToDevice, h->copy_stream));
+            if (p) PCF_CUDA_TRY(cudaMemcpyAsync(h->p + off, p + off, cnt, cudaMemcpyHostToDevice, h->copy_stream));
+            up = end;
+        }
+        PCF_CUDA_TRY(cudaEventRecord(h->slab_ev[sl], h->copy_stream));
+        PCF_CUDA_TRY(cudaStreamWaitEvent(h->stream, h->slab_ev[sl], 0));
+        if (sl == 0) PCF_CUDA_TRY(cudaEventRecord(h->ev[1], h->stream));
+        if ((rc = assemble_chunks(h, dt, rayleigh_factor, prm->damp_horizontal_wind_on_rhs, c0, c1))) break;
+    }
     PCF_CUDA_TRY(cudaMemcpyAsync(h->b64, rhs, sizeof(double) * h->d.n, cudaMemcpyHostToDevice, h->copy_stream));
     PCF_CUDA_TRY(cudaEventRecord(h->ev[7], h->copy_stream));
     const double *x = nullptr;
-    int rc = solve_common(h, dt, rayleigh_factor, tolref, prm, res, &x, h->ev[7]);
+    if (!rc) rc = solve_common(h, dt, rayleigh_factor, tolref, prm, res, &x, h->ev[7], true);
     if (rc) {
         cudaStreamWaitEvent(h->stream, h->ev[7], 0);  // no later call may meet the copy in flight
         return rc;
