@@ -412,7 +412,7 @@ def run_step(args, rank, world, local_rank):
     wold = torch.zeros(dom.halo_shape, dtype=torch.float64, device=dev)
     kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000, residual="true")
     nl_fast = pcf.PoissonNamelist(**kw, precision="fp64" if args.method == "fp64" else "mixed",
-                                  multigrid=args.method == "mg", mg_dtau=args.mg_dtau, mg_fused_coarse=args.fused_coarse)
+                                  multigrid=args.method == "mg", mg_dtau=args.mg_dtau, mg_fused_coarse=FUSED[args.fused_coarse])
     nl_plain = pcf.PoissonNamelist(**kw, precision="fp64")
 
     def step(nl):
@@ -530,7 +530,7 @@ def run_c1(args, rank, world, local_rank):
     d_dpip = torch.zeros(dom.halo_shape, dtype=torch.float64, device=dev)
     kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000, residual="true")
     nl_fast = pcf.PoissonNamelist(**kw, precision="fp64" if args.method == "fp64" else "mixed",
-                                  multigrid=args.method == "mg", mg_dtau=args.mg_dtau, mg_fused_coarse=args.fused_coarse)
+                                  multigrid=args.method == "mg", mg_dtau=args.mg_dtau, mg_fused_coarse=FUSED[args.fused_coarse])
     nl_plain = pcf.PoissonNamelist(**kw, precision="fp64")
 
     def all_solves(nl):
@@ -626,7 +626,7 @@ def run_ensemble(args, rank, world, local_rank):
         members.append((cfg, s, d))
     torch.cuda.synchronize()
     kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000, residual="true")
-    nl_ens = pcf.PoissonNamelist(**kw, precision="mixed", multigrid=True, mg_dtau=args.mg_dtau, mg_fused_coarse=args.fused_coarse, autotune=True)
+    nl_ens = pcf.PoissonNamelist(**kw, precision="mixed", multigrid=True, mg_dtau=args.mg_dtau, mg_fused_coarse=FUSED[args.fused_coarse], autotune=True)
     nl_plain = pcf.PoissonNamelist(**kw, precision="fp64")
     ens = pcf.Ensemble([m[1] for m in members])
     cols = lambda key: [m[2][key].data_ptr() for m in members]
@@ -663,7 +663,7 @@ def run_ensemble(args, rank, world, local_rank):
     value = world * n / (ms / 1e3)
 
     # the same members one after another: plain FP64, and the single-handle multigrid solve
-    nl_single = pcf.PoissonNamelist(**kw, precision="mixed", multigrid=True, mg_dtau=args.mg_dtau, mg_fused_coarse=args.fused_coarse, autotune=True)
+    nl_single = pcf.PoissonNamelist(**kw, precision="mixed", multigrid=True, mg_dtau=args.mg_dtau, mg_fused_coarse=FUSED[args.fused_coarse], autotune=True)
 
     def sequential(nl):
         tot, iters = 0.0, []
@@ -826,7 +826,7 @@ def learned_arm(args, s, cfg, d_rhs, d_rho, d_betar, d_dpip, local_rank):
                              device=local_rank)
     t2 = time.perf_counter()
     kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000, precision="mixed",
-              residual="true", multigrid=args.method == "mg", mg_dtau=args.mg_dtau, mg_fused_coarse=args.fused_coarse)
+              residual="true", multigrid=args.method == "mg", mg_dtau=args.mg_dtau, mg_fused_coarse=FUSED[args.fused_coarse])
     out = {"training": {"configuration": "c3: 128x128x64 Boussinesq, 1-5 Gaussian hills, N ~ U(0.005, 0.02); "
                                          "stage_c5_patches: 128x128x192 patches of the c5 family at its resolution",
                         "pairs": {r: len(p) for r, p in pairs.items()}, "epochs": args.learned_epochs,
@@ -907,7 +907,7 @@ def run_ours(args, rank, world, local_rank):
 
     nl_fast = pcf.PoissonNamelist(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000,
                                   precision="fp64" if args.method == "fp64" else "mixed", residual="true",
-                                  multigrid=args.method == "mg", mg_dtau=args.mg_dtau, mg_fused_coarse=args.fused_coarse)
+                                  multigrid=args.method == "mg", mg_dtau=args.mg_dtau, mg_fused_coarse=FUSED[args.fused_coarse])
     nl_plain = pcf.PoissonNamelist(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=20000,
                                    precision="fp64", residual="true")
 
@@ -1069,6 +1069,9 @@ def run_ours(args, rank, world, local_rank):
     s.close()
 
 
+FUSED = {"auto": None, "on": True, "off": False}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1079,8 +1082,9 @@ def main():
     ap.add_argument("--size", default=None, help="c2 only: NXxNYxNZ instead of 256x256x128 (profiling captures)")
     ap.add_argument("--method", default="mg", choices=sorted(METHODS))
     ap.add_argument("--mg-dtau", type=float, default=2.5)
-    ap.add_argument("--fused-coarse", action="store_true",
-                    help="multigrid: the coarse levels in one cooperative launch per cycle (mg_fused_coarse = 1)")
+    ap.add_argument("--fused-coarse", default="auto", choices=["auto", "on", "off"],
+                    help="multigrid: the coarse levels as one cluster launch per cycle (mg_fused_coarse; auto: "
+                         "in the ensemble only)")
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--ref-sample-iters", type=int, default=None,
                     help="BiCGSTAB iterations per CPU sample (default: 20 on c2 and step, 4 on c5, 3 on c4)")

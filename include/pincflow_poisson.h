@@ -145,10 +145,12 @@ typedef struct {
                                       multiple of 8 those stencils load the BF16 tiles into shared memory by TMA
                                       (same arithmetic, same results); the learned preconditioner stage
                                       (learned & 2) runs the same V-cycle, which its training pairs come from (1) */
-    int mg_fused_coarse;           /* multigrid: 1: the levels of at most 1024 columns (nz <= 256) run as one
-                                      cooperative launch per cycle (column solves by warp scans, grid barriers
-                                      between the steps); 0: one kernel per step as on the finer levels (0:
-                                      measured no faster at 256 x 256 x 128 and slower for the ensemble) */
+    int mg_fused_coarse;           /* multigrid: the levels of at most 1024 columns (nz <= 256) as ONE launch
+                                      per cycle: a cluster of 16 thread blocks with the hardware cluster barrier
+                                      between the steps (column solves by warp scans).  1: on; 0: one kernel per
+                                      step as on the finer levels; -1 (default): on in pcf_ensemble_solve_device
+                                      (whose members' launches then leave the other SMs to one another), off in
+                                      single solves (measured slower there) */
 } pcf_params;
 
 typedef struct {

@@ -299,14 +299,18 @@ __global__ void __launch_bounds__(256) k_mg_prolong4(const float *__restrict__ e
 // their ~40 kernels per cycle moves a few MB.  k_mg_coarse runs that whole
 // part of the cycle -- the same steps as the per-kernel path (column solve
 // from zero, residual, restriction, ..., coarsest smoothing, prolongation,
-// pseudo-time step, column solve) -- as phases of one cooperative launch
-// separated by grid barriers.  Phases are cell-parallel (stencils and grid
+// pseudo-time step, column solve) -- as phases of ONE thread-block cluster
+// of kCoarseCluster CTAs, separated by the hardware cluster barrier
+// (barrier.cluster with release / acquire semantics: every global write of a
+// phase is visible to the whole cluster in the next).  The coarse levels'
+// data (a few MB) stay in L2.  Phases are cell-parallel (stencils and grid
 // transfers, the stencil's terms summed in k_stencil's order) or
 // column-parallel (the Thomas sweeps: one warp per column, each lane a run of
 // at most 8 levels, the runs' affine maps chained by warp-shuffle scans).
 constexpr int kCoarseColumns = 1024;   // levels of at most 32 x 32 columns
 constexpr int kCoarseMaxLevels = 12;
 constexpr int kCoarseThreads = 256;
+constexpr int kCoarseCluster = 16;     // CTAs of the cluster (the non-portable maximum; 8 where 16 is refused)
 
 struct CoarseLevel {
     int nx, ny, nz, cx, cy;  // cx, cy: the aggregation from the next finer level
@@ -321,40 +325,14 @@ struct CoarseArgs {
     int nlev;          // lv[0] is the first level of the coarse part
     int coarse_iters;  // smoothing steps on the coarsest level
     const KrylovScalars *guard;
-    unsigned *bar;     // grid barrier counter, zero at launch
 };
 
-// Grid-wide barrier number `gen` (0, 1, ...) of the launch; bounded (2 s):
-// a barrier that gives up marks the solve failed (PCF_ECUDA) and returns false.
-__device__ __forceinline__ bool coarse_barrier(const CoarseArgs &a, unsigned gen) {
-    __syncthreads();
-    __shared__ int fail;
-    if (threadIdx.x == 0) {
-        fail = 0;
-        __threadfence();
-        atomicAdd(a.bar, 1u);
-        const unsigned target = (gen + 1u) * gridDim.x;
-        uint64_t t0, t1;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-        for (;;) {
-            unsigned v;
-            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a.bar) : "memory");
-            if (v >= target) break;
-            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-            if (t1 - t0 > 2000000000ull) {
-                fail = 1;
-                KrylovScalars *g = const_cast<KrylovScalars *>(a.guard);
-                if (g) {
-                    g->status = PCF_ECUDA;
-                    g->done = 1;
-                }
-                break;
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return !fail;
+// Barrier of the whole cluster (every thread of every CTA arrives; the CTAs
+// of a cluster are co-scheduled, so it needs no bound).
+__device__ __forceinline__ void coarse_barrier() {
+    __syncwarp();  // the .aligned form wants the whole warp at the same instruction
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
 // Column solves of level L, one warp per column: mode TH_B solves from -deta b
@@ -507,29 +485,29 @@ __device__ void coarse_prolong(const CoarseLevel &F, const CoarseLevel &C, const
 }
 
 __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(const __grid_constant__ CoarseArgs a) {
+    // the guard is written by earlier kernels only: every CTA takes the same branch
     if (krylov_done(a.guard)) return;
-    unsigned gen = 0;
     const int top = a.nlev - 1;
     // descent: column solve from zero, residual, restriction
     for (int l = 0; l < top; ++l) {
         const CoarseLevel &L = a.lv[l];
         coarse_thomas<TH_B>(L, L.b, L.s);
-        if (!coarse_barrier(a, gen++)) return;
+        coarse_barrier();
         coarse_stencil<false>(L, L.s, L.b, L.t);
-        if (!coarse_barrier(a, gen++)) return;
+        coarse_barrier();
         coarse_restrict(L, a.lv[l + 1], L.t);
-        if (!coarse_barrier(a, gen++)) return;
+        coarse_barrier();
     }
     // the coarsest level: a column solve from zero, then pseudo-time steps
     const CoarseLevel &Z = a.lv[top];
     coarse_thomas<TH_B>(Z, Z.b, Z.s);
-    if (!coarse_barrier(a, gen++)) return;
+    coarse_barrier();
     float *cur = Z.s, *oth = Z.t;
     for (int q = 1; q < a.coarse_iters; ++q) {
         coarse_stencil<true>(Z, cur, Z.b, oth);
-        if (!coarse_barrier(a, gen++)) return;
+        coarse_barrier();
         coarse_thomas<TH_T>(Z, oth, oth);
-        if (!coarse_barrier(a, gen++)) return;
+        coarse_barrier();
         float *w = cur;
         cur = oth;
         oth = w;
@@ -539,11 +517,11 @@ __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(const __grid_const
     for (int l = top - 1; l >= 0; --l) {
         const CoarseLevel &L = a.lv[l];
         coarse_prolong(L, a.lv[l + 1], e);
-        if (!coarse_barrier(a, gen++)) return;
+        coarse_barrier();
         coarse_stencil<true>(L, L.s, L.b, L.t);
-        if (!coarse_barrier(a, gen++)) return;
+        coarse_barrier();
         coarse_thomas<TH_T>(L, L.t, L.t);
-        if (l > 0 && !coarse_barrier(a, gen++)) return;
+        if (l > 0) coarse_barrier();
         e = L.t;
     }
 }

@@ -667,8 +667,7 @@ struct MgState {
     double dtau = 0;
     bool bf16 = false;       // the finest level's stencils read h->coef16
     int fused_from = -1;     // first level of the one-launch coarse cycle (k_mg_coarse), -1: none
-    unsigned *coarse_bar = nullptr;  // its grid barrier counter
-    int coarse_grid = 0;     // its CTAs (co-resident)
+    int coarse_cluster = 0;  // its cluster's CTAs (16, or 8 where 16 is refused)
 };
 
 __global__ void k_to_float(const double *__restrict__ a, float *__restrict__ b, long long n, double scale);
@@ -821,20 +820,20 @@ static int mg_coarse_launch(pcf_handle *h, int l, const KrylovScalars *guard, fl
     }
     a.coarse_iters = m.coarse_iters;
     a.guard = guard;
-    a.bar = m.coarse_bar;
     ProfScope ps(h, PCF_PROF_MG, bytes);
-    PCF_CUDA_TRY(cudaMemsetAsync(m.coarse_bar, 0, sizeof(unsigned), h->stream));
     cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3((unsigned)m.coarse_grid);
+    cfg.gridDim = dim3((unsigned)m.coarse_cluster);
     cfg.blockDim = dim3(kCoarseThreads);
     cfg.stream = h->stream;
     cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)m.coarse_cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     PCF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_mg_coarse, a));
-    h->launches += 1;  // the memset is not a kernel
+    h->launches += 1;
     if (a.nlev == 1)
         *result = (m.coarse_iters - 1) % 2 == 0 ? m.lv[l].s : m.lv[l].t;
     else
@@ -938,7 +937,8 @@ static void clear_graphs(pcf_handle *h);
 
 // Builds (on the first call or when the level layout changes) and refreshes
 // (when the operator or the smoother's step changed) the hierarchy.
-static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
+// ensemble: called for a member of pcf_ensemble_solve_device (mg_fused_coarse = -1 fuses there only)
+static int mg_prepare(pcf_handle *h, const pcf_params *prm, bool ensemble = false) {
     if (!(prm->mg_dtau > 0) || prm->mg_coarse_iterations < 1 || prm->mg_min_columns < 1) return PCF_EINVAL;
     if (!h->mg) h->mg = new MgState();
     MgState &m = *h->mg;
@@ -999,23 +999,35 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm) {
     // kCoarseColumns columns (from level 2 on when level 1 reads a BF16 copy),
     // if its columns fit the warp sweeps (nz <= 256)
     m.fused_from = -1;
-    if (prm->mg_fused_coarse && h->d.nz <= 256) {
+    const bool fuse = prm->mg_fused_coarse > 0 || (prm->mg_fused_coarse < 0 && ensemble);
+    if (fuse && h->d.nz <= 256) {
         for (int l = m.bf16 ? 2 : 1; l < (int)m.lv.size(); ++l)
             if (m.lv[l].d.plane <= kCoarseColumns) {
                 if ((int)m.lv.size() - l <= kCoarseMaxLevels) m.fused_from = l;
                 break;
             }
     }
-    if (m.fused_from >= 0 && !m.coarse_bar) {
-        void *p = nullptr;
-        const cudaError_t e = cudaMalloc(&p, sizeof(unsigned));
-        if (e != cudaSuccess) return pcf_set_cuda_error(e);
-        m.allocs.push_back(p);
-        m.coarse_bar = static_cast<unsigned *>(p);
-        int per_sm = 0;
-        PCF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_coarse, kCoarseThreads, 0));
-        if (per_sm < 1) return PCF_ECUDA;
-        m.coarse_grid = num_sms();  // one CTA per SM: the cheapest grid barrier
+    if (m.fused_from >= 0 && !m.coarse_cluster) {
+        // the largest cluster the device schedules: 16 CTAs (non-portable), else 8
+        PCF_CUDA_TRY(cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        for (int size = kCoarseCluster; size >= 8 && !m.coarse_cluster; size /= 2) {
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3((unsigned)size);
+            cfg.blockDim = dim3(kCoarseThreads);
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = (unsigned)size;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, k_mg_coarse, &cfg) == cudaSuccess && clusters > 0)
+                m.coarse_cluster = size;
+            else
+                cudaGetLastError();
+        }
+        if (!m.coarse_cluster) m.fused_from = -1;  // no cluster: one kernel per step
     }
     if (m.bf16 && !h->coef16) {
         // first use: allocate and convert; later assemblies and pcf_set_operator write it themselves
@@ -1567,7 +1579,7 @@ int pcf_params_default(pcf_params *p) {
     p->mg_min_columns = 16;
     p->autotune = 0;
     p->mg_operator_bf16 = 1;
-    p->mg_fused_coarse = 0;
+    p->mg_fused_coarse = -1;
     return PCF_OK;
 }
 
@@ -3023,7 +3035,7 @@ int pcf_ensemble_solve_device(pcf_ensemble *e, const double *const *d_rhs, const
         PCF_CUDA_TRY(cudaEventRecord(h->ev[1], h->stream));
         if ((rc = assemble_device(h, dt[q], rayleigh_factor[q], prm->damp_horizontal_wind_on_rhs))) return rc;
         if (prm->preconditioner && (rc = ensure_factors(h, deta_of(h, prm->dtau)))) return rc;
-        if (prm->multigrid && (rc = mg_prepare(h, prm))) return rc;
+        if (prm->multigrid && (rc = mg_prepare(h, prm, true))) return rc;
         if (prm->autotune && (rc = autotune_handle(h, prm))) return rc;
         PCF_CUDA_TRY(cudaEventRecord(h->ev[2], h->stream));
         PCF_CUDA_TRY(cudaMemsetAsync(h->x64, 0, sizeof(double) * h->d.n, h->stream));

@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import ctypes
 from dataclasses import dataclass, field
+from typing import Optional
 
 import numpy as np
 
@@ -54,7 +55,8 @@ class PoissonNamelist:
     mg_min_columns: int = 16          # multigrid: a level with at most this many columns is the coarsest
     autotune: bool = False            # time the stencil tile shapes of each new grid size on first use
     mg_operator_bf16: bool = True     # multigrid: finest and first coarse level stencils read BF16 copies
-    mg_fused_coarse: bool = False     # multigrid: levels of <= 1024 columns in one cooperative launch per cycle
+    mg_fused_coarse: Optional[bool] = None  # multigrid: levels of <= 1024 columns as one cluster launch per cycle
+    #                                         (None: in ensembles only)
 
     def to_c(self) -> _lib.PcfParams:
         p = _lib.PcfParams()
@@ -79,7 +81,7 @@ class PoissonNamelist:
         p.mg_min_columns = int(self.mg_min_columns)
         p.autotune = int(bool(self.autotune))
         p.mg_operator_bf16 = int(bool(self.mg_operator_bf16))
-        p.mg_fused_coarse = int(bool(self.mg_fused_coarse))
+        p.mg_fused_coarse = -1 if self.mg_fused_coarse is None else int(bool(self.mg_fused_coarse))
         return p
 
 

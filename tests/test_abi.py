@@ -93,7 +93,7 @@ def test_params_default_mirror_poisson_namelist(pcf):
     assert p.tolerance == 1e-8 and p.poisson_iterations == 1000 and p.preconditioner == 1
     assert p.dtau == 1.0 and p.preconditioner_iterations == 2 and p.tolerance_is_relative == 0
     assert p.damp_horizontal_wind_on_rhs == 0 and p.precision == 0 and p.residual == 0 and p.learned == 0
-    assert p.multigrid == 0
+    assert p.multigrid == 0 and p.mg_fused_coarse == -1  # the fused coarse cycle: ensembles only
     nl = pcf.PoissonNamelist().to_c()
     for name, _ in pcf._lib.PcfParams._fields_:
         assert getattr(nl, name) == getattr(p, name), name

@@ -46,8 +46,11 @@ def _solve_ensemble(pcf, ens, members, nl):
                                     [d["dpip"].data_ptr() for _, _, d in members])
 
 
-def test_ensemble_matches_single_solves(pcf, members):
-    nl = pcf.PoissonNamelist(**NL)
+@pytest.mark.parametrize("fused", [None, False])
+def test_ensemble_matches_single_solves(pcf, members, fused):
+    """fused None: the default, the coarse levels as one cluster launch in the
+    ensemble; False: one kernel per step as in single solves."""
+    nl = pcf.PoissonNamelist(**NL, mg_fused_coarse=fused)
     with pcf.Ensemble([s for _, s, _ in members]) as ens:
         infos = _solve_ensemble(pcf, ens, members, nl)
         got = [d["dpip"].cpu().numpy().copy() for _, _, d in members]
@@ -65,8 +68,12 @@ def test_ensemble_matches_single_solves(pcf, members):
             continue
         assert info.true_residual <= 1e-10
         d["dpip"].zero_()
+        # the ensemble runs the coarse levels as one cluster launch by default
+        # (mg_fused_coarse = -1); the single solve is asked for the same
         single = s.solve_poisson_device(d["rhs"].data_ptr(), d["rho"].data_ptr(), d["betar"].data_ptr(), cfg["dt"],
-                                        cfg["rayleigh_factor"], cfg["tolref"], nl, d["dpip"].data_ptr())
+                                        cfg["rayleigh_factor"], cfg["tolref"],
+                                        pcf.PoissonNamelist(**NL, mg_fused_coarse=fused is None),
+                                        d["dpip"].data_ptr())
         ref = d["dpip"].cpu().numpy()
         assert single.niter == info.niter, (q, single.niter, info.niter)
         assert rel_err(got[q], ref) <= 1e-12, (q, rel_err(got[q], ref))
