@@ -151,6 +151,12 @@ typedef struct {
                                       step as on the finer levels; -1 (default): on in pcf_ensemble_solve_device
                                       (whose members' launches then leave the other SMs to one another), off in
                                       single solves (measured slower there) */
+    int mg_smoother_fp8;           /* multigrid with mg_operator_bf16: the finest level's pseudo-time steps read
+                                      an FP8 E4M3 copy of their 22 planes (each plane scaled by a power of 2 so
+                                      that its largest value lands in [64, 128)), a quarter of the FP32 planes'
+                                      bytes; the residual keeps the BF16 copy.  Off by default (0): measured
+                                      slower at 512 x 512 x 192, where widening FP8 to FP32 runs on the
+                                      conversion pipe and takes about as long as the launch itself */
 } pcf_params;
 
 typedef struct {

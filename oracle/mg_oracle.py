@@ -54,6 +54,31 @@ def bf16(a):
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+def e4m3(a):
+    """Rounding to FP8 E4M3 (to nearest, ties to even; saturating at 448;
+    subnormal step 2^-9), as cvt.rn.satfinite.e4m3x2.f32 does; float64 out."""
+    a = np.asarray(a, dtype=np.float64)
+    m = np.minimum(np.abs(a), 448.0)
+    _, e = np.frexp(m)                      # m = f 2^e, f in [0.5, 1)
+    e = np.maximum(e - 1, -6)               # the binade's exponent; subnormals share 2^-6's step
+    q = np.ldexp(1.0, e - 3)                # 3 mantissa bits
+    return np.sign(a) * np.minimum(np.round(m / q) * q, 448.0)
+
+
+def fp8_planes(planes):
+    """The GPU's FP8 copy of BF16-rounded planes, widened back: plane p as
+    E4M3(c scale_p) / scale_p with scale_p = 2^(7 - e_p), max |c| = f 2^e_p."""
+    out = np.zeros_like(planes)
+    for p in range(planes.shape[0]):
+        mx = np.abs(planes[p]).max()
+        if mx == 0:
+            continue
+        _, e = np.frexp(np.float32(mx))
+        sc = np.ldexp(1.0, 7 - int(e))
+        out[p] = e4m3(planes[p] * sc) / sc
+    return out
+
+
 def factors(coef, deta):
     """Thomas pivots P, M, Q (k_factors)."""
     ac, ad, au = coef[AC], coef[AD], coef[AU]
@@ -136,10 +161,13 @@ def coarsen(coef, fc, cx, cy):
 class Multigrid:
     """The hierarchy and V-cycle of the GPU preconditioner (mg_prepare, mg_precond, mg_cycle)."""
 
-    def __init__(self, coef, fcscal, dx, dy, dtau=1.0, coarse_iterations=4, min_columns=16, bf16_planes=False):
+    def __init__(self, coef, fcscal, dx, dy, dtau=1.0, coarse_iterations=4, min_columns=16, bf16_planes=False,
+                 fp8_smoother=False):
         """bf16_planes: the residual and pseudo-step stencils of level 0, and
         of level 1 unless it is the coarsest, read BF16-rounded planes (the
-        GPU's mg_operator_bf16); the Thomas pivots keep the unrounded operator."""
+        GPU's mg_operator_bf16); the Thomas pivots keep the unrounded operator.
+        fp8_smoother (with bf16_planes): level 0's pseudo-time steps read the
+        FP8 copy of those planes (the GPU's mg_smoother_fp8)."""
         nz, ny, nx = fcscal.shape
         self.dims = level_dims(nx, ny, nz, min_columns)
         self.ci = coarse_iterations
@@ -155,12 +183,13 @@ class Multigrid:
         for l, L in enumerate(self.levels):
             rounded = bf16_planes and (l == 0 or (l == 1 and l < len(self.levels) - 1))
             L["scoef"] = bf16(L["coef"]) if rounded else L["coef"]
+            L["pcoef"] = fp8_planes(L["scoef"]) if (fp8_smoother and bf16_planes and l == 0) else L["scoef"]
 
     def smooth(self, l, b, steps):
         L = self.levels[l]
-        s = pseudo_step(L["scoef"], L["fac"], L["deta"], b, None)
+        s = pseudo_step(L["pcoef"], L["fac"], L["deta"], b, None)
         for _ in range(steps - 1):
-            s = pseudo_step(L["scoef"], L["fac"], L["deta"], b, s)
+            s = pseudo_step(L["pcoef"], L["fac"], L["deta"], b, s)
         return s
 
     def cycle(self, b, l=0):
@@ -175,7 +204,7 @@ class Multigrid:
         bc = (L["fc"] * r).reshape(nz, ny // cy, cy, nx // cx, cx).sum(axis=(2, 4)) / (cx * cy * C["fc"])
         e = self.cycle(bc, l + 1)
         s = s + np.repeat(np.repeat(C["fc"] * e, cy, axis=1), cx, axis=2) / L["fc"]
-        return pseudo_step(L["scoef"], L["fac"], L["deta"], b, s)
+        return pseudo_step(L["pcoef"], L["fac"], L["deta"], b, s)
 
 
 def bicgstab(coef, M, b, tol=1e-10, maxit=1000):

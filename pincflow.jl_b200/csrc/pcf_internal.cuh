@@ -14,6 +14,7 @@
 #pragma once
 
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
@@ -213,6 +214,13 @@ struct pcf_handle {
     double *corr;        // corx, cory of the corrector (2 haloed arrays, on first use)
     double *istage;      // staging of pcf_implicit_step: 12 haloed arrays + 1 interior (on first use)
     __nv_bfloat16 *coef16;  // BF16 copy of the 25 planes for the V-cycle's finest level (on first use)
+    // FP8 E4M3 copy of those planes for the finest level's pseudo-time steps
+    // (on first use), the planes' scales and inverse scales (25 + 25 floats),
+    // their maxima (25 words), and the operator version it was made from
+    uint8_t *coef8;
+    float *scale8;
+    unsigned *amax8;
+    long long coef8_version;
     float *rfc32;        // 1 / fcscal on the interior
     double fac_deta;  // d_eta the factors were built with (NaN: none)
     // FP64 Krylov vectors

@@ -65,6 +65,20 @@ __device__ __forceinline__ void unpack_bf16x4(uint2 x, float (&v)[4]) {
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
+// two and four FP8 E4M3 values widened to FP32 (exact, through FP16)
+__device__ __forceinline__ float2 fp8x2_to_float2(unsigned short x) {
+    const __half2_raw h = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)x, __NV_E4M3);
+    return __half22float2(*reinterpret_cast<const __half2 *>(&h));
+}
+__device__ __forceinline__ void unpack_fp8x2(unsigned short x, float scale, float (&v)[2]) {
+    const float2 a = fp8x2_to_float2(x);
+    v[0] = a.x * scale; v[1] = a.y * scale;
+}
+__device__ __forceinline__ void unpack_fp8x4(unsigned x, float scale, float (&v)[4]) {
+    const float2 a = fp8x2_to_float2((unsigned short)(x & 0xffffu)), b = fp8x2_to_float2((unsigned short)(x >> 16));
+    v[0] = a.x * scale; v[1] = a.y * scale; v[2] = b.x * scale; v[3] = b.y * scale;
+}
+
 // V consecutive BF16 values (2V bytes, 2V-byte aligned) widened to FP32
 template <int V>
 __device__ __forceinline__ void load_bf16(const __nv_bfloat16 *__restrict__ p, float (&v)[V]) {
@@ -348,6 +362,9 @@ struct StencilArgs {
     const T *coef;        // 25 planes
     const __nv_bfloat16 *coef16 = nullptr;  // the same planes in BF16, read by the C16 kernels
     const void *tmap16 = nullptr;           // device array of the three tensor maps of coef16 (make_coef16_maps)
+    // C16 = 3: the pseudo-step's planes in FP8 E4M3, plane p scaled by 1 / inv8[p] (a power of 2)
+    const void *tmap8 = nullptr;            // device array of the tensor maps of that copy (make_coef8_maps)
+    const float *inv8 = nullptr;            // device array of the 25 inverse scales
     const T *s;           // input vector
     T *out;
     const T *w1;          // EPI_DOT1/2: second operand; EPI_PSEUDO/RESID: b
@@ -446,11 +463,14 @@ __device__ __forceinline__ void ring_store(T *slot, const T (&rv)[Ring<T, V, TX,
 // (128-wide tiles) or 2 (64-wide), the tensor maps a.tmap16
 // (make_coef16_maps: three of box width 128, then three of box width 64)
 // and stencil_bulk_smem bytes of dynamic shared memory.  A wait that gives
-// up (2 s) marks the iteration failed (guard status PCF_ECUDA).
+// up (2 s) marks the iteration failed (guard status PCF_ECUDA).  C16 = 3 is
+// the same staging of the pseudo-step's 22 planes from an FP8 E4M3 copy
+// (a.tmap8, make_coef8_maps), each plane widened and multiplied by its
+// power-of-2 inverse scale a.inv8[p]: a quarter of the FP32 planes' bytes.
 constexpr int kStencilStages = 2;  // 3 measured slower: 2 instead of 3 resident blocks per SM
-template <int V, int TX, int TY, bool HORIZ>
+template <int V, int TX, int TY, bool HORIZ, int EB = 2>
 constexpr int stencil_stage_bytes() {
-    return (HORIZ ? PCF_NCOEF - 3 : PCF_NCOEF) * TY * TX * V * 2;
+    return (HORIZ ? PCF_NCOEF - 3 : PCF_NCOEF) * TY * TX * V * EB;
 }
 
 // stage slot of plane p: the Horizontal operator skips AC, AD and AU
@@ -462,18 +482,21 @@ __host__ __device__ constexpr int slot_of_plane(int p) {
 template <typename T, int V, int TX, int TY, bool HORIZ, int EPI, bool DIFF = false, int C16 = 0>
 __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
     static_assert(C16 == 0 || sizeof(T) == 4, "BF16 planes feed the FP32 stencil only");
-    static_assert(C16 != 2 || ((V == 4 || V == 2) && TX == 32 && TY == 4), "the tensor maps' boxes are 32 V x 4");
+    static_assert(C16 < 2 || ((V == 4 || V == 2) && TX == 32 && TY == 4), "the tensor maps' boxes are 32 V x 4");
+    static_assert(C16 != 3 || (HORIZ && EPI == EPI_PSEUDO && !DIFF), "the FP8 copy feeds the pseudo-time step only");
     static_assert(PCF_AC == 0 && PCF_AL == 1 && PCF_AD == 5 && PCF_AU == 6 && PCF_ALD == 7, "plane order");
     using R = Ring<T, V, TX, TY>;
     __shared__ __align__(16) T sm[R::NS][R::NR * R::RW];
     if (a.guard_update ? no_update_pending(a.guard) : krylov_done(a.guard)) return;
-    // C16 == 2: kStencilStages coefficient stages, then one mbarrier per stage
+    // C16 >= 2: kStencilStages coefficient stages, then one mbarrier per stage
     constexpr int NST = kStencilStages;
     constexpr int NPL = HORIZ ? PCF_NCOEF - 3 : PCF_NCOEF;
-    constexpr int STAGE = NPL * TY * R::W;  // BF16 values per stage
+    constexpr int STAGE = NPL * TY * R::W;  // values per stage
+    constexpr int EB = C16 == 3 ? 1 : 2;    // bytes per value: FP8 or BF16
     extern __shared__ __align__(128) unsigned char stencil_dyn[];
-    __nv_bfloat16 *stg = reinterpret_cast<__nv_bfloat16 *>(stencil_dyn);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(stencil_dyn + NST * STAGE * sizeof(__nv_bfloat16));
+    unsigned char *stg = stencil_dyn;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(stencil_dyn + NST * STAGE * EB);
+    __shared__ float sinv[C16 == 3 ? PCF_NCOEF : 1];  // C16 == 3: the planes' inverse scales
 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int x0 = blockIdx.x * R::W, y0 = blockIdx.y * TY;
@@ -488,28 +511,37 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
     T rv[R::ROWS_PER_THREAD][V];
     T hv;
     const int lt = tx + TX * ty;
-    // C16 == 2: thread 0 loads level kk's tile of every plane into stage st
-    const char *maps = C16 == 2 ? static_cast<const char *>(a.tmap16) + (V == 2 ? 3 * 128 : 0) : nullptr;
+    // C16 >= 2: thread 0 loads level kk's tile of every plane into stage st.
+    // BF16 maps: [0] all planes, [1] AL..AF, [2] ALD..AFUU (box width 128,
+    // then the same at 64); FP8 maps: [0] AL..AF, [1] ALD..AFUU (128, then 64)
+    const char *maps = C16 == 2   ? static_cast<const char *>(a.tmap16) + (V == 2 ? 3 * 128 : 0)
+                       : C16 == 3 ? static_cast<const char *>(a.tmap8) + (V == 2 ? 2 * 128 : 0)
+                                  : nullptr;
+    const char *maps_h = C16 == 3 ? maps : C16 == 2 ? maps + 128 : nullptr;  // the Horizontal pair
     auto issue = [&](int kk, int st) {
         if (kk == a.stall_level) return;  // test hook: no copy in flight, the wait for it runs out
-        const uint32_t bar = smem_u32(bars + st), dst = smem_u32(stg + st * STAGE);
-        mbar_arrive_expect(bar, (uint32_t)(STAGE * sizeof(__nv_bfloat16)));  // whole boxes, zero-filled outside
+        const uint32_t bar = smem_u32(bars + st), dst = smem_u32(stg + st * STAGE * EB);
+        mbar_arrive_expect(bar, (uint32_t)(STAGE * EB));  // whole boxes, zero-filled outside
         if (HORIZ) {
-            tma_load_4d(dst, maps + 128, x0, y0, kk, PCF_AL, bar);
-            tma_load_4d(dst + 4 * TY * R::W * 2, maps + 256, x0, y0, kk, PCF_ALD, bar);
+            tma_load_4d(dst, maps_h, x0, y0, kk, PCF_AL, bar);
+            tma_load_4d(dst + 4 * TY * R::W * EB, maps_h + 128, x0, y0, kk, PCF_ALD, bar);
         } else {
             tma_load_4d(dst, maps, x0, y0, kk, 0, bar);
         }
     };
-    if constexpr (C16 == 2) {
+    if constexpr (C16 == 3) {
+        if (lt < PCF_NCOEF) sinv[lt] = a.inv8[lt];  // visible after the prologue's barrier
+    }
+    if constexpr (C16 >= 2) {
         if (lt == 0) {
 #pragma unroll
             for (int q = 0; q < NST; ++q)
                 asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bars + q)));
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
             // the maps were written to global memory before the launch
-            for (int q = HORIZ ? 1 : 0; q < (HORIZ ? 3 : 1); ++q)
-                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(maps + 128 * q) : "memory");
+            for (int q = 0; q < (HORIZ ? 2 : 1); ++q)
+                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"((HORIZ ? maps_h : maps) + 128 * q)
+                             : "memory");
             for (int q = 0; q < NST - 1 && k0 + q < k1; ++q) issue(k0 + q, q);
         }
         __syncthreads();
@@ -523,10 +555,10 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
         ring_store<T, V, TX, TY>(sm[(kk + 12) % R::NS], rv, hv);
     }
     __syncthreads();
-    // C16 == 2: the ring's next plane and the level's b are loaded one level
+    // C16 >= 2: the ring's next plane and the level's b are loaded one level
     // earlier than in the other variants (registers rv / wn hold them across
     // the barrier), so that their DRAM latency overlaps a whole level
-    constexpr bool AHEAD = C16 == 2;
+    constexpr bool AHEAD = C16 >= 2;
     T rv2[R::ROWS_PER_THREAD][V];
     T hv2;
     T wn[V];
@@ -538,7 +570,7 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
     const int r = ty + 1;
     for (int k = k0; k < k1; ++k) {
         const int j = k - k0;
-        if constexpr (C16 == 2) {
+        if constexpr (C16 >= 2) {
             // stage (j + NST - 1) % NST held level k - 1, which every thread finished before the barrier below
             if (lt == 0 && k + NST - 1 < k1) issue(k + NST - 1, (j + NST - 1) % NST);
         }
@@ -554,17 +586,24 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
         if (active && PCF_IN(base, n - (V - 1), 103) &&
             (!AHEAD || k + 1 >= k1 || PCF_IN(base + plane, n - (V - 1), 104))) {
             T c[PCF_NCOEF][V];
-            if constexpr (C16 == 2) {
+            if constexpr (C16 >= 2) {
                 failed = !mbar_wait(smem_u32(bars + j % NST), (uint32_t)((j / NST) & 1), a.wait_ns);
-                const __nv_bfloat16 *cs = stg + (j % NST) * STAGE + ty * R::W + tx * V;
+                const unsigned char *cs = stg + ((j % NST) * STAGE + ty * R::W + tx * V) * EB;
 #pragma unroll
                 for (int p = 0; p < PCF_NCOEF; ++p) {
                     if (HORIZ && (p == PCF_AC || p == PCF_AD || p == PCF_AU)) continue;
-                    const __nv_bfloat16 *cp = cs + slot_of_plane<HORIZ>(p) * TY * R::W;
-                    if constexpr (V == 4)
+                    const unsigned char *cp = cs + slot_of_plane<HORIZ>(p) * TY * R::W * EB;
+                    if constexpr (C16 == 3) {
+                        if constexpr (V == 4)
+                            unpack_fp8x4(failed ? 0u : *reinterpret_cast<const unsigned *>(cp), sinv[p], c[p]);
+                        else
+                            unpack_fp8x2(failed ? (unsigned short)0 : *reinterpret_cast<const unsigned short *>(cp),
+                                         sinv[p], c[p]);
+                    } else if constexpr (V == 4) {
                         unpack_bf16x4(failed ? make_uint2(0u, 0u) : *reinterpret_cast<const uint2 *>(cp), c[p]);
-                    else if constexpr (V == 2)
+                    } else if constexpr (V == 2) {
                         unpack_bf16x2(failed ? 0u : *reinterpret_cast<const unsigned *>(cp), c[p]);
+                    }
                 }
             } else {
 #pragma unroll
@@ -694,7 +733,7 @@ __global__ void __launch_bounds__(TX *TY) k_stencil(StencilArgs<T> a, int kc) {
                 for (int e = 0; e < V; ++e) rv[q][e] = rv2[q][e];
             hv = hv2;
         }
-        if constexpr (C16 == 2) {
+        if constexpr (C16 >= 2) {
             if (__syncthreads_or(failed)) {
                 // a stage never completed: record it, let the copies still in
                 // flight land (bounded), and leave

@@ -152,10 +152,11 @@ static int pick_kc(long long xyblocks, int nz) {
     return (int)kc;
 }
 
-// dynamic shared memory of the staged BF16 stencil: the stages, one mbarrier each
-template <int V, int TX, int TY, bool HORIZ>
+// dynamic shared memory of the staged stencil (C16 = 2: BF16 planes, 3:
+// FP8): the stages, one mbarrier each
+template <int V, int TX, int TY, bool HORIZ, int C16 = 2>
 constexpr int stencil_bulk_smem() {
-    return kStencilStages * (stencil_stage_bytes<V, TX, TY, HORIZ>() + (int)sizeof(uint64_t));
+    return kStencilStages * (stencil_stage_bytes<V, TX, TY, HORIZ, C16 == 3 ? 1 : 2>() + (int)sizeof(uint64_t));
 }
 
 // The tensor maps of a BF16 operator copy (25 planes of nx x ny x nz values)
@@ -195,10 +196,45 @@ static bool make_coef16_maps(const __nv_bfloat16 *coef16, const Dims &d, void *m
     return cudaMemcpy(maps, host, sizeof(host), cudaMemcpyHostToDevice) == cudaSuccess;
 }
 
+// The tensor maps of an FP8 operator copy (25 planes of nx x ny x nz bytes)
+// for the staged pseudo-time step, written to the device array maps (4 x 128
+// bytes): boxes of 128 x 4 x 1 values of [0] the 4 planes AL..AF and [1] the
+// 18 planes ALD..AFUU, then [2..3] the same with 64-wide boxes.  False when
+// the grid breaks the alignment rules (rows of a multiple of 16 bytes, at
+// least one 128-wide box wide) or no encoder is available.
+static bool make_coef8_maps(const uint8_t *coef8, const Dims &d, void *maps) {
+    using Encode = decltype(&cuTensorMapEncodeTiled);
+    static Encode encode = [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            fn = nullptr;
+        }
+        return reinterpret_cast<Encode>(fn);
+    }();
+    if (!encode || !coef8 || d.nx % 16 != 0 || d.nx < 128 || (reinterpret_cast<uintptr_t>(coef8) & 15) != 0)
+        return false;
+    CUtensorMap host[4];
+    const cuuint64_t dims[4] = {(cuuint64_t)d.nx, (cuuint64_t)d.ny, (cuuint64_t)d.nz, (cuuint64_t)PCF_NCOEF};
+    const cuuint64_t strides[3] = {(cuuint64_t)d.nx, (cuuint64_t)d.plane, (cuuint64_t)d.n};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const cuuint32_t planes[2] = {PCF_AD - PCF_AL, PCF_NCOEF - PCF_ALD};
+    for (int q = 0; q < 4; ++q) {
+        const cuuint32_t box[4] = {q < 2 ? 128u : 64u, 4, 1, planes[q % 2]};
+        if (encode(&host[q], CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<uint8_t *>(coef8), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    return cudaMemcpy(maps, host, sizeof(host), cudaMemcpyHostToDevice) == cudaSuccess;
+}
+
 // Raises the staged stencil's dynamic shared-memory limit on the current
 // device (once per device) and returns how many of its blocks the device
 // holds at once (resident blocks per SM x SMs); 0 if the device refuses.
-template <typename T, int V, int TX, int TY, bool HORIZ, int EPI, bool DIFF>
+template <typename T, int V, int TX, int TY, bool HORIZ, int EPI, bool DIFF, int C16 = 2>
 static int stencil_bulk_ready() {
     static std::atomic<int> state[64];  // per device: 0 unknown, -1 refused, else the capacity
     int dev = 0;
@@ -208,12 +244,11 @@ static int stencil_bulk_ready() {
     }
     int st = state[dev].load();
     if (st == 0) {
-        auto kern = k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF, 2>;
+        auto kern = k_stencil<T, V, TX, TY, HORIZ, EPI, DIFF, C16>;
+        constexpr int smem = stencil_bulk_smem<V, TX, TY, HORIZ, C16>();
         int per_sm = 0;
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 stencil_bulk_smem<V, TX, TY, HORIZ>()) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TX * TY, stencil_bulk_smem<V, TX, TY, HORIZ>()) ==
-                cudaSuccess &&
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TX * TY, smem) == cudaSuccess &&
             per_sm > 0) {
             st = per_sm * num_sms();
         } else {
@@ -225,15 +260,16 @@ static int stencil_bulk_ready() {
     return st > 0 ? st : 0;
 }
 
-// Launches the TMA-staged BF16 stencil with SV x values per thread (tiles of
-// 32 SV x 4 cells) on the handle's stream; false (nothing launched) if the
-// device refuses its shared memory or the grid exceeds the partials buffer.
-template <typename T, int SV, bool HORIZ, int EPI, bool DIFF>
+// Launches the TMA-staged stencil (C16 = 2: BF16 planes, 3: FP8) with SV x
+// values per thread (tiles of 32 SV x 4 cells) on the handle's stream; false
+// (nothing launched) if the device refuses its shared memory or the grid
+// exceeds the partials buffer.
+template <typename T, int SV, bool HORIZ, int EPI, bool DIFF, int C16 = 2>
 static bool launch_staged(pcf_handle *h, const StencilArgs<T> &a0) {
     StencilArgs<T> a = a0;
     if (h->test_stall) a.stall_level = h->test_stall - 1;
     if (h->test_wait_ns) a.wait_ns = h->test_wait_ns;
-    const int cap = stencil_bulk_ready<T, SV, 32, 4, HORIZ, EPI, DIFF>();
+    const int cap = stencil_bulk_ready<T, SV, 32, 4, HORIZ, EPI, DIFF, C16>();
     if (cap <= 0) return false;
     constexpr int W = 32 * SV;
     const long long gx = (a.nx + W - 1) / W, gy = (a.ny + 3) / 4, xy = gx * gy;
@@ -254,8 +290,8 @@ static bool launch_staged(pcf_handle *h, const StencilArgs<T> &a0) {
     }
     const long long gz = (a.nz + kc - 1) / kc;
     if (xy * gz > kMaxPartials) return false;
-    k_stencil<T, SV, 32, 4, HORIZ, EPI, DIFF, 2><<<dim3((unsigned)gx, (unsigned)gy, (unsigned)gz), dim3(32, 4, 1),
-                                                     stencil_bulk_smem<SV, 32, 4, HORIZ>(), h->stream>>>(a, kc);
+    k_stencil<T, SV, 32, 4, HORIZ, EPI, DIFF, C16><<<dim3((unsigned)gx, (unsigned)gy, (unsigned)gz), dim3(32, 4, 1),
+                                                       stencil_bulk_smem<SV, 32, 4, HORIZ, C16>(), h->stream>>>(a, kc);
     return true;
 }
 
@@ -279,6 +315,18 @@ static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_ov
                                      : (sizeof(T) == 4 ? PCF_PROF_APPLY32 : PCF_PROF_APPLY64);
     // the preconditioner's stencils may read BF16 planes (a.coef16)
     constexpr bool c16_ok = sizeof(T) == 4 && !DIFF && (EPI == EPI_PSEUDO || EPI == EPI_RESNR);
+    if constexpr (c16_ok && HORIZ && EPI == EPI_PSEUDO && V == 4 && TX == 32) {
+        // the finest level's pseudo-time step on the FP8 copy of its planes
+        if (a.tmap8 && a.inv8) {
+            ProfScope ps(h, tag_override >= 0 ? tag_override : PCF_PROF_MG_BF16,
+                         ((double)planes + (double)(words - planes) * sizeof(T)) * (double)a.n);
+            const bool narrow = a.n >= 10000000 || a.nx >= 512;
+            if (narrow ? launch_staged<T, 2, HORIZ, EPI, DIFF, 3>(h, a) : launch_staged<T, 4, HORIZ, EPI, DIFF, 3>(h, a)) {
+                PCF_CUDA_TRY(cudaGetLastError());
+                return PCF_OK;
+            }
+        }
+    }
     if constexpr (c16_ok) {
         if (a.coef16) {
             ProfScope ps(h, tag_override >= 0 ? tag_override : PCF_PROF_MG_BF16,
@@ -657,6 +705,7 @@ struct MgLevel {
     float *coef = nullptr, *fac = nullptr, *fc = nullptr, *b = nullptr, *s = nullptr, *t = nullptr;
     __nv_bfloat16 *coef16 = nullptr;  // level 1: BF16 copy of coef (multigrid BF16 mode)
     void *tmap16 = nullptr;           // levels 0 and 1: tensor maps of the BF16 copy (make_coef16_maps), or null
+    void *tmap8 = nullptr;            // level 0: tensor maps of the FP8 copy (make_coef8_maps) while it is used
 };
 struct MgState {
     std::vector<MgLevel> lv;  // lv[0] is the handle's grid (its planes are the handle's)
@@ -666,11 +715,63 @@ struct MgState {
     long long version = -1;  // operator version the coarse operators were built from
     double dtau = 0;
     bool bf16 = false;       // the finest level's stencils read h->coef16
+    void *maps8 = nullptr;   // the FP8 copy's tensor maps (made once)
     int fused_from = -1;     // first level of the one-launch coarse cycle (k_mg_coarse), -1: none
     int coarse_cluster = 0;  // its cluster's CTAs (16, or 8 where 16 is refused)
 };
 
 __global__ void k_to_float(const double *__restrict__ a, float *__restrict__ b, long long n, double scale);
+
+// ---- the FP8 copy of the finest level's planes (the pseudo-time step's) ----
+// Plane p is stored as E4M3(c16 * scale_p) with scale_p = 2^(7 - e_p), where
+// max |c16| over the plane is f 2^e_p (f in [0.5, 1)): the plane's largest
+// value lands in [64, 128), below E4M3's 448, and values under 2^-16 of it
+// flush to zero.  Scales are powers of 2, so scaling and unscaling are exact.
+
+// max |value| of each of the 25 BF16 planes (blockIdx.y) as the bits of a
+// non-negative float, atomically combined into amax (zero beforehand)
+__global__ void __launch_bounds__(256) k_plane_absmax(const __nv_bfloat16 *__restrict__ c, long long n,
+                                                      unsigned *amax) {
+    const __nv_bfloat16 *pl = c + (long long)blockIdx.y * n;
+    float m = 0.f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(__bfloat162float(pl[i])));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+    __shared__ float wmax[8];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, wmax[w]);
+        atomicMax(amax + blockIdx.y, __float_as_uint(m));
+    }
+}
+
+// scale[p] and 1 / scale[p] (at scale + 25) from the planes' maxima
+__global__ void k_fp8_scales(const unsigned *amax, float *scale) {
+    const int p = threadIdx.x;
+    if (p >= PCF_NCOEF) return;
+    const float m = __uint_as_float(amax[p]);
+    int e = 0;
+    if (m > 0.f) frexpf(m, &e);
+    scale[p] = m > 0.f ? ldexpf(1.f, 7 - e) : 1.f;
+    scale[PCF_NCOEF + p] = m > 0.f ? ldexpf(1.f, e - 7) : 1.f;
+}
+
+// c8 = E4M3(c16 * scale) (round to nearest even, saturating), two values per thread
+__global__ void __launch_bounds__(256) k_to_fp8(const __nv_bfloat16 *__restrict__ c, long long n,
+                                                const float *__restrict__ scale, uint8_t *__restrict__ c8) {
+    const float sc = scale[blockIdx.y];
+    const __nv_bfloat162 *src = reinterpret_cast<const __nv_bfloat162 *>(c + (long long)blockIdx.y * n);
+    __nv_fp8x2_storage_t *dst = reinterpret_cast<__nv_fp8x2_storage_t *>(c8 + (long long)blockIdx.y * n);
+    const long long n2 = n / 2;  // n is even (nx % 16 == 0)
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n2; i += (long long)gridDim.x * blockDim.x) {
+        float2 v = __bfloat1622float2(src[i]);
+        v.x *= sc;
+        v.y *= sc;
+        dst[i] = __nv_cvt_float2_to_fp8x2(v, __NV_SATFINITE, __NV_E4M3);
+    }
+}
 
 __global__ void k_float_to_bf16(const float *__restrict__ a, __nv_bfloat16 *__restrict__ b, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -780,6 +881,8 @@ static int mg_pseudo_step(pcf_handle *h, const MgLevel &L, const float *coef, co
     sa.coef = coef;
     sa.coef16 = coef16;
     sa.tmap16 = coef16 ? L.tmap16 : nullptr;
+    sa.tmap8 = coef16 ? L.tmap8 : nullptr;  // the finest level: its FP8 copy when in use
+    sa.inv8 = sa.tmap8 ? h->scale8 + PCF_NCOEF : nullptr;
     sa.s = s;
     sa.out = out;
     sa.w1 = b;
@@ -931,6 +1034,7 @@ static void mg_free(pcf_handle *h) {
     for (void *q : h->mg->allocs) cudaFree(q);
     h->mg->allocs.clear();
     h->mg->lv.clear();
+    h->mg->maps8 = nullptr;
 }
 
 static void clear_graphs(pcf_handle *h);
@@ -1049,6 +1153,44 @@ static int mg_prepare(pcf_handle *h, const pcf_params *prm, bool ensemble = fals
         if (e != cudaSuccess) return pcf_set_cuda_error(e);
         m.allocs.push_back(maps);
         if (make_coef16_maps(h->coef16, h->d, maps)) m.lv[0].tmap16 = maps;
+    }
+    // the finest level's pseudo-time steps on an FP8 copy of its planes
+    // (mg_smoother_fp8), made from the BF16 copy once per operator
+    const bool fp8 = m.bf16 && prm->mg_smoother_fp8 && m.lv[0].tmap16 && h->d.nx % 16 == 0;
+    if (fp8 && !h->coef8) {
+        const size_t bytes = (size_t)h->d.n * PCF_NCOEF;
+        cudaError_t e = cudaMalloc((void **)&h->coef8, bytes);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&h->scale8, 2 * PCF_NCOEF * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc((void **)&h->amax8, PCF_NCOEF * sizeof(unsigned));
+        if (e != cudaSuccess) {
+            cudaFree(h->coef8);
+            cudaFree(h->scale8);
+            h->coef8 = nullptr;
+            h->scale8 = nullptr;
+            return pcf_set_cuda_error(e);
+        }
+        h->bytes += (long long)bytes + 3 * PCF_NCOEF * 4;
+        h->coef8_version = -1;
+    }
+    if (fp8 && !m.maps8) {  // once per hierarchy
+        void *maps = nullptr;
+        const cudaError_t e = cudaMalloc(&maps, 4 * 128);
+        if (e != cudaSuccess) return pcf_set_cuda_error(e);
+        m.allocs.push_back(maps);
+        if (make_coef8_maps(h->coef8, h->d, maps)) m.maps8 = maps;
+    }
+    m.lv[0].tmap8 = fp8 ? m.maps8 : nullptr;
+    if (m.lv[0].tmap8 && h->coef8_version != h->op_version) {
+        // BF16 planes read twice (maxima, conversion), FP8 planes written
+        ProfScope ps(h, PCF_PROF_ASSEMBLE, (2.0 * 2 + 1.0) * PCF_NCOEF * (double)h->d.n);
+        PCF_CUDA_TRY(cudaMemsetAsync(h->amax8, 0, PCF_NCOEF * sizeof(unsigned), h->stream));
+        const dim3 g((unsigned)std::max(1, num_sms() * 8 / PCF_NCOEF), PCF_NCOEF);
+        k_plane_absmax<<<g, 256, 0, h->stream>>>(h->coef16, h->d.n, h->amax8);
+        k_fp8_scales<<<1, 32, 0, h->stream>>>(h->amax8, h->scale8);
+        k_to_fp8<<<g, 256, 0, h->stream>>>(h->coef16, h->d.n, h->scale8, h->coef8);
+        h->launches += 3;
+        PCF_CUDA_TRY(cudaGetLastError());
+        h->coef8_version = h->op_version;
     }
     for (MgLevel &L : m.lv) L.deta = prm->mg_dtau / (2 * (1 / (L.dx * L.dx) + 1 / (L.dy * L.dy)));
     // the finest level's pivots are the handle's (shared with the reference preconditioner)
@@ -1429,7 +1571,7 @@ static int run_finish(pcf_handle *h, const Work<T> &w, const LoopCfg &c, bool pr
 static GraphKey graph_key(const pcf_handle *h, int tsize, const LoopCfg &c, bool pi, int check_interval) {
     return GraphKey{tsize, c.precond, c.pc_iters, c.flex, c.reliable, pi, check_interval, c.deta, c.mg,
                     c.mg && h->mg ? (int)h->mg->lv.size() : 0, c.mg && h->mg ? h->mg->coarse_iters : 0,
-                    c.mg && h->mg ? (int)h->mg->bf16 | (h->mg->fused_from + 1) << 1 : 0,
+                    c.mg && h->mg ? (int)h->mg->bf16 | (h->mg->lv[0].tmap8 ? 2 : 0) | (h->mg->fused_from + 1) << 2 : 0,
                     c.learned_pc ? (const void *)h->net : nullptr};
 }
 
@@ -1580,6 +1722,7 @@ int pcf_params_default(pcf_params *p) {
     p->autotune = 0;
     p->mg_operator_bf16 = 1;
     p->mg_fused_coarse = -1;
+    p->mg_smoother_fp8 = 0;
     return PCF_OK;
 }
 
@@ -1595,7 +1738,7 @@ int pcf_destroy(pcf_handle *h) {
     int dev = h->dims.device;
     cudaSetDevice(dev);
     void *ptrs[] = {h->jac, h->met13, h->met23, h->met33, h->pbar, h->rhobar, h->thetabar, h->n2, h->rho, h->betar,
-                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch, h->stage, h->corr, h->istage, h->coef16, h->lr32,
+                    h->p, h->coef64, h->coef32, h->fac64, h->fac32, h->coefB32, h->fc64, h->rfc32, h->fch, h->rfch, h->stage, h->corr, h->istage, h->coef16, h->coef8, h->scale8, h->amax8, h->lr32,
                     h->x64, h->r64, h->r064, h->p64, h->v64, h->s64,
                     h->t64, h->za64, h->zb64, h->b64, h->w64, h->x32, h->r32, h->r032, h->p32, h->v32, h->s32,
                     h->t32, h->za32, h->zb32, h->zc32, h->zd32, h->partials, h->ticket, h->scal64, h->scal32,
@@ -1649,9 +1792,12 @@ int pcf_create(pcf_handle **out, const pcf_dims *dims) {
     stencil_bulk_ready<float, 4, 32, 4, true, EPI_PSEUDO, false>();
     stencil_bulk_ready<float, 2, 32, 4, false, EPI_RESNR, false>();
     stencil_bulk_ready<float, 2, 32, 4, true, EPI_PSEUDO, false>();
+    stencil_bulk_ready<float, 4, 32, 4, true, EPI_PSEUDO, false, 3>();
+    stencil_bulk_ready<float, 2, 32, 4, true, EPI_PSEUDO, false, 3>();
 
     pcf_handle *h = new pcf_handle;
     std::memset(h, 0, sizeof(*h));
+    h->coef8_version = -1;
     h->dims = *dims;
     h->d.nx = dims->nx;
     h->d.ny = dims->ny;

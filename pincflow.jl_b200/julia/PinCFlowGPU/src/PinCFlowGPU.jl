@@ -50,6 +50,7 @@ mutable struct PcfParams
     autotune::Cint
     mg_operator_bf16::Cint
     mg_fused_coarse::Cint
+    mg_smoother_fp8::Cint
 end
 
 mutable struct PcfResult
@@ -117,7 +118,7 @@ and the GPU path's SETTINGS.
 """
 function params(; tolerance, poisson_iterations, preconditioner, dtau, preconditioner_iterations,
                 tolerance_is_relative, damp_horizontal_wind_on_rhs)
-    p = PcfParams(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
+    p = PcfParams(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
     ccall((:pcf_params_default, LIB), Cint, (Ref{PcfParams},), p)
     p.tolerance = tolerance
     p.poisson_iterations = poisson_iterations

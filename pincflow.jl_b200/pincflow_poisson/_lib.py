@@ -69,7 +69,7 @@ class PcfParams(ctypes.Structure):
                 ("multigrid", ctypes.c_int), ("mg_dtau", ctypes.c_double),
                 ("mg_coarse_iterations", ctypes.c_int), ("mg_min_columns", ctypes.c_int),
                 ("autotune", ctypes.c_int), ("mg_operator_bf16", ctypes.c_int),
-                ("mg_fused_coarse", ctypes.c_int)]
+                ("mg_fused_coarse", ctypes.c_int), ("mg_smoother_fp8", ctypes.c_int)]
 
 
 class PcfTuneEntry(ctypes.Structure):

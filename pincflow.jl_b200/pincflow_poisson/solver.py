@@ -57,6 +57,7 @@ class PoissonNamelist:
     mg_operator_bf16: bool = True     # multigrid: finest and first coarse level stencils read BF16 copies
     mg_fused_coarse: Optional[bool] = None  # multigrid: levels of <= 1024 columns as one cluster launch per cycle
     #                                         (None: in ensembles only)
+    mg_smoother_fp8: bool = False     # multigrid: finest level's pseudo-time steps read an FP8 copy of their planes
 
     def to_c(self) -> _lib.PcfParams:
         p = _lib.PcfParams()
@@ -82,6 +83,7 @@ class PoissonNamelist:
         p.autotune = int(bool(self.autotune))
         p.mg_operator_bf16 = int(bool(self.mg_operator_bf16))
         p.mg_fused_coarse = -1 if self.mg_fused_coarse is None else int(bool(self.mg_fused_coarse))
+        p.mg_smoother_fp8 = int(bool(self.mg_smoother_fp8))
         return p
 
 

@@ -54,7 +54,7 @@ int main(void) {
   printf("pcf_dims %zu\npcf_params %zu\npcf_result %zu\n", sizeof(pcf_dims), sizeof(pcf_params), sizeof(pcf_result));
   F(pcf_params, dtau) F(pcf_params, inner_tolerance) F(pcf_params, check_interval)
   F(pcf_params, mg_dtau) F(pcf_params, mg_min_columns) F(pcf_params, mg_operator_bf16)
-  F(pcf_params, mg_fused_coarse)
+  F(pcf_params, mg_fused_coarse) F(pcf_params, mg_smoother_fp8)
   F(pcf_result, residual) F(pcf_result, ms_total) F(pcf_dims, device)
   return 0;
 }
@@ -81,6 +81,7 @@ def test_struct_layouts_match_header(pcf):
     assert L.PcfParams.mg_min_columns.offset == c["pcf_params.mg_min_columns"]
     assert L.PcfParams.mg_operator_bf16.offset == c["pcf_params.mg_operator_bf16"]
     assert L.PcfParams.mg_fused_coarse.offset == c["pcf_params.mg_fused_coarse"]
+    assert L.PcfParams.mg_smoother_fp8.offset == c["pcf_params.mg_smoother_fp8"]
     assert L.PcfResult.residual.offset == c["pcf_result.residual"]
     assert L.PcfResult.ms_total.offset == c["pcf_result.ms_total"]
     assert L.PcfDims.device.offset == c["pcf_dims.device"]

@@ -54,7 +54,14 @@ def _oracle_mg(cfg, coef, **kw):
     f = cfg["fields"]
     return Multigrid(coef, F.fcscal(cfg["dom"], f), f["dx"], f["dy"], dtau=kw.get("mg_dtau", 2.0),
                      coarse_iterations=kw.get("mg_coarse_iterations", 4), min_columns=kw.get("mg_min_columns", 16),
-                     bf16_planes=kw.get("bf16_planes", False))
+                     bf16_planes=kw.get("bf16_planes", False), fp8_smoother=kw.get("fp8_smoother", False))
+
+
+def _fp8_active(cfg):
+    """mg_smoother_fp8 takes effect where the finest level's copies are staged
+    by TMA: rows of a multiple of 16 bytes in FP8, at least 128 wide."""
+    nx = cfg["dom"].nx
+    return nx % 16 == 0 and nx >= 128
 
 
 @pytest.mark.parametrize("name", MG_CASES)
@@ -83,10 +90,17 @@ def test_vcycle_matches_oracle(name, solvers, oracle, pcf):
     assert rel_err(got, want) < 1e-4, rel_err(got, want)
     # the BF16 operator copies (shared-memory staged stencils on wide grids)
     # against the oracle's V-cycle on the same BF16-rounded planes
-    got16 = s.apply_multigrid(b, pcf.PoissonNamelist(precision="mixed", **MG))
+    got16 = s.apply_multigrid(b, pcf.PoissonNamelist(precision="mixed", mg_smoother_fp8=False, **MG))
     want16 = _oracle_mg(cfg, coef, bf16_planes=True, **MG).cycle(b)
     assert rel_err(got16, want16) < 1e-4, rel_err(got16, want16)
     assert rel_err(got16, want) > 10 * rel_err(got16, want16), (rel_err(got16, want), rel_err(got16, want16))
+    # mg_smoother_fp8: the finest level's pseudo-time steps on the FP8 copy
+    # (where it is staged), against the oracle's V-cycle on the same FP8 planes
+    got8 = s.apply_multigrid(b, pcf.PoissonNamelist(precision="mixed", mg_smoother_fp8=True, **MG))
+    want8 = _oracle_mg(cfg, coef, bf16_planes=True, fp8_smoother=_fp8_active(cfg), **MG).cycle(b)
+    assert rel_err(got8, want8) < 1e-4, rel_err(got8, want8)
+    if _fp8_active(cfg):
+        assert rel_err(got8, want16) > 10 * rel_err(got8, want8), (rel_err(got8, want16), rel_err(got8, want8))
 
 
 @pytest.mark.parametrize("name", MG_CASES)
@@ -100,7 +114,7 @@ def test_fused_coarse_cycle_matches_oracle(name, solvers, oracle, pcf):
     b = np.random.default_rng(17).standard_normal(cfg["dom"].interior_shape)
     for bf16 in (False, True):
         got = s.apply_multigrid(b, pcf.PoissonNamelist(precision="mixed", mg_operator_bf16=bf16,
-                                                       mg_fused_coarse=True, **MG))
+                                                       mg_smoother_fp8=False, mg_fused_coarse=True, **MG))
         want = _oracle_mg(cfg, coef, bf16_planes=bf16, **MG).cycle(b)
         assert rel_err(got, want) < 1e-4, (bf16, rel_err(got, want))
     if name not in CASES:
@@ -151,6 +165,28 @@ def test_bf16_operator_copy_keeps_the_iteration_count(name, solvers, oracle, pcf
         _, i32 = s.apply_bicgstab(rhs, 1.0, pcf.PoissonNamelist(mg_operator_bf16=False, **kw))
         assert not i16.errflag and not i32.errflag and i16.true_residual <= 1e-10
         assert iterations_agree(i16.niter, i32.niter), (scale, i16.niter, i32.niter)
+
+
+def test_fp8_smoother_keeps_the_iteration_count(pcf):
+    """Stretched 128 x 96 x 48 mountain grid (the FP8 copy staged): the mixed
+    solve with the finest level's pseudo-time steps on the FP8 copy reaches
+    the FP64 true residual 1e-10 in the iterations of the BF16 copy (within
+    the rounding noise of BiCGSTAB counts), and the same solution within 1e-6
+    once the null-space component is removed."""
+    from pincflow_poisson import configs as C
+    cfg = C.c2(nx=128, ny=96, nz=48)
+    with pcf.PoissonSolver(cfg["dom"], cfg["model"]) as s:
+        s.set_grid(cfg["fields"])
+        s.set_background(cfg["fields"])
+        s.compute_operator(cfg["rho"], cfg["betar"], cfg["dt"], cfg["rayleigh_factor"], return_coef=False)
+        kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=4000, residual="true",
+                  precision="mixed", **dict(MG, mg_dtau=2.5))
+        x8, i8 = s.apply_bicgstab(cfg["rhs"], 1.0, pcf.PoissonNamelist(mg_smoother_fp8=True, **kw))
+        x16, i16 = s.apply_bicgstab(cfg["rhs"], 1.0, pcf.PoissonNamelist(**kw))
+    assert not i8.errflag and not i16.errflag and i8.true_residual <= 1e-10, (i8, i16)
+    assert iterations_agree(i8.niter, i16.niter), (i8.niter, i16.niter)
+    # the two solutions may differ by a multiple of the null vector fcscal
+    assert rel_err(_drop_null(cfg, x8), _drop_null(cfg, x16)) < 1e-6
 
 
 def test_multigrid_rejected_outside_the_mixed_solve(solvers, pcf):

@@ -118,3 +118,32 @@ def test_vcycle_bf16_planes_differ_only_by_rounding(mtn):
     assert m16.levels[-1]["scoef"] is m16.levels[-1]["coef"]
     rel = np.linalg.norm(e16 - e32) / np.linalg.norm(e32)
     assert 1e-6 < rel < 5e-2, rel
+
+
+def test_e4m3_rounding_known_values():
+    """The oracle's FP8 E4M3 rounding (the GPU's mg_smoother_fp8 copy) on the
+    format's known values: normals, the largest finite value (saturation),
+    subnormals (step 2^-9) and ties to even."""
+    from oracle.mg_oracle import e4m3
+    cases = [(1.0, 1.0), (-1.0, -1.0), (1.0625, 1.0), (1.1875, 1.25), (0.0625, 0.0625), (448.0, 448.0),
+             (1000.0, 448.0), (2.0 ** -9, 2.0 ** -9), (2.0 ** -10, 0.0), (3 * 2.0 ** -10, 2.0 ** -8),
+             (2.0 ** -6, 2.0 ** -6), (7 * 2.0 ** -9, 7 * 2.0 ** -9), (240.0, 240.0), (250.0, 256.0), (0.0, 0.0)]
+    got = e4m3(np.array([c[0] for c in cases]))
+    assert np.array_equal(got, np.array([c[1] for c in cases])), list(zip(cases, got))
+
+
+def test_fp8_planes_scale_each_plane_to_the_top_binades():
+    """Each plane's largest value lands in [64, 128) before rounding, so the
+    FP8 copy keeps 3 bits of every value within 2^-6 of the plane's maximum
+    and flushes values below 2^-16 of it."""
+    from oracle.mg_oracle import fp8_planes
+    rng = np.random.default_rng(3)
+    planes = rng.standard_normal((3, 4, 5, 6)) * np.array([1e-6, 1.0, 3e4])[:, None, None, None]
+    out = fp8_planes(planes)
+    for p in range(3):
+        big = np.abs(planes[p]) > np.abs(planes[p]).max() * 2.0 ** -6
+        assert np.all(np.abs(out[p][big] - planes[p][big]) <= 2.0 ** -4 * np.abs(planes[p][big]))
+    tiny = np.zeros((1, 2, 2, 2))
+    tiny[0, 0, 0, 0] = 1.0
+    tiny[0, 1, 1, 1] = 2.0 ** -18
+    assert fp8_planes(tiny)[0, 1, 1, 1] == 0.0
