@@ -2538,6 +2538,11 @@ static int tiny_solve(pcf_handle *h, double tol, const pcf_params *prm, const do
     return PCF_OK;
 }
 
+// Iterations the mixed solve gives the learned preconditioner stage to
+// converge; a stage that has not by then (the multigrid alone takes 11-16 on
+// the benchmark grids) is dropped like one that breaks down.
+constexpr int kStageIterations = 60;
+
 // Solves A x = b64 (device) according to prm; the solution ends in *xres
 // (a device FP64 buffer owned by the handle).
 static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, const double **xres, pcf_result *res) {
@@ -2638,19 +2643,23 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
         PCF_CUDA_TRY(cudaGetLastError());
         float *e = nullptr;
         RunOut ro;
-        rc = bicgstab_run<float>(h, w, w.s, tol, maxit - res->niter, cm, prm->check_interval, false, &e, &ro,
-                                 res->niter, 1.0, b_norm, prm->inner_tolerance, prm->restart_interval);
+        // with the learned stage the iteration gets kStageIterations to converge
+        const int cap = cm.learned_pc ? std::min(maxit - res->niter, kStageIterations) : maxit - res->niter;
+        rc = bicgstab_run<float>(h, w, w.s, tol, cap, cm, prm->check_interval, false, &e, &ro, res->niter, 1.0,
+                                 b_norm, prm->inner_tolerance, prm->restart_interval);
         if (rc) return rc;
         res->niter += ro.iters;
         res->nrefine += ro.nupdates;
         reliable_bytes(h, ro.nupdates);
         if (ro.nupdates > 0) rel = ro.res;
         if (ro.converged) break;
-        if (ro.status == PCF_EBREAKDOWN && restarts < prm->max_refinements && res->niter < maxit) {
+        const bool stalled = cm.learned_pc && ro.iters >= cap && res->niter < maxit;
+        if ((ro.status == PCF_EBREAKDOWN || stalled) && restarts < prm->max_refinements && res->niter < maxit) {
             if (cm.learned_pc) {
-                // the plain preconditioner is the fallback: a breakdown or divergence
-                // with the learned stage drops the stage for the rest of the solve and
-                // discards the FP32 correction since the last reliable update
+                // the plain preconditioner is the fallback: a breakdown, divergence or
+                // stall with the learned stage drops the stage for the rest of the solve
+                // and discards the FP32 correction since the last reliable update
+                // (the FP64 solution keeps every reliable update made with it)
                 cm.learned_pc = 0;
             } else {
                 // fold what the broken-down iteration accumulated

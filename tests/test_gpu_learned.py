@@ -224,3 +224,26 @@ def test_diverging_stage_falls_back_to_the_preconditioner(netmod):
         assert not on.errflag and on.true_residual <= 1e-10, on
         r = cfg["rhs"] - s.apply_operator(x)
         assert np.sqrt(np.mean(r ** 2)) / np.sqrt(np.mean(cfg["rhs"] ** 2)) <= 1.5e-10
+
+
+@pytest.mark.parametrize("scale", [0.25, 1.0])
+def test_unhelpful_stage_costs_a_bounded_number_of_iterations(netmod, scale):
+    """Whatever the stage network does -- diverge, stall or merely not help --
+    the mixed solve drops it after at most 60 iterations without convergence
+    and finishes with the multigrid alone: it reaches 1e-10 in at most the
+    multigrid's own count plus those 60 (and 8 of rounding slack)."""
+    learned, NO = netmod
+    import pincflow_poisson as pcf
+    from pincflow_poisson import configs as C
+    p = _random_params(NO, 12) * scale
+    cfg = C.c3(101, nx=32, ny=32, nz=64)
+    with learned.LearnedNet(max_columns=32 * 32) as net, _solver(pcf, cfg) as s:
+        net.set_params(p)
+        net.set_bias_free(True)
+        s.attach_network(net)
+        kw = dict(tolerance=1e-10, tolerance_is_relative=True, poisson_iterations=4000, precision="mixed",
+                  multigrid=True)
+        _, off = s.apply_bicgstab(cfg["rhs"], 1.0, pcf.PoissonNamelist(**kw))
+        _, on = s.apply_bicgstab(cfg["rhs"], 1.0, pcf.PoissonNamelist(learned=2, **kw))
+    assert not on.errflag and on.true_residual <= 1e-10, on
+    assert on.niter <= off.niter + 60 + 8, (on.niter, off.niter)
