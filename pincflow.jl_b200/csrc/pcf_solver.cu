@@ -320,7 +320,7 @@ static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_ov
         if (a.tmap8 && a.inv8) {
             ProfScope ps(h, tag_override >= 0 ? tag_override : PCF_PROF_MG_BF16,
                          ((double)planes + (double)(words - planes) * sizeof(T)) * (double)a.n);
-            const bool narrow = a.n >= 10000000 || a.nx >= 512;
+            const bool narrow = a.n >= 10000000 || a.nx >= 512 || (a.nx % 128 != 0 && a.nx % 64 == 0);
             if (narrow ? launch_staged<T, 2, HORIZ, EPI, DIFF, 3>(h, a) : launch_staged<T, 4, HORIZ, EPI, DIFF, 3>(h, a)) {
                 PCF_CUDA_TRY(cudaGetLastError());
                 return PCF_OK;
@@ -344,7 +344,9 @@ static int launch_stencil_cfg(pcf_handle *h, const StencilArgs<T> &a, int tag_ov
                 // (measured per launch: 512x512x192 0.512 vs 0.561 ms, and the
                 // 256x256x192 level below it faster too; 256x256x128 0.116 vs
                 // 0.113 ms)
-                const bool narrow = a.n >= 10000000 || a.nx >= 512;
+                // (and 64-wide where 128-wide tiles would leave a half-empty
+                // column of tiles, nx = 192 for instance)
+                const bool narrow = a.n >= 10000000 || a.nx >= 512 || (a.nx % 128 != 0 && a.nx % 64 == 0);
                 if (a.tmap16 && (narrow ? launch_staged<T, 2, HORIZ, EPI, DIFF>(h, a)
                                         : launch_staged<T, 4, HORIZ, EPI, DIFF>(h, a))) {
                     PCF_CUDA_TRY(cudaGetLastError());
