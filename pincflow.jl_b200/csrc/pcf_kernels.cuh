@@ -1034,6 +1034,21 @@ __global__ void __launch_bounds__(256) k_init(const T *__restrict__ b, T *x, T *
     reduce_finalize<1>(red, v);
 }
 
+// r = b and the sum of b^2: the residual b - A x of the zero initial guess
+// (apply_bicgstab!.jl:63-67 with x = 0), without applying the operator.
+__global__ void __launch_bounds__(256) k_copy_sumsq(const double *__restrict__ b, double *r, long long n,
+                                                    ReduceCtx red) {
+    double bb = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double v = b[i];
+        r[i] = v;
+        bb += v * v;
+    }
+    double v[1] = {bb};
+    reduce_finalize<1>(red, v);
+}
+
 // Generic sum of a*b (compute_global_dot_product).
 template <typename T>
 __global__ void __launch_bounds__(256) k_dot(const T *__restrict__ a, const T *__restrict__ b, long long n,

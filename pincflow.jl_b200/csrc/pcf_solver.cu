@@ -2478,6 +2478,20 @@ static int true_residual(pcf_handle *h, const double *b, const double *x, double
     return PCF_OK;
 }
 
+// The FP64 residual of the zero initial guess, r64 = b (into w64, as
+// true_residual leaves it), and its RMS: one pass over b instead of an
+// operator apply.
+static int zero_guess_residual(pcf_handle *h, const double *b, double *rms) {
+    k_copy_sumsq<<<vec_grid(h->d.n), 256, 0, h->stream>>>(b, h->w64, h->d.n, red(h, nullptr, FIN_STORE, h->dot_out));
+    h->launches += 1;
+    PCF_CUDA_TRY(cudaGetLastError());
+    double rr = 0;
+    PCF_CUDA_TRY(cudaMemcpyAsync(&rr, h->dot_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    PCF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    *rms = std::sqrt(rr / (double)h->d.n);
+    return PCF_OK;
+}
+
 // Grids of at most kTinyMaxCells cells: the reference FP64 BiCGSTAB in one
 // thread block (pcf_tiny.cuh), whatever the precision and multigrid settings
 // (on such grids the solve is bound by launch latency, so neither reduced
@@ -2587,7 +2601,7 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
     // x64 accumulates the correction; r64 = b - A x64 is the FP64 true residual.
     PCF_CUDA_TRY(cudaMemsetAsync(h->x64, 0, sizeof(double) * h->d.n, h->stream));
     double rnorm = 0;
-    if ((rc = true_residual(h, h->b64, h->x64, &rnorm))) return rc;
+    if ((rc = zero_guess_residual(h, h->b64, &rnorm))) return rc;
     const double b_norm = rnorm;
     res->b_norm = b_norm;
     if ((prm->learned & 1) && h->net && b_norm > 0 && std::isfinite(b_norm)) {
@@ -3196,15 +3210,11 @@ int pcf_ensemble_solve_device(pcf_ensemble *e, const double *const *d_rhs, const
         if (prm->autotune && (rc = autotune_handle(h, prm))) return rc;
         PCF_CUDA_TRY(cudaEventRecord(h->ev[2], h->stream));
         PCF_CUDA_TRY(cudaMemsetAsync(h->x64, 0, sizeof(double) * h->d.n, h->stream));
-        StencilArgs<double> a;
-        a.coef = h->coef64;
-        a.s = h->x64;
-        a.out = h->w64;
-        a.w1 = h->b64;
-        a.deta = 0;
-        a.guard = nullptr;
-        a.red = red(h, nullptr, FIN_STORE, h->dot_out);
-        if ((rc = launch_stencil<double, false, EPI_RESID>(h, a))) return rc;
+        // r = b - A 0 = b and its sum of squares
+        k_copy_sumsq<<<vec_grid(h->d.n), 256, 0, h->stream>>>(h->b64, h->w64, h->d.n,
+                                                               red(h, nullptr, FIN_STORE, h->dot_out));
+        h->launches += 1;
+        PCF_CUDA_TRY(cudaGetLastError());
         PCF_CUDA_TRY(cudaMemcpyAsync(e->h_norm + q, h->dot_out, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     }
     for (int q = 0; q < n; ++q) PCF_CUDA_TRY(cudaStreamSynchronize(e->m[q]->stream));
