@@ -2574,7 +2574,8 @@ static int krylov_solve(pcf_handle *h, double tolref, const pcf_params *prm, con
     if (prm->multigrid && (prm->precision != PCF_PRECISION_MIXED || !c.precond)) return PCF_EINVAL;
     if (h->d.n <= kTinyMaxCells) return tiny_solve(h, tol, prm, xres, res);
     int rc;
-    if (c.precond && (rc = ensure_factors(h, c.deta))) return rc;
+    // (the multigrid mixed solve builds the pivots of its own d_eta in mg_prepare)
+    if (c.precond && !prm->multigrid && (rc = ensure_factors(h, c.deta))) return rc;
     const int maxit = prm->poisson_iterations;
 
     if (prm->precision != PCF_PRECISION_MIXED) {
@@ -2721,7 +2722,9 @@ static int solve_common(pcf_handle *h, double dt, double rf, double tolref, cons
     {
         NvtxScope r("pcf assemble");
         if (!assembled && (rc = assemble_device(h, dt, rf, prm->damp_horizontal_wind_on_rhs))) return rc;
-        if (prm->preconditioner && (rc = ensure_factors(h, deta_of(h, prm->dtau)))) return rc;
+        // the multigrid mixed solve builds the pivots of its own d_eta (mg_prepare)
+        const bool mg = prm->multigrid && prm->precision == PCF_PRECISION_MIXED;
+        if (prm->preconditioner && !mg && (rc = ensure_factors(h, deta_of(h, prm->dtau)))) return rc;
     }
     if (rhs_ready) PCF_CUDA_TRY(cudaStreamWaitEvent(h->stream, rhs_ready, 0));
     PCF_CUDA_TRY(cudaEventRecord(h->ev[2], h->stream));
@@ -3205,7 +3208,7 @@ int pcf_ensemble_solve_device(pcf_ensemble *e, const double *const *d_rhs, const
         PCF_CUDA_TRY(cudaMemcpyAsync(h->b64, d_rhs[q], sizeof(double) * h->d.n, cudaMemcpyDeviceToDevice, h->stream));
         PCF_CUDA_TRY(cudaEventRecord(h->ev[1], h->stream));
         if ((rc = assemble_device(h, dt[q], rayleigh_factor[q], prm->damp_horizontal_wind_on_rhs))) return rc;
-        if (prm->preconditioner && (rc = ensure_factors(h, deta_of(h, prm->dtau)))) return rc;
+        if (prm->preconditioner && !prm->multigrid && (rc = ensure_factors(h, deta_of(h, prm->dtau)))) return rc;
         if (prm->multigrid && (rc = mg_prepare(h, prm, true))) return rc;
         if (prm->autotune && (rc = autotune_handle(h, prm))) return rc;
         PCF_CUDA_TRY(cudaEventRecord(h->ev[2], h->stream));
