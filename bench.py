@@ -1079,7 +1079,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c5", choices=sorted(WORKLOADS))
-    ap.add_argument("--size", default=None, help="c2 only: NXxNYxNZ instead of 256x256x128 (profiling captures)")
+    ap.add_argument("--size", default=None,
+                    help="c2 and step only: NXxNYxNZ instead of 256x256x128 (profiling captures)")
     ap.add_argument("--method", default="mg", choices=sorted(METHODS))
     ap.add_argument("--mg-dtau", type=float, default=2.5)
     ap.add_argument("--fused-coarse", default="auto", choices=["auto", "on", "off"],
@@ -1097,6 +1098,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
+    if args.size and args.config not in ("c2", "step"):
+        raise SystemExit("--size applies to --config c2 and step only")
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
